@@ -1,0 +1,205 @@
+/*
+ * rfxb200 -- C ABI of the B200 FDTD time-stepping library.
+ *
+ * The reference (bk-squared/rfx 1.6.7) is pure Python/JAX and has no plugin or
+ * FFI API of its own.  Its seam for this path is the pure-Python function
+ *   rfx.simulation.run(grid, materials, n_steps, *, boundary, cpml_axes,
+ *                      pec_axes, sources, probes, dft_planes, pec_mask,
+ *                      checkpoint, checkpoint_segments, ...)   rfx/simulation.py:1686
+ * and its graded-mesh twin
+ *   rfx.nonuniform.run_nonuniform(...)                          rfx/nonuniform.py:1589
+ * whose bodies run one jax.lax.scan over the step function built by
+ *   make_core_step                                              rfx/simulation.py:1227
+ *   _build_nu_scan                                              rfx/nonuniform.py:998
+ * Each entry point below names the piece of that seam it replaces.
+ *
+ * Conventions
+ *  - All functions return 0 on success or a negative RFXB_E_* code; the
+ *    message of the last failure on the calling thread is rfxb_last_error().
+ *    Nothing raises inside a kernel; device-side status is read back.
+ *  - Array arguments named *_dev are device pointers, *_host host pointers.
+ *    Field and material arrays use the reference layout: (nx, ny, nz)
+ *    C-order float32, z fastest.
+ *  - A plan owns its internal state (padded double-buffered fields, CPML
+ *    psi, update coefficients, Kahan DFT compensation, checkpoints).  The
+ *    caller owns everything it passes in: materials, source tables, probe
+ *    outputs, DFT accumulators, adjoint tables, gradient buffers.
+ *  - Work is stream-ordered on the cudaStream_t given (0 = legacy default).
+ *    A plan must not be used from two threads at once.
+ */
+#ifndef RFXB200_H
+#define RFXB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RFXB_OK 0
+#define RFXB_E_INVALID (-1)   /* bad descriptor or argument */
+#define RFXB_E_SHAPE (-2)     /* inconsistent sizes */
+#define RFXB_E_NOMEM (-3)     /* device allocation failed */
+#define RFXB_E_LAUNCH (-4)    /* kernel launch or CUDA runtime failure */
+#define RFXB_E_STATE (-5)     /* call out of order (e.g. adjoint before forward) */
+
+#define RFXB_AXIS_X 1u
+#define RFXB_AXIS_Y 2u
+#define RFXB_AXIS_Z 4u
+
+/* field component codes (ex ey ez hx hy hz) */
+#define RFXB_EX 0
+#define RFXB_EY 1
+#define RFXB_EZ 2
+#define RFXB_HX 3
+#define RFXB_HY 4
+#define RFXB_HZ 5
+/* probe flag: sample before soft-source injection (lumped-port V/I,
+ * rfx/simulation.py:1449-1500) */
+#define RFXB_PROBE_PRESOURCE 16
+
+typedef struct RfxbPlan RfxbPlan;
+typedef struct RfxbBatch RfxbBatch;
+
+/* One running-DFT plane (rfx/probes/probes.py:379-449). */
+typedef struct {
+  int axis;        /* normal axis 0/1/2 */
+  int index;       /* plane index along the axis */
+  int component;   /* RFXB_EX..RFXB_HZ */
+  int n_freqs;
+} RfxbDftDesc;
+
+/* Static description of one simulation (grid, boundaries, monitors).
+ * Replaces the trace-time setup of _build_step_setup (rfx/simulation.py:626)
+ * and _build_nu_scan (rfx/nonuniform.py:998). */
+typedef struct {
+  int nx, ny, nz;
+  double dt;
+  /* inverse spacing tables, length nx / ny / nz (host).  E-update tables
+   * ("inv_d_e") and H-update tables ("inv_d_h") as built by
+   * rfx/nonuniform.py:187-224; for a uniform grid every entry is 1/dx. */
+  const float* inv_xe_host; const float* inv_xh_host;
+  const float* inv_ye_host; const float* inv_yh_host;
+  const float* inv_ze_host; const float* inv_zh_host;
+  /* CPML (rfx/boundaries/cpml.py:346-478): layers per face (0 = none), the
+   * axes that absorb, and per face (x_lo, x_hi, y_lo, y_hi, z_lo, z_hi) the
+   * float32 b, c, kappa profiles of length cpml_layers with the hi faces
+   * pre-flipped, plus each face's boundary cell size. */
+  int cpml_layers;
+  unsigned cpml_axes;
+  const float* cpml_b_host;      /* [6][cpml_layers] */
+  const float* cpml_c_host;      /* [6][cpml_layers] */
+  const float* cpml_kappa_host;  /* [6][cpml_layers] */
+  double cpml_cell[6];
+  /* PEC faces applied after every E update (rfx/boundaries/pec.py:13-47) */
+  unsigned pec_axes;
+  /* soft sources: n_src x (i, j, k, component) (rfx/simulation.py:44-54) */
+  int n_src;
+  const int32_t* src_cells_host;
+  /* point probes: n_probe x (i, j, k, component | flags) (rfx/simulation.py:75-80) */
+  int n_probe;
+  const int32_t* probe_cells_host;
+  /* running-DFT planes */
+  int n_dft;
+  const RfxbDftDesc* dft_host;
+  /* gradient region [i0,i1) x [j0,j1) x [k0,k1) whose forward history the
+   * adjoint needs; i0 >= i1 means none */
+  int grad_box[6];
+} RfxbDesc;
+
+/* Per-call device buffers of the forward path. */
+typedef struct {
+  const float* src_wave_dev;   /* [n_total_steps][n_src], row = global step */
+  float* probe_out_dev;        /* [n_total_steps][n_probe], may be NULL */
+  void* const* dft_acc_dev;    /* n_dft complex64 arrays (n_freqs, n1, n2), accumulated */
+  const void* const* dft_phase_dev; /* n_dft float2 arrays [n_total_steps][n_freqs]: (cos, sin)*dt */
+} RfxbStepIO;
+
+/* Per-call device buffers of the adjoint path. */
+typedef struct {
+  const float* g_dev;          /* dJ/d(probe samples) [n_total_steps][n_probe] */
+  double* grad_dev;            /* dJ/d eps_r over grad_box, accumulated (C order) */
+  const float* dca_dev;        /* d ca / d eps_r over grad_box */
+  const float* dcb_dev;        /* d cb / d eps_r over grad_box */
+  float* src_adj_dev;          /* dJ/d(source table) [n_total_steps][n_src], may be NULL */
+} RfxbAdjointIO;
+
+int rfxb_version(void);
+const char* rfxb_last_error(void);
+
+/* Create / destroy a plan.  Replaces the trace-time setup named above. */
+int rfxb_plan_create(const RfxbDesc* desc, RfxbPlan** out);
+void rfxb_plan_destroy(RfxbPlan* plan);
+
+/* Materials -> per-cell update coefficients (ca, cb of rfx/core/yee.py:387-393,
+ * ce of rfx/boundaries/cpml.py:536, ch of cpml.py:818), computed on device in
+ * float32.  mu_r_dev may be NULL (mu_r = 1).  edge_mask_dev (uint8, bits
+ * 1/2/4 = ex/ey/ez zeroed after each E update, the output of
+ * tangential_edge_masks at rfx/boundaries/pec.py:90-176) may be NULL. */
+int rfxb_plan_set_materials(RfxbPlan* plan, const float* eps_r_dev, const float* sigma_dev,
+                            const float* mu_r_dev, const uint8_t* edge_mask_dev, void* stream);
+
+/* Zero fields, psi, DFT compensation and the step parity (init_state +
+ * init_cpml, rfx/core/yee.py:42-58, rfx/boundaries/cpml.py:346). */
+int rfxb_plan_reset(RfxbPlan* plan, void* stream);
+/* Copy fields between caller arrays (reference layout) and the plan state.
+ * fields_dev: 6 pointers ex ey ez hx hy hz. */
+int rfxb_plan_load_fields(RfxbPlan* plan, const float* const* fields_dev, void* stream);
+int rfxb_plan_store_fields(RfxbPlan* plan, float* const* fields_dev, void* stream);
+
+/* Advance n_steps steps starting at global step step0 (the scan of
+ * rfx/simulation.py:1969-1977 / rfx/nonuniform.py:1796 over the body of
+ * rfx/simulation.py:1255-1685 / rfx/nonuniform.py:1256-1568).  The uniform
+ * or graded lane is selected by the spacing tables; the DFT sample time is
+ * encoded in the caller's phase table. */
+int rfxb_plan_advance(RfxbPlan* plan, const RfxbStepIO* io, int step0, int n_steps, void* stream);
+
+/* load_fields + advance + store_fields in one call: the shape of an XLA
+ * custom call that aliases the fields in and out. */
+int rfxb_forward(RfxbPlan* plan, const RfxbStepIO* io, float* const* fields_dev,
+                 int step0, int n_steps, void* stream);
+
+/* Forward history of the gradient region for steps [step0, step0+n_steps):
+ * the plan keeps E^n and curl H^{n+1/2} there, for the adjoint.  Must be
+ * called before the advance that produces those steps. */
+int rfxb_plan_record_history(RfxbPlan* plan, int step0, int n_steps);
+
+/* Checkpoints of the full state (fields, psi, parity) in plan-owned HBM:
+ * the storage of checkpoint-every-K with segment recompute, replacing
+ * jax.checkpoint segments (rfx/simulation.py:2011-2058,
+ * rfx/nonuniform.py:1755-1794). */
+int rfxb_plan_checkpoint_reserve(RfxbPlan* plan, int n_slots);
+int rfxb_plan_checkpoint_save(RfxbPlan* plan, int slot, void* stream);
+int rfxb_plan_checkpoint_load(RfxbPlan* plan, int slot, void* stream);
+
+/* Reverse-time adjoint: the transpose of the forward step, replacing
+ * jax.grad through the scan.  adjoint_begin zeroes the adjoint state and
+ * injects the probe cotangent of the last step n_total-1; adjoint_advance
+ * runs the reverse steps step_hi-1 down to step_hi-n_steps, whose history
+ * must have been recorded. */
+int rfxb_plan_adjoint_begin(RfxbPlan* plan, const RfxbAdjointIO* aio, int n_total, void* stream);
+int rfxb_plan_adjoint_advance(RfxbPlan* plan, const RfxbAdjointIO* aio, int step_hi, int n_steps,
+                              void* stream);
+
+/* Batched sweep: many plans (uneven grid sizes) advanced together, one
+ * launch per step for all of them, the step loop captured in a CUDA graph.
+ * Replaces a Python loop of independent run()/forward() calls, the only
+ * batching the reference offers for uneven grids (rfx/vmap_sweep.py:871
+ * batches equal grids only). */
+int rfxb_batch_create(RfxbPlan* const* plans, int n_plans, RfxbBatch** out);
+void rfxb_batch_destroy(RfxbBatch* batch);
+int rfxb_batch_advance(RfxbBatch* batch, const RfxbStepIO* ios, int step0, int n_steps, void* stream);
+int rfxb_batch_record_history(RfxbBatch* batch, int step0, int n_steps);
+int rfxb_batch_adjoint_begin(RfxbBatch* batch, const RfxbAdjointIO* aios, int n_total, void* stream);
+int rfxb_batch_adjoint_advance(RfxbBatch* batch, const RfxbAdjointIO* aios, int step_hi, int n_steps,
+                               void* stream);
+
+/* Bytes of device memory a plan holds (state, coefficients, psi, history,
+ * checkpoints). */
+int64_t rfxb_plan_device_bytes(const RfxbPlan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RFXB200_H */

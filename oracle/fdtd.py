@@ -1,0 +1,595 @@
+"""NumPy restatement of the rfx scan body (uniform and graded lanes).
+
+TEST INFRASTRUCTURE ONLY -- see the package docstring.  The arithmetic follows
+the reference operation by operation so that a float32 run reproduces the
+reference's float32 rounding pattern closely; ``dtype=np.float64`` gives the
+FP64 oracle in which, as in the reference's float64 mode, the material arrays
+and CPML profile coefficients keep their float32 values
+(rfx/api/__init__.py precision docstring, rfx/boundaries/cpml.py:165-171) and
+only the state and the arithmetic are promoted.
+
+Reference anchors (paths relative to the rfx project root):
+  grid geometry           rfx/grid.py:105-279
+  graded grid             rfx/nonuniform.py:101-224, 274-422
+  Yee updates             rfx/core/yee.py:121-138, 226-404, 411-492
+  CPML                    rfx/boundaries/cpml.py:101-171, 346-478, 522-1065
+  PEC / PEC mask          rfx/boundaries/pec.py:13-47, 90-208
+  sources                 rfx/simulation.py:181-293, rfx/nonuniform.py:588-691,
+                          rfx/sources/sources.py:31-103, 238-247
+  uniform scan order      rfx/simulation.py:1255-1685, 1958-1977
+  graded scan order       rfx/nonuniform.py:1256-1568
+  DFT plane accumulation  rfx/simulation.py:1574-1588, rfx/nonuniform.py:1458-1472
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import NamedTuple
+
+import numpy as np
+
+# rfx/core/yee.py:117-118 and rfx/grid.py:8
+EPS_0 = 8.8541878128e-12
+MU_0 = 1.25663706212e-6
+C0 = 299_792_458.0
+# rfx/nonuniform.py:34 uses the constant implied by EPS_0/MU_0
+C0_NU = 1.0 / math.sqrt(EPS_0 * MU_0)
+
+COMPONENTS = ("ex", "ey", "ez", "hx", "hy", "hz")
+
+
+# ---------------------------------------------------------------------------
+# Grids
+# ---------------------------------------------------------------------------
+
+@dataclass
+class UniformGrid:
+    """Geometry of ``rfx.grid.Grid`` (rfx/grid.py:105-246)."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dt: float
+    cpml_layers: int
+    pads: tuple  # (x_lo, x_hi, y_lo, y_hi, z_lo, z_hi)
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz)
+
+    def position_to_index(self, pos):
+        """rfx/grid.py:258-279: round-to-nearest plus the lo pad."""
+        i = int(round(pos[0] / self.dx)) + self.pads[0]
+        j = int(round(pos[1] / self.dx)) + self.pads[2]
+        k = int(round(pos[2] / self.dx)) + self.pads[4]
+        if not (0 <= i < self.nx and 0 <= j < self.ny and 0 <= k < self.nz):
+            raise ValueError(f"position {pos} maps outside the grid")
+        return (i, j, k)
+
+
+def make_uniform_grid(domain, dx, cpml_layers=8, cpml_axes="xyz"):
+    """rfx/grid.py:88-239 (3-D mode, no per-face overrides)."""
+    dt = dx / (C0 * np.sqrt(3.0)) * 0.99
+    pad = [cpml_layers if ax in cpml_axes else 0 for ax in "xyz"]
+    nx = int(np.ceil(domain[0] / dx)) + 1 + 2 * pad[0]
+    ny = int(np.ceil(domain[1] / dx)) + 1 + 2 * pad[1]
+    nz = int(np.ceil(domain[2] / dx)) + 1 + 2 * pad[2]
+    return UniformGrid(nx, ny, nz, float(dx), float(dt), int(cpml_layers),
+                       (pad[0], pad[0], pad[1], pad[1], pad[2], pad[2]))
+
+
+@dataclass
+class NonUniformGrid:
+    """Geometry of ``rfx.nonuniform.NonUniformGrid`` (rfx/nonuniform.py:37-98)."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dy: float
+    dx_arr: np.ndarray
+    dy_arr: np.ndarray
+    dz: np.ndarray
+    dt: float
+    cpml_layers: int
+    inv_dx: np.ndarray
+    inv_dy: np.ndarray
+    inv_dz: np.ndarray
+    inv_dx_h: np.ndarray
+    inv_dy_h: np.ndarray
+    inv_dz_h: np.ndarray
+    pads: tuple
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz)
+
+
+def profile_to_inv_arrays(profile_full):
+    """rfx/nonuniform.py:187-224 (float32 arithmetic)."""
+    arr = np.asarray(profile_full, dtype=np.float32)
+    inv_local = np.float32(1.0) / arr
+    inv_mean = np.float32(2.0) / (arr[:-1] + arr[1:])
+    inv_d_h = np.concatenate([inv_local[:-1], np.zeros(1, np.float32)])
+    inv_d_e = np.concatenate([inv_local[:1], inv_mean])
+    return inv_d_e, inv_d_h
+
+
+def _pad_profile(profile, pad_lo, pad_hi):
+    """rfx/nonuniform.py:101-127 (concrete numpy branch)."""
+    lo = np.full(pad_lo, float(profile[0]))
+    hi = np.full(pad_hi, float(profile[-1]))
+    return np.concatenate([lo, np.asarray(profile, dtype=np.float64), hi])
+
+
+def _append_bounding_node(profile_full):
+    """rfx/nonuniform.py:130-152."""
+    return np.concatenate([profile_full, profile_full[-1:]])
+
+
+def make_nonuniform_grid(domain_xy, dz_profile, dx, cpml_layers=8):
+    """rfx/nonuniform.py:274-422 with uniform x/y and CPML on every face."""
+    pad = int(cpml_layers)
+    nxi = int(round(domain_xy[0] / dx))
+    nyi = int(round(domain_xy[1] / dx))
+    dx_full = _append_bounding_node(_pad_profile(np.full(nxi, float(dx)), pad, pad))
+    dy_full = _append_bounding_node(_pad_profile(np.full(nyi, float(dx)), pad, pad))
+    dz_full = _append_bounding_node(_pad_profile(np.asarray(dz_profile, np.float64), pad, pad))
+    dt = float(0.99 / (C0_NU * np.sqrt(1 / float(np.min(dx_full)) ** 2
+                                       + 1 / float(np.min(dy_full)) ** 2
+                                       + 1 / float(np.min(dz_full)) ** 2)))
+    ix, ixh = profile_to_inv_arrays(dx_full)
+    iy, iyh = profile_to_inv_arrays(dy_full)
+    iz, izh = profile_to_inv_arrays(dz_full)
+    return NonUniformGrid(
+        nx=len(dx_full), ny=len(dy_full), nz=len(dz_full),
+        dx=float(dx), dy=float(dx),
+        dx_arr=dx_full.astype(np.float32), dy_arr=dy_full.astype(np.float32),
+        dz=dz_full.astype(np.float32), dt=dt, cpml_layers=pad,
+        inv_dx=ix, inv_dy=iy, inv_dz=iz, inv_dx_h=ixh, inv_dy_h=iyh, inv_dz_h=izh,
+        pads=(pad,) * 6)
+
+
+# ---------------------------------------------------------------------------
+# CPML profiles
+# ---------------------------------------------------------------------------
+
+class CPMLProfile(NamedTuple):
+    sigma: np.ndarray
+    kappa: np.ndarray
+    alpha: np.ndarray
+    b: np.ndarray
+    c: np.ndarray
+
+
+def cpml_profile(n_layers, dt, dx, order=3, kappa_max=1.0, R_asymptotic=1e-15):
+    """rfx/boundaries/cpml.py:101-171 (concrete float64 branch, float32 out)."""
+    eta = float(np.sqrt(MU_0 / EPS_0))
+    d = n_layers * dx
+    sigma_max = -float(np.log(R_asymptotic)) * (order + 1) / (2.0 * eta * d)
+    sigma_max = sigma_max * kappa_max
+    rho = 1.0 - np.arange(n_layers, dtype=np.float64) / max(n_layers - 1, 1)
+    sigma = sigma_max * rho ** order
+    kappa = 1.0 + (kappa_max - 1.0) * rho ** order
+    alpha = 0.05 * (1.0 - rho)
+    denom = sigma * kappa + kappa ** 2 * alpha
+    b = np.exp(-(sigma / kappa + alpha) * dt / EPS_0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        c = np.where(denom > 1e-30, sigma * (b - 1.0) / denom, 0.0)
+    f = np.float32
+    return CPMLProfile(sigma.astype(f), kappa.astype(f), alpha.astype(f),
+                       b.astype(f), c.astype(f))
+
+
+def build_cpml(grid, kappa_max=1.0):
+    """Per-face profiles and boundary cell sizes (rfx/boundaries/cpml.py:346-478).
+
+    Returns ``{face: (b, c, kappa, cell_size)}`` with the hi faces pre-flipped
+    (rfx/boundaries/cpml.py:404-409).  Uniform grids use ``dx`` on every face;
+    graded grids use ``dx``, ``dy``, ``dz[0]``, ``dz[-1]``
+    (rfx/boundaries/cpml.py:174-197).
+    """
+    n = grid.cpml_layers
+    if isinstance(grid, NonUniformGrid):
+        sizes = {"x": (grid.dx, grid.dx), "y": (grid.dy, grid.dy),
+                 "z": (float(grid.dz[0]), float(grid.dz[-1]))}
+    else:
+        sizes = {a: (grid.dx, grid.dx) for a in "xyz"}
+    out = {}
+    for a in "xyz":
+        lo = cpml_profile(n, grid.dt, sizes[a][0], kappa_max=kappa_max)
+        hi = cpml_profile(n, grid.dt, sizes[a][1], kappa_max=kappa_max)
+        out[a + "_lo"] = (lo.b, lo.c, lo.kappa, sizes[a][0])
+        out[a + "_hi"] = (hi.b[::-1].copy(), hi.c[::-1].copy(), hi.kappa[::-1].copy(), sizes[a][1])
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Sources
+# ---------------------------------------------------------------------------
+
+def gaussian_pulse(t, f0, bandwidth=0.5, amplitude=1.0, cutoff=3.0):
+    """rfx/sources/sources.py:56-103, evaluated in the dtype of ``t``."""
+    tau = 1.0 / (f0 * bandwidth * math.pi)
+    t0 = cutoff * tau
+    arg = (t - t0) / tau
+    return amplitude * (-2.0 * arg) * np.exp(-(arg ** 2))
+
+
+def _times(n_steps, dt):
+    """``jnp.arange(n_steps, dtype=float32) * dt`` (rfx/simulation.py:277)."""
+    return np.arange(n_steps, dtype=np.float32) * dt
+
+
+def _cell_cb(eps_r_cell, sigma_cell, dt):
+    """rfx/simulation.py:181-194 in float32."""
+    eps = np.float32(eps_r_cell) * EPS_0
+    loss = np.float32(sigma_cell) * dt / (2.0 * eps)
+    return np.float32((dt / eps) / (1.0 + loss))
+
+
+def j_source_waveform(grid, idx, materials, n_steps, f0, bandwidth=0.5, amplitude=1.0):
+    """``make_j_source`` (rfx/simulation.py:239-293): ``cb * pulse(n dt)``."""
+    i, j, k = idx
+    cb = _cell_cb(materials[0][i, j, k], materials[1][i, j, k], grid.dt)
+    w = gaussian_pulse(_times(n_steps, grid.dt), f0, bandwidth, amplitude)
+    return (cb * w).astype(np.float32)
+
+
+def port_sigma(d_par, d_perp1, d_perp2, impedance):
+    """rfx/sources/sources.py:31-45."""
+    return d_par / (impedance * d_perp1 * d_perp2)
+
+
+def port_source_waveform(grid, idx, materials, n_steps, f0, bandwidth=0.5, d_par=None):
+    """``make_port_source`` (rfx/simulation.py:296-314): ``cb/d_par * pulse``."""
+    i, j, k = idx
+    cb = _cell_cb(materials[0][i, j, k], materials[1][i, j, k], grid.dt)
+    d_par = grid.dx if d_par is None else d_par
+    w = gaussian_pulse(_times(n_steps, grid.dt), f0, bandwidth)
+    return ((cb / d_par) * w).astype(np.float32)
+
+
+def current_source_waveform(grid, idx, component, materials, n_steps, f0, bandwidth=0.5):
+    """``make_current_source`` (rfx/nonuniform.py:588-691): ``cb/dV * pulse``
+    with the primal width on the component axis and dual widths across."""
+    i, j, k = idx
+    eps = float(materials[0][i, j, k]) * EPS_0
+    sigma = float(materials[1][i, j, k])
+    loss = sigma * grid.dt / (2.0 * eps)
+    cb = (grid.dt / eps) / (1.0 + loss)
+    p_axis = {"ex": 0, "ey": 1, "ez": 2}[component]
+    profiles = (grid.dx_arr, grid.dy_arr, grid.dz)
+    widths = []
+    for a, ii in enumerate((i, j, k)):
+        prof = np.asarray(profiles[a], dtype=np.float64)
+        if a == p_axis:
+            widths.append(float(prof[ii]))
+        elif ii <= 0:
+            widths.append(float(prof[0]))
+        else:
+            widths.append(float(0.5 * (prof[ii - 1] + prof[ii])))
+    dV = widths[0] * widths[1] * widths[2]
+    w = gaussian_pulse(_times(n_steps, grid.dt), f0, bandwidth)
+    return ((cb / dV) * w).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Stencil helpers
+# ---------------------------------------------------------------------------
+
+def _sf(a, ax):
+    """``_shift_fwd`` (rfx/core/yee.py:121-128): a[i+1], zero past the end."""
+    out = np.zeros_like(a)
+    d = [slice(None)] * 3
+    s = [slice(None)] * 3
+    d[ax] = slice(0, -1)
+    s[ax] = slice(1, None)
+    out[tuple(d)] = a[tuple(s)]
+    return out
+
+
+def _sb(a, ax):
+    """``_shift_bwd`` (rfx/core/yee.py:131-138): a[i-1], zero before the start."""
+    out = np.zeros_like(a)
+    d = [slice(None)] * 3
+    s = [slice(None)] * 3
+    d[ax] = slice(1, None)
+    s[ax] = slice(0, -1)
+    out[tuple(d)] = a[tuple(s)]
+    return out
+
+
+def tangential_edge_masks(cell_mask):
+    """rfx/boundaries/pec.py:90-176 on non-periodic 3-D axes."""
+    m = np.asarray(cell_mask, dtype=bool)
+    out = []
+    for ax in range(3):
+        nb = _sb(m, ax) | _sf(m, ax)
+        out.append(m & nb)
+    return tuple(out)
+
+
+def _slab(ax, lo, n):
+    s = [slice(None)] * 3
+    s[ax] = slice(0, n) if lo else slice(-n, None)
+    return tuple(s)
+
+
+def _col(v, ax):
+    shp = [1, 1, 1]
+    shp[ax] = -1
+    return v.reshape(shp)
+
+
+# ---------------------------------------------------------------------------
+# One step
+# ---------------------------------------------------------------------------
+
+# (field corrected, field differentiated, sign) per CPML axis, in the order
+# the reference applies them (rfx/boundaries/cpml.py:874-1043 and 604-777).
+_CPML_H = {0: (("hy", "ez", +1), ("hz", "ey", -1)),
+           1: (("hx", "ez", -1), ("hz", "ex", +1)),
+           2: (("hx", "ey", +1), ("hy", "ex", -1))}
+_CPML_E = {0: (("ey", "hz", -1), ("ez", "hy", +1)),
+           1: (("ex", "hz", +1), ("ez", "hx", -1)),
+           2: (("ex", "hy", -1), ("ey", "hx", +1))}
+
+
+class _Stepper:
+    def __init__(self, grid, materials, *, dtype, nonuniform, cpml_axes,
+                 pec_axes, pec_mask, kappa_max=1.0):
+        self.g = grid
+        self.f = np.dtype(dtype)
+        self.nu = nonuniform
+        shape = grid.shape
+        eps_r, sigma, mu_r = materials
+        f = self.f
+        self.eps_r = np.asarray(eps_r, np.float32).astype(f)
+        self.sigma = np.asarray(sigma, np.float32).astype(f)
+        self.mu_r = np.asarray(mu_r, np.float32).astype(f)
+        self.F = {c: np.zeros(shape, f) for c in COMPONENTS}
+        self.step_count = 0
+        self.cpml_axes = cpml_axes
+        self.pec_axes = pec_axes
+        self.n = grid.cpml_layers
+        self.psi = {}
+        if cpml_axes and self.n > 0:
+            self.prof = build_cpml(grid, kappa_max)
+            for ax in range(3):
+                if "xyz"[ax] not in cpml_axes:
+                    continue
+                for side in ("lo", "hi"):
+                    sl_shape = list(shape)
+                    sl_shape[ax] = self.n
+                    for (fc, _, _) in _CPML_H[ax] + _CPML_E[ax]:
+                        self.psi[(fc, ax, side)] = np.zeros(sl_shape, f)
+        self.emask = None
+        if pec_mask is not None:
+            self.emask = tuple(m.astype(f) for m in tangential_edge_masks(pec_mask))
+        if nonuniform:
+            g = grid
+            self.tab = {k: np.asarray(getattr(g, k), np.float32).astype(f) for k in
+                        ("inv_dx", "inv_dy", "inv_dz", "inv_dx_h", "inv_dy_h", "inv_dz_h")}
+
+    # rfx/core/yee.py:226-291 (uniform) and :411-453 (graded)
+    def update_h(self):
+        F, dt, f = self.F, self.g.dt, self.f
+        ex, ey, ez = F["ex"], F["ey"], F["ez"]
+        mu = self.mu_r * MU_0
+        if self.nu:
+            t = self.tab
+            iyh, izh, ixh = _col(t["inv_dy_h"], 1), _col(t["inv_dz_h"], 2), _col(t["inv_dx_h"], 0)
+            cx = (_sf(ez, 1) - ez) * iyh - (_sf(ey, 2) - ey) * izh
+            cy = (_sf(ex, 2) - ex) * izh - (_sf(ez, 0) - ez) * ixh
+            cz = (_sf(ey, 0) - ey) * ixh - (_sf(ex, 1) - ex) * iyh
+        else:
+            dx = self.g.dx
+            cx = (_sf(ez, 1) - ez) / dx - (_sf(ey, 2) - ey) / dx
+            cy = (_sf(ex, 2) - ex) / dx - (_sf(ez, 0) - ez) / dx
+            cz = (_sf(ey, 0) - ey) / dx - (_sf(ex, 1) - ex) / dx
+        k = dt / mu
+        F["hx"] = F["hx"] - k * cx
+        F["hy"] = F["hy"] - k * cy
+        F["hz"] = F["hz"] - k * cz
+
+    # rfx/core/yee.py:347-404 (uniform) and :456-492 (graded)
+    def update_e(self):
+        F, dt = self.F, self.g.dt
+        hx, hy, hz = F["hx"], F["hy"], F["hz"]
+        eps = self.eps_r * EPS_0
+        s2 = self.sigma * dt / (2.0 * eps)
+        ca = (1.0 - s2) / (1.0 + s2)
+        cb = (dt / eps) / (1.0 + s2)
+        if self.nu:
+            t = self.tab
+            iy, iz, ix = _col(t["inv_dy"], 1), _col(t["inv_dz"], 2), _col(t["inv_dx"], 0)
+            cx = (hz - _sb(hz, 1)) * iy - (hy - _sb(hy, 2)) * iz
+            cy = (hx - _sb(hx, 2)) * iz - (hz - _sb(hz, 0)) * ix
+            cz = (hy - _sb(hy, 0)) * ix - (hx - _sb(hx, 1)) * iy
+        else:
+            dx = self.g.dx
+            cx = (hz - _sb(hz, 1)) / dx - (hy - _sb(hy, 2)) / dx
+            cy = (hx - _sb(hx, 2)) / dx - (hz - _sb(hz, 0)) / dx
+            cz = (hy - _sb(hy, 0)) / dx - (hx - _sb(hx, 1)) / dx
+        F["ex"] = ca * F["ex"] + cb * cx
+        F["ey"] = ca * F["ey"] + cb * cy
+        F["ez"] = ca * F["ez"] + cb * cz
+        self.step_count += 1
+
+    def _apply_cpml(self, table, coef_full, fwd):
+        """rfx/boundaries/cpml.py:522-801 (E) and :804-1065 (H).  The curl
+        slices read the field values from before this correction pass."""
+        F, n = self.F, self.n
+        src = {c: F[c] for c in COMPONENTS}
+        work = {c: F[c].copy() for c in COMPONENTS}
+        for ax in range(3):
+            if "xyz"[ax] not in self.cpml_axes:
+                continue
+            name = "xyz"[ax]
+            for (fc, dc, sgn) in table[ax]:
+                for side in ("lo", "hi"):
+                    b, c, kap, d = self.prof[f"{name}_{side}"]
+                    b = _col(b.astype(self.f), ax)
+                    c = _col(c.astype(self.f), ax)
+                    kap = _col(kap.astype(self.f), ax)
+                    sl = _slab(ax, side == "lo", n)
+                    a = src[dc]
+                    if fwd:
+                        curl = (_sf(a, ax)[sl] - a[sl]) / d
+                    else:
+                        curl = (a[sl] - _sb(a, ax)[sl]) / d
+                    key = (fc, ax, side)
+                    psi = b * self.psi[key] + c * curl
+                    self.psi[key] = psi
+                    cf = coef_full[sl]
+                    if sgn < 0:
+                        cf = -cf
+                    km = (1.0 / kap - 1.0)
+                    if ax == 0:
+                        work[fc][sl] = work[fc][sl] + cf * psi
+                        work[fc][sl] = work[fc][sl] + cf * km * curl
+                    else:
+                        work[fc][sl] = work[fc][sl] + cf * psi
+                        work[fc][sl] = work[fc][sl] + cf * (km * curl)
+        for c in COMPONENTS:
+            F[c] = work[c]
+
+    def cpml_h(self):
+        if self.psi:
+            ch = self.g.dt / (self.mu_r * MU_0)
+            self._apply_cpml(_CPML_H, ch, fwd=True)
+
+    def cpml_e(self):
+        if self.psi:
+            ce = self.g.dt / (self.eps_r * EPS_0)
+            self._apply_cpml(_CPML_E, ce, fwd=False)
+
+    # rfx/boundaries/pec.py:13-47
+    def pec(self):
+        F, ax = self.F, self.pec_axes
+        if "x" in ax:
+            for c in ("ey", "ez"):
+                F[c][0, :, :] = 0.0
+                F[c][-1, :, :] = 0.0
+        if "y" in ax:
+            for c in ("ex", "ez"):
+                F[c][:, 0, :] = 0.0
+                F[c][:, -1, :] = 0.0
+        if "z" in ax:
+            for c in ("ex", "ey"):
+                F[c][:, :, 0] = 0.0
+                F[c][:, :, -1] = 0.0
+            F["ez"][:, :, -1] = 0.0
+
+    # rfx/boundaries/pec.py:179-208
+    def pec_mask(self):
+        if self.emask is not None:
+            for c, m in zip(("ex", "ey", "ez"), self.emask):
+                self.F[c] = self.F[c] * (1.0 - m)
+
+
+class OracleResult(NamedTuple):
+    time_series: np.ndarray           # (n_steps, n_probes)
+    dft_planes: list                  # [(n_freqs, n1, n2) complex]
+    state: dict                       # final fields
+    vi: np.ndarray | None             # (n_steps, n_ports, 2) pre-source V, I
+    psi: dict
+
+
+def _plane(a, axis, index):
+    if axis == 0:
+        return a[index, :, :]
+    if axis == 1:
+        return a[:, index, :]
+    return a[:, :, index]
+
+
+def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
+         probes_before_dft, dx_vi):
+    f = st.f
+    cdt = np.complex64 if f == np.float32 else np.complex128
+    ts = np.zeros((n_steps, len(probes)), f)
+    accs = []
+    for (axis, index, comp, freqs) in dft_planes:
+        shp = list(st.g.shape)
+        del shp[axis]
+        accs.append(np.zeros([len(freqs)] + shp, cdt))
+    vi = np.zeros((n_steps, len(vi_ports), 2), f) if vi_ports else None
+    dt = st.g.dt
+    for n in range(n_steps):
+        st.update_h()
+        st.cpml_h()
+        st.update_e()
+        st.cpml_e()
+        st.pec()
+        st.pec_mask()
+        F = st.F
+        # Lumped-port V/I sampling happens before source injection
+        # (rfx/simulation.py:1480-1500).
+        for p, (i, j, k, comp) in enumerate(vi_ports or ()):
+            v = -F[comp][i, j, k] * dx_vi
+            if comp == "ez":
+                iv = (F["hy"][i, j, k] - F["hy"][i - 1, j, k] - F["hx"][i, j, k] + F["hx"][i, j - 1, k]) * dx_vi
+            elif comp == "ex":
+                iv = (F["hz"][i, j, k] - F["hz"][i, j - 1, k] - F["hy"][i, j, k] + F["hy"][i, j, k - 1]) * dx_vi
+            else:
+                iv = (F["hx"][i, j, k] - F["hx"][i, j, k - 1] - F["hz"][i, j, k] + F["hz"][i - 1, j, k]) * dx_vi
+            vi[n, p, 0] = v
+            vi[n, p, 1] = iv
+        for (i, j, k, comp, wave) in sources:
+            F[comp][i, j, k] = F[comp][i, j, k] + f.type(wave[n])
+
+        def _probes():
+            for p, (i, j, k, comp) in enumerate(probes):
+                ts[n, p] = F[comp][i, j, k]
+
+        def _dft():
+            t = np.float32(n + dft_time_offset) * np.float32(dt) if f == np.float32 \
+                else float(n + dft_time_offset) * dt
+            for q, (axis, index, comp, freqs) in enumerate(dft_planes):
+                fr = np.asarray(freqs, dtype=f)
+                arg = (fr * (-2.0 * math.pi)).astype(f) * t
+                phase = (np.cos(arg) + 1j * np.sin(arg)).astype(cdt)
+                plane = _plane(F[comp], axis, index)
+                accs[q] = accs[q] + (plane[None, :, :] * phase[:, None, None]) * dt
+
+        if probes_before_dft:
+            _probes()
+            _dft()
+        else:
+            _dft()
+            _probes()
+    return OracleResult(ts, accs, {c: st.F[c].copy() for c in COMPONENTS}, vi, st.psi)
+
+
+def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
+                pec_axes=None, sources=(), probes=(), dft_planes=(), pec_mask=None,
+                vi_ports=(), kappa_max=1.0, dtype=np.float32):
+    """``rfx.simulation.run`` (rfx/simulation.py:1686-2138), scan body order of
+    rfx/simulation.py:1255-1685.  ``pec_axes=None`` means all axes
+    (rfx/simulation.py:684-691).  ``sources`` are ``(i, j, k, comp, waveform)``,
+    ``probes`` ``(i, j, k, comp)``, ``dft_planes`` ``(axis, index, comp, freqs)``.
+    The uniform DFT time stamp is ``(n+1) dt`` (rfx/simulation.py:1574)."""
+    if pec_axes is None:
+        pec_axes = "xyz"
+    st = _Stepper(grid, materials, dtype=dtype, nonuniform=False,
+                  cpml_axes=cpml_axes if boundary == "cpml" else "",
+                  pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=kappa_max)
+    return _run(st, n_steps, sources, probes, dft_planes, vi_ports, 1,
+                probes_before_dft=True, dx_vi=grid.dx)
+
+
+def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_planes=(),
+                   pec_mask=None, kappa_max=1.0, dtype=np.float32):
+    """``rfx.nonuniform.run_nonuniform`` (rfx/nonuniform.py:1589-1804), scan body
+    of rfx/nonuniform.py:1256-1568: PEC on every axis, DFT time stamp ``n dt``
+    (rfx/nonuniform.py:1461), DFT before probes."""
+    axes = "".join(a for a, p in zip("xyz", (grid.pads[0] + grid.pads[1],
+                                             grid.pads[2] + grid.pads[3],
+                                             grid.pads[4] + grid.pads[5])) if p > 0)
+    st = _Stepper(grid, materials, dtype=dtype, nonuniform=True,
+                  cpml_axes=axes if grid.cpml_layers > 0 else "",
+                  pec_axes="xyz", pec_mask=pec_mask, kappa_max=kappa_max)
+    return _run(st, n_steps, sources, probes, dft_planes, (), 0,
+                probes_before_dft=False, dx_vi=grid.dx)

@@ -1,0 +1,115 @@
+"""ctypes binding of the C ABI in ``include/rfxb200.h``.
+
+The product path has no CPU fallback: if ``librfxb200.so`` cannot be loaded
+(or built, where nvcc is available) every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librfxb200.so")
+
+c_float_p = C.POINTER(C.c_float)
+c_int32_p = C.POINTER(C.c_int32)
+
+
+class RfxbDftDesc(C.Structure):
+    _fields_ = [("axis", C.c_int), ("index", C.c_int), ("component", C.c_int), ("n_freqs", C.c_int)]
+
+
+class RfxbDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dt", C.c_double),
+        ("inv_xe_host", c_float_p), ("inv_xh_host", c_float_p),
+        ("inv_ye_host", c_float_p), ("inv_yh_host", c_float_p),
+        ("inv_ze_host", c_float_p), ("inv_zh_host", c_float_p),
+        ("cpml_layers", C.c_int),
+        ("cpml_axes", C.c_uint),
+        ("cpml_b_host", c_float_p), ("cpml_c_host", c_float_p), ("cpml_kappa_host", c_float_p),
+        ("cpml_cell", C.c_double * 6),
+        ("pec_axes", C.c_uint),
+        ("n_src", C.c_int), ("src_cells_host", c_int32_p),
+        ("n_probe", C.c_int), ("probe_cells_host", c_int32_p),
+        ("n_dft", C.c_int), ("dft_host", C.POINTER(RfxbDftDesc)),
+        ("grad_box", C.c_int * 6),
+    ]
+
+
+class RfxbStepIO(C.Structure):
+    _fields_ = [
+        ("src_wave_dev", C.c_void_p),
+        ("probe_out_dev", C.c_void_p),
+        ("dft_acc_dev", C.POINTER(C.c_void_p)),
+        ("dft_phase_dev", C.POINTER(C.c_void_p)),
+    ]
+
+
+class RfxbAdjointIO(C.Structure):
+    _fields_ = [
+        ("g_dev", C.c_void_p),
+        ("grad_dev", C.c_void_p),
+        ("dca_dev", C.c_void_p),
+        ("dcb_dev", C.c_void_p),
+        ("src_adj_dev", C.c_void_p),
+    ]
+
+
+# name -> (restype, argtypes); the set of exported symbols the header declares
+SIGNATURES = {
+    "rfxb_version": (C.c_int, []),
+    "rfxb_last_error": (C.c_char_p, []),
+    "rfxb_plan_create": (C.c_int, [C.POINTER(RfxbDesc), C.POINTER(C.c_void_p)]),
+    "rfxb_plan_destroy": (None, [C.c_void_p]),
+    "rfxb_plan_set_materials": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rfxb_plan_reset": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rfxb_plan_load_fields": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p]),
+    "rfxb_plan_store_fields": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p]),
+    "rfxb_plan_advance": (C.c_int, [C.c_void_p, C.POINTER(RfxbStepIO), C.c_int, C.c_int, C.c_void_p]),
+    "rfxb_forward": (C.c_int, [C.c_void_p, C.POINTER(RfxbStepIO), C.POINTER(C.c_void_p), C.c_int, C.c_int,
+                               C.c_void_p]),
+    "rfxb_plan_record_history": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "rfxb_plan_checkpoint_reserve": (C.c_int, [C.c_void_p, C.c_int]),
+    "rfxb_plan_checkpoint_save": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "rfxb_plan_checkpoint_load": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "rfxb_plan_adjoint_begin": (C.c_int, [C.c_void_p, C.POINTER(RfxbAdjointIO), C.c_int, C.c_void_p]),
+    "rfxb_plan_adjoint_advance": (C.c_int, [C.c_void_p, C.POINTER(RfxbAdjointIO), C.c_int, C.c_int, C.c_void_p]),
+    "rfxb_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
+    "rfxb_batch_destroy": (None, [C.c_void_p]),
+    "rfxb_batch_advance": (C.c_int, [C.c_void_p, C.POINTER(RfxbStepIO), C.c_int, C.c_int, C.c_void_p]),
+    "rfxb_batch_record_history": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "rfxb_batch_adjoint_begin": (C.c_int, [C.c_void_p, C.POINTER(RfxbAdjointIO), C.c_int, C.c_void_p]),
+    "rfxb_batch_adjoint_advance": (C.c_int, [C.c_void_p, C.POINTER(RfxbAdjointIO), C.c_int, C.c_int, C.c_void_p]),
+    "rfxb_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Load (building first if the library file is missing) and type the ABI."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            from . import build as _build
+            _build.build()
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        msg = load().rfxb_last_error().decode(errors="replace")
+        raise RuntimeError(f"{what} failed (rfxb code {rc}): {msg}")

@@ -1,0 +1,738 @@
+// Host side of the C ABI declared in include/rfxb200.h: plan and batch
+// objects, device allocation, descriptor upload, launch sequencing and the
+// CUDA-graph replay of step chunks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <utility>
+#include <vector>
+
+#include "../../include/rfxb200.h"
+#include "rfxb_common.cuh"
+
+namespace rfxb {
+template <int TY>
+__global__ void fwd_step_kernel(const RfxbInst*, const RfxbWork*, int, int);
+__global__ void dft_kernel(const RfxbInst*, const RfxbDftPlane*, int, int, int);
+__global__ void pack_kernel(float*, const float*, RfxbInst);
+__global__ void unpack_kernel(float*, const float*, RfxbInst);
+__global__ void coef_kernel(RfxbInst, float*, float*, float*, float*, const float*, const float*,
+                            const float*, const unsigned char*, unsigned char*, float);
+__global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int);
+__global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int);
+__global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int);
+}  // namespace rfxb
+
+using namespace rfxb;
+
+namespace {
+
+constexpr int kTY = 8;
+constexpr int kBlockThreads = 32 * kTY;
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define RFXB_CUDA(call)                                                                         \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess)                                                                      \
+      return fail(RFXB_E_LAUNCH, std::string(#call) + ": " + cudaGetErrorString(_e));          \
+  } while (0)
+
+int sm_count() {
+  static int n = -1;
+  if (n < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) n = 148;
+  }
+  return n;
+}
+
+}  // namespace
+
+struct RfxbPlan {
+  RfxbInst inst{};             // host copy of the device descriptor
+  int nx = 0, ny = 0, nz = 0;
+  double dt = 0.0;
+  long long elems = 0;         // floats per padded per-cell array
+  int par = 0;                 // parity of the buffers holding the current state
+  std::vector<void*> allocs;
+  // per-cell and table arrays
+  float* ca = nullptr; float* cb = nullptr; float* ce = nullptr; float* ch = nullptr;
+  unsigned char* emask = nullptr;
+  bool has_mu = false;
+  std::vector<int4> src, prb;
+  std::vector<RfxbDftDesc> dft;
+  std::vector<float2*> dft_cmp;
+  std::vector<long long> dft_cells;
+  long long psi_elems[3] = {0, 0, 0};
+  // history
+  float* hist = nullptr;
+  long long hist_cap = 0;      // floats
+  long long hcells = 0;
+  // checkpoints
+  std::vector<float*> ckpt;
+  std::vector<int> ckpt_valid;
+  // adjoint
+  AdjInst adj{};
+  bool adj_alloc = false;
+  int adj_par = 0;
+  // single-plan group state
+  RfxbBatch* self_group = nullptr;
+
+  ~RfxbPlan() {
+    for (void* p : allocs) cudaFree(p);
+  }
+
+  template <typename T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) return fail(RFXB_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return 0;
+  }
+  int64_t bytes = 0;
+};
+
+struct GraphKey {
+  int k, par0, dft, prb;
+  bool operator<(const GraphKey& o) const {
+    return std::tie(k, par0, dft, prb) < std::tie(o.k, o.par0, o.dft, o.prb);
+  }
+};
+
+struct RfxbBatch {
+  std::vector<RfxbPlan*> plans;
+  RfxbInst* d_inst = nullptr;
+  AdjInst* d_adj = nullptr;
+  RfxbWork* d_work = nullptr;
+  int n_work = 0;
+  RfxbDftPlane* d_dft = nullptr;
+  std::vector<RfxbDftPlane> dft;
+  int dft_blocks = 0;
+  std::vector<void*> allocs;
+  cudaStream_t cap_stream = nullptr;
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  ~RfxbBatch() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    for (void* p : allocs) cudaFree(p);
+  }
+};
+
+namespace {
+
+// Work list: (TY x 32) tiles of (y, z), each over an x range.  The x split
+// is chosen so the whole launch holds a few waves of CTAs.
+void make_work(const RfxbPlan& p, int inst_index, int target_ctas, std::vector<RfxbWork>& out) {
+  const int ty_tiles = (p.ny + kTY - 1) / kTY;
+  const int tz_tiles = (p.nz + 31) / 32;
+  const long long tiles = (long long)ty_tiles * tz_tiles;
+  int chunks = (int)std::max<long long>(1, (target_ctas + tiles - 1) / tiles);
+  chunks = std::min(chunks, std::max(1, p.nx / 8));
+  const int xlen = (p.nx + chunks - 1) / chunks;
+  for (int xa = 0; xa < p.nx; xa += xlen)
+    for (int y = 0; y < ty_tiles; ++y)
+      for (int z = 0; z < tz_tiles; ++z)
+        out.push_back(RfxbWork{inst_index, y * kTY, z * 32, xa, std::min(p.nx, xa + xlen)});
+}
+
+int upload_tables(RfxbPlan* p, const float* h, int n, const float** dst) {
+  std::vector<float> t(n + 2, 0.f);
+  for (int i = 0; i < n; ++i) t[i + 1] = h[i];
+  float* d = nullptr;
+  if (int rc = p->alloc(&d, t.size())) return rc;
+  RFXB_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
+  *dst = d + 1;
+  return 0;
+}
+
+int build_group(RfxbBatch* g) {
+  std::vector<RfxbInst> insts;
+  std::vector<RfxbWork> work;
+  long long total_cells = 0;
+  for (auto* p : g->plans) total_cells += (long long)p->nx * p->ny * p->nz;
+  const int target = sm_count() * 8;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    RfxbPlan* p = g->plans[q];
+    const long long cells = (long long)p->nx * p->ny * p->nz;
+    // each instance gets a share of the target proportional to its cells
+    const int share = (int)std::max<long long>(1, (long long)target * cells / std::max<long long>(1, total_cells));
+    make_work(*p, (int)q, share, work);
+  }
+  g->n_work = (int)work.size();
+  auto galloc = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
+    if (e != cudaSuccess) return fail(RFXB_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    g->allocs.push_back(*ptr);
+    return 0;
+  };
+  if (int rc = galloc((void**)&g->d_inst, sizeof(RfxbInst) * g->plans.size())) return rc;
+  if (int rc = galloc((void**)&g->d_adj, sizeof(AdjInst) * g->plans.size())) return rc;
+  if (int rc = galloc((void**)&g->d_work, sizeof(RfxbWork) * work.size())) return rc;
+  RFXB_CUDA(cudaMemcpy(g->d_work, work.data(), sizeof(RfxbWork) * work.size(), cudaMemcpyHostToDevice));
+  // DFT planes
+  g->dft.clear();
+  int blocks = 0;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    RfxbPlan* p = g->plans[q];
+    for (size_t d = 0; d < p->dft.size(); ++d) {
+      const RfxbDftDesc& dd = p->dft[d];
+      RfxbDftPlane pl{};
+      pl.inst = (int)q;
+      pl.axis = dd.axis;
+      pl.index = dd.index;
+      pl.comp = dd.component;
+      pl.nf = dd.n_freqs;
+      pl.n1 = dd.axis == 0 ? p->ny : p->nx;
+      pl.n2 = dd.axis == 2 ? p->ny : p->nz;
+      pl.cmp = p->dft_cmp[d];
+      pl.block0 = blocks;
+      blocks += (int)((p->dft_cells[d] + 255) / 256);
+      g->dft.push_back(pl);
+    }
+  }
+  g->dft_blocks = blocks;
+  if (!g->dft.empty()) {
+    if (int rc = galloc((void**)&g->d_dft, sizeof(RfxbDftPlane) * g->dft.size())) return rc;
+  }
+  RFXB_CUDA(cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking));
+  return 0;
+}
+
+// Upload descriptors with this call's IO pointers.
+int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_prb, cudaStream_t st) {
+  std::vector<RfxbInst> insts(g->plans.size());
+  *has_dft = false;
+  *has_prb = false;
+  size_t di = 0;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    RfxbPlan* p = g->plans[q];
+    insts[q] = p->inst;
+    const RfxbStepIO* io = ios ? &ios[q] : nullptr;
+    insts[q].srcw = io ? io->src_wave_dev : nullptr;
+    if (p->inst.nsrc > 0 && insts[q].srcw == nullptr) insts[q].nsrc = 0;
+    insts[q].prb_out = io ? io->probe_out_dev : nullptr;
+    if (insts[q].prb_out) *has_prb = true;
+    for (size_t d = 0; d < p->dft.size(); ++d, ++di) {
+      const bool on = io && io->dft_acc_dev && io->dft_phase_dev && io->dft_acc_dev[d] && io->dft_phase_dev[d];
+      g->dft[di].acc = on ? static_cast<float2*>(io->dft_acc_dev[d]) : nullptr;
+      g->dft[di].phase = on ? static_cast<const float2*>(io->dft_phase_dev[d]) : nullptr;
+      if (on) *has_dft = true;
+    }
+  }
+  for (const auto& pl : g->dft)
+    if (*has_dft && pl.acc == nullptr)
+      return fail(RFXB_E_INVALID, "either every DFT plane of a group gets accumulator and phase table, or none");
+  RFXB_CUDA(cudaMemcpyAsync(g->d_inst, insts.data(), sizeof(RfxbInst) * insts.size(), cudaMemcpyHostToDevice, st));
+  if (!g->dft.empty())
+    RFXB_CUDA(cudaMemcpyAsync(g->d_dft, g->dft.data(), sizeof(RfxbDftPlane) * g->dft.size(),
+                              cudaMemcpyHostToDevice, st));
+  // cudaMemcpyAsync from pageable memory stages the source before returning
+  return 0;
+}
+
+int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, cudaStream_t st) {
+  int par = par0;
+  for (int s = 0; s < n_steps; ++s) {
+    const int n = step0 + s;
+    fwd_step_kernel<kTY><<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_work, n, par);
+    if (has_dft)
+      dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, par ^ 1);
+    par ^= 1;
+  }
+  RFXB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, cudaStream_t st) {
+  if (n_steps < 0 || step0 < 0) return fail(RFXB_E_INVALID, "negative step range");
+  if (n_steps == 0) return 0;
+  const int par0 = g->plans[0]->par;
+  for (auto* p : g->plans)
+    if (p->par != par0) return fail(RFXB_E_STATE, "plans of a batch must share the step parity");
+  bool has_dft = false, has_prb = false;
+  if (int rc = upload_group(g, ios, &has_dft, &has_prb, st)) return rc;
+  if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, st)) return rc;
+  for (auto* p : g->plans) p->par = (par0 + n_steps) & 1;
+  return 0;
+}
+
+int ensure_adjoint(RfxbPlan* p, cudaStream_t st) {
+  if (!p->adj_alloc) {
+    for (int c = 0; c < 6; ++c)
+      if (int rc = p->alloc(&p->adj.aF[c], p->elems)) return rc;
+    for (int s = 0; s < 2; ++s)
+      for (int a = 0; a < 3; ++a) {
+        if (int rc = p->alloc(&p->adj.aPsiH[s][a], p->psi_elems[a])) return rc;
+        if (int rc = p->alloc(&p->adj.aPsiE[s][a], p->psi_elems[a])) return rc;
+      }
+    p->adj_alloc = true;
+  }
+  for (int c = 0; c < 6; ++c) RFXB_CUDA(cudaMemsetAsync(p->adj.aF[c], 0, p->elems * sizeof(float), st));
+  for (int s = 0; s < 2; ++s)
+    for (int a = 0; a < 3; ++a) {
+      RFXB_CUDA(cudaMemsetAsync(p->adj.aPsiH[s][a], 0, std::max<long long>(1, p->psi_elems[a]) * sizeof(float), st));
+      RFXB_CUDA(cudaMemsetAsync(p->adj.aPsiE[s][a], 0, std::max<long long>(1, p->psi_elems[a]) * sizeof(float), st));
+    }
+  p->adj_par = 0;
+  return 0;
+}
+
+int upload_adjoint(RfxbBatch* g, const RfxbAdjointIO* aios, cudaStream_t st) {
+  std::vector<RfxbInst> insts(g->plans.size());
+  std::vector<AdjInst> adjs(g->plans.size());
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    RfxbPlan* p = g->plans[q];
+    const RfxbAdjointIO& a = aios[q];
+    insts[q] = p->inst;
+    insts[q].prb_out = nullptr;
+    insts[q].srcw = nullptr;
+    insts[q].g = a.g_dev;
+    insts[q].g_ld = p->inst.nprb;
+    insts[q].grad = a.grad_dev;
+    insts[q].dca = a.dca_dev;
+    insts[q].dcb = a.dcb_dev;
+    insts[q].src_adj = a.src_adj_dev;
+    if (a.grad_dev && (a.dca_dev == nullptr || a.dcb_dev == nullptr || p->hist == nullptr))
+      return fail(RFXB_E_STATE, "gradient requested without coefficient derivatives or recorded history");
+    adjs[q] = p->adj;
+  }
+  RFXB_CUDA(cudaMemcpyAsync(g->d_inst, insts.data(), sizeof(RfxbInst) * insts.size(), cudaMemcpyHostToDevice, st));
+  RFXB_CUDA(cudaMemcpyAsync(g->d_adj, adjs.data(), sizeof(AdjInst) * adjs.size(), cudaMemcpyHostToDevice, st));
+  return 0;
+}
+
+int group_adjoint_begin(RfxbBatch* g, const RfxbAdjointIO* aios, int n_total, cudaStream_t st) {
+  if (n_total < 1) return fail(RFXB_E_INVALID, "n_total must be >= 1");
+  for (auto* p : g->plans)
+    if (int rc = ensure_adjoint(p, st)) return rc;
+  if (int rc = upload_adjoint(g, aios, st)) return rc;
+  adj_init_kernel<<<(unsigned)g->plans.size(), 32, 0, st>>>(g->d_inst, g->d_adj, (int)g->plans.size(), n_total - 1);
+  RFXB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, int n_steps, cudaStream_t st) {
+  if (n_steps <= 0) return 0;
+  if (step_hi - n_steps < 0) return fail(RFXB_E_INVALID, "reverse range reaches below step 0");
+  const int par0 = g->plans[0]->adj_par;
+  for (auto* p : g->plans) {
+    if (!p->adj_alloc) return fail(RFXB_E_STATE, "adjoint_advance before adjoint_begin");
+    if (p->adj_par != par0) return fail(RFXB_E_STATE, "plans of a batch must share the adjoint parity");
+  }
+  if (int rc = upload_adjoint(g, aios, st)) return rc;
+  int par = par0;
+  for (int s = step_hi - 1; s >= step_hi - n_steps; --s) {
+    adj_pass_a<<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_adj, g->d_work, s, par);
+    adj_pass_b<<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_adj, g->d_work, s, par);
+    par ^= 1;
+  }
+  RFXB_CUDA(cudaGetLastError());
+  for (auto* p : g->plans) p->adj_par = (par0 + n_steps) & 1;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rfxb_version(void) { return 10000; }
+
+const char* rfxb_last_error(void) { return g_last_error.c_str(); }
+
+int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
+  if (!d || !out) return fail(RFXB_E_INVALID, "null descriptor or output");
+  *out = nullptr;
+  if (d->nx < 2 || d->ny < 2 || d->nz < 2) return fail(RFXB_E_SHAPE, "grid must be at least 2 cells on every axis");
+  if ((long long)d->nx * d->ny * d->nz > (1LL << 34)) return fail(RFXB_E_SHAPE, "grid too large");
+  if (!(d->dt > 0.0)) return fail(RFXB_E_INVALID, "dt must be positive");
+  if (!d->inv_xe_host || !d->inv_xh_host || !d->inv_ye_host || !d->inv_yh_host || !d->inv_ze_host ||
+      !d->inv_zh_host)
+    return fail(RFXB_E_INVALID, "inverse spacing tables are required");
+  const int ncp = d->cpml_layers;
+  if (ncp < 0) return fail(RFXB_E_INVALID, "cpml_layers must be >= 0");
+  if (ncp > 0) {
+    if (!d->cpml_b_host || !d->cpml_c_host || !d->cpml_kappa_host)
+      return fail(RFXB_E_INVALID, "CPML profiles are required when cpml_layers > 0");
+    const int dims[3] = {d->nx, d->ny, d->nz};
+    for (int a = 0; a < 3; ++a)
+      if ((d->cpml_axes >> a) & 1u)
+        if (dims[a] < 2 * ncp) return fail(RFXB_E_SHAPE, "CPML slabs of one axis overlap (axis shorter than 2*cpml_layers)");
+  }
+  for (int s = 0; s < d->n_src; ++s) {
+    const int32_t* c = d->src_cells_host + 4 * s;
+    if (c[0] < 0 || c[0] >= d->nx || c[1] < 0 || c[1] >= d->ny || c[2] < 0 || c[2] >= d->nz || c[3] < 0 || c[3] > 2)
+      return fail(RFXB_E_INVALID, "source cell or component out of range");
+  }
+  for (int p = 0; p < d->n_probe; ++p) {
+    const int32_t* c = d->probe_cells_host + 4 * p;
+    if (c[0] < 0 || c[0] >= d->nx || c[1] < 0 || c[1] >= d->ny || c[2] < 0 || c[2] >= d->nz ||
+        (c[3] & 7) > 5 || (c[3] & ~(7 | RFXB_PROBE_PRESOURCE)) != 0)
+      return fail(RFXB_E_INVALID, "probe cell or component out of range");
+  }
+  for (int q = 0; q < d->n_dft; ++q) {
+    const RfxbDftDesc& dd = d->dft_host[q];
+    const int dims[3] = {d->nx, d->ny, d->nz};
+    if (dd.axis < 0 || dd.axis > 2 || dd.index < 0 || dd.index >= dims[dd.axis] || dd.component < 0 ||
+        dd.component > 5 || dd.n_freqs < 1)
+      return fail(RFXB_E_INVALID, "DFT plane descriptor out of range");
+  }
+  const int* hb = d->grad_box;
+  if (hb[0] < hb[1]) {
+    if (hb[0] < 0 || hb[1] > d->nx || hb[2] < 0 || hb[3] > d->ny || hb[4] < 0 || hb[5] > d->nz || hb[2] >= hb[3] ||
+        hb[4] >= hb[5])
+      return fail(RFXB_E_INVALID, "gradient region out of range");
+  }
+
+  RfxbPlan* p = new RfxbPlan();
+  p->nx = d->nx; p->ny = d->ny; p->nz = d->nz; p->dt = d->dt;
+  RfxbInst& I = p->inst;
+  I.nx = d->nx; I.ny = d->ny; I.nz = d->nz;
+  I.zs = ((d->nz + 1) + 31) / 32 * 32;
+  I.ps = (long long)(d->ny + 2) * I.zs;
+  const long long base = 32;
+  I.off0 = base + I.ps + I.zs;
+  p->elems = base + (long long)(d->nx + 2) * I.ps + I.zs + 64;
+  auto bail = [&](int rc) { delete p; return rc; };
+  for (int s = 0; s < 2; ++s)
+    for (int c = 0; c < 6; ++c) {
+      float* q = nullptr;
+      if (int rc = p->alloc(&q, p->elems)) return bail(rc);
+      I.F[s][c] = q;
+    }
+  if (int rc = p->alloc(&p->ca, p->elems)) return bail(rc);
+  if (int rc = p->alloc(&p->cb, p->elems)) return bail(rc);
+  if (int rc = p->alloc(&p->ce, p->elems)) return bail(rc);
+  for (float* q : {p->ca, p->cb, p->ce})
+    if (cudaMemset(q, 0, p->elems * sizeof(float)) != cudaSuccess) return bail(fail(RFXB_E_LAUNCH, "cudaMemset"));
+  I.ca = p->ca; I.cb = p->cb; I.ce = p->ce; I.ch = nullptr;
+  I.ch0 = (float)d->dt / (float)kMu0;
+  if (int rc = upload_tables(p, d->inv_xe_host, d->nx, &I.xe)) return bail(rc);
+  if (int rc = upload_tables(p, d->inv_xh_host, d->nx, &I.xh)) return bail(rc);
+  if (int rc = upload_tables(p, d->inv_ye_host, d->ny, &I.ye)) return bail(rc);
+  if (int rc = upload_tables(p, d->inv_yh_host, d->ny, &I.yh)) return bail(rc);
+  if (int rc = upload_tables(p, d->inv_ze_host, d->nz, &I.ze)) return bail(rc);
+  if (int rc = upload_tables(p, d->inv_zh_host, d->nz, &I.zh)) return bail(rc);
+  // CPML
+  I.ncp = ncp;
+  I.cpml_axes = ncp > 0 ? (d->cpml_axes & 7u) : 0u;
+  if (I.cpml_axes == 0) I.ncp = 0;
+  if (I.ncp > 0) {
+    std::vector<float> tb(6 * 3 * ncp);
+    for (int f = 0; f < 6; ++f)
+      for (int s = 0; s < ncp; ++s) {
+        tb[(f * 3 + 0) * ncp + s] = d->cpml_b_host[f * ncp + s];
+        tb[(f * 3 + 1) * ncp + s] = d->cpml_c_host[f * ncp + s];
+        const float kap = d->cpml_kappa_host[f * ncp + s];
+        tb[(f * 3 + 2) * ncp + s] = 1.0f / kap - 1.0f;  // rfx/boundaries/cpml.py:616
+      }
+    float* dcp = nullptr;
+    if (int rc = p->alloc(&dcp, tb.size())) return bail(rc);
+    if (cudaMemcpy(dcp, tb.data(), tb.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(RFXB_E_LAUNCH, "cudaMemcpy"));
+    I.cpb = dcp;
+    for (int f = 0; f < 6; ++f) {
+      if (!(d->cpml_cell[f] > 0.0)) return bail(fail(RFXB_E_INVALID, "CPML cell sizes must be positive"));
+      I.ib[f] = (float)(1.0 / d->cpml_cell[f]);
+    }
+    p->psi_elems[0] = 4LL * ncp * d->ny * I.zs;
+    p->psi_elems[1] = 4LL * d->nx * ncp * I.zs;
+    p->psi_elems[2] = 4LL * d->nx * d->ny * ncp;
+    for (int a = 0; a < 3; ++a) {
+      if (!((I.cpml_axes >> a) & 1u)) { p->psi_elems[a] = 0; }
+      for (int s = 0; s < 2; ++s) {
+        float* q1 = nullptr; float* q2 = nullptr;
+        if (int rc = p->alloc(&q1, p->psi_elems[a])) return bail(rc);
+        if (int rc = p->alloc(&q2, p->psi_elems[a])) return bail(rc);
+        I.psH[s][a] = q1;
+        I.psE[s][a] = q2;
+      }
+    }
+  }
+  I.pec_axes = d->pec_axes & 7u;
+  // sources / probes
+  I.nsrc = d->n_src;
+  I.nprb = d->n_probe;
+  for (int s = 0; s < d->n_src; ++s) {
+    const int32_t* c = d->src_cells_host + 4 * s;
+    p->src.push_back(make_int4(c[0], c[1], c[2], c[3]));
+  }
+  for (int q = 0; q < d->n_probe; ++q) {
+    const int32_t* c = d->probe_cells_host + 4 * q;
+    p->prb.push_back(make_int4(c[0], c[1], c[2], c[3]));
+  }
+  int4* dsrc = nullptr; int4* dprb = nullptr;
+  if (int rc = p->alloc(&dsrc, p->src.size())) return bail(rc);
+  if (int rc = p->alloc(&dprb, p->prb.size())) return bail(rc);
+  if (!p->src.empty() && cudaMemcpy(dsrc, p->src.data(), p->src.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(RFXB_E_LAUNCH, "cudaMemcpy"));
+  if (!p->prb.empty() && cudaMemcpy(dprb, p->prb.data(), p->prb.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(RFXB_E_LAUNCH, "cudaMemcpy"));
+  I.src = dsrc; I.src_ld = d->n_src;
+  I.prb = dprb; I.prb_ld = d->n_probe;
+  // DFT compensation buffers
+  for (int q = 0; q < d->n_dft; ++q) {
+    const RfxbDftDesc& dd = d->dft_host[q];
+    p->dft.push_back(dd);
+    const long long n1 = dd.axis == 0 ? d->ny : d->nx;
+    const long long n2 = dd.axis == 2 ? d->ny : d->nz;
+    float2* c = nullptr;
+    if (int rc = p->alloc(&c, (size_t)dd.n_freqs * n1 * n2)) return bail(rc);
+    p->dft_cmp.push_back(c);
+    p->dft_cells.push_back(n1 * n2);
+  }
+  for (int k = 0; k < 6; ++k) I.hb[k] = hb[k];
+  if (hb[0] >= hb[1]) { I.hb[0] = 0; I.hb[1] = 0; }
+  p->hcells = (long long)(I.hb[1] - I.hb[0]) * (I.hb[3] - I.hb[2]) * (I.hb[5] - I.hb[4]);
+  I.hist = nullptr;
+  // own single-plan group
+  RfxbBatch* g = new RfxbBatch();
+  g->plans.push_back(p);
+  if (int rc = build_group(g)) { delete g; return bail(rc); }
+  p->self_group = g;
+  if (cudaDeviceSynchronize() != cudaSuccess) { delete g; return bail(fail(RFXB_E_LAUNCH, "setup failed")); }
+  if (int rc = rfxb_plan_reset(p, nullptr)) { delete g; return bail(rc); }
+  if (cudaStreamSynchronize(nullptr) != cudaSuccess) { delete g; return bail(fail(RFXB_E_LAUNCH, "reset failed")); }
+  *out = p;
+  return 0;
+}
+
+void rfxb_plan_destroy(RfxbPlan* p) {
+  if (!p) return;
+  cudaDeviceSynchronize();
+  delete p->self_group;
+  delete p;
+}
+
+int rfxb_plan_set_materials(RfxbPlan* p, const float* eps_r, const float* sigma, const float* mu_r,
+                            const uint8_t* edge_mask, void* stream) {
+  if (!p || !eps_r || !sigma) return fail(RFXB_E_INVALID, "plan, eps_r and sigma are required");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (mu_r && !p->ch) {
+    if (int rc = p->alloc(&p->ch, p->elems)) return rc;
+    RFXB_CUDA(cudaMemsetAsync(p->ch, 0, p->elems * sizeof(float), st));
+  }
+  p->inst.ch = mu_r ? p->ch : nullptr;
+  if (edge_mask && !p->emask) {
+    if (int rc = p->alloc(&p->emask, p->elems)) return rc;
+    RFXB_CUDA(cudaMemsetAsync(p->emask, 0, p->elems, st));
+  }
+  p->inst.emask = edge_mask ? p->emask : nullptr;
+  const long long cells = (long long)p->nx * p->ny * p->nz;
+  const int blocks = (int)std::min<long long>((cells + 255) / 256, 65535LL * 8);
+  coef_kernel<<<blocks, 256, 0, st>>>(p->inst, p->ca, p->cb, p->ce, mu_r ? p->ch : nullptr, eps_r, sigma, mu_r,
+                                      edge_mask, edge_mask ? p->emask : nullptr, (float)p->dt);
+  RFXB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int rfxb_plan_reset(RfxbPlan* p, void* stream) {
+  if (!p) return fail(RFXB_E_INVALID, "null plan");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (int s = 0; s < 2; ++s)
+    for (int c = 0; c < 6; ++c) RFXB_CUDA(cudaMemsetAsync(p->inst.F[s][c], 0, p->elems * sizeof(float), st));
+  for (int s = 0; s < 2; ++s)
+    for (int a = 0; a < 3; ++a) {
+      if (p->psi_elems[a] > 0) {
+        RFXB_CUDA(cudaMemsetAsync(p->inst.psH[s][a], 0, p->psi_elems[a] * sizeof(float), st));
+        RFXB_CUDA(cudaMemsetAsync(p->inst.psE[s][a], 0, p->psi_elems[a] * sizeof(float), st));
+      }
+    }
+  for (size_t q = 0; q < p->dft_cmp.size(); ++q)
+    RFXB_CUDA(cudaMemsetAsync(p->dft_cmp[q], 0, p->dft[q].n_freqs * p->dft_cells[q] * sizeof(float2), st));
+  p->par = 0;
+  return 0;
+}
+
+int rfxb_plan_load_fields(RfxbPlan* p, const float* const* fields, void* stream) {
+  if (!p || !fields) return fail(RFXB_E_INVALID, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long cells = (long long)p->nx * p->ny * p->nz;
+  const int blocks = (int)std::min<long long>((cells + 255) / 256, 65535LL * 8);
+  for (int c = 0; c < 6; ++c) {
+    if (!fields[c]) return fail(RFXB_E_INVALID, "null field pointer");
+    pack_kernel<<<blocks, 256, 0, st>>>(p->inst.F[p->par][c], fields[c], p->inst);
+  }
+  RFXB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int rfxb_plan_store_fields(RfxbPlan* p, float* const* fields, void* stream) {
+  if (!p || !fields) return fail(RFXB_E_INVALID, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long cells = (long long)p->nx * p->ny * p->nz;
+  const int blocks = (int)std::min<long long>((cells + 255) / 256, 65535LL * 8);
+  for (int c = 0; c < 6; ++c) {
+    if (!fields[c]) return fail(RFXB_E_INVALID, "null field pointer");
+    unpack_kernel<<<blocks, 256, 0, st>>>(fields[c], p->inst.F[p->par][c], p->inst);
+  }
+  RFXB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int rfxb_plan_advance(RfxbPlan* p, const RfxbStepIO* io, int step0, int n_steps, void* stream) {
+  if (!p) return fail(RFXB_E_INVALID, "null plan");
+  return group_advance(p->self_group, io, step0, n_steps, static_cast<cudaStream_t>(stream));
+}
+
+int rfxb_forward(RfxbPlan* p, const RfxbStepIO* io, float* const* fields, int step0, int n_steps, void* stream) {
+  if (int rc = rfxb_plan_load_fields(p, fields, stream)) return rc;
+  if (int rc = rfxb_plan_advance(p, io, step0, n_steps, stream)) return rc;
+  return rfxb_plan_store_fields(p, fields, stream);
+}
+
+int rfxb_plan_record_history(RfxbPlan* p, int step0, int n_steps) {
+  if (!p) return fail(RFXB_E_INVALID, "null plan");
+  if (p->hcells == 0) return fail(RFXB_E_STATE, "plan has no gradient region");
+  if (n_steps < 0 || step0 < 0) return fail(RFXB_E_INVALID, "negative history range");
+  const long long need = (long long)n_steps * 6 * p->hcells;
+  if (need > p->hist_cap) {
+    cudaDeviceSynchronize();
+    if (p->hist) {
+      auto it = std::find(p->allocs.begin(), p->allocs.end(), (void*)p->hist);
+      if (it != p->allocs.end()) p->allocs.erase(it);
+      cudaFree(p->hist);
+      p->hist = nullptr;
+    }
+    if (int rc = p->alloc(&p->hist, need)) return rc;
+    p->hist_cap = need;
+  }
+  p->inst.hist = p->hist;
+  p->inst.hist_ld = 6 * p->hcells;
+  p->inst.hist_step0 = step0;
+  p->inst.hist_nsteps = n_steps;
+  return 0;
+}
+
+int rfxb_plan_checkpoint_reserve(RfxbPlan* p, int n_slots) {
+  if (!p || n_slots < 0) return fail(RFXB_E_INVALID, "bad checkpoint request");
+  const long long per = 6 * p->elems + 2 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2]);
+  while ((int)p->ckpt.size() < n_slots) {
+    float* q = nullptr;
+    if (int rc = p->alloc(&q, per)) return rc;
+    p->ckpt.push_back(q);
+    p->ckpt_valid.push_back(0);
+  }
+  return 0;
+}
+
+int rfxb_plan_checkpoint_save(RfxbPlan* p, int slot, void* stream) {
+  if (!p || slot < 0 || slot >= (int)p->ckpt.size()) return fail(RFXB_E_INVALID, "checkpoint slot out of range");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float* dst = p->ckpt[slot];
+  for (int c = 0; c < 6; ++c) {
+    RFXB_CUDA(cudaMemcpyAsync(dst, p->inst.F[p->par][c], p->elems * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    dst += p->elems;
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (p->psi_elems[a] == 0) continue;
+    RFXB_CUDA(cudaMemcpyAsync(dst, p->inst.psH[p->par][a], p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    dst += p->psi_elems[a];
+    RFXB_CUDA(cudaMemcpyAsync(dst, p->inst.psE[p->par][a], p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    dst += p->psi_elems[a];
+  }
+  p->ckpt_valid[slot] = 1;
+  return 0;
+}
+
+int rfxb_plan_checkpoint_load(RfxbPlan* p, int slot, void* stream) {
+  if (!p || slot < 0 || slot >= (int)p->ckpt.size()) return fail(RFXB_E_INVALID, "checkpoint slot out of range");
+  if (!p->ckpt_valid[slot]) return fail(RFXB_E_STATE, "checkpoint slot was never saved");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float* src = p->ckpt[slot];
+  for (int c = 0; c < 6; ++c) {
+    RFXB_CUDA(cudaMemcpyAsync(p->inst.F[p->par][c], src, p->elems * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    src += p->elems;
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (p->psi_elems[a] == 0) continue;
+    RFXB_CUDA(cudaMemcpyAsync(p->inst.psH[p->par][a], src, p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    src += p->psi_elems[a];
+    RFXB_CUDA(cudaMemcpyAsync(p->inst.psE[p->par][a], src, p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    src += p->psi_elems[a];
+  }
+  return 0;
+}
+
+int rfxb_plan_adjoint_begin(RfxbPlan* p, const RfxbAdjointIO* aio, int n_total, void* stream) {
+  if (!p || !aio) return fail(RFXB_E_INVALID, "null argument");
+  return group_adjoint_begin(p->self_group, aio, n_total, static_cast<cudaStream_t>(stream));
+}
+
+int rfxb_plan_adjoint_advance(RfxbPlan* p, const RfxbAdjointIO* aio, int step_hi, int n_steps, void* stream) {
+  if (!p || !aio) return fail(RFXB_E_INVALID, "null argument");
+  return group_adjoint_advance(p->self_group, aio, step_hi, n_steps, static_cast<cudaStream_t>(stream));
+}
+
+int rfxb_batch_create(RfxbPlan* const* plans, int n_plans, RfxbBatch** out) {
+  if (!plans || n_plans < 1 || !out) return fail(RFXB_E_INVALID, "bad batch arguments");
+  *out = nullptr;
+  RfxbBatch* g = new RfxbBatch();
+  for (int q = 0; q < n_plans; ++q) {
+    if (!plans[q]) { delete g; return fail(RFXB_E_INVALID, "null plan in batch"); }
+    g->plans.push_back(plans[q]);
+  }
+  if (int rc = build_group(g)) { delete g; return rc; }
+  *out = g;
+  return 0;
+}
+
+void rfxb_batch_destroy(RfxbBatch* g) {
+  if (!g) return;
+  cudaDeviceSynchronize();
+  delete g;
+}
+
+int rfxb_batch_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, void* stream) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  return group_advance(g, ios, step0, n_steps, static_cast<cudaStream_t>(stream));
+}
+
+int rfxb_batch_record_history(RfxbBatch* g, int step0, int n_steps) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  for (auto* p : g->plans)
+    if (p->hcells > 0)
+      if (int rc = rfxb_plan_record_history(p, step0, n_steps)) return rc;
+  return 0;
+}
+
+int rfxb_batch_adjoint_begin(RfxbBatch* g, const RfxbAdjointIO* aios, int n_total, void* stream) {
+  if (!g || !aios) return fail(RFXB_E_INVALID, "null argument");
+  return group_adjoint_begin(g, aios, n_total, static_cast<cudaStream_t>(stream));
+}
+
+int rfxb_batch_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, int n_steps, void* stream) {
+  if (!g || !aios) return fail(RFXB_E_INVALID, "null argument");
+  return group_adjoint_advance(g, aios, step_hi, n_steps, static_cast<cudaStream_t>(stream));
+}
+
+int64_t rfxb_plan_device_bytes(const RfxbPlan* p) {
+  if (!p) return 0;
+  int64_t b = 0;
+  b += 12 * p->elems * 4;                  // fields
+  b += 3 * p->elems * 4;                   // ca cb ce
+  if (p->ch) b += p->elems * 4;
+  if (p->emask) b += p->elems;
+  b += 4 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2]) * 4;
+  if (p->adj_alloc) b += (6 * p->elems + 4 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2])) * 4;
+  b += p->hist_cap * 4;
+  b += (int64_t)p->ckpt.size() * (6 * p->elems + 2 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2])) * 4;
+  return b;
+}
+
+}  // extern "C"

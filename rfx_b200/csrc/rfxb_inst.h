@@ -1,0 +1,96 @@
+// Device-side descriptors shared by the forward, adjoint and DFT kernels.
+//
+// Internal state layout (one simulation, "instance"): every per-cell array
+// (fields, coefficients) uses a padded copy of the reference's (nx, ny, nz)
+// C-order layout with z fastest:
+//
+//   element(i, j, k) = off0 + i*ps + j*zs + k,   i in [-1, nx], j in [-1, ny]
+//
+// zs = round_up(nz + 1, 32) is the row stride (128-byte aligned rows), and
+// ps = (ny + 2) * zs the plane stride.  Planes i = -1 and i = nx, rows j = -1
+// and j = ny, and the row tail k in [nz, zs) are zero guards that are never
+// written.  Because the element before a row start is the previous row's
+// tail, k = -1 also reads zero.  The guards are exactly the reference's
+// zero padding in _shift_fwd / _shift_bwd (rfx/core/yee.py:121-138), so the
+// stencils carry no boundary branches.
+#pragma once
+#include <cstdint>
+
+#define RFXB_TZ 32          // tile extent along z (one warp)
+#define RFXB_MAXC 6
+
+// CPML psi layout per axis (q = which of the two corrected components):
+//   x: ((side*2 + q)*n + s)*ny*zs + j*zs + k
+//   y: ((side*2 + q)*nx + i)*n*zs + s*zs + k
+//   z: ((side*2 + q)*nx + i)*ny*n + j*n + s
+struct RfxbInst {
+  int nx, ny, nz, zs;
+  long long ps;            // plane stride (elements)
+  long long off0;          // element offset of cell (0,0,0)
+  float* F[2][6];          // ping-pong field buffers: ex ey ez hx hy hz
+  const float* ca;         // per cell, E decay coefficient
+  const float* cb;         // per cell, E curl coefficient
+  const float* ce;         // per cell, dt/(eps_r eps0) for CPML-E
+  const float* ch;         // per cell dt/(mu_r mu0), or null -> ch0
+  float ch0;
+  // inverse spacing tables; pointers address entry 0, entries -1 and n valid
+  const float* xe; const float* xh;
+  const float* ye; const float* yh;
+  const float* ze; const float* zh;
+  // CPML
+  int ncp;                 // layers per face (0 = none)
+  unsigned cpml_axes;      // bit a set -> axis a absorbs
+  const float* cpb;        // [face][3][ncp]: b, c, (1/kappa - 1); face = 2*axis + side
+  float ib[6];             // 1 / boundary cell size per face
+  float* psH[2][3];        // H-side psi per axis, ping-pong
+  float* psE[2][3];        // E-side psi per axis, ping-pong
+  // PEC
+  unsigned pec_axes;       // bit a set -> zero tangential E on both faces of axis a
+  const unsigned char* emask;  // per cell bits (1 ex, 2 ey, 4 ez) zeroed, or null
+  // sources: E_c[i,j,k] += w[n*src_ld + s]
+  int nsrc;
+  const int4* src;         // (i, j, k, comp)
+  const float* srcw;
+  int src_ld;
+  // probes: out[n*prb_ld + p] = field; comp bits 0..2, bit 4 = sample before sources
+  int nprb;
+  const int4* prb;
+  float* prb_out;
+  int prb_ld;
+  // gradient-region history: per step 6 * hcells floats (E_old xyz, curl xyz)
+  int hb[6];               // i0 i1 j0 j1 k0 k1 (half-open), empty if i0 >= i1
+  float* hist;
+  long long hist_ld;
+  int hist_step0;
+  int hist_nsteps;
+  // adjoint-only inputs
+  const float* g;          // dJ/d(probe) table [n*g_ld + p]
+  int g_ld;
+  const float* dca;        // d ca / d eps_r over the gradient region
+  const float* dcb;        // d cb / d eps_r over the gradient region
+  double* grad;            // accumulated dJ/d eps_r over the gradient region
+  float* src_adj;          // dJ/d w[n, s] output [n*src_ld + s]
+};
+
+struct AdjInst {           // adjoint state of one instance (same layouts as the forward state)
+  float* aF[6];            // aex aey aez ahx ahy ahz
+  float* aPsiH[2][3];      // ping-pong
+  float* aPsiE[2][3];
+};
+
+struct RfxbWork {          // one CTA: a (y, z) tile over an x range
+  int inst;
+  int y0, z0;
+  int xa, xb;
+};
+
+struct RfxbDftPlane {      // one running-DFT plane of one instance
+  int inst;
+  int axis, index, comp;
+  int nf;
+  int n1, n2;              // plane extents (reference order)
+  float2* acc;             // caller accumulator (nf, n1, n2) complex64
+  float2* cmp;             // Kahan compensation, same shape
+  const float2* phase;     // [n][nf]: (cos, sin) * dt of the sample time
+  int block0;              // first CTA of this plane in the launch
+};

@@ -1,0 +1,291 @@
+"""Drop-in ``run()`` for the uniform lane, backed by the CUDA step kernel.
+
+Mirrors ``rfx.simulation.run`` (rfx/simulation.py:1686-2138): the same
+arguments for the features on this path, the same source / probe / DFT-plane
+specs, the same ``SimResult`` fields, and the same errors for bad
+``checkpoint_segments``.  The whole ``jax.lax.scan`` (rfx/simulation.py:1977)
+runs as one resident device simulation; features outside this path
+(dispersion, TFSF, NTFF, waveguide ports, conformal PEC, periodic axes, ...)
+raise ``NotImplementedError`` instead of silently changing the physics.
+"""
+
+from __future__ import annotations
+
+from typing import NamedTuple
+
+import numpy as np
+import torch
+
+from .cpml import build_cpml
+from .engine import Plan, PlanSpec, require_cuda
+from .grid import face_pads, spacing_tables
+from .sources import SourceSpec  # noqa: F401  (re-export: the reference's spec type)
+
+
+class MaterialArrays(NamedTuple):
+    """rfx/core/yee.py:31-39."""
+    eps_r: np.ndarray
+    sigma: np.ndarray
+    mu_r: np.ndarray
+
+
+class FDTDState(NamedTuple):
+    """rfx/core/yee.py:16-28 (final fields of a run)."""
+    ex: np.ndarray
+    ey: np.ndarray
+    ez: np.ndarray
+    hx: np.ndarray
+    hy: np.ndarray
+    hz: np.ndarray
+    step: int
+
+
+class ProbeSpec(NamedTuple):
+    """rfx/simulation.py:75-80."""
+    i: int
+    j: int
+    k: int
+    component: str
+
+
+class LumpedPortSParamSpec(NamedTuple):
+    """rfx/simulation.py:102-132: V/I DFT at a single-cell lumped port."""
+    i: int
+    j: int
+    k: int
+    component: str
+    freqs: np.ndarray
+    impedance: float
+
+
+class DFTPlaneProbe(NamedTuple):
+    """rfx/probes/probes.py:379-405."""
+    accumulator: np.ndarray
+    freqs: np.ndarray
+    component: str
+    axis: int
+    index: int
+    total_steps: int = 0
+    window: str = "rect"
+    window_alpha: float = 0.25
+
+
+class SimResult(NamedTuple):
+    """rfx/simulation.py:135-178 (fields on this path)."""
+    state: FDTDState | None
+    time_series: np.ndarray
+    ntff_data: object = None
+    dft_planes: tuple | None = None
+    flux_monitors: tuple | None = None
+    waveguide_ports: tuple | None = None
+    wire_port_sparams: tuple | None = None
+    lumped_port_sparams: tuple | None = None
+    snapshots: dict | None = None
+    ntff_box: object = None
+    grid: object = None
+    wire_refplane_sparams: tuple | None = None
+
+
+def init_dft_plane_probe(axis, index, component, freqs, grid_shape, dft_total_steps=0,
+                         dft_window="rect", dft_window_alpha=0.25) -> DFTPlaneProbe:
+    """rfx/probes/probes.py:408-449 (complex64 accumulator)."""
+    if axis == 0:
+        plane = (grid_shape[1], grid_shape[2])
+    elif axis == 1:
+        plane = (grid_shape[0], grid_shape[2])
+    else:
+        plane = (grid_shape[0], grid_shape[1])
+    freqs = np.asarray(freqs, np.float32)
+    return DFTPlaneProbe(np.zeros((len(freqs),) + plane, np.complex64), freqs, component, int(axis),
+                         int(index), int(dft_total_steps), dft_window, float(dft_window_alpha))
+
+
+def tangential_edge_masks(cell_mask):
+    """Per-component tangential edge masks of a PEC cell mask on non-periodic
+    3-D axes (rfx/boundaries/pec.py:90-176), packed as bits 1/2/4."""
+    m = np.asarray(cell_mask, dtype=bool)
+    bits = np.zeros(m.shape, np.uint8)
+    for ax in range(3):
+        nb = np.zeros_like(m)
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[ax] = slice(1, None)
+        hi[ax] = slice(0, -1)
+        nb[tuple(lo)] |= m[tuple(hi)]
+        nb[tuple(hi)] |= m[tuple(lo)]
+        bits |= ((m & nb).astype(np.uint8) << ax)
+    return bits
+
+
+def dft_phase_table(freqs, n_steps, dt, time_offset):
+    """(n_steps, n_freqs, 2) float32 of ``(cos, sin)(-2 pi f t) * dt``.
+
+    The sample time follows the reference: ``t = (n + 1) dt`` on the uniform
+    lane (rfx/simulation.py:1574) and ``n dt`` on the graded lane
+    (rfx/nonuniform.py:1461), with the float32 phase argument
+    ``f32(-2 pi f) * f32(t)`` of those lines.
+    """
+    fr = np.asarray(freqs, np.float32)
+    w = (fr * np.float32(-2.0 * np.pi)).astype(np.float32)
+    t = np.arange(time_offset, time_offset + n_steps, dtype=np.float32) * np.float32(dt)
+    arg = (t[:, None] * w[None, :]).astype(np.float32).astype(np.float64)
+    out = np.empty((n_steps, len(fr), 2), np.float32)
+    out[..., 0] = np.cos(arg) * dt
+    out[..., 1] = np.sin(arg) * dt
+    return out
+
+
+def _vi_probes(spec: LumpedPortSParamSpec):
+    """Probe cells whose pre-source samples give the port V and I
+    (rfx/simulation.py:1480-1500)."""
+    i, j, k, c = spec.i, spec.j, spec.k, spec.component
+    if c == "ez":
+        h = [(i, j, k, "hy", 1.0), (i - 1, j, k, "hy", -1.0), (i, j, k, "hx", -1.0), (i, j - 1, k, "hx", 1.0)]
+    elif c == "ex":
+        h = [(i, j, k, "hz", 1.0), (i, j - 1, k, "hz", -1.0), (i, j, k, "hy", -1.0), (i, j, k - 1, "hy", 1.0)]
+    else:
+        h = [(i, j, k, "hx", 1.0), (i, j, k - 1, "hx", -1.0), (i, j, k, "hz", -1.0), (i - 1, j, k, "hz", 1.0)]
+    return [(i, j, k, c, -1.0)] + h
+
+
+def _unsupported(**kw):
+    bad = [k for k, v in kw.items() if v not in (None, False, (), [], 0, "")]
+    if bad:
+        raise NotImplementedError(
+            "rfx_b200 runs the Yee/CPML/source/probe/DFT-plane scan body only; these features are outside that "
+            "path: " + ", ".join(sorted(bad)))
+
+
+def _to_np(a, dtype=np.float32):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return np.asarray(a, dtype=dtype)
+
+
+def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
+               dft_time_offset, lumped_specs=(), return_state=True, report_every=None, report_label="",
+               kappa_max=None, noop_faces=(), device=None):
+    """Shared driver of the uniform and graded lanes."""
+    dev = require_cuda(device)
+    shape = tuple(int(v) for v in grid.shape)
+    n_steps = int(n_steps)
+    srcs = [(int(s[0]), int(s[1]), int(s[2]), s[3], s[4]) for s in sources]
+    prb = [(int(p[0]), int(p[1]), int(p[2]), p[3], False) for p in probes]
+    vi_rows = []
+    for spec in lumped_specs:
+        rows = []
+        for (i, j, k, c, sgn) in _vi_probes(spec):
+            rows.append((len(prb), sgn))
+            prb.append((i, j, k, c, True))
+        vi_rows.append(rows)
+    cp = build_cpml(grid, cpml_axes, kappa_max=kappa_max, noop_faces=noop_faces) if cpml_axes else None
+    plan = Plan(PlanSpec(shape=shape, dt=float(grid.dt), tables=spacing_tables(grid), cpml=cp,
+                         pec_axes=pec_axes, sources=[s[:4] for s in srcs], probes=prb,
+                         dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in dft_planes]), dev)
+    try:
+        em = tangential_edge_masks(_to_np(pec_mask, bool)) if pec_mask is not None else None
+        mu = getattr(materials, "mu_r", None)
+        plan.set_materials(_to_np(materials.eps_r), _to_np(materials.sigma),
+                           None if mu is None else _to_np(mu), em)
+        plan.reset()
+        src_table = None
+        if srcs:
+            tab = np.stack([_to_np(s[4])[:n_steps] for s in srcs], axis=-1)
+            if tab.shape[0] < n_steps:
+                raise ValueError("source waveform shorter than n_steps")
+            src_table = torch.from_numpy(np.ascontiguousarray(tab, np.float32)).to(dev)
+        probe_out = torch.zeros((n_steps, len(prb)), device=dev, dtype=torch.float32) if prb else None
+        accs, phases = [], []
+        for d in dft_planes:
+            accs.append(torch.from_numpy(np.ascontiguousarray(np.asarray(d.accumulator, np.complex64))).to(dev))
+            phases.append(torch.from_numpy(dft_phase_table(d.freqs, n_steps, grid.dt, dft_time_offset)).to(dev))
+        chunk = int(report_every) if report_every else n_steps
+        done = 0
+        while done < n_steps:
+            k = min(chunk, n_steps - done)
+            plan.advance(done, k, src_table, probe_out, accs, phases)
+            done += k
+            if report_every:
+                torch.cuda.current_stream().synchronize()
+                print(f"[PROGRESS] {report_label} step {done}/{n_steps}", flush=True)
+        torch.cuda.current_stream().synchronize()
+        ts_all = probe_out.cpu().numpy() if probe_out is not None else np.zeros((n_steps, 0), np.float32)
+        ts = ts_all[:, :len(probes)]
+        out_planes = tuple(d._replace(accumulator=a.cpu().numpy()) for d, a in zip(dft_planes, accs))
+        lumped = None
+        if lumped_specs:
+            lumped = []
+            for spec, rows in zip(lumped_specs, vi_rows):
+                dx = float(grid.dx)
+                v = ts_all[:, rows[0][0]].astype(np.float64) * rows[0][1] * dx
+                iv = sum(ts_all[:, r].astype(np.float64) * s for r, s in rows[1:]) * dx
+                lumped.append((spec, _vi_dft(v, iv, spec.freqs, float(grid.dt))))
+            lumped = tuple(lumped)
+        state = None
+        if return_state:
+            f = [t.cpu().numpy() for t in plan.store_fields()]
+            state = FDTDState(*f, step=n_steps)
+        return ts, out_planes, lumped, state
+    finally:
+        plan.close()
+
+
+def _vi_dft(v, i, freqs, dt):
+    """Port V/I DFT with the reference's sample time ``n dt``
+    (rfx/simulation.py:1447, 1480-1500), summed in float64."""
+    n = np.arange(len(v), dtype=np.float64)
+    ph = np.exp(-1j * 2.0 * np.pi * np.asarray(freqs, np.float64)[:, None] * (n[None, :] * dt)) * dt
+    return ((ph @ v).astype(np.complex64), (ph @ i).astype(np.complex64))
+
+
+def run(grid, materials, n_steps, *, boundary="pec", cpml_axes="xyz", pec_axes=None, periodic=None, debye=None,
+        lorentz=None, tfsf=None, sources=None, probes=None, dft_planes=None, flux_monitors=None,
+        waveguide_ports=None, ntff=None, snapshot=None, checkpoint=False, checkpoint_segments=None,
+        aniso_eps=None, aniso_inv_eps=None, aniso_inv_eps_smooth=False, pec_mask=None, pec_occupancy=None,
+        conformal_weights=None, wire_port_sparams=None, lumped_port_sparams=None, wire_refplane_sparams=None,
+        lumped_rlc=None, kerr_chi3=None, field_dtype=None, return_state=True, mag_sources=None,
+        stencil_order=2, report_every=None, report_label="", sheet_impedance=None, device=None) -> SimResult:
+    """Uniform-grid scan (rfx/simulation.py:1686).  Step order per
+    rfx/simulation.py:1255-1685: H, CPML-H, E, CPML-E, PEC faces, PEC mask,
+    soft sources, probes, DFT planes at ``t = (n+1) dt``."""
+    _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf, flux_monitors=flux_monitors,
+                 waveguide_ports=waveguide_ports, ntff=ntff, snapshot=snapshot, aniso_eps=aniso_eps,
+                 aniso_inv_eps=aniso_inv_eps, pec_occupancy=pec_occupancy, conformal_weights=conformal_weights,
+                 wire_port_sparams=wire_port_sparams, wire_refplane_sparams=wire_refplane_sparams,
+                 lumped_rlc=lumped_rlc, kerr_chi3=kerr_chi3, mag_sources=mag_sources,
+                 sheet_impedance=sheet_impedance)
+    if periodic is not None and any(periodic):
+        raise NotImplementedError("periodic axes are outside this path")
+    if stencil_order != 2:
+        raise NotImplementedError("only the (2,2) Yee stencil is on this path")
+    if field_dtype not in (None, np.float32, "float32", torch.float32):
+        raise NotImplementedError("fields are float32 on this path")
+    if checkpoint_segments is not None:
+        K = int(checkpoint_segments)
+        if K < 1:
+            raise ValueError(f"checkpoint_segments must be ≥ 1, got {checkpoint_segments}")
+        if n_steps % K != 0:
+            raise ValueError(f"checkpoint_segments={K} does not divide n_steps={n_steps}; pick a divisor")
+        if report_every is not None:
+            raise NotImplementedError("report_every is not supported together with checkpoint_segments")
+    if pec_axes is None:
+        pec_axes = "xyz"
+    use_cpml = boundary == "cpml" and int(grid.cpml_layers) > 0
+    if boundary not in ("pec", "cpml"):
+        raise NotImplementedError(f"boundary={boundary!r} is outside this path")
+    srcs = [(s.i, s.j, s.k, s.component, s.waveform) for s in (sources or [])]
+    prbs = [(p.i, p.j, p.k, p.component) for p in (probes or [])]
+    ts, planes, lumped, state = run_device(
+        grid, materials, n_steps, cpml_axes=cpml_axes if use_cpml else "", pec_axes=pec_axes, sources=srcs,
+        probes=prbs, dft_planes=list(dft_planes or []), pec_mask=pec_mask, dft_time_offset=1,
+        lumped_specs=list(lumped_port_sparams or []), return_state=return_state, report_every=report_every,
+        report_label=report_label, noop_faces=set(getattr(grid, "pec_faces", None) or ()), device=device)
+    return SimResult(state=state, time_series=ts, dft_planes=planes if dft_planes else None,
+                     lumped_port_sparams=lumped, grid=grid)
+
+
+def extract_lumped_s11(v_dft, i_dft, z0=50.0):
+    """rfx/probes/probes.py:1240-1274."""
+    denom = v_dft - z0 * i_dft
+    safe = np.where(np.abs(denom) > 0.0, denom, np.ones_like(denom))
+    return (v_dft + z0 * i_dft) / safe

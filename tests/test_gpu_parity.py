@@ -1,0 +1,99 @@
+"""GPU parity of the CUDA forward path against the oracle and the reference's
+golden vector.  Tolerance: 1e-4 relative L2 against the float32 oracle (the
+acceptance bar for probe traces and DFT fields); the error against the float64
+oracle is printed per result."""
+
+import os
+
+import numpy as np
+import pytest
+
+from tests.scenarios import c1_readme, rel_l2, small_nonuniform, small_uniform
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-4
+
+
+def _check(sc, ts, planes, ref, label):
+    for p in range(ts.shape[1]):
+        e32 = rel_l2(ts[:, p], ref["ts_f32"][:, p])
+        e64 = rel_l2(ts[:, p], ref["ts_f64"][:, p])
+        print(f"{label} probe {p}: relL2 vs oracle f32 {e32:.2e}, vs f64 {e64:.2e}")
+        assert e32 < TOL
+    for q, acc in enumerate(planes):
+        e32 = rel_l2(acc, ref[f"dft{q}_f32"])
+        e64 = rel_l2(acc, ref[f"dft{q}_f64"])
+        print(f"{label} dft {q}: relL2 vs oracle f32 {e32:.2e}, vs f64 {e64:.2e}")
+        assert e32 < TOL
+
+
+@pytest.mark.parametrize("build", [small_uniform, small_nonuniform, c1_readme])
+def test_forward_matches_oracle(cuda, build):
+    sc = build()
+    ref = np.load(os.path.join(GOLDEN, f"oracle_{sc.name}.npz"))
+    ts, planes, _ = sc.run_product()
+    assert ts.shape == ref["ts_f32"].shape
+    _check(sc, ts, planes, ref, sc.name)
+
+
+@pytest.mark.parametrize("build", [small_uniform, small_nonuniform])
+def test_final_fields_match_oracle(cuda, build):
+    sc = build(n_steps=120)
+    ts, planes, fields = sc.run_product()
+    r = sc.run_oracle(np.float32)
+    for c, f in fields.items():
+        e = rel_l2(f, r.state[c])
+        print(f"{sc.name} {c}: relL2 {e:.2e}")
+        assert e < TOL
+
+
+def test_reference_golden_s11_through_device(cuda):
+    """The reference fixture golden_forward_no_rlc_s11.npy (CPML-6 lumped port,
+    1200 steps) reproduced through rfx_b200.run with a lumped-port spec."""
+    import rfx_b200
+    golden = np.load(os.path.join(GOLDEN, "forward_no_rlc_s11.npy"))
+    g = rfx_b200.Grid(freq_max=10e9, domain=(0.02, 0.02, 0.02), dx=0.02 / 15, cpml_layers=6)
+    shape = g.shape
+    mats = rfx_b200.MaterialArrays(np.ones(shape, np.float32), np.zeros(shape, np.float32),
+                                   np.ones(shape, np.float32))
+    lp = rfx_b200.LumpedPort((0.0093, 0.0093, 0.0093), "ez", 50.0, rfx_b200.GaussianPulse(f0=5e9, bandwidth=0.9))
+    mats = rfx_b200.setup_lumped_port(g, lp, mats)
+    src = rfx_b200.make_port_source(g, lp, mats, 1200)
+    i, j, k = g.position_to_index(lp.position)
+    spec = rfx_b200.LumpedPortSParamSpec(i, j, k, "ez", np.array([3., 4., 5., 6., 7.]) * 1e9, 50.0)
+    r = rfx_b200.run(g, mats, 1200, boundary="cpml", pec_axes="", sources=[src], lumped_port_sparams=[spec],
+                     return_state=False)
+    (_, (v, iv)), = r.lumped_port_sparams
+    s11 = rfx_b200.extract_lumped_s11(v, iv, 50.0)
+    print("S11 device", s11, "golden", golden, "rel", np.abs(s11 - golden) / np.abs(golden))
+    np.testing.assert_allclose(s11, golden, rtol=1e-5, atol=1e-6)
+
+
+def test_chunked_advance_is_bit_identical(cuda):
+    """Host-driven chunks continue the same state (tests/test_run_progress_reporting.py)."""
+    import rfx_b200
+    sc = small_uniform(n_steps=100)
+    g = sc.product_grid()
+    mats = rfx_b200.MaterialArrays(*sc.materials)
+    srcs = [rfx_b200.SourceSpec(i, j, k, c, w) for (i, j, k, c, w) in sc.sources]
+    prbs = [rfx_b200.ProbeSpec(i, j, k, c) for (i, j, k, c) in sc.probes]
+    a = rfx_b200.run(g, mats, 100, boundary="cpml", sources=srcs, probes=prbs)
+    b = rfx_b200.run(g, mats, 100, boundary="cpml", sources=srcs, probes=prbs, report_every=37)
+    c = rfx_b200.run(g, mats, 100, boundary="cpml", sources=srcs, probes=prbs)
+    assert np.array_equal(a.time_series, b.time_series)
+    assert np.array_equal(a.time_series, c.time_series)
+    for comp in ("ex", "ey", "ez", "hx", "hy", "hz"):
+        assert np.array_equal(getattr(a.state, comp), getattr(b.state, comp))
+
+
+def test_pec_boundary_without_cpml(cuda):
+    """boundary='pec' cavity (no CPML): tangential E vanishes on every face."""
+    import rfx_b200
+    sc = small_uniform(n_steps=60)
+    sc.boundary = "pec"
+    ref = sc.run_oracle(np.float32)
+    ts, _, fields = sc.run_product()
+    assert rel_l2(ts, ref.time_series) < TOL
+    ey = fields["ey"]
+    assert np.all(ey[0] == 0) and np.all(ey[-1] == 0) and np.all(ey[:, :, 0] == 0)
