@@ -1,0 +1,359 @@
+"""Benchmark of the rfx time-stepping hot path on B200.
+
+Workload (default, the configuration the metric names): a batched design
+sweep -- 64 independent simulations of uneven size (n^3 interior, n ~ U{64..160}
+seeded, CPML 8, +1 fence -> (n+17)^3 cells, 161 M cells in total for seed 0),
+each with 8 seeded dielectric boxes, a 16x16x2 design region, an Ez 12 GHz
+soft source and 4 Ez probes, 2000 time steps; one bench step = forward of all
+64 (one step-kernel launch per time step for the whole batch) + per-instance
+probe-DFT objective + hand-written adjoint sweep giving dJ/d eps_r over every
+design region.  Metric: Mcell-steps/s = total cells x time steps / time,
+counting forward+adjoint once.  Inputs are seeded synthetic data with the
+configuration's shapes (the reference publishes no dataset).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own seeded sweep (independent instances, no
+data-path collective: weak scaling); the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import re
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s fwd+adjoint grad, batched vs single, 1 B200; % HBM roofline"
+UNIT = "Mcell-steps/s"
+
+
+def _workload_config(args, cells, world):
+    return {"workload": f"batched_sweep: {args.instances} instances (n+17)^3, n~U{{64..160}} seed {{rank}}, "
+                        f"CPML 8, {args.time_steps} time steps, forward + probe-DFT objective + adjoint "
+                        f"dJ/d eps_r over 16x16x2 regions",
+            "instances_per_gpu": args.instances, "time_steps": args.time_steps,
+            "cells_per_gpu": int(cells), "adjoint_mode": "history (design-region E^n and curl H recorded in HBM)",
+            "l2": "inputs larger than L2 (state of 161 M cells)", "parallelism": f"independent instances x {world} GPU"}
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.1)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.nv is not None:
+            self.t.join(timeout=2)
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the oracle port; never part of the measured GPU path)
+# ---------------------------------------------------------------------------
+
+def _oracle_sample(args_tuple):
+    """Forward + adjoint of one instance on the oracle for a few time steps."""
+    q, n_time, seed, n_inst = args_tuple
+    import oracle  # noqa: F401
+    from oracle.adjoint import forward_adjoint
+    from oracle.fdtd import make_uniform_grid
+    from rfx_b200.workloads import batched_sweep
+    inst = batched_sweep(seed=seed, n_inst=n_inst, n_steps=n_time)[q]
+    g = inst.grid
+    og = make_uniform_grid(g.domain, g.dx, cpml_layers=g.cpml_layers)
+    assert og.shape == tuple(g.shape)
+    mats = (inst.eps_r, inst.sigma, np.ones(g.shape, np.float32))
+    freqs = inst.freqs
+    dt = g.dt
+
+    def obj_grad(ts):
+        n = np.arange(ts.shape[0])
+        ph = np.exp(-2j * np.pi * freqs[:, None] * n[None, :] * dt) * dt
+        X = ph @ ts.astype(np.float64)
+        return 2.0 * np.real(np.conj(X)[:, None, :] * ph[:, :, None]).sum(0)
+
+    t0 = time.perf_counter()
+    forward_adjoint(og, mats, n_time, boundary="cpml", pec_axes="", sources=inst.sources, probes=inst.probes,
+                    box=inst.box, objective_grad=obj_grad, dtype=np.float32)
+    dt_s = time.perf_counter() - t0
+    return int(np.prod(g.shape)) * n_time, dt_s
+
+
+def _smallest(n_inst, seed):
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(64, 161, n_inst)
+    return int(np.argmin(sizes)), int(sizes.min())
+
+
+def cpu_baseline_port(args, n_workers=1, n_time=60):
+    q, n = _smallest(args.instances, 0)
+    jobs = [(q, n_time, 0, args.instances)] * n_workers
+    t0 = time.perf_counter()
+    if n_workers == 1:
+        res = [_oracle_sample(jobs[0])]
+    else:
+        with mp.get_context("spawn").Pool(n_workers) as pool:
+            res = pool.map(_oracle_sample, jobs)
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    return {"value": work / wall / 1e6, "unit": UNIT, "cores": n_workers, "kind": "port",
+            "sample": f"{n_workers} x instance {q} of seed 0 ({n + 17}^3 cells), {n_time} time steps, forward + "
+                      f"adjoint on the NumPy float32 oracle (the reference's own JAX solver is not installable "
+                      f"here), timed on the host"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def _traffic_per_cell():
+    """DRAM bytes per cell and launch of fwd_step_kernel from the committed
+    ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "fwd_step_kernel.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_cell_per_launch:\s*([0-9.eE+-]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from rfx_b200.batch import Sweep
+    from rfx_b200.workloads import batched_sweep
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    insts = batched_sweep(seed=rank, n_inst=args.instances, n_steps=args.time_steps)
+    sw = Sweep(insts, args.time_steps, device=dev, batched=True)
+    cells = sw.cells()
+    N = args.time_steps
+    stream = torch.cuda.current_stream()
+
+    def one_step():
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sw.forward()
+        e1.record(stream)
+        _, gs = sw.objectives()
+        sw.backward(gs)
+        e2.record(stream)
+        return e0, e1, e2
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    events = []
+    with ClockSampler(local_rank) as clk:
+        t_host0 = time.perf_counter()
+        for _ in range(args.steps):
+            events.append(one_step())
+        torch.cuda.synchronize()
+        t_host = time.perf_counter() - t_host0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms = sum(a.elapsed_time(c) for a, b, c in events)
+    fwd_ms = sum(a.elapsed_time(b) for a, b, c in events)
+    t = torch.tensor([total_ms, fwd_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, fwd_ms = float(t[0]), float(t[1])
+    value = cells * N * args.steps * world / (total_ms / 1e3) / 1e6
+
+    # roofline of the forward step kernel: algorithmic bytes per launch over
+    # its average launch time (forward phase = one launch per time step)
+    alg_bytes = sum(p.algorithmic_bytes_per_step() for p in sw.plans)
+    fwd_launch_s = fwd_ms / 1e3 / (N * args.steps)
+    achieved = alg_bytes / fwd_launch_s / 1e9
+    tpc = _traffic_per_cell()
+    roofline = {"kernel": "fwd_step_kernel<8>", "bound": "hbm", "achieved": round(achieved, 1),
+                "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                "traffic": (round(tpc * cells) if tpc else None),
+                "algorithmic_bytes_per_launch": int(alg_bytes),
+                "fwd_share_of_step": round(fwd_ms / total_ms, 3)}
+
+    # single-instance comparison (each simulation launched on its own)
+    single = None
+    if rank == 0 and not args.no_single:
+        sw1 = Sweep(insts, N, device=dev, batched=False)
+        sw1.forward()
+        _, gs = sw1.objectives()
+        sw1.backward(gs)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sw1.forward()
+        _, gs = sw1.objectives()
+        sw1.backward(gs)
+        b.record(stream)
+        torch.cuda.synchronize()
+        sms = a.elapsed_time(b)
+        single_rate = cells * N / (sms / 1e3) / 1e6
+        batched_rate = cells * N * args.steps / (total_ms / 1e3) / 1e6
+        single = {"value": round(single_rate, 1), "unit": UNIT,
+                  "what": f"same {args.instances} simulations, forward+adjoint launched one simulation at a time",
+                  "batched_over_single": round(batched_rate / single_rate, 3)}
+        sw1.close()
+
+    # end to end through the public API with host buffers: upload every
+    # instance's eps_r / sigma from pinned host memory, run, read J and grads back
+    e2e = None
+    if not args.no_e2e:
+        host_eps = [torch.from_numpy(s.eps_r).pin_memory() for s in insts]
+        host_sig = [torch.from_numpy(s.sigma).pin_memory() for s in insts]
+        h2d = sum(x.numel() * 4 for x in host_eps) + sum(x.numel() * 4 for x in host_sig)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        d2h = 0
+        a.record(stream)
+        for _ in range(args.steps):
+            sw.set_materials([x.to(dev, non_blocking=True) for x in host_eps],
+                             [x.to(dev, non_blocking=True) for x in host_sig])
+            Js, grads = sw.run()
+            outs = [g.to("cpu", non_blocking=True) for g in grads] + [torch.stack(Js).to("cpu", non_blocking=True)]
+            d2h = sum(o.numel() * o.element_size() for o in outs)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ems = a.elapsed_time(b)
+        et = torch.tensor([ems], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": round(cells * N * args.steps * world / (float(et[0]) / 1e3) / 1e6, 1), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "path": "rfx_b200.batch.Sweep.set_materials + run (host pinned eps_r/sigma in, J and dJ/d eps_r out)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_port(args, n_workers=1, n_time=args.cpu_time_steps)
+
+    launches = args.steps * (N + 2 * N + 1)
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 2), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                "config": _workload_config(args, cells, world), "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "single": single, "gpu_launches": launches,
+                "clocks": clk.summary(), "host_wall_s_timed": round(t_host, 3)}
+        print(json.dumps(line), flush=True)
+    sw.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    workers = max(1, min(len(os.sched_getaffinity(0)), 16))
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline_port(args, n_workers=workers, n_time=args.ref_time_steps)
+    for _ in range(args.steps):
+        vals.append(cpu_baseline_port(args, n_workers=workers, n_time=args.ref_time_steps))
+    v = statistics.mean(x["value"] for x in vals)
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": _workload_config(args, 0, world), "cpu_baseline": cb,
+            "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference = NumPy float32 restatement of rfx's scan body and its transpose (oracle port); "
+                    "rfx itself needs JAX, which is not installable offline here"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--time-steps", type=int, default=2000)
+    ap.add_argument("--cpu-time-steps", type=int, default=40)
+    ap.add_argument("--ref-time-steps", type=int, default=20)
+    ap.add_argument("--no-single", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

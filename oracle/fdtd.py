@@ -338,16 +338,19 @@ _CPML_E = {0: (("ey", "hz", -1), ("ez", "hy", +1)),
 
 class _Stepper:
     def __init__(self, grid, materials, *, dtype, nonuniform, cpml_axes,
-                 pec_axes, pec_mask, kappa_max=1.0):
+                 pec_axes, pec_mask, kappa_max=1.0, exact_materials=False):
         self.g = grid
         self.f = np.dtype(dtype)
         self.nu = nonuniform
         shape = grid.shape
         eps_r, sigma, mu_r = materials
         f = self.f
-        self.eps_r = np.asarray(eps_r, np.float32).astype(f)
-        self.sigma = np.asarray(sigma, np.float32).astype(f)
-        self.mu_r = np.asarray(mu_r, np.float32).astype(f)
+        # exact_materials keeps float64 material values (finite-difference
+        # checks); otherwise they are float32 as in the reference.
+        mdt = f if exact_materials else np.float32
+        self.eps_r = np.asarray(eps_r, mdt).astype(f)
+        self.sigma = np.asarray(sigma, mdt).astype(f)
+        self.mu_r = np.asarray(mu_r, mdt).astype(f)
         self.F = {c: np.zeros(shape, f) for c in COMPONENTS}
         self.step_count = 0
         self.cpml_axes = cpml_axes
@@ -565,7 +568,7 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
 
 def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
                 pec_axes=None, sources=(), probes=(), dft_planes=(), pec_mask=None,
-                vi_ports=(), kappa_max=1.0, dtype=np.float32):
+                vi_ports=(), kappa_max=1.0, dtype=np.float32, exact_materials=False):
     """``rfx.simulation.run`` (rfx/simulation.py:1686-2138), scan body order of
     rfx/simulation.py:1255-1685.  ``pec_axes=None`` means all axes
     (rfx/simulation.py:684-691).  ``sources`` are ``(i, j, k, comp, waveform)``,
@@ -575,13 +578,14 @@ def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
         pec_axes = "xyz"
     st = _Stepper(grid, materials, dtype=dtype, nonuniform=False,
                   cpml_axes=cpml_axes if boundary == "cpml" else "",
-                  pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=kappa_max)
+                  pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=kappa_max,
+                  exact_materials=exact_materials)
     return _run(st, n_steps, sources, probes, dft_planes, vi_ports, 1,
                 probes_before_dft=True, dx_vi=grid.dx)
 
 
 def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_planes=(),
-                   pec_mask=None, kappa_max=1.0, dtype=np.float32):
+                   pec_mask=None, kappa_max=1.0, dtype=np.float32, exact_materials=False):
     """``rfx.nonuniform.run_nonuniform`` (rfx/nonuniform.py:1589-1804), scan body
     of rfx/nonuniform.py:1256-1568: PEC on every axis, DFT time stamp ``n dt``
     (rfx/nonuniform.py:1461), DFT before probes."""
@@ -590,6 +594,7 @@ def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_plane
                                              grid.pads[4] + grid.pads[5])) if p > 0)
     st = _Stepper(grid, materials, dtype=dtype, nonuniform=True,
                   cpml_axes=axes if grid.cpml_layers > 0 else "",
-                  pec_axes="xyz", pec_mask=pec_mask, kappa_max=kappa_max)
+                  pec_axes="xyz", pec_mask=pec_mask, kappa_max=kappa_max,
+                  exact_materials=exact_materials)
     return _run(st, n_steps, sources, probes, dft_planes, (), 0,
                 probes_before_dft=False, dx_vi=grid.dx)

@@ -33,7 +33,6 @@ using namespace rfxb;
 namespace {
 
 constexpr int kTY = 8;
-constexpr int kBlockThreads = 32 * kTY;
 
 thread_local std::string g_last_error;
 
@@ -136,19 +135,46 @@ struct RfxbBatch {
 
 namespace {
 
-// Work list: (TY x 32) tiles of (y, z), each over an x range.  The x split
-// is chosen so the whole launch holds a few waves of CTAs.
-void make_work(const RfxbPlan& p, int inst_index, int target_ctas, std::vector<RfxbWork>& out) {
+// Work list: (TY x 32) tiles of (y, z), each over an x range [xa, xb).
+// The x split is chosen for the whole group so the CTA count fills whole
+// waves of the resident capacity (tail waves idle most SMs) while keeping
+// x ranges long enough that the one-plane prologue of each CTA stays cheap.
+int pick_chunks(long long tiles, int min_nx, int resident) {
+  int best = 1;
+  double best_eff = -1.0;
+  for (int c = 1; c <= 64; ++c) {
+    if (c > 1 && min_nx / c < 8) break;
+    const long long total = tiles * c;
+    const long long waves = (total + resident - 1) / resident;
+    const double fill = (double)total / (double)(waves * resident);
+    const double xlen = (double)min_nx / c;
+    const double eff = fill * xlen / (xlen + 1.5);
+    if (eff > best_eff + 1e-9) { best_eff = eff; best = c; }
+  }
+  return best;
+}
+
+void make_work(const RfxbPlan& p, int inst_index, int chunks, std::vector<RfxbWork>& out) {
   const int ty_tiles = (p.ny + kTY - 1) / kTY;
   const int tz_tiles = (p.nz + 31) / 32;
-  const long long tiles = (long long)ty_tiles * tz_tiles;
-  int chunks = (int)std::max<long long>(1, (target_ctas + tiles - 1) / tiles);
-  chunks = std::min(chunks, std::max(1, p.nx / 8));
+  chunks = std::max(1, std::min(chunks, p.nx));
   const int xlen = (p.nx + chunks - 1) / chunks;
   for (int xa = 0; xa < p.nx; xa += xlen)
     for (int y = 0; y < ty_tiles; ++y)
       for (int z = 0; z < tz_tiles; ++z)
         out.push_back(RfxbWork{inst_index, y * kTY, z * 32, xa, std::min(p.nx, xa + xlen)});
+}
+
+int resident_ctas() {
+  static int r = -1;
+  if (r < 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fwd_step_kernel<kTY>, 32 * kTY, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 4;
+    r = per_sm * sm_count();
+  }
+  return r;
 }
 
 int upload_tables(RfxbPlan* p, const float* h, int n, const float** dst) {
@@ -164,16 +190,14 @@ int upload_tables(RfxbPlan* p, const float* h, int n, const float** dst) {
 int build_group(RfxbBatch* g) {
   std::vector<RfxbInst> insts;
   std::vector<RfxbWork> work;
-  long long total_cells = 0;
-  for (auto* p : g->plans) total_cells += (long long)p->nx * p->ny * p->nz;
-  const int target = sm_count() * 8;
-  for (size_t q = 0; q < g->plans.size(); ++q) {
-    RfxbPlan* p = g->plans[q];
-    const long long cells = (long long)p->nx * p->ny * p->nz;
-    // each instance gets a share of the target proportional to its cells
-    const int share = (int)std::max<long long>(1, (long long)target * cells / std::max<long long>(1, total_cells));
-    make_work(*p, (int)q, share, work);
+  long long tiles = 0;
+  int min_nx = 1 << 30;
+  for (auto* p : g->plans) {
+    tiles += (long long)((p->ny + kTY - 1) / kTY) * ((p->nz + 31) / 32);
+    min_nx = std::min(min_nx, p->nx);
   }
+  const int chunks = pick_chunks(tiles, min_nx, resident_ctas());
+  for (size_t q = 0; q < g->plans.size(); ++q) make_work(*g->plans[q], (int)q, chunks, work);
   g->n_work = (int)work.size();
   auto galloc = [&](void** ptr, size_t bytes) -> int {
     cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
@@ -308,8 +332,8 @@ int upload_adjoint(RfxbBatch* g, const RfxbAdjointIO* aios, cudaStream_t st) {
     insts[q].dca = a.dca_dev;
     insts[q].dcb = a.dcb_dev;
     insts[q].src_adj = a.src_adj_dev;
-    if (a.grad_dev && (a.dca_dev == nullptr || a.dcb_dev == nullptr || p->hist == nullptr))
-      return fail(RFXB_E_STATE, "gradient requested without coefficient derivatives or recorded history");
+    if (a.grad_dev && (a.dca_dev == nullptr || a.dcb_dev == nullptr || p->hcells == 0))
+      return fail(RFXB_E_STATE, "gradient requested without a gradient region or coefficient derivatives");
     adjs[q] = p->adj;
   }
   RFXB_CUDA(cudaMemcpyAsync(g->d_inst, insts.data(), sizeof(RfxbInst) * insts.size(), cudaMemcpyHostToDevice, st));

@@ -17,12 +17,26 @@
 
 namespace rfxb {
 
+#define RFXB_NSTAGE 4
+
+// One pipeline stage holds everything the step reads from plane i of the
+// input state: E with a one-cell halo on every side, H with the low y/z halo,
+// and the ca/cb coefficients of the tile.
+template <int TY>
+struct FwdStage {
+  float e[3][TY + 2][RFXB_TZ + 2];     // [ex,ey,ez][y - y0 + 1][z - z0 + 1]
+  float h[3][TY + 1][RFXB_TZ + 1];     // [hx,hy,hz][y - y0 + 1][z - z0 + 1] (H^{n-1/2})
+  float cab[2][TY][RFXB_TZ];           // [ca,cb][y - y0][z - z0]
+};
+
 template <int TY>
 struct FwdSmem {
-  float e[3][3][TY + 2][RFXB_TZ + 2];  // [plane buffer][ex,ey,ez][y + 1][z + 1]
-  float h[3][TY + 1][RFXB_TZ + 1];     // [hx,hy,hz][y - y0 + 1][z - z0 + 1]
+  FwdStage<TY> st[RFXB_NSTAGE];        // planes i-1 .. i+2 (buffer (p + 1) & 3)
+  float h[3][TY + 1][RFXB_TZ + 1];     // H^{n+1/2} of plane i with the low y/z halo
   RfxbInst P;
 };
+
+__device__ __forceinline__ int stage_of(int p) { return (p + 1) & (RFXB_NSTAGE - 1); }
 
 // H^{n+1/2} components selected by MASK (1 hx, 2 hy, 4 hz) at (i, jj, kk).
 // E of plane i is in buffer b0 and of plane i+1 in b1; (ly, lz) are the
@@ -31,19 +45,21 @@ template <int TY, int MASK>
 __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, int par,
                                        int b0, int b1, int i, int jj, int kk, int ly, int lz,
                                        bool write_psi, float& hx, float& hy, float& hz) {
-  const long long e = P.off0 + (long long)i * P.ps + (long long)jj * P.zs + kk;
-  const float Ex = S.e[b0][0][ly][lz], Ey = S.e[b0][1][ly][lz], Ez = S.e[b0][2][ly][lz];
-  const float dEz_y = S.e[b0][2][ly + 1][lz] - Ez;
-  const float dEy_z = S.e[b0][1][ly][lz + 1] - Ey;
-  const float dEx_z = S.e[b0][0][ly][lz + 1] - Ex;
-  const float dEz_x = S.e[b1][2][ly][lz] - Ez;
-  const float dEy_x = S.e[b1][1][ly][lz] - Ey;
-  const float dEx_y = S.e[b0][0][ly + 1][lz] - Ex;
-  const float chc = P.ch ? P.ch[e] : P.ch0;
+  const FwdStage<TY>& A = S.st[b0];
+  const FwdStage<TY>& B = S.st[b1];
+  const float Ex = A.e[0][ly][lz], Ey = A.e[1][ly][lz], Ez = A.e[2][ly][lz];
+  const float dEz_y = A.e[2][ly + 1][lz] - Ez;
+  const float dEy_z = A.e[1][ly][lz + 1] - Ey;
+  const float dEx_z = A.e[0][ly][lz + 1] - Ex;
+  const float dEz_x = B.e[2][ly][lz] - Ez;
+  const float dEy_x = B.e[1][ly][lz] - Ey;
+  const float dEx_y = A.e[0][ly + 1][lz] - Ex;
+  float chc = P.ch0;
+  if (P.ch) chc = P.ch[P.off0 + (long long)i * P.ps + (long long)jj * P.zs + kk];
   const float xh = __ldg(P.xh + i), yh = __ldg(P.yh + jj), zh = __ldg(P.zh + kk);
-  if (MASK & 1) hx = P.F[par][3][e] - chc * (dEz_y * yh - dEy_z * zh);
-  if (MASK & 2) hy = P.F[par][4][e] - chc * (dEx_z * zh - dEz_x * xh);
-  if (MASK & 4) hz = P.F[par][5][e] - chc * (dEy_x * xh - dEx_y * yh);
+  if (MASK & 1) hx = A.h[0][ly][lz] - chc * (dEz_y * yh - dEy_z * zh);
+  if (MASK & 2) hy = A.h[1][ly][lz] - chc * (dEx_z * zh - dEz_x * xh);
+  if (MASK & 4) hz = A.h[2][ly][lz] - chc * (dEy_x * xh - dEx_y * yh);
   const int n = P.ncp;
   if (n == 0) return;
   int s, sd;
@@ -121,18 +137,35 @@ __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, 
   }
 }
 
+// Stage plane ip of the input state: E (rows y0-1..y0+TY, cols z0-1..z0+32),
+// H (rows y0-1..y0+TY-1, cols z0-1..z0+31) and ca/cb of the tile.  Rows past
+// the grid read the zero guard row j = ny.
 template <int TY>
-__device__ __forceinline__ void load_e_plane(const RfxbInst& P, FwdSmem<TY>& S, const float* const* F,
-                                             int y0, int z0, int ip, int ty, int lane) {
-  const int b = (ip + 3) % 3;
-  for (int c = 0; c < 3; ++c) {
-    const float* base = F[c] + P.off0 + (long long)ip * P.ps + (z0 - 1);
-    for (int r = ty; r < TY + 2; r += TY) {
-      const int jj = min(y0 - 1 + r, P.ny);
-      const float* row = base + (long long)jj * P.zs;
-      cp_async4(&S.e[b][c][r][lane], row + lane);
-      if (lane < 2) cp_async4(&S.e[b][c][r][32 + lane], row + 32 + lane);
+__device__ __forceinline__ void load_stage(const RfxbInst& P, FwdSmem<TY>& S, const float* const* F,
+                                           int y0, int z0, int ip, int ty, int lane) {
+  FwdStage<TY>& D = S.st[stage_of(ip)];
+  const long long pbase = P.off0 + (long long)ip * P.ps + (z0 - 1);
+  for (int r = ty; r < TY + 2; r += TY) {
+    const int jj = min(y0 - 1 + r, P.ny);
+    const long long rb = pbase + (long long)jj * P.zs;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cp_async4(&D.e[c][r][lane], F[c] + rb + lane);
+      if (lane < 2) cp_async4(&D.e[c][r][32 + lane], F[c] + rb + 32 + lane);
     }
+    if (r < TY + 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cp_async4(&D.h[c][r][lane], F[3 + c] + rb + lane);
+        if (lane == 0) cp_async4(&D.h[c][r][32], F[3 + c] + rb + 32);
+      }
+    }
+  }
+  {
+    const int jj = min(y0 + ty, P.ny);
+    const long long o = P.off0 + (long long)ip * P.ps + (long long)jj * P.zs + z0 + lane;
+    cp_async4(&D.cab[0][ty][lane], P.ca + o);
+    cp_async4(&D.cab[1][ty][lane], P.cb + o);
   }
 }
 
@@ -169,19 +202,22 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   float* const* Fout = P.F[par ^ 1];
 
   const int xa = w.xa, xb = w.xb;
-  load_e_plane<TY>(P, S, Fin, w.y0, w.z0, xa - 1, ty, lane);
-  load_e_plane<TY>(P, S, Fin, w.y0, w.z0, xa, ty, lane);
+  // pipeline: planes xa-1 and xa (group 0), xa+1 (group 1), xa+2 (group 2)
+  load_stage<TY>(P, S, Fin, w.y0, w.z0, xa - 1, ty, lane);
+  load_stage<TY>(P, S, Fin, w.y0, w.z0, xa, ty, lane);
   cp_async_commit();
-  load_e_plane<TY>(P, S, Fin, w.y0, w.z0, xa + 1, ty, lane);
+  load_stage<TY>(P, S, Fin, w.y0, w.z0, xa + 1, ty, lane);
   cp_async_commit();
-  cp_async_wait<1>();
+  if (xa + 2 <= P.nx) load_stage<TY>(P, S, Fin, w.y0, w.z0, xa + 2, ty, lane);
+  cp_async_commit();
+  cp_async_wait<2>();
   __syncthreads();
 
   // H of plane xa-1 at this column (computed, not stored: its owner stores it).
   float hy_prev = 0.f, hz_prev = 0.f;
   if (xa > 0 && own) {
     float hx_, hy_, hz_;
-    h_cell<TY, 6>(P, S, par, (xa + 2) % 3, xa % 3, xa - 1, j, k, ly, lz, false, hx_, hy_, hz_);
+    h_cell<TY, 6>(P, S, par, stage_of(xa - 1), stage_of(xa), xa - 1, j, k, ly, lz, false, hx_, hy_, hz_);
     hy_prev = hy_;
     hz_prev = hz_;
   }
@@ -189,11 +225,11 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   const bool has_hist = P.hist != nullptr && (n - P.hist_step0) >= 0 && (n - P.hist_step0) < P.hist_nsteps;
 
   for (int i = xa; i < xb; ++i) {
-    cp_async_wait<0>();
-    __syncthreads();
-    if (i + 2 <= P.nx) load_e_plane<TY>(P, S, Fin, w.y0, w.z0, i + 2, ty, lane);
+    cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
+    __syncthreads();      // ... for every thread; plane i-1's stage is free
+    if (i + 3 <= P.nx) load_stage<TY>(P, S, Fin, w.y0, w.z0, i + 3, ty, lane);
     cp_async_commit();
-    const int b0 = i % 3, b1 = (i + 1) % 3;
+    const int b0 = stage_of(i), b1 = stage_of(i + 1);
 
     // ---- H phase ----
     float hx = 0.f, hy = 0.f, hz = 0.f;
@@ -227,7 +263,8 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
 
     // ---- E phase ----
     if (own) {
-      const float Ex = S.e[b0][0][ly][lz], Ey = S.e[b0][1][ly][lz], Ez = S.e[b0][2][ly][lz];
+      const FwdStage<TY>& A = S.st[b0];
+      const float Ex = A.e[0][ly][lz], Ey = A.e[1][ly][lz], Ez = A.e[2][ly][lz];
       const float dHz_y = hz - S.h[2][ly - 1][lz];
       const float dHy_z = hy - S.h[1][ly][lz - 1];
       const float dHx_z = hx - S.h[0][ly][lz - 1];
@@ -238,7 +275,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
       const float cx = dHz_y * ye - dHy_z * ze;
       const float cy = dHx_z * ze - dHz_x * xe;
       const float cz = dHy_x * xe - dHx_y * ye;
-      const float ca = P.ca[e], cb = P.cb[e];
+      const float ca = A.cab[0][ty][lane], cb = A.cab[1][ty][lane];
       float ex = ca * Ex + cb * cx;
       float ey = ca * Ey + cb * cy;
       float ez = ca * Ez + cb * cz;

@@ -160,6 +160,22 @@ class Plan:
     def handle(self):
         return self._h
 
+    def psi_entries(self) -> int:
+        """CPML psi entries, E and H side, over all absorbing faces."""
+        cp = self.spec.cpml
+        if cp is None or cp.layers <= 0:
+            return 0
+        nx, ny, nz = self.shape
+        cross = {"x": ny * nz, "y": nx * nz, "z": nx * ny}
+        return sum(2 * 2 * 2 * cp.layers * cross[a] for a in cp.axes)
+
+    def algorithmic_bytes_per_step(self) -> int:
+        """Bytes one forward step must move at minimum: six fields read and
+        written (48 B/cell), the ca/cb coefficients (8 B/cell), every psi entry
+        read and written (8 B)."""
+        nx, ny, nz = self.shape
+        return 56 * nx * ny * nz + 8 * self.psi_entries()
+
     def device_bytes(self) -> int:
         return int(self._lib.rfxb_plan_device_bytes(self._h))
 

@@ -28,13 +28,15 @@ class Scenario:
     domain: tuple | None = None
     dx: float | None = None
 
-    def run_oracle(self, dtype=np.float32):
+    def run_oracle(self, dtype=np.float32, exact_materials=False):
         if self.lane == "uniform":
             return oracle.run_uniform(self.ogrid, self.materials, self.n_steps, boundary=self.boundary,
                                       pec_axes=self.pec_axes, sources=self.sources, probes=self.probes,
-                                      dft_planes=self.dft, pec_mask=self.pec_mask, dtype=dtype)
+                                      dft_planes=self.dft, pec_mask=self.pec_mask, dtype=dtype,
+                                      exact_materials=exact_materials)
         return oracle.run_nonuniform(self.ogrid, self.materials, self.n_steps, sources=self.sources,
-                                     probes=self.probes, dft_planes=self.dft, pec_mask=self.pec_mask, dtype=dtype)
+                                     probes=self.probes, dft_planes=self.dft, pec_mask=self.pec_mask, dtype=dtype,
+                                     exact_materials=exact_materials)
 
     def product_grid(self):
         import rfx_b200
