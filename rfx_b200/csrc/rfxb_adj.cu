@@ -21,7 +21,7 @@ namespace rfxb {
 // Pass A: one thread per (j, k) column marching along x.
 __global__ void __launch_bounds__(256)
 adj_pass_a(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
-           const RfxbWork* __restrict__ work, int n, int par) {
+           const RfxbWork* __restrict__ work, int n, int par, int apar) {
   const RfxbWork w = work[blockIdx.x];
   const RfxbInst& P = insts[w.inst];
   const AdjInst& A = adjs[w.inst];
@@ -40,15 +40,15 @@ adj_pass_a(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
     const long long e = P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
     const long long ex1 = e + P.ps, ey1 = e + P.zs, ez1 = e + 1;
     const float cb0 = P.cb[e];
-    const float qx = cb0 * A.aF[0][e], qy = cb0 * A.aF[1][e], qz = cb0 * A.aF[2][e];
+    const float qx = cb0 * A.aF[apar][0][e], qy = cb0 * A.aF[apar][1][e], qz = cb0 * A.aF[apar][2][e];
     const float cbx = P.cb[ex1], cby = P.cb[ey1], cbz = P.cb[ez1];
-    const float qy_x1 = cbx * A.aF[1][ex1], qz_x1 = cbx * A.aF[2][ex1];
-    const float qx_y1 = cby * A.aF[0][ey1], qz_y1 = cby * A.aF[2][ey1];
-    const float qx_z1 = cbz * A.aF[0][ez1], qy_z1 = cbz * A.aF[1][ez1];
+    const float qy_x1 = cbx * A.aF[apar][1][ex1], qz_x1 = cbx * A.aF[apar][2][ex1];
+    const float qx_y1 = cby * A.aF[apar][0][ey1], qz_y1 = cby * A.aF[apar][2][ey1];
+    const float qx_z1 = cbz * A.aF[apar][0][ez1], qy_z1 = cbz * A.aF[apar][1][ez1];
     const float xe0 = __ldg(P.xe + i), xe1 = __ldg(P.xe + i + 1);
-    float ahx = A.aF[3][e] + ((ze0 * qy - ze1 * qy_z1) - (ye0 * qz - ye1 * qz_y1));
-    float ahy = A.aF[4][e] + ((xe0 * qz - xe1 * qz_x1) - (ze0 * qx - ze1 * qx_z1));
-    float ahz = A.aF[5][e] + ((ye0 * qx - ye1 * qx_y1) - (xe0 * qy - xe1 * qy_x1));
+    float ahx = A.aF[apar][3][e] + ((ze0 * qy - ze1 * qy_z1) - (ye0 * qz - ye1 * qz_y1));
+    float ahy = A.aF[apar][4][e] + ((xe0 * qz - xe1 * qz_x1) - (ze0 * qx - ze1 * qx_z1));
+    float ahz = A.aF[apar][5][e] + ((ye0 * qx - ye1 * qx_y1) - (xe0 * qy - xe1 * qy_x1));
     if (ncp) {
       // r(y) = ib (c nu + s ce km aE_t), nu = aPsiE + s ce aE_t, at slab cells y
       // aH_h(x) += r(x) - r(x + 1 along the axis)
@@ -66,7 +66,7 @@ adj_pass_a(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
         const float b = __ldg(tb + s), c = __ldg(tb + ncp + s), km = __ldg(tb + 2 * ncp + s);
         const long long ee = P.off0 + (long long)ii * P.ps + (long long)jj * P.zs + kk;
         const float ce = P.ce[ee];
-        const float at = A.aF[t][ee];
+        const float at = A.aF[apar][t][ee];
         long long qi;
         if (axis == 0) qi = psi_index_x(P, sd, q, s, jj, kk);
         else if (axis == 1) qi = psi_index_y(P, sd, q, s, ii, kk);
@@ -96,15 +96,15 @@ adj_pass_a(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
         }
       }
     }
-    A.aF[3][e] = ahx;
-    A.aF[4][e] = ahy;
-    A.aF[5][e] = ahz;
+    A.aF[apar][3][e] = ahx;
+    A.aF[apar][4][e] = ahy;
+    A.aF[apar][5][e] = ahz;
     // gradient over the recorded region
     if (in_hy && hist_ok && i >= P.hb[0] && i < P.hb[1]) {
       const int ci = ((i - P.hb[0]) * sy + (j - P.hb[2])) * sz + (k - P.hb[4]);
       const float* hp = P.hist + (long long)(n - P.hist_step0) * P.hist_ld + ci;
       const float dca = P.dca[ci], dcb = P.dcb[ci];
-      const float ax = A.aF[0][e], ay = A.aF[1][e], az = A.aF[2][e];
+      const float ax = A.aF[apar][0][e], ay = A.aF[apar][1][e], az = A.aF[apar][2][e];
       double acc = (double)ax * ((double)dca * hp[0] + (double)dcb * hp[3 * hc])
                  + (double)ay * ((double)dca * hp[hc] + (double)dcb * hp[4 * hc])
                  + (double)az * ((double)dca * hp[2 * hc] + (double)dcb * hp[5 * hc]);
@@ -117,7 +117,7 @@ adj_pass_a(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
 // of y_{n-1}, the source adjoint dJ/dw_{n-1}, and the mask for storage.
 __global__ void __launch_bounds__(256)
 adj_pass_b(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
-           const RfxbWork* __restrict__ work, int n, int par) {
+           const RfxbWork* __restrict__ work, int n, int par, int apar) {
   const RfxbWork w = work[blockIdx.x];
   const RfxbInst& P = insts[w.inst];
   const AdjInst& A = adjs[w.inst];
@@ -131,16 +131,16 @@ adj_pass_b(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
     const long long exm = e - P.ps, eym = e - P.zs, ezm = e - 1;
     auto chat = [&](long long ee) { return P.ch ? P.ch[ee] : P.ch0; };
     const float c0 = chat(e);
-    const float px = c0 * A.aF[3][e], py = c0 * A.aF[4][e], pz = c0 * A.aF[5][e];
+    const float px = c0 * A.aF[apar][3][e], py = c0 * A.aF[apar][4][e], pz = c0 * A.aF[apar][5][e];
     const float cxm = chat(exm), cym = chat(eym), czm = chat(ezm);
-    const float py_xm = cxm * A.aF[4][exm], pz_xm = cxm * A.aF[5][exm];
-    const float px_ym = cym * A.aF[3][eym], pz_ym = cym * A.aF[5][eym];
-    const float px_zm = czm * A.aF[3][ezm], py_zm = czm * A.aF[4][ezm];
+    const float py_xm = cxm * A.aF[apar][4][exm], pz_xm = cxm * A.aF[apar][5][exm];
+    const float px_ym = cym * A.aF[apar][3][eym], pz_ym = cym * A.aF[apar][5][eym];
+    const float px_zm = czm * A.aF[apar][3][ezm], py_zm = czm * A.aF[apar][4][ezm];
     const float xh0 = __ldg(P.xh + i), xhm = __ldg(P.xh + i - 1);
     const float ca = P.ca[e];
-    float ax = ca * A.aF[0][e] + ((zh0 * py - zhm * py_zm) - (yh0 * pz - yhm * pz_ym));
-    float ay = ca * A.aF[1][e] + ((xh0 * pz - xhm * pz_xm) - (zh0 * px - zhm * px_zm));
-    float az = ca * A.aF[2][e] + ((yh0 * px - yhm * px_ym) - (xh0 * py - xhm * py_xm));
+    float ax = ca * A.aF[apar][0][e] + ((zh0 * py - zhm * py_zm) - (yh0 * pz - yhm * pz_ym));
+    float ay = ca * A.aF[apar][1][e] + ((xh0 * pz - xhm * pz_xm) - (zh0 * px - zhm * px_zm));
+    float az = ca * A.aF[apar][2][e] + ((yh0 * px - yhm * px_ym) - (xh0 * py - xhm * py_xm));
     if (ncp) {
       // r(y) = ib (c nu + s km p_t), nu = aPsiH + s p_t, p = ch aH1
       // aE_e(x) += r(x - 1 along the axis) - r(x)
@@ -157,7 +157,7 @@ adj_pass_b(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
         const float* tb = P.cpb + (size_t)face * 3 * ncp;
         const float b = __ldg(tb + s), c = __ldg(tb + ncp + s), km = __ldg(tb + 2 * ncp + s);
         const long long ee = P.off0 + (long long)ii * P.ps + (long long)jj * P.zs + kk;
-        const float pt = chat(ee) * A.aF[t][ee];
+        const float pt = chat(ee) * A.aF[apar][t][ee];
         long long qi;
         if (axis == 0) qi = psi_index_x(P, sd, q, s, jj, kk);
         else if (axis == 1) qi = psi_index_y(P, sd, q, s, ii, kk);
@@ -207,16 +207,16 @@ adj_pass_b(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
       if (m & 2u) ay = 0.f;
       if (m & 4u) az = 0.f;
     }
-    A.aF[0][e] = ax;
-    A.aF[1][e] = ay;
-    A.aF[2][e] = az;
+    A.aF[apar][0][e] = ax;
+    A.aF[apar][1][e] = ay;
+    A.aF[apar][2][e] = az;
   }
 }
 
 // mu_N = Q^T g_{N-1} on the E probes (H probes are injected by pass A of the
 // first reverse step), dJ/dw_{N-1} at the sources, stored masked.
 __global__ void adj_init_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
-                                int ninst, int nlast) {
+                                int ninst, int nlast, int apar) {
   const int q = blockIdx.x;
   if (q >= ninst) return;
   const RfxbInst& P = insts[q];
@@ -229,14 +229,14 @@ __global__ void adj_init_kernel(const RfxbInst* __restrict__ insts, const AdjIns
       const int comp = c.w & 7;
       if (comp >= 3) continue;
       const long long e = P.off0 + (long long)c.x * P.ps + (long long)c.y * P.zs + c.z;
-      A.aF[comp][e] += P.g[(long long)nlast * P.g_ld + p];
+      A.aF[apar][comp][e] += P.g[(long long)nlast * P.g_ld + p];
     }
   }
   if (P.src_adj) {
     for (int s = 0; s < P.nsrc; ++s) {
       const int4 c = P.src[s];
       const long long e = P.off0 + (long long)c.x * P.ps + (long long)c.y * P.zs + c.z;
-      P.src_adj[(long long)nlast * P.src_ld + s] = A.aF[c.w][e];
+      P.src_adj[(long long)nlast * P.src_ld + s] = A.aF[apar][c.w][e];
     }
   }
   if (P.g) {
@@ -252,7 +252,7 @@ __global__ void adj_init_kernel(const RfxbInst* __restrict__ insts, const AdjIns
       if ((P.pec_axes & 4u) && (k == 0 || k == P.nz - 1) && comp != 2) zero = true;
       if ((P.pec_axes & 4u) && k == P.nz - 1 && comp == 2) zero = true;
       if (P.emask && (P.emask[e] >> comp) & 1u) zero = true;
-      if (zero) A.aF[comp][e] = 0.f;
+      if (zero) A.aF[apar][comp][e] = 0.f;
     }
   }
 }

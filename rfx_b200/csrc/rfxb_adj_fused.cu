@@ -1,0 +1,456 @@
+// Fused reverse step of the adjoint: the same tiling, x-march, 4-stage
+// cp.async pipeline and halo recomputation as the forward step kernel.
+//
+// The transpose of one forward step (see rfxb_adj.cu for the derivation)
+// has the forward's dependency shape with the roles swapped:
+//   phase A (H-like, needs aE at x and x+1 along each axis):
+//     aH1 = aH + C_H^T(cb aEm) + sum_slabs [r_E(x) - r_E(x+1)]
+//     r_E = ib (c nu + s ce km aE_t),  nu = aPsiE + s ce aE_t,  aPsiE' = b nu
+//   phase B (E-like, needs p = ch aH1 at x and x-1 along each axis):
+//     aE  = ca aEm + C_E^T(p) + sum_slabs [r_H(x-1) - r_H(x)]
+//     r_H = ib (c nu + s km p_t),       nu = aPsiH + s p_t,       aPsiH' = b nu
+// followed by the probe cotangent of y_{n-1}, the source adjoint and the
+// PEC/edge mask.  Adjoint fields and psi are ping-ponged like the forward
+// state, so halo cells recomputed by a neighbour CTA read step-consistent
+// values.  The eps_r gradient over the recorded region is accumulated in
+// phase A from the forward history.
+#include "rfxb_common.cuh"
+
+namespace rfxb {
+
+#define RFXB_ANSTAGE 4
+#define RFXB_AEW 40
+#define RFXB_AHW 36
+
+template <int TY>
+struct __align__(16) AdjStage {
+  float ae[3][TY + 2][RFXB_AEW];   // masked adjoint E, rows y0-1 .. y0+TY, z from z0-4
+  float cbp[TY + 2][RFXB_AEW];     // cb on the same footprint
+  float ah[3][TY + 1][RFXB_AHW];   // adjoint H, rows y0-1 .. y0+TY-1, z from z0-4
+  float ca[TY][RFXB_TZ];           // ca of the tile
+};
+
+template <int TY>
+struct AdjSmem {
+  AdjStage<TY> st[RFXB_ANSTAGE];
+  float p[3][TY + 1][RFXB_TZ + 1];   // ch * aH1 of plane i, [y - y0 + 1][z - z0 + 1]
+  RfxbInst P;
+  AdjInst A;
+};
+
+__device__ __forceinline__ int astage_of(int p) { return (p + 1) & (RFXB_ANSTAGE - 1); }
+
+struct AdjCtx {
+  int nx, ny, nz, zs, ncp, par, apar;
+  long long ps, off0, cs;
+  const float* ch;
+  float ch0;
+  bool cpx, cpy, cpz;
+};
+
+__device__ __forceinline__ long long cell_index(const AdjCtx& C, int i, int j, int k) {
+  return C.off0 + (long long)i * C.ps + (long long)j * C.zs + k;
+}
+
+__device__ __forceinline__ long long psi_q(const RfxbInst& P, int axis, int sd, int q, int s, int i, int j, int k) {
+  if (axis == 0) return psi_index_x(P, sd, q, s, j, k);
+  if (axis == 1) return psi_index_y(P, sd, q, s, i, k);
+  return psi_index_z(P, sd, q, s, i, j);
+}
+
+// r_E of one CPML-E relation at cell (i, j, k) whose masked adjoint E
+// component t is at: the transposed psi recursion and kappa term.
+__device__ __forceinline__ float r_e(const RfxbInst& P, const AdjInst& A, const AdjCtx& C, int axis, int q, float sgn,
+                                     int i, int j, int k, float at, bool write) {
+  const int coord = axis == 0 ? i : axis == 1 ? j : k;
+  const int nax = axis == 0 ? C.nx : axis == 1 ? C.ny : C.nz;
+  if (coord < 0 || coord >= nax) return 0.f;
+  int s;
+  const int sd = cpml_side(coord, nax, C.ncp, s);
+  if (sd < 0) return 0.f;
+  const int face = 2 * axis + sd;
+  const float* tb = P.cpb + (size_t)face * 3 * C.ncp;
+  const float b = __ldg(tb + s), c = __ldg(tb + C.ncp + s), km = __ldg(tb + 2 * C.ncp + s);
+  const float ce = P.ce[cell_index(C, i, j, k)];
+  const long long qi = psi_q(P, axis, sd, q, s, i, j, k);
+  const float nu = A.aPsiE[C.par][axis][qi] + sgn * ce * at;
+  if (write) A.aPsiE[C.par ^ 1][axis][qi] = b * nu;
+  return P.ib[face] * (c * nu + sgn * ce * km * at);
+}
+
+// r_H of one CPML-H relation at cell (i, j, k) with p_t = ch aH1_t there.
+__device__ __forceinline__ float r_h(const RfxbInst& P, const AdjInst& A, const AdjCtx& C, int axis, int q, float sgn,
+                                     int i, int j, int k, float pt, bool write) {
+  const int coord = axis == 0 ? i : axis == 1 ? j : k;
+  const int nax = axis == 0 ? C.nx : axis == 1 ? C.ny : C.nz;
+  if (coord < 0 || coord >= nax) return 0.f;
+  int s;
+  const int sd = cpml_side(coord, nax, C.ncp, s);
+  if (sd < 0) return 0.f;
+  const int face = 2 * axis + sd;
+  const float* tb = P.cpb + (size_t)face * 3 * C.ncp;
+  const float b = __ldg(tb + s), c = __ldg(tb + C.ncp + s), km = __ldg(tb + 2 * C.ncp + s);
+  const long long qi = psi_q(P, axis, sd, q, s, i, j, k);
+  const float nu = A.aPsiH[C.par][axis][qi] + sgn * pt;
+  if (write) A.aPsiH[C.par ^ 1][axis][qi] = b * nu;
+  return P.ib[face] * (c * nu + sgn * km * pt);
+}
+
+// Phase A at (i, jj, kk): aH1 components selected by MASK (1 hx, 2 hy, 4 hz).
+template <int TY, int MASK>
+__device__ __forceinline__ void adj_a_cell(const RfxbInst& P, const AdjInst& A, const AdjSmem<TY>& S,
+                                           const AdjCtx& C, int b0, int b1, int i, int jj, int kk, int ly, int lz,
+                                           float xe0, float xe1, float ye0, float ye1, float ze0, float ze1,
+                                           bool own, float& ahx, float& ahy, float& ahz) {
+  const AdjStage<TY>& X = S.st[b0];
+  const AdjStage<TY>& Y = S.st[b1];
+  const float cb0 = X.cbp[ly][lz];
+  const float ax0 = X.ae[0][ly][lz], ay0 = X.ae[1][ly][lz], az0 = X.ae[2][ly][lz];
+  const float qx = cb0 * ax0, qy = cb0 * ay0, qz = cb0 * az0;
+  const float cbx = Y.cbp[ly][lz];
+  const float ay_x1 = Y.ae[1][ly][lz], az_x1 = Y.ae[2][ly][lz];
+  const float cby = X.cbp[ly + 1][lz];
+  const float ax_y1 = X.ae[0][ly + 1][lz], az_y1 = X.ae[2][ly + 1][lz];
+  const float cbz = X.cbp[ly][lz + 1];
+  const float ax_z1 = X.ae[0][ly][lz + 1], ay_z1 = X.ae[1][ly][lz + 1];
+  if (MASK & 1) ahx = X.ah[0][ly][lz] + ((ze0 * qy - ze1 * (cbz * ay_z1)) - (ye0 * qz - ye1 * (cby * az_y1)));
+  if (MASK & 2) ahy = X.ah[1][ly][lz] + ((xe0 * qz - xe1 * (cbx * az_x1)) - (ze0 * qx - ze1 * (cbz * ax_z1)));
+  if (MASK & 4) ahz = X.ah[2][ly][lz] + ((ye0 * qx - ye1 * (cby * ax_y1)) - (xe0 * qy - xe1 * (cbx * ay_x1)));
+  // CPML-E^T: aH_h(x) += r_E(x) - r_E(x + 1 along the axis); own cells write aPsiE'
+  if (C.cpx) {
+    if (own || (MASK & 4)) ahz += r_e(P, A, C, 0, 0, -1.f, i, jj, kk, ay0, own) -
+                                  r_e(P, A, C, 0, 0, -1.f, i + 1, jj, kk, ay_x1, false);   // (ey <- hz)
+    if (own || (MASK & 2)) ahy += r_e(P, A, C, 0, 1, +1.f, i, jj, kk, az0, own) -
+                                  r_e(P, A, C, 0, 1, +1.f, i + 1, jj, kk, az_x1, false);   // (ez <- hy)
+  }
+  if (C.cpy) {
+    if (own || (MASK & 4)) ahz += r_e(P, A, C, 1, 0, +1.f, i, jj, kk, ax0, own) -
+                                  r_e(P, A, C, 1, 0, +1.f, i, jj + 1, kk, ax_y1, false);   // (ex <- hz)
+    if (own || (MASK & 1)) ahx += r_e(P, A, C, 1, 1, -1.f, i, jj, kk, az0, own) -
+                                  r_e(P, A, C, 1, 1, -1.f, i, jj + 1, kk, az_y1, false);   // (ez <- hx)
+  }
+  if (C.cpz) {
+    if (own || (MASK & 2)) ahy += r_e(P, A, C, 2, 0, -1.f, i, jj, kk, ax0, own) -
+                                  r_e(P, A, C, 2, 0, -1.f, i, jj, kk + 1, ax_z1, false);   // (ex <- hy)
+    if (own || (MASK & 1)) ahx += r_e(P, A, C, 2, 1, +1.f, i, jj, kk, ay0, own) -
+                                  r_e(P, A, C, 2, 1, +1.f, i, jj, kk + 1, ay_z1, false);   // (ey <- hx)
+  }
+}
+
+template <int TY>
+__device__ __forceinline__ void adj_load_stage(AdjSmem<TY>& S, const AdjCtx& C, const float* aF0, const float* ca,
+                                               const float* cb, int y0, int z0, int ip, int tid) {
+  AdjStage<TY>& D = S.st[astage_of(ip)];
+  const long long pb = C.off0 + (long long)ip * C.ps;
+  constexpr int RE = (TY + 2) * 10, RH = (TY + 1) * 9, RC = TY * 8;
+  constexpr int NE = 4 * RE, NH = 3 * RH, NC = RC;
+  for (int t = tid; t < NE + NH + NC; t += 32 * TY) {
+    if (t < NE) {
+      const int c = t / RE, u = t - c * RE, r = u / 10, q = u - r * 10;
+      const int jj = min(y0 - 1 + r, C.ny);
+      const long long off = pb + (long long)jj * C.zs + (z0 - 4 + 4 * q);
+      if (c < 3) cp_async16(&D.ae[c][r][4 * q], aF0 + c * C.cs + off);
+      else cp_async16(&D.cbp[r][4 * q], cb + off);
+    } else if (t < NE + NH) {
+      const int v = t - NE, c = v / RH, u = v - c * RH, r = u / 9, q = u - r * 9;
+      const int jj = min(y0 - 1 + r, C.ny);
+      cp_async16(&D.ah[c][r][4 * q], aF0 + (3 + c) * C.cs + pb + (long long)jj * C.zs + (z0 - 4 + 4 * q));
+    } else {
+      const int v = t - NE - NH, r = v / 8, q = v - r * 8;
+      const int jj = min(y0 + r, C.ny);
+      cp_async16(&D.ca[r][4 * q], ca + pb + (long long)jj * C.zs + (z0 + 4 * q));
+    }
+  }
+}
+
+template <int TY>
+__global__ void __launch_bounds__(32 * TY, 4)
+adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
+                const RfxbWork* __restrict__ work, int n, int par, int apar) {
+  extern __shared__ __align__(16) unsigned char adj_smem_raw[];
+  AdjSmem<TY>& S = *reinterpret_cast<AdjSmem<TY>*>(adj_smem_raw);
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * 32 + lane;
+  const RfxbWork w = work[blockIdx.x];
+  load_inst(S.P, insts + w.inst, tid, 32 * TY);
+  {
+    const int nw = sizeof(AdjInst) / 4;
+    const int* s = reinterpret_cast<const int*>(adjs + w.inst);
+    int* d = reinterpret_cast<int*>(&S.A);
+    for (int t = tid; t < nw; t += 32 * TY) d[t] = __ldg(s + t);
+  }
+  __syncthreads();
+  const RfxbInst& P = S.P;
+  const AdjInst& A = S.A;
+  AdjCtx C;
+  C.nx = P.nx; C.ny = P.ny; C.nz = P.nz; C.zs = P.zs; C.ncp = P.ncp; C.par = par; C.apar = apar;
+  C.ps = P.ps; C.off0 = P.off0; C.cs = P.cs;
+  C.ch = P.ch;
+  C.ch0 = P.ch0;
+  const int y0 = w.y0, z0 = w.z0;
+  // the +1 neighbours of the tile (row y0+TY, column z0+32) also read CPML terms
+  C.cpx = C.ncp > 0 && (P.cpml_axes & 1u);
+  C.cpy = C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY >= C.ny - C.ncp);
+  C.cpz = C.ncp > 0 && (P.cpml_axes & 4u) && (z0 - 1 < C.ncp || z0 + 32 >= C.nz - C.ncp);
+  const float* aF0 = A.aF[apar][0];
+  float* aFo = A.aF[apar ^ 1][0];
+  const int j = y0 + ty, k = z0 + lane;
+  const bool own = (j < C.ny) && (k < C.nz);
+  const int ly = ty + 1, lz = lane + 4, lh = lane + 1;
+  auto chat = [&](int i_, int j_, int k_) { return C.ch ? C.ch[cell_index(C, i_, j_, k_)] : C.ch0; };
+  const float ye0 = own ? __ldg(P.ye + j) : 0.f, ye1 = own ? __ldg(P.ye + j + 1) : 0.f;
+  const float ze0 = own ? __ldg(P.ze + k) : 0.f, ze1 = own ? __ldg(P.ze + k + 1) : 0.f;
+  const float yh0 = own ? __ldg(P.yh + j) : 0.f, yhm = own ? __ldg(P.yh + j - 1) : 0.f;
+  const float zh0 = own ? __ldg(P.zh + k) : 0.f, zhm = own ? __ldg(P.zh + k - 1) : 0.f;
+  const bool row_halo = (ty == 0) && (y0 >= 1) && (k < C.nz);
+  const float ye0_r = row_halo ? __ldg(P.ye + y0 - 1) : 0.f, ye1_r = row_halo ? __ldg(P.ye + y0) : 0.f;
+  const float ze0_r = row_halo ? __ldg(P.ze + k) : 0.f, ze1_r = row_halo ? __ldg(P.ze + k + 1) : 0.f;
+  const int hcw = TY > 1 ? 1 : 0;
+  const bool col_halo = (ty == hcw) && (lane < TY) && (z0 >= 1) && (y0 + lane < C.ny);
+  const float ye0_c = col_halo ? __ldg(P.ye + y0 + lane) : 0.f, ye1_c = col_halo ? __ldg(P.ye + y0 + lane + 1) : 0.f;
+  const float ze0_c = col_halo ? __ldg(P.ze + z0 - 1) : 0.f, ze1_c = col_halo ? __ldg(P.ze + z0) : 0.f;
+  const unsigned pec = P.pec_axes;
+  const bool pec_j = ((pec & 2u) != 0) && (j == 0 || j == C.ny - 1);
+  const bool pec_k0 = ((pec & 4u) != 0) && (k == 0 || k == C.nz - 1);
+  const bool pec_kz = ((pec & 4u) != 0) && (k == C.nz - 1);
+  // probes (cotangent injection) and sources (adjoint read-out) on this column
+  unsigned pmask = 0u, smask = 0u;
+  if (own) {
+    const int np = min(P.nprb, 32);
+    for (int q = 0; q < np; ++q) { const int4 c = __ldg(P.prb + q); if (c.y == j && c.z == k) pmask |= 1u << q; }
+    const int ns = min(P.nsrc, 32);
+    for (int q = 0; q < ns; ++q) { const int4 c = __ldg(P.src + q); if (c.y == j && c.z == k) smask |= 1u << q; }
+  }
+  const bool prb_tail = P.nprb > 32, src_tail = P.nsrc > 32;
+  const bool in_gyz = P.grad && j >= P.hb[2] && j < P.hb[3] && k >= P.hb[4] && k < P.hb[5];
+  const bool hist_ok = P.hist && (n - P.hist_step0) >= 0 && (n - P.hist_step0) < P.hist_nsteps;
+
+  const int xa = w.xa, xb = w.xb;
+  const float* ca = P.ca;
+  const float* cb = P.cb;
+  adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa - 1, tid);
+  adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa, tid);
+  cp_async_commit();
+  adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 1, tid);
+  cp_async_commit();
+  if (xa + 2 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 2, tid);
+  cp_async_commit();
+  cp_async_wait<2>();
+  __syncthreads();
+
+  // phase A of plane xa-1 at this column: p and r_H there (not stored)
+  float py_prev = 0.f, pz_prev = 0.f, rhy_prev = 0.f, rhz_prev = 0.f;
+  if (xa > 0 && own) {
+    float a1, a2, a3;
+    const int im = xa - 1;
+    adj_a_cell<TY, 6>(P, A, S, C, astage_of(im), astage_of(xa), im, j, k, ly, lz, __ldg(P.xe + im),
+                      __ldg(P.xe + xa), ye0, ye1, ze0, ze1, false, a1, a2, a3);
+    if (P.g) {   // H-probe cotangent of y_n at plane xa-1
+      for (unsigned m = pmask; m; m &= m - 1) {
+        const int q = __ffs(m) - 1;
+        const int4 c = __ldg(P.prb + q);
+        if (c.x == im && (c.w & 7) >= 4) {
+          const float gv = __ldg(P.g + (long long)n * P.g_ld + q);
+          if ((c.w & 7) == 4) a2 += gv; else a3 += gv;
+        }
+      }
+      if (prb_tail)
+        for (int q = 32; q < P.nprb; ++q) {
+          const int4 c = __ldg(P.prb + q);
+          if (c.x == im && c.y == j && c.z == k && (c.w & 7) >= 4) {
+            const float gv = __ldg(P.g + (long long)n * P.g_ld + q);
+            if ((c.w & 7) == 4) a2 += gv; else a3 += gv;
+          }
+        }
+    }
+    const float chc = chat(im, j, k);
+    py_prev = chc * a2;
+    pz_prev = chc * a3;
+    if (C.cpx) {
+      rhy_prev = r_h(P, A, C, 0, 0, +1.f, im, j, k, py_prev, false);
+      rhz_prev = r_h(P, A, C, 0, 1, -1.f, im, j, k, pz_prev, false);
+    }
+  }
+
+  for (int i = xa; i < xb; ++i) {
+    cp_async_wait<1>();
+    __syncthreads();
+    if (i + 3 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, i + 3, tid);
+    cp_async_commit();
+    const int b0 = astage_of(i), b1 = astage_of(i + 1);
+    const float xe0 = __ldg(P.xe + i), xe1 = __ldg(P.xe + i + 1);
+    const float xh0 = __ldg(P.xh + i), xhm = __ldg(P.xh + i - 1);
+    const long long e = cell_index(C, i, j, k);
+
+    // ---- phase A ----
+    float ahx = 0.f, ahy = 0.f, ahz = 0.f;
+    if (own) {
+      adj_a_cell<TY, 7>(P, A, S, C, b0, b1, i, j, k, ly, lz, xe0, xe1, ye0, ye1, ze0, ze1, true, ahx, ahy, ahz);
+      if (P.g && (pmask || prb_tail)) {   // H-probe cotangent of y_n
+        for (unsigned m = pmask; m; m &= m - 1) {
+          const int q = __ffs(m) - 1;
+          const int4 c = __ldg(P.prb + q);
+          if (c.x == i && (c.w & 7) >= 3) {
+            const float gv = __ldg(P.g + (long long)n * P.g_ld + q);
+            if ((c.w & 7) == 3) ahx += gv; else if ((c.w & 7) == 4) ahy += gv; else ahz += gv;
+          }
+        }
+        if (prb_tail)
+          for (int q = 32; q < P.nprb; ++q) {
+            const int4 c = __ldg(P.prb + q);
+            if (c.x == i && c.y == j && c.z == k && (c.w & 7) >= 3) {
+              const float gv = __ldg(P.g + (long long)n * P.g_ld + q);
+              if ((c.w & 7) == 3) ahx += gv; else if ((c.w & 7) == 4) ahy += gv; else ahz += gv;
+            }
+          }
+      }
+      aFo[3 * C.cs + e] = ahx;
+      aFo[4 * C.cs + e] = ahy;
+      aFo[5 * C.cs + e] = ahz;
+      if (in_gyz && hist_ok && i >= P.hb[0] && i < P.hb[1]) {
+        const int sy = P.hb[3] - P.hb[2], sz = P.hb[5] - P.hb[4];
+        const int hc = (P.hb[1] - P.hb[0]) * sy * sz;
+        const int ci = ((i - P.hb[0]) * sy + (j - P.hb[2])) * sz + (k - P.hb[4]);
+        const float* hp = P.hist + (long long)(n - P.hist_step0) * P.hist_ld + ci;
+        const float dca = P.dca[ci], dcb = P.dcb[ci];
+        const AdjStage<TY>& X = S.st[b0];
+        const double acc = (double)X.ae[0][ly][lz] * ((double)dca * hp[0] + (double)dcb * hp[3 * hc]) +
+                           (double)X.ae[1][ly][lz] * ((double)dca * hp[hc] + (double)dcb * hp[4 * hc]) +
+                           (double)X.ae[2][ly][lz] * ((double)dca * hp[2 * hc] + (double)dcb * hp[5 * hc]);
+        P.grad[ci] += acc;
+      }
+    }
+    const float chc = own ? chat(i, j, k) : 0.f;
+    S.p[0][ly][lh] = chc * ahx;
+    S.p[1][ly][lh] = chc * ahy;
+    S.p[2][ly][lh] = chc * ahz;
+    if (ty == 0) {   // halo row j = y0 - 1: hx, hz
+      float a1 = 0.f, a2 = 0.f, a3 = 0.f;
+      float chr = 0.f;
+      if (row_halo) {
+        adj_a_cell<TY, 5>(P, A, S, C, b0, b1, i, y0 - 1, k, 0, lz, xe0, xe1, ye0_r, ye1_r, ze0_r, ze1_r, false,
+                          a1, a2, a3);
+        chr = chat(i, y0 - 1, k);
+        if (P.g) {
+          for (int q = 0; q < P.nprb; ++q) {
+            const int4 c = __ldg(P.prb + q);
+            if (c.x == i && c.y == y0 - 1 && c.z == k && ((c.w & 7) == 3 || (c.w & 7) == 5)) {
+              const float gv = __ldg(P.g + (long long)n * P.g_ld + q);
+              if ((c.w & 7) == 3) a1 += gv; else a3 += gv;
+            }
+          }
+        }
+      }
+      S.p[0][0][lh] = chr * a1;
+      S.p[2][0][lh] = chr * a3;
+    }
+    if (ty == hcw && lane < TY) {   // halo column k = z0 - 1: hx, hy
+      float a1 = 0.f, a2 = 0.f, a3 = 0.f;
+      float chz = 0.f;
+      if (col_halo) {
+        adj_a_cell<TY, 3>(P, A, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xe0, xe1, ye0_c, ye1_c, ze0_c, ze1_c,
+                          false, a1, a2, a3);
+        chz = chat(i, y0 + lane, z0 - 1);
+        if (P.g) {
+          for (int q = 0; q < P.nprb; ++q) {
+            const int4 c = __ldg(P.prb + q);
+            if (c.x == i && c.y == y0 + lane && c.z == z0 - 1 && ((c.w & 7) == 3 || (c.w & 7) == 4)) {
+              const float gv = __ldg(P.g + (long long)n * P.g_ld + q);
+              if ((c.w & 7) == 3) a1 += gv; else a2 += gv;
+            }
+          }
+        }
+      }
+      S.p[0][lane + 1][0] = chz * a1;
+      S.p[1][lane + 1][0] = chz * a2;
+    }
+    __syncthreads();
+
+    // ---- phase B ----
+    float py = 0.f, pz = 0.f;
+    float rhy = 0.f, rhz = 0.f;
+    if (own) {
+      const AdjStage<TY>& X = S.st[b0];
+      const float px = S.p[0][ly][lh];
+      py = S.p[1][ly][lh];
+      pz = S.p[2][ly][lh];
+      const float px_ym = S.p[0][ly - 1][lh], pz_ym = S.p[2][ly - 1][lh];
+      const float px_zm = S.p[0][ly][lh - 1], py_zm = S.p[1][ly][lh - 1];
+      const float cav = X.ca[ty][lane];
+      float ax = cav * X.ae[0][ly][lz] + ((zh0 * py - zhm * py_zm) - (yh0 * pz - yhm * pz_ym));
+      float ay = cav * X.ae[1][ly][lz] + ((xh0 * pz - xhm * pz_prev) - (zh0 * px - zhm * px_zm));
+      float az = cav * X.ae[2][ly][lz] + ((yh0 * px - yhm * px_ym) - (xh0 * py - xhm * py_prev));
+      if (C.cpx) {   // (hy <- ez, +1, q0), (hz <- ey, -1, q1): aE(x) += r(x-1) - r(x)
+        rhy = r_h(P, A, C, 0, 0, +1.f, i, j, k, py, true);
+        rhz = r_h(P, A, C, 0, 1, -1.f, i, j, k, pz, true);
+        az += rhy_prev - rhy;
+        ay += rhz_prev - rhz;
+      }
+      if (C.cpy) {   // (hx <- ez, -1, q0), (hz <- ex, +1, q1)
+        az += r_h(P, A, C, 1, 0, -1.f, i, j - 1, k, px_ym, false) - r_h(P, A, C, 1, 0, -1.f, i, j, k, px, true);
+        ax += r_h(P, A, C, 1, 1, +1.f, i, j - 1, k, pz_ym, false) - r_h(P, A, C, 1, 1, +1.f, i, j, k, pz, true);
+      }
+      if (C.cpz) {   // (hx <- ey, +1, q0), (hy <- ex, -1, q1)
+        ay += r_h(P, A, C, 2, 0, +1.f, i, j, k - 1, px_zm, false) - r_h(P, A, C, 2, 0, +1.f, i, j, k, px, true);
+        ax += r_h(P, A, C, 2, 1, -1.f, i, j, k - 1, py_zm, false) - r_h(P, A, C, 2, 1, -1.f, i, j, k, py, true);
+      }
+      if (n >= 1 && (pmask | smask | (unsigned)prb_tail | (unsigned)src_tail)) {
+        if (P.g) {   // E-probe cotangent of y_{n-1}
+          for (unsigned m = pmask; m; m &= m - 1) {
+            const int q = __ffs(m) - 1;
+            const int4 c = __ldg(P.prb + q);
+            if (c.x == i && (c.w & 7) < 3) {
+              const float gv = __ldg(P.g + (long long)(n - 1) * P.g_ld + q);
+              if ((c.w & 7) == 0) ax += gv; else if ((c.w & 7) == 1) ay += gv; else az += gv;
+            }
+          }
+          if (prb_tail)
+            for (int q = 32; q < P.nprb; ++q) {
+              const int4 c = __ldg(P.prb + q);
+              if (c.x == i && c.y == j && c.z == k && (c.w & 7) < 3) {
+                const float gv = __ldg(P.g + (long long)(n - 1) * P.g_ld + q);
+                if ((c.w & 7) == 0) ax += gv; else if ((c.w & 7) == 1) ay += gv; else az += gv;
+              }
+            }
+        }
+        if (P.src_adj) {
+          for (unsigned m = smask; m; m &= m - 1) {
+            const int q = __ffs(m) - 1;
+            const int4 c = __ldg(P.src + q);
+            if (c.x == i) P.src_adj[(long long)(n - 1) * P.src_ld + q] = c.w == 0 ? ax : c.w == 1 ? ay : az;
+          }
+          if (src_tail)
+            for (int q = 32; q < P.nsrc; ++q) {
+              const int4 c = __ldg(P.src + q);
+              if (c.x == i && c.y == j && c.z == k)
+                P.src_adj[(long long)(n - 1) * P.src_ld + q] = c.w == 0 ? ax : c.w == 1 ? ay : az;
+            }
+        }
+      }
+      if ((pec & 1u) && (i == 0 || i == C.nx - 1)) { ay = 0.f; az = 0.f; }
+      if (pec_j) { ax = 0.f; az = 0.f; }
+      if (pec_k0) { ax = 0.f; ay = 0.f; }
+      if (pec_kz) az = 0.f;
+      if (P.emask) {
+        const unsigned m = P.emask[e];
+        if (m & 1u) ax = 0.f;
+        if (m & 2u) ay = 0.f;
+        if (m & 4u) az = 0.f;
+      }
+      aFo[e] = ax;
+      aFo[C.cs + e] = ay;
+      aFo[2 * C.cs + e] = az;
+    }
+    py_prev = py;
+    pz_prev = pz;
+    rhy_prev = rhy;
+    rhz_prev = rhz;
+  }
+  cp_async_wait<0>();
+}
+
+template __global__ void adj_step_kernel<8>(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
+
+size_t adj_step_smem_bytes() { return sizeof(AdjSmem<8>); }
+
+}  // namespace rfxb

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -23,9 +24,12 @@ __global__ void pack_kernel(float*, const float*, RfxbInst);
 __global__ void unpack_kernel(float*, const float*, RfxbInst);
 __global__ void coef_kernel(RfxbInst, float*, float*, float*, float*, const float*, const float*,
                             const float*, const unsigned char*, unsigned char*, float);
-__global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int);
-__global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int);
-__global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int);
+__global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
+__global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
+__global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
+template <int TY>
+__global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
+size_t adj_step_smem_bytes();
 }  // namespace rfxb
 
 using namespace rfxb;
@@ -86,7 +90,8 @@ struct RfxbPlan {
   // adjoint
   AdjInst adj{};
   bool adj_alloc = false;
-  int adj_par = 0;
+  int adj_par = 0;    // parity of the adjoint psi buffers
+  int adj_fpar = 0;   // parity of the adjoint field buffers
   // single-plan group state
   RfxbBatch* self_group = nullptr;
 
@@ -107,10 +112,12 @@ struct RfxbPlan {
   int64_t bytes = 0;
 };
 
+// A cached CUDA graph of a launch sequence: kind 0 forward steps
+// [step0, step0+k), kind 1 reverse steps [step0-k, step0) of the adjoint.
 struct GraphKey {
-  int k, par0, dft, prb;
+  int kind, step0, k, par0, fpar0, dft;
   bool operator<(const GraphKey& o) const {
-    return std::tie(k, par0, dft, prb) < std::tie(o.k, o.par0, o.dft, o.prb);
+    return std::tie(kind, step0, k, par0, fpar0, dft) < std::tie(o.kind, o.step0, o.k, o.par0, o.fpar0, o.dft);
   }
 };
 
@@ -283,6 +290,45 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, c
   return 0;
 }
 
+// Launch sequences of more than a few steps are captured once into a CUDA
+// graph (keyed by step range and parities) and replayed; the descriptors the
+// kernels read are uploaded before each replay.  RFXB_GRAPHS=0 disables it.
+bool graphs_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_GRAPHS");
+    v = (e && std::string(e) == "0") ? 0 : 1;
+  }
+  return v == 1;
+}
+
+template <typename F>
+int run_graph(RfxbBatch* g, const GraphKey& key, cudaStream_t st, F&& launch) {
+  auto it = g->graphs.find(key);
+  if (it == g->graphs.end()) {
+    if (g->graphs.size() >= 64) {   // bound the cache
+      for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
+      g->graphs.clear();
+    }
+    RFXB_CUDA(cudaStreamBeginCapture(g->cap_stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = launch(g->cap_stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(g->cap_stream, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (ec != cudaSuccess) return fail(RFXB_E_LAUNCH, std::string("graph capture: ") + cudaGetErrorString(ec));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(RFXB_E_LAUNCH, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    it = g->graphs.emplace(key, exec).first;
+  }
+  RFXB_CUDA(cudaGraphLaunch(it->second, st));
+  return 0;
+}
+
 int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, cudaStream_t st) {
   if (n_steps < 0 || step0 < 0) return fail(RFXB_E_INVALID, "negative step range");
   if (n_steps == 0) return 0;
@@ -291,15 +337,26 @@ int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, c
     if (p->par != par0) return fail(RFXB_E_STATE, "plans of a batch must share the step parity");
   bool has_dft = false, has_prb = false;
   if (int rc = upload_group(g, ios, &has_dft, &has_prb, st)) return rc;
-  if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, st)) return rc;
+  if (graphs_enabled() && n_steps >= 4) {
+    const GraphKey key{0, step0, n_steps, par0, 0, has_dft ? 1 : 0};
+    if (int rc = run_graph(g, key, st, [&](cudaStream_t cs) {
+          return launch_steps(g, step0, n_steps, par0, has_dft, cs);
+        }))
+      return rc;
+  } else {
+    if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, st)) return rc;
+  }
   for (auto* p : g->plans) p->par = (par0 + n_steps) & 1;
   return 0;
 }
 
 int ensure_adjoint(RfxbPlan* p, cudaStream_t st) {
   if (!p->adj_alloc) {
-    for (int c = 0; c < 6; ++c)
-      if (int rc = p->alloc(&p->adj.aF[c], p->elems)) return rc;
+    for (int s = 0; s < 2; ++s) {
+      float* q = nullptr;
+      if (int rc = p->alloc(&q, 6 * p->elems)) return rc;
+      for (int c = 0; c < 6; ++c) p->adj.aF[s][c] = q + c * p->elems;
+    }
     for (int s = 0; s < 2; ++s)
       for (int a = 0; a < 3; ++a) {
         if (int rc = p->alloc(&p->adj.aPsiH[s][a], p->psi_elems[a])) return rc;
@@ -307,14 +364,26 @@ int ensure_adjoint(RfxbPlan* p, cudaStream_t st) {
       }
     p->adj_alloc = true;
   }
-  for (int c = 0; c < 6; ++c) RFXB_CUDA(cudaMemsetAsync(p->adj.aF[c], 0, p->elems * sizeof(float), st));
+  for (int s = 0; s < 2; ++s) RFXB_CUDA(cudaMemsetAsync(p->adj.aF[s][0], 0, 6 * p->elems * sizeof(float), st));
   for (int s = 0; s < 2; ++s)
     for (int a = 0; a < 3; ++a) {
       RFXB_CUDA(cudaMemsetAsync(p->adj.aPsiH[s][a], 0, std::max<long long>(1, p->psi_elems[a]) * sizeof(float), st));
       RFXB_CUDA(cudaMemsetAsync(p->adj.aPsiE[s][a], 0, std::max<long long>(1, p->psi_elems[a]) * sizeof(float), st));
     }
   p->adj_par = 0;
+  p->adj_fpar = 0;
   return 0;
+}
+
+// The fused reverse step is the default; RFXB_ADJOINT_KERNEL=twopass selects
+// the two unfused passes (an independent cross-check of the same transpose).
+bool use_twopass() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_ADJOINT_KERNEL");
+    v = (e && std::string(e) == "twopass") ? 1 : 0;
+  }
+  return v == 1;
 }
 
 int upload_adjoint(RfxbBatch* g, const RfxbAdjointIO* aios, cudaStream_t st) {
@@ -346,7 +415,8 @@ int group_adjoint_begin(RfxbBatch* g, const RfxbAdjointIO* aios, int n_total, cu
   for (auto* p : g->plans)
     if (int rc = ensure_adjoint(p, st)) return rc;
   if (int rc = upload_adjoint(g, aios, st)) return rc;
-  adj_init_kernel<<<(unsigned)g->plans.size(), 32, 0, st>>>(g->d_inst, g->d_adj, (int)g->plans.size(), n_total - 1);
+  adj_init_kernel<<<(unsigned)g->plans.size(), 32, 0, st>>>(g->d_inst, g->d_adj, (int)g->plans.size(), n_total - 1,
+                                                             g->plans[0]->adj_fpar);
   RFXB_CUDA(cudaGetLastError());
   return 0;
 }
@@ -355,19 +425,50 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
   if (n_steps <= 0) return 0;
   if (step_hi - n_steps < 0) return fail(RFXB_E_INVALID, "reverse range reaches below step 0");
   const int par0 = g->plans[0]->adj_par;
+  const int fpar0 = g->plans[0]->adj_fpar;
   for (auto* p : g->plans) {
     if (!p->adj_alloc) return fail(RFXB_E_STATE, "adjoint_advance before adjoint_begin");
-    if (p->adj_par != par0) return fail(RFXB_E_STATE, "plans of a batch must share the adjoint parity");
+    if (p->adj_par != par0 || p->adj_fpar != fpar0)
+      return fail(RFXB_E_STATE, "plans of a batch must share the adjoint parity");
   }
   if (int rc = upload_adjoint(g, aios, st)) return rc;
-  int par = par0;
-  for (int s = step_hi - 1; s >= step_hi - n_steps; --s) {
-    adj_pass_a<<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_adj, g->d_work, s, par);
-    adj_pass_b<<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_adj, g->d_work, s, par);
-    par ^= 1;
+  const bool two = use_twopass();
+  if (!two) {
+    static bool attr = false;
+    if (!attr) {
+      RFXB_CUDA(cudaFuncSetAttribute(adj_step_kernel<kTY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)adj_step_smem_bytes()));
+      attr = true;
+    }
   }
-  RFXB_CUDA(cudaGetLastError());
-  for (auto* p : g->plans) p->adj_par = (par0 + n_steps) & 1;
+  auto launch = [&](cudaStream_t cs) -> int {
+    int par = par0, fpar = fpar0;
+    for (int s = step_hi - 1; s >= step_hi - n_steps; --s) {
+      if (two) {
+        adj_pass_a<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
+        adj_pass_b<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
+      } else {
+        adj_step_kernel<kTY><<<g->n_work, dim3(32, kTY), adj_step_smem_bytes(), cs>>>(g->d_inst, g->d_adj,
+                                                                                      g->d_work, s, par, fpar);
+        fpar ^= 1;
+      }
+      par ^= 1;
+    }
+    RFXB_CUDA(cudaGetLastError());
+    return 0;
+  };
+  if (graphs_enabled() && n_steps >= 4) {
+    const GraphKey key{1 + (two ? 1 : 0), step_hi, n_steps, par0, fpar0, 0};
+    if (int rc = run_graph(g, key, st, launch)) return rc;
+  } else {
+    if (int rc = launch(st)) return rc;
+  }
+  const int par = (par0 + n_steps) & 1;
+  const int fpar = two ? fpar0 : ((fpar0 + n_steps) & 1);
+  for (auto* p : g->plans) {
+    p->adj_par = par;
+    p->adj_fpar = fpar;
+  }
   return 0;
 }
 
@@ -431,14 +532,15 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
   I.ps = (long long)(d->ny + 2) * I.zs;
   const long long base = 32;
   I.off0 = base + I.ps + I.zs;
-  p->elems = base + (long long)(d->nx + 2) * I.ps + I.zs + 64;
+  // a multiple of 32 elements, so every component block starts 128-byte aligned
+  p->elems = (base + (long long)(d->nx + 2) * I.ps + I.zs + 64 + 31) / 32 * 32;
+  I.cs = p->elems;
   auto bail = [&](int rc) { delete p; return rc; };
-  for (int s = 0; s < 2; ++s)
-    for (int c = 0; c < 6; ++c) {
-      float* q = nullptr;
-      if (int rc = p->alloc(&q, p->elems)) return bail(rc);
-      I.F[s][c] = q;
-    }
+  for (int s = 0; s < 2; ++s) {
+    float* q = nullptr;
+    if (int rc = p->alloc(&q, 6 * p->elems)) return bail(rc);
+    for (int c = 0; c < 6; ++c) I.F[s][c] = q + c * p->elems;
+  }
   if (int rc = p->alloc(&p->ca, p->elems)) return bail(rc);
   if (int rc = p->alloc(&p->cb, p->elems)) return bail(rc);
   if (int rc = p->alloc(&p->ce, p->elems)) return bail(rc);
@@ -753,7 +855,7 @@ int64_t rfxb_plan_device_bytes(const RfxbPlan* p) {
   if (p->ch) b += p->elems * 4;
   if (p->emask) b += p->elems;
   b += 4 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2]) * 4;
-  if (p->adj_alloc) b += (6 * p->elems + 4 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2])) * 4;
+  if (p->adj_alloc) b += (12 * p->elems + 4 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2])) * 4;
   b += p->hist_cap * 4;
   b += (int64_t)p->ckpt.size() * (6 * p->elems + 2 * (p->psi_elems[0] + p->psi_elems[1] + p->psi_elems[2])) * 4;
   return b;

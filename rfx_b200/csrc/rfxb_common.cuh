@@ -13,6 +13,11 @@ __device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+// 16-byte copy; both addresses must be 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }

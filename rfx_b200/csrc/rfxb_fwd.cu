@@ -1,9 +1,10 @@
 // Forward time step of the Yee/CPML leapfrog: one fused kernel per step.
 //
 // One CTA owns a (TY x 32) tile of the (y, z) plane and marches along x over
-// an x range [xa, xb).  For each x plane it
-//   1. stages E^n of planes i and i+1 (with a one-cell y/z halo) in shared
-//      memory through cp.async, prefetching plane i+2 one iteration ahead;
+// an x range [xa, xb).  For each x plane i it
+//   1. keeps a 4-stage cp.async pipeline of the input planes i-1 .. i+2 in
+//      shared memory, 16-byte copies of: E with a one-cell halo on every side,
+//      H with the low y/z halo, and the ca/cb coefficients of the tile;
 //   2. computes H^{n+1/2} on the tile plus the low y row / low z column halo
 //      (rfx/core/yee.py:226-291 / :411-453, then rfx/boundaries/cpml.py:804-1065);
 //   3. computes E^{n+1} on the tile from those H values and the H of plane
@@ -11,40 +12,51 @@
 //      rfx/boundaries/cpml.py:522-801), applies the PEC faces
 //      (rfx/boundaries/pec.py:13-47), the PEC edge mask (pec.py:179-208),
 //      soft sources (rfx/simulation.py:1518-1523) and probes (:1565-1567).
-// Fields and H-side CPML psi are ping-ponged between two buffers, so halo
-// cells recomputed by a neighbour CTA always read step-n values.
+// Fields and psi are ping-ponged between two buffers, so halo cells
+// recomputed by a neighbour CTA always read step-n values.  CPML work is
+// confined to CTAs whose tile touches a y/z slab and to x-slab planes.
 #include "rfxb_common.cuh"
 
 namespace rfxb {
 
 #define RFXB_NSTAGE 4
+#define RFXB_EW 40   // staged E row: z in [z0 - 4, z0 + 36)
+#define RFXB_HW 36   // staged H row: z in [z0 - 4, z0 + 32)
 
-// One pipeline stage holds everything the step reads from plane i of the
-// input state: E with a one-cell halo on every side, H with the low y/z halo,
-// and the ca/cb coefficients of the tile.
 template <int TY>
-struct FwdStage {
-  float e[3][TY + 2][RFXB_TZ + 2];     // [ex,ey,ez][y - y0 + 1][z - z0 + 1]
-  float h[3][TY + 1][RFXB_TZ + 1];     // [hx,hy,hz][y - y0 + 1][z - z0 + 1] (H^{n-1/2})
-  float cab[2][TY][RFXB_TZ];           // [ca,cb][y - y0][z - z0]
+struct __align__(16) FwdStage {
+  float e[3][TY + 2][RFXB_EW];   // ex ey ez, rows y0-1 .. y0+TY
+  float h[3][TY + 1][RFXB_HW];   // hx hy hz (H^{n-1/2}), rows y0-1 .. y0+TY-1
+  float cab[2][TY][RFXB_TZ];     // ca cb, rows y0 .. y0+TY-1, z from z0
 };
 
 template <int TY>
 struct FwdSmem {
-  FwdStage<TY> st[RFXB_NSTAGE];        // planes i-1 .. i+2 (buffer (p + 1) & 3)
-  float h[3][TY + 1][RFXB_TZ + 1];     // H^{n+1/2} of plane i with the low y/z halo
+  FwdStage<TY> st[RFXB_NSTAGE];      // plane p lives in stage (p + 1) & 3
+  float h[3][TY + 1][RFXB_TZ + 1];   // H^{n+1/2} of plane i: [y - y0 + 1][z - z0 + 1]
   RfxbInst P;
 };
 
 __device__ __forceinline__ int stage_of(int p) { return (p + 1) & (RFXB_NSTAGE - 1); }
 
+// Per-CTA constants kept in registers.
+struct FwdCtx {
+  int nx, ny, nz, zs, ncp, par;
+  long long ps, off0, cs;
+  const float* Fi;
+  float* Fo;
+  const float* ch;
+  float ch0;
+  bool cpx, cpy, cpz;      // CPML axis active (y/z: and this tile touches a slab)
+};
+
 // H^{n+1/2} components selected by MASK (1 hx, 2 hy, 4 hz) at (i, jj, kk).
-// E of plane i is in buffer b0 and of plane i+1 in b1; (ly, lz) are the
-// cell's shared-memory coordinates.  psi is written only for owned cells.
+// (ly, lz): the cell's row and z index in the staged planes (lz = k - z0 + 4).
 template <int TY, int MASK>
-__device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, int par,
+__device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, const FwdCtx& C,
                                        int b0, int b1, int i, int jj, int kk, int ly, int lz,
-                                       bool write_psi, float& hx, float& hy, float& hz) {
+                                       float xh, float yh, float zh, bool write_psi,
+                                       float& hx, float& hy, float& hz) {
   const FwdStage<TY>& A = S.st[b0];
   const FwdStage<TY>& B = S.st[b1];
   const float Ex = A.e[0][ly][lz], Ey = A.e[1][ly][lz], Ez = A.e[2][ly][lz];
@@ -54,17 +66,16 @@ __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, 
   const float dEz_x = B.e[2][ly][lz] - Ez;
   const float dEy_x = B.e[1][ly][lz] - Ey;
   const float dEx_y = A.e[0][ly + 1][lz] - Ex;
-  float chc = P.ch0;
-  if (P.ch) chc = P.ch[P.off0 + (long long)i * P.ps + (long long)jj * P.zs + kk];
-  const float xh = __ldg(P.xh + i), yh = __ldg(P.yh + jj), zh = __ldg(P.zh + kk);
+  float chc = C.ch0;
+  if (C.ch) chc = C.ch[C.off0 + (long long)i * C.ps + (long long)jj * C.zs + kk];
   if (MASK & 1) hx = A.h[0][ly][lz] - chc * (dEz_y * yh - dEy_z * zh);
   if (MASK & 2) hy = A.h[1][ly][lz] - chc * (dEx_z * zh - dEz_x * xh);
   if (MASK & 4) hz = A.h[2][ly][lz] - chc * (dEy_x * xh - dEx_y * yh);
-  const int n = P.ncp;
-  if (n == 0) return;
+  const int n = C.ncp;
+  const int par = C.par;
   int s, sd;
-  if (P.cpml_axes & 1u) {
-    sd = cpml_side(i, P.nx, n, s);
+  if (C.cpx) {
+    sd = cpml_side(i, C.nx, n, s);
     if (sd >= 0) {
       const float* tb = P.cpb + (size_t)sd * 3 * n;
       const float b = __ldg(tb + s), c = __ldg(tb + n + s), km = __ldg(tb + 2 * n + s);
@@ -87,8 +98,8 @@ __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, 
       }
     }
   }
-  if (P.cpml_axes & 2u) {
-    sd = cpml_side(jj, P.ny, n, s);
+  if (C.cpy) {
+    sd = cpml_side(jj, C.ny, n, s);
     if (sd >= 0) {
       const float* tb = P.cpb + (size_t)(2 + sd) * 3 * n;
       const float b = __ldg(tb + s), c = __ldg(tb + n + s), km = __ldg(tb + 2 * n + s);
@@ -111,8 +122,8 @@ __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, 
       }
     }
   }
-  if (P.cpml_axes & 4u) {
-    sd = cpml_side(kk, P.nz, n, s);
+  if (C.cpz) {
+    sd = cpml_side(kk, C.nz, n, s);
     if (sd >= 0) {
       const float* tb = P.cpb + (size_t)(4 + sd) * 3 * n;
       const float b = __ldg(tb + s), c = __ldg(tb + n + s), km = __ldg(tb + 2 * n + s);
@@ -137,40 +148,35 @@ __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, 
   }
 }
 
-// Stage plane ip of the input state: E (rows y0-1..y0+TY, cols z0-1..z0+32),
-// H (rows y0-1..y0+TY-1, cols z0-1..z0+31) and ca/cb of the tile.  Rows past
-// the grid read the zero guard row j = ny.
+// Stage plane ip of the input state with 16-byte copies.  Every copy starts on
+// a 16-byte boundary: off0, ps, zs, cs and z0 are multiples of 32 elements.
+// Rows past the grid read the zero guard row j = ny.
 template <int TY>
-__device__ __forceinline__ void load_stage(const RfxbInst& P, FwdSmem<TY>& S, const float* const* F,
-                                           int y0, int z0, int ip, int ty, int lane) {
+__device__ __forceinline__ void load_stage(FwdSmem<TY>& S, const FwdCtx& C, const float* ca, const float* cb,
+                                           int y0, int z0, int ip, int tid) {
   FwdStage<TY>& D = S.st[stage_of(ip)];
-  const long long pbase = P.off0 + (long long)ip * P.ps + (z0 - 1);
-  for (int r = ty; r < TY + 2; r += TY) {
-    const int jj = min(y0 - 1 + r, P.ny);
-    const long long rb = pbase + (long long)jj * P.zs;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      cp_async4(&D.e[c][r][lane], F[c] + rb + lane);
-      if (lane < 2) cp_async4(&D.e[c][r][32 + lane], F[c] + rb + 32 + lane);
+  const long long pb = C.off0 + (long long)ip * C.ps;
+  constexpr int RE = (TY + 2) * 10, RH = (TY + 1) * 9, RC = TY * 8;
+  constexpr int NE = 3 * RE, NH = 3 * RH, NC = 2 * RC;
+  for (int t = tid; t < NE + NH + NC; t += 32 * TY) {
+    if (t < NE) {
+      const int c = t / RE, u = t - c * RE, r = u / 10, q = u - r * 10;
+      const int jj = min(y0 - 1 + r, C.ny);
+      cp_async16(&D.e[c][r][4 * q], C.Fi + c * C.cs + pb + (long long)jj * C.zs + (z0 - 4 + 4 * q));
+    } else if (t < NE + NH) {
+      const int v = t - NE, c = v / RH, u = v - c * RH, r = u / 9, q = u - r * 9;
+      const int jj = min(y0 - 1 + r, C.ny);
+      cp_async16(&D.h[c][r][4 * q], C.Fi + (3 + c) * C.cs + pb + (long long)jj * C.zs + (z0 - 4 + 4 * q));
+    } else {
+      const int v = t - NE - NH, c = v / RC, u = v - c * RC, r = u / 8, q = u - r * 8;
+      const int jj = min(y0 + r, C.ny);
+      cp_async16(&D.cab[c][r][4 * q], (c ? cb : ca) + pb + (long long)jj * C.zs + (z0 + 4 * q));
     }
-    if (r < TY + 1) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        cp_async4(&D.h[c][r][lane], F[3 + c] + rb + lane);
-        if (lane == 0) cp_async4(&D.h[c][r][32], F[3 + c] + rb + 32);
-      }
-    }
-  }
-  {
-    const int jj = min(y0 + ty, P.ny);
-    const long long o = P.off0 + (long long)ip * P.ps + (long long)jj * P.zs + z0 + lane;
-    cp_async4(&D.cab[0][ty][lane], P.ca + o);
-    cp_async4(&D.cab[1][ty][lane], P.cb + o);
   }
 }
 
 template <int TY>
-__global__ void __launch_bounds__(32 * TY)
+__global__ void __launch_bounds__(32 * TY, 4)
 fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work, int n, int par) {
   __shared__ FwdSmem<TY> S;
   const int lane = threadIdx.x, ty = threadIdx.y;
@@ -179,9 +185,31 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   load_inst(S.P, insts + w.inst, tid, 32 * TY);
   __syncthreads();
   const RfxbInst& P = S.P;
-  const int j = w.y0 + ty, k = w.z0 + lane;
-  const bool own = (j < P.ny) && (k < P.nz);
-  const int ly = ty + 1, lz = lane + 1;
+  FwdCtx C;
+  C.nx = P.nx; C.ny = P.ny; C.nz = P.nz; C.zs = P.zs; C.ncp = P.ncp; C.par = par;
+  C.ps = P.ps; C.off0 = P.off0; C.cs = P.cs;
+  C.Fi = P.F[par][0];
+  C.Fo = P.F[par ^ 1][0];
+  C.ch = P.ch;
+  C.ch0 = P.ch0;
+  const int y0 = w.y0, z0 = w.z0;
+  C.cpx = C.ncp > 0 && (P.cpml_axes & 1u);
+  C.cpy = C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY - 1 >= C.ny - C.ncp);
+  C.cpz = C.ncp > 0 && (P.cpml_axes & 4u) && (z0 - 1 < C.ncp || z0 + 31 >= C.nz - C.ncp);
+  const float* ca = P.ca;
+  const float* cb = P.cb;
+  const int j = y0 + ty, k = z0 + lane;
+  const bool own = (j < C.ny) && (k < C.nz);
+  const int ly = ty + 1, lz = lane + 4, lh = lane + 1;
+  // spacing table entries of this thread's column and of the halo cells
+  const float yh = own ? __ldg(P.yh + j) : 0.f, ye = own ? __ldg(P.ye + j) : 0.f;
+  const float zh = own ? __ldg(P.zh + k) : 0.f, ze = own ? __ldg(P.ze + k) : 0.f;
+  const bool row_halo = (ty == 0) && (y0 >= 1) && (k < C.nz);
+  const float yh_row = row_halo ? __ldg(P.yh + y0 - 1) : 0.f;
+  const int hcw = TY > 1 ? 1 : 0;                       // warp computing the z halo column
+  const bool col_halo = (ty == hcw) && (lane < TY) && (z0 >= 1) && (y0 + lane < C.ny);
+  const float yh_col = col_halo ? __ldg(P.yh + y0 + lane) : 0.f;
+  const float zh_col = col_halo ? __ldg(P.zh + z0 - 1) : 0.f;
 
   // Sources and probes whose (j, k) is this thread's column.
   unsigned smask = 0u, pmask = 0u;
@@ -198,17 +226,19 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     }
   }
   const bool src_tail = P.nsrc > 32, prb_tail = P.nprb > 32;
-  const float* const* Fin = P.F[par];
-  float* const* Fout = P.F[par ^ 1];
+  const unsigned pec = P.pec_axes;
+  const bool pec_j = ((pec & 2u) != 0) && (j == 0 || j == C.ny - 1);
+  const bool pec_k0 = ((pec & 4u) != 0) && (k == 0 || k == C.nz - 1);
+  const bool pec_kz = ((pec & 4u) != 0) && (k == C.nz - 1);
 
   const int xa = w.xa, xb = w.xb;
   // pipeline: planes xa-1 and xa (group 0), xa+1 (group 1), xa+2 (group 2)
-  load_stage<TY>(P, S, Fin, w.y0, w.z0, xa - 1, ty, lane);
-  load_stage<TY>(P, S, Fin, w.y0, w.z0, xa, ty, lane);
+  load_stage<TY>(S, C, ca, cb, y0, z0, xa - 1, tid);
+  load_stage<TY>(S, C, ca, cb, y0, z0, xa, tid);
   cp_async_commit();
-  load_stage<TY>(P, S, Fin, w.y0, w.z0, xa + 1, ty, lane);
+  load_stage<TY>(S, C, ca, cb, y0, z0, xa + 1, tid);
   cp_async_commit();
-  if (xa + 2 <= P.nx) load_stage<TY>(P, S, Fin, w.y0, w.z0, xa + 2, ty, lane);
+  if (xa + 2 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, xa + 2, tid);
   cp_async_commit();
   cp_async_wait<2>();
   __syncthreads();
@@ -217,47 +247,48 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   float hy_prev = 0.f, hz_prev = 0.f;
   if (xa > 0 && own) {
     float hx_, hy_, hz_;
-    h_cell<TY, 6>(P, S, par, stage_of(xa - 1), stage_of(xa), xa - 1, j, k, ly, lz, false, hx_, hy_, hz_);
+    const float xhp = __ldg(P.xh + xa - 1);
+    h_cell<TY, 6>(P, S, C, stage_of(xa - 1), stage_of(xa), xa - 1, j, k, ly, lz, xhp, yh, zh, false,
+                  hx_, hy_, hz_);
     hy_prev = hy_;
     hz_prev = hz_;
   }
 
   const bool has_hist = P.hist != nullptr && (n - P.hist_step0) >= 0 && (n - P.hist_step0) < P.hist_nsteps;
+  const bool has_emask = P.emask != nullptr;
 
   for (int i = xa; i < xb; ++i) {
     cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
     __syncthreads();      // ... for every thread; plane i-1's stage is free
-    if (i + 3 <= P.nx) load_stage<TY>(P, S, Fin, w.y0, w.z0, i + 3, ty, lane);
+    if (i + 3 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, i + 3, tid);
     cp_async_commit();
     const int b0 = stage_of(i), b1 = stage_of(i + 1);
+    const float xh = __ldg(P.xh + i), xe = __ldg(P.xe + i);
 
     // ---- H phase ----
     float hx = 0.f, hy = 0.f, hz = 0.f;
-    const long long e = P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
+    const long long e = C.off0 + (long long)i * C.ps + (long long)j * C.zs + k;
     if (own) {
-      h_cell<TY, 7>(P, S, par, b0, b1, i, j, k, ly, lz, true, hx, hy, hz);
-      Fout[3][e] = hx;
-      Fout[4][e] = hy;
-      Fout[5][e] = hz;
+      h_cell<TY, 7>(P, S, C, b0, b1, i, j, k, ly, lz, xh, yh, zh, true, hx, hy, hz);
+      C.Fo[3 * C.cs + e] = hx;
+      C.Fo[4 * C.cs + e] = hy;
+      C.Fo[5 * C.cs + e] = hz;
     }
-    S.h[0][ly][lz] = hx;
-    S.h[1][ly][lz] = hy;
-    S.h[2][ly][lz] = hz;
+    S.h[0][ly][lh] = hx;
+    S.h[1][ly][lh] = hy;
+    S.h[2][ly][lh] = hz;
     if (ty == 0) {  // halo row j = y0 - 1: hx, hz
       float a = 0.f, bq = 0.f, cq = 0.f;
-      const int jh = w.y0 - 1;
-      if (jh >= 0 && k < P.nz) h_cell<TY, 5>(P, S, par, b0, b1, i, jh, k, 0, lz, false, a, bq, cq);
-      S.h[0][0][lz] = a;
-      S.h[1][0][lz] = 0.f;
-      S.h[2][0][lz] = cq;
+      if (row_halo) h_cell<TY, 5>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
+      S.h[0][0][lh] = a;
+      S.h[2][0][lh] = cq;
     }
-    if (ty == (TY > 1 ? 1 : 0) && lane < TY) {  // halo column k = z0 - 1: hx, hy
+    if (ty == hcw && lane < TY) {  // halo column k = z0 - 1: hx, hy
       float a = 0.f, bq = 0.f, cq = 0.f;
-      const int jc = w.y0 + lane, kh = w.z0 - 1;
-      if (kh >= 0 && jc < P.ny) h_cell<TY, 3>(P, S, par, b0, b1, i, jc, kh, lane + 1, 0, false, a, bq, cq);
+      if (col_halo) h_cell<TY, 3>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false,
+                                  a, bq, cq);
       S.h[0][lane + 1][0] = a;
       S.h[1][lane + 1][0] = bq;
-      S.h[2][lane + 1][0] = 0.f;
     }
     __syncthreads();
 
@@ -265,27 +296,26 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     if (own) {
       const FwdStage<TY>& A = S.st[b0];
       const float Ex = A.e[0][ly][lz], Ey = A.e[1][ly][lz], Ez = A.e[2][ly][lz];
-      const float dHz_y = hz - S.h[2][ly - 1][lz];
-      const float dHy_z = hy - S.h[1][ly][lz - 1];
-      const float dHx_z = hx - S.h[0][ly][lz - 1];
+      const float dHz_y = hz - S.h[2][ly - 1][lh];
+      const float dHy_z = hy - S.h[1][ly][lh - 1];
+      const float dHx_z = hx - S.h[0][ly][lh - 1];
       const float dHz_x = hz - hz_prev;
       const float dHy_x = hy - hy_prev;
-      const float dHx_y = hx - S.h[0][ly - 1][lz];
-      const float xe = __ldg(P.xe + i), ye = __ldg(P.ye + j), ze = __ldg(P.ze + k);
+      const float dHx_y = hx - S.h[0][ly - 1][lh];
       const float cx = dHz_y * ye - dHy_z * ze;
       const float cy = dHx_z * ze - dHz_x * xe;
       const float cz = dHy_x * xe - dHx_y * ye;
-      const float ca = A.cab[0][ty][lane], cb = A.cab[1][ty][lane];
-      float ex = ca * Ex + cb * cx;
-      float ey = ca * Ey + cb * cy;
-      float ez = ca * Ez + cb * cz;
-      const int ncp = P.ncp;
-      if (ncp) {
+      const float cav = A.cab[0][ty][lane], cbv = A.cab[1][ty][lane];
+      float ex = cav * Ex + cbv * cx;
+      float ey = cav * Ey + cbv * cy;
+      float ez = cav * Ez + cbv * cz;
+      const int ncp = C.ncp;
+      if (C.cpx || C.cpy || C.cpz) {
         int s, sd;
         float ce = 0.f;
         bool ce_loaded = false;
-        if (P.cpml_axes & 1u) {
-          sd = cpml_side(i, P.nx, ncp, s);
+        if (C.cpx) {
+          sd = cpml_side(i, C.nx, ncp, s);
           if (sd >= 0) {
             ce = P.ce[e];
             ce_loaded = true;
@@ -310,8 +340,8 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
             }
           }
         }
-        if (P.cpml_axes & 2u) {
-          sd = cpml_side(j, P.ny, ncp, s);
+        if (C.cpy) {
+          sd = cpml_side(j, C.ny, ncp, s);
           if (sd >= 0) {
             if (!ce_loaded) { ce = P.ce[e]; ce_loaded = true; }
             const float* tb = P.cpb + (size_t)(2 + sd) * 3 * ncp;
@@ -335,8 +365,8 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
             }
           }
         }
-        if (P.cpml_axes & 4u) {
-          sd = cpml_side(k, P.nz, ncp, s);
+        if (C.cpz) {
+          sd = cpml_side(k, C.nz, ncp, s);
           if (sd >= 0) {
             if (!ce_loaded) { ce = P.ce[e]; ce_loaded = true; }
             const float* tb = P.cpb + (size_t)(4 + sd) * 3 * ncp;
@@ -362,13 +392,11 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
         }
       }
       // PEC faces
-      if (P.pec_axes & 1u) if (i == 0 || i == P.nx - 1) { ey = 0.f; ez = 0.f; }
-      if (P.pec_axes & 2u) if (j == 0 || j == P.ny - 1) { ex = 0.f; ez = 0.f; }
-      if (P.pec_axes & 4u) {
-        if (k == 0 || k == P.nz - 1) { ex = 0.f; ey = 0.f; }
-        if (k == P.nz - 1) ez = 0.f;
-      }
-      if (P.emask) {
+      if ((pec & 1u) && (i == 0 || i == C.nx - 1)) { ey = 0.f; ez = 0.f; }
+      if (pec_j) { ex = 0.f; ez = 0.f; }
+      if (pec_k0) { ex = 0.f; ey = 0.f; }
+      if (pec_kz) ez = 0.f;
+      if (has_emask) {
         const unsigned m = P.emask[e];
         if (m) {
           ex = ex * (1.f - (float)(m & 1u));
@@ -386,32 +414,37 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
           hp[3 * hc] = cx; hp[4 * hc] = cy; hp[5 * hc] = cz;
         }
       }
-      auto sample = [&](int p, int pre) {
-        const int4 c = __ldg(P.prb + p);
-        if (c.x != i || ((c.w >> 4) & 1) != pre) return;
-        const int comp = c.w & 7;
-        const float v = comp == 0 ? ex : comp == 1 ? ey : comp == 2 ? ez : comp == 3 ? hx : comp == 4 ? hy : hz;
-        P.prb_out[(long long)n * P.prb_ld + p] = v;
-      };
-      auto inject = [&](int s) {
-        const int4 c = __ldg(P.src + s);
-        if (c.x != i) return;
-        const float v = __ldg(P.srcw + (long long)n * P.src_ld + s);
-        if (c.w == 0) ex = ex + v; else if (c.w == 1) ey = ey + v; else ez = ez + v;
-      };
-      if (P.prb_out) {
-        for (unsigned m = pmask; m; m &= m - 1) sample(__ffs(m) - 1, 1);
-        if (prb_tail) for (int p = 32; p < P.nprb; ++p) { const int4 c = __ldg(P.prb + p); if (c.y == j && c.z == k) sample(p, 1); }
+      if (pmask | smask | (unsigned)src_tail | (unsigned)prb_tail) {
+        auto sample = [&](int p, int pre) {
+          const int4 c = __ldg(P.prb + p);
+          if (c.x != i || ((c.w >> 4) & 1) != pre) return;
+          const int comp = c.w & 7;
+          const float v = comp == 0 ? ex : comp == 1 ? ey : comp == 2 ? ez : comp == 3 ? hx : comp == 4 ? hy : hz;
+          P.prb_out[(long long)n * P.prb_ld + p] = v;
+        };
+        auto inject = [&](int s) {
+          const int4 c = __ldg(P.src + s);
+          if (c.x != i) return;
+          const float v = __ldg(P.srcw + (long long)n * P.src_ld + s);
+          if (c.w == 0) ex = ex + v; else if (c.w == 1) ey = ey + v; else ez = ez + v;
+        };
+        if (P.prb_out) {
+          for (unsigned m = pmask; m; m &= m - 1) sample(__ffs(m) - 1, 1);
+          if (prb_tail)
+            for (int p = 32; p < P.nprb; ++p) { const int4 c = __ldg(P.prb + p); if (c.y == j && c.z == k) sample(p, 1); }
+        }
+        for (unsigned m = smask; m; m &= m - 1) inject(__ffs(m) - 1);
+        if (src_tail)
+          for (int s = 32; s < P.nsrc; ++s) { const int4 c = __ldg(P.src + s); if (c.y == j && c.z == k) inject(s); }
+        if (P.prb_out) {
+          for (unsigned m = pmask; m; m &= m - 1) sample(__ffs(m) - 1, 0);
+          if (prb_tail)
+            for (int p = 32; p < P.nprb; ++p) { const int4 c = __ldg(P.prb + p); if (c.y == j && c.z == k) sample(p, 0); }
+        }
       }
-      for (unsigned m = smask; m; m &= m - 1) inject(__ffs(m) - 1);
-      if (src_tail) for (int s = 32; s < P.nsrc; ++s) { const int4 c = __ldg(P.src + s); if (c.y == j && c.z == k) inject(s); }
-      if (P.prb_out) {
-        for (unsigned m = pmask; m; m &= m - 1) sample(__ffs(m) - 1, 0);
-        if (prb_tail) for (int p = 32; p < P.nprb; ++p) { const int4 c = __ldg(P.prb + p); if (c.y == j && c.z == k) sample(p, 0); }
-      }
-      Fout[0][e] = ex;
-      Fout[1][e] = ey;
-      Fout[2][e] = ez;
+      C.Fo[e] = ex;
+      C.Fo[C.cs + e] = ey;
+      C.Fo[2 * C.cs + e] = ez;
     }
     hy_prev = hy;
     hz_prev = hz;

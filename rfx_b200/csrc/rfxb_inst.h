@@ -27,6 +27,7 @@ struct RfxbInst {
   int nx, ny, nz, zs;
   long long ps;            // plane stride (elements)
   long long off0;          // element offset of cell (0,0,0)
+  long long cs;            // component stride: F[p][c] = F[p][0] + c * cs (multiple of 32)
   float* F[2][6];          // ping-pong field buffers: ex ey ez hx hy hz
   const float* ca;         // per cell, E decay coefficient
   const float* cb;         // per cell, E curl coefficient
@@ -73,7 +74,7 @@ struct RfxbInst {
 };
 
 struct AdjInst {           // adjoint state of one instance (same layouts as the forward state)
-  float* aF[6];            // aex aey aez ahx ahy ahz
+  float* aF[2][6];         // ping-pong: aex aey aez ahx ahy ahz (component stride cs)
   float* aPsiH[2][3];      // ping-pong
   float* aPsiE[2][3];
 };

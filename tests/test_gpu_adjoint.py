@@ -120,3 +120,55 @@ def test_autograd_function(cuda):
     assert eps_box.grad is not None and torch.isfinite(eps_box.grad).all()
     assert float(eps_box.grad.abs().sum()) > 0
     r.close()
+
+
+@pytest.mark.parametrize("build,box", [(small_uniform, (14, 20, 14, 20, 12, 14)),
+                                       (small_nonuniform, (12, 18, 12, 18, 11, 13))])
+def test_gradient_matches_oracle_adjoint(cuda, build, box):
+    """dJ/d eps_r of the CUDA adjoint against the oracle's float64 transpose
+    for J = <G, ts> with a seeded G (relative L2 below 1e-4)."""
+    from oracle.adjoint import forward_adjoint
+    from tests.scenarios import rel_l2
+    sc = build(n_steps=140)
+    G = np.random.default_rng(7).standard_normal((sc.n_steps, len(sc.probes)))
+    _, og, osrc = forward_adjoint(sc.ogrid, sc.materials, sc.n_steps, nonuniform=sc.lane == "nonuniform",
+                                  boundary=sc.boundary, pec_axes=sc.pec_axes, sources=sc.sources, probes=sc.probes,
+                                  pec_mask=sc.pec_mask, box=box, objective_grad=lambda ts: G)
+    r = _runner(sc, box)
+    r.forward()
+    grad, src_adj = r.backward(torch.from_numpy(G.astype(np.float32)).cuda())
+    e = rel_l2(grad.cpu().numpy(), og)
+    es = rel_l2(src_adj.cpu().numpy(), osrc)
+    print(sc.name, "grad relL2 vs oracle adjoint", e, "source adjoint", es)
+    assert e < 1e-4 and es < 1e-4
+    r.close()
+
+
+def test_twopass_adjoint_matches_fused(cuda, tmp_path):
+    """The two unfused passes (RFXB_ADJOINT_KERNEL=twopass) and the fused
+    reverse step give the same gradient."""
+    import subprocess
+    import sys
+    script = tmp_path / "g.py"
+    script.write_text(
+        "import sys, numpy as np, torch\n"
+        f"sys.path.insert(0, {repr(str(__import__('os').path.dirname(__import__('os').path.dirname(__file__))))})\n"
+        "from tests.test_gpu_adjoint import _runner\n"
+        "from tests.scenarios import small_uniform\n"
+        "sc = small_uniform(n_steps=120)\n"
+        "r = _runner(sc, (14, 20, 14, 20, 12, 14))\n"
+        "r.forward()\n"
+        "G = torch.from_numpy(np.random.default_rng(9).standard_normal((120, len(sc.probes))).astype(np.float32)).cuda()\n"
+        "g, s = r.backward(G)\n"
+        "np.save(sys.argv[1], np.concatenate([g.cpu().numpy().ravel(), s.cpu().numpy().ravel().astype(np.float64)]))\n")
+    import os
+    outs = []
+    for mode in ("fused", "twopass"):
+        out = tmp_path / f"{mode}.npy"
+        env = dict(os.environ, RFXB_ADJOINT_KERNEL=mode)
+        subprocess.run([sys.executable, str(script), str(out)], check=True, env=env, timeout=600)
+        outs.append(np.load(out))
+    from tests.scenarios import rel_l2
+    e = rel_l2(outs[0], outs[1])
+    print("fused vs twopass relL2", e)
+    assert e < 1e-5

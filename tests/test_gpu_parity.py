@@ -97,3 +97,27 @@ def test_pec_boundary_without_cpml(cuda):
     assert rel_l2(ts, ref.time_series) < TOL
     ey = fields["ey"]
     assert np.all(ey[0] == 0) and np.all(ey[-1] == 0) and np.all(ey[:, :, 0] == 0)
+
+
+def test_graph_replay_matches_direct_launches(cuda, tmp_path):
+    """Step sequences replayed from captured CUDA graphs equal direct launches
+    bit for bit (RFXB_GRAPHS=0 disables the graphs)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = tmp_path / "r.py"
+    script.write_text(
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {root!r})\n"
+        "from tests.scenarios import small_uniform\n"
+        "sc = small_uniform(n_steps=90)\n"
+        "ts, planes, fields = sc.run_product()\n"
+        "np.save(sys.argv[1], np.concatenate([ts.ravel(), np.abs(planes[0]).ravel(), fields['ez'].ravel()]))\n")
+    outs = []
+    for flag in ("1", "0"):
+        out = tmp_path / f"g{flag}.npy"
+        subprocess.run([sys.executable, str(script), str(out)], check=True, timeout=600,
+                       env=dict(os.environ, RFXB_GRAPHS=flag))
+        outs.append(np.load(out))
+    assert np.array_equal(outs[0], outs[1])
