@@ -42,6 +42,7 @@ extern "C" {
 #define RFXB_E_NOMEM (-3)     /* device allocation failed */
 #define RFXB_E_LAUNCH (-4)    /* kernel launch or CUDA runtime failure */
 #define RFXB_E_STATE (-5)     /* call out of order (e.g. adjoint before forward) */
+#define RFXB_E_TIMEOUT (-6)   /* a bounded wait inside a kernel ran out (device status word) */
 
 #define RFXB_AXIS_X 1u
 #define RFXB_AXIS_Y 2u
@@ -193,6 +194,12 @@ int rfxb_batch_record_history(RfxbBatch* batch, int step0, int n_steps);
 int rfxb_batch_adjoint_begin(RfxbBatch* batch, const RfxbAdjointIO* aios, int n_total, void* stream);
 int rfxb_batch_adjoint_advance(RfxbBatch* batch, const RfxbAdjointIO* aios, int step_hi, int n_steps,
                                void* stream);
+
+/* Synchronise the stream and read the device status word of the plan's (or
+ * batch's) launches: RFXB_E_TIMEOUT if a bounded pipeline wait inside a step
+ * kernel ran out (the kernel then left without hanging the GPU). */
+int rfxb_plan_device_status(RfxbPlan* plan, void* stream);
+int rfxb_batch_device_status(RfxbBatch* batch, void* stream);
 
 /* Bytes of device memory a plan holds (state, coefficients, psi, history,
  * checkpoints). */

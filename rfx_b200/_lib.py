@@ -85,6 +85,8 @@ SIGNATURES = {
     "rfxb_batch_adjoint_begin": (C.c_int, [C.c_void_p, C.POINTER(RfxbAdjointIO), C.c_int, C.c_void_p]),
     "rfxb_batch_adjoint_advance": (C.c_int, [C.c_void_p, C.POINTER(RfxbAdjointIO), C.c_int, C.c_int, C.c_void_p]),
     "rfxb_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+    "rfxb_plan_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "rfxb_batch_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 
 _lock = threading.Lock()

@@ -123,6 +123,7 @@ class AdjointRunner:
             for q, s0 in enumerate(range(0, N, self.K)):
                 p.checkpoint_save(q)
                 p.advance(s0, min(self.K, N - s0), st, ts)
+        p.check_device()
         self.ts = ts
         return ts
 
@@ -154,6 +155,7 @@ class AdjointRunner:
                 p.record_history(s0, L)
                 p.advance(s0, L, st, None)
                 p.adjoint_advance(s0 + L, L, **kw)
+        p.check_device()
         return grad.view(self.box_shape), src_adj
 
     def close(self):

@@ -130,6 +130,13 @@ class Sweep:
         Js, gs = self.objectives()
         return Js, self.backward(gs)
 
+    def check_device(self):
+        """Synchronise and raise if a bounded wait inside a kernel ran out."""
+        if self.batch is not None:
+            self.batch.check_device()
+        for p in self.plans:
+            p.check_device()
+
     def close(self):
         if self.batch is not None:
             self.batch.close()

@@ -22,11 +22,28 @@ namespace rfxb {
 #define RFXB_AEW 40
 #define RFXB_AHW 36
 
+__host__ __device__ constexpr int apad128(int nfloats) { return (nfloats % 32) ? 32 - (nfloats % 32) : 32; }
+
 template <int TY>
-struct __align__(16) AdjStage {
+struct AdjDims {
+  static constexpr int NE = 3 * (TY + 2) * RFXB_AEW;
+  static constexpr int NB = (TY + 2) * RFXB_AEW;
+  static constexpr int NH = 3 * (TY + 1) * RFXB_AHW;
+  static constexpr int NC = TY * RFXB_TZ;
+  static constexpr int P0 = apad128(NE);
+  static constexpr int P1 = apad128(NE + P0 + NB);
+  static constexpr int P2 = apad128(NE + P0 + NB + P1 + NH);
+  static constexpr unsigned BYTES = 4u * (NE + NB + NH + NC);
+};
+
+template <int TY>
+struct __align__(128) AdjStage {
   float ae[3][TY + 2][RFXB_AEW];   // masked adjoint E, rows y0-1 .. y0+TY, z from z0-4
+  float p0[AdjDims<TY>::P0];
   float cbp[TY + 2][RFXB_AEW];     // cb on the same footprint
+  float p1[AdjDims<TY>::P1];
   float ah[3][TY + 1][RFXB_AHW];   // adjoint H, rows y0-1 .. y0+TY-1, z from z0-4
+  float p2[AdjDims<TY>::P2];
   float ca[TY][RFXB_TZ];           // ca of the tile
 };
 
@@ -36,6 +53,7 @@ struct AdjSmem {
   float p[3][TY + 1][RFXB_TZ + 1];   // ch * aH1 of plane i, [y - y0 + 1][z - z0 + 1]
   RfxbInst P;
   AdjInst A;
+  unsigned long long mbar[RFXB_ANSTAGE];
 };
 
 __device__ __forceinline__ int astage_of(int p) { return (p + 1) & (RFXB_ANSTAGE - 1); }
@@ -163,11 +181,27 @@ __device__ __forceinline__ void adj_load_stage(AdjSmem<TY>& S, const AdjCtx& C, 
   }
 }
 
+// TMA boxes of plane ip (one thread): adjoint E and H of parity apar, cb with
+// the E footprint, ca of the tile.
 template <int TY>
+__device__ __forceinline__ void adj_tma_stage(AdjSmem<TY>& S, const CUtensorMap* tm, int apar, int y0, int z0,
+                                              int ip) {
+  const int s = astage_of(ip);
+  const uint32_t mb = smem_u32(&S.mbar[s]);
+  mbar_expect_tx(mb, AdjDims<TY>::BYTES);
+  tma_load_4d(smem_u32(&S.st[s].ae[0][0][0]), tm + 5 + apar, z0 - 4, y0, ip + 1, 0, mb);
+  tma_load_4d(smem_u32(&S.st[s].cbp[0][0]), tm + 9, z0 - 4, y0, ip + 1, 1, mb);
+  tma_load_4d(smem_u32(&S.st[s].ah[0][0][0]), tm + 7 + apar, z0 - 4, y0, ip + 1, 3, mb);
+  tma_load_4d(smem_u32(&S.st[s].ca[0][0]), tm + 10, z0, y0 + 1, ip + 1, 0, mb);
+}
+
+__device__ __forceinline__ uint32_t astage_parity(int p, int xa) { return (uint32_t)(((p - xa + 1) >> 2) & 1); }
+
+template <int TY, bool TMA>
 __global__ void __launch_bounds__(32 * TY, 4)
 adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
-                const RfxbWork* __restrict__ work, int n, int par, int apar) {
-  extern __shared__ __align__(16) unsigned char adj_smem_raw[];
+                const RfxbWork* __restrict__ work, const CUtensorMap* __restrict__ maps, int n, int par, int apar) {
+  extern __shared__ __align__(128) unsigned char adj_smem_raw[];
   AdjSmem<TY>& S = *reinterpret_cast<AdjSmem<TY>*>(adj_smem_raw);
   const int lane = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * 32 + lane;
@@ -179,7 +213,12 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     int* d = reinterpret_cast<int*>(&S.A);
     for (int t = tid; t < nw; t += 32 * TY) d[t] = __ldg(s + t);
   }
+  if (TMA && tid == 0) {
+    for (int q = 0; q < RFXB_ANSTAGE; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
+    mbar_fence_init();
+  }
   __syncthreads();
+  const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const RfxbInst& P = S.P;
   const AdjInst& A = S.A;
   AdjCtx C;
@@ -228,15 +267,30 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   const int xa = w.xa, xb = w.xb;
   const float* ca = P.ca;
   const float* cb = P.cb;
-  adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa - 1, tid);
-  adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa, tid);
-  cp_async_commit();
-  adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 1, tid);
-  cp_async_commit();
-  if (xa + 2 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 2, tid);
-  cp_async_commit();
-  cp_async_wait<2>();
-  __syncthreads();
+  auto bail = [&](int last_issued, int from) {
+    if (tid == 0) {
+      atomicOr(P.status, 1);
+      for (int p = from; p <= last_issued; ++p)
+        mbar_wait_bounded(smem_u32(&S.mbar[astage_of(p)]), astage_parity(p, xa));
+    }
+  };
+  if (TMA) {
+    if (tid == 0)
+      for (int p = xa - 1; p <= min(xa + 2, C.nx); ++p) adj_tma_stage<TY>(S, tm, apar, y0, z0, p);
+    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of(xa - 1)]), astage_parity(xa - 1, xa)) &&
+                    mbar_wait_bounded(smem_u32(&S.mbar[astage_of(xa)]), astage_parity(xa, xa));
+    if (__syncthreads_or(!ok)) { bail(min(xa + 2, C.nx), xa - 1); return; }
+  } else {
+    adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa - 1, tid);
+    adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa, tid);
+    cp_async_commit();
+    adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 1, tid);
+    cp_async_commit();
+    if (xa + 2 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 2, tid);
+    cp_async_commit();
+    cp_async_wait<2>();
+    __syncthreads();
+  }
 
   // phase A of plane xa-1 at this column: p and r_H there (not stored)
   float py_prev = 0.f, pz_prev = 0.f, rhy_prev = 0.f, rhz_prev = 0.f;
@@ -273,10 +327,16 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   }
 
   for (int i = xa; i < xb; ++i) {
-    cp_async_wait<1>();
-    __syncthreads();
-    if (i + 3 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, i + 3, tid);
-    cp_async_commit();
+    if (TMA) {
+      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of(i + 1)]), astage_parity(i + 1, xa));
+      if (__syncthreads_or(!ok)) { bail(min(i + 2, C.nx), i + 1); return; }
+      if (tid == 0 && i + 3 <= C.nx) adj_tma_stage<TY>(S, tm, apar, y0, z0, i + 3);
+    } else {
+      cp_async_wait<1>();
+      __syncthreads();
+      if (i + 3 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, i + 3, tid);
+      cp_async_commit();
+    }
     const int b0 = astage_of(i), b1 = astage_of(i + 1);
     const float xe0 = __ldg(P.xe + i), xe1 = __ldg(P.xe + i + 1);
     const float xh0 = __ldg(P.xh + i), xhm = __ldg(P.xh + i - 1);
@@ -446,10 +506,13 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     rhy_prev = rhy;
     rhz_prev = rhz;
   }
-  cp_async_wait<0>();
+  if (!TMA) cp_async_wait<0>();
 }
 
-template __global__ void adj_step_kernel<8>(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
+template __global__ void adj_step_kernel<8, true>(const RfxbInst*, const AdjInst*, const RfxbWork*,
+                                                  const CUtensorMap*, int, int, int);
+template __global__ void adj_step_kernel<8, false>(const RfxbInst*, const AdjInst*, const RfxbWork*,
+                                                   const CUtensorMap*, int, int, int);
 
 size_t adj_step_smem_bytes() { return sizeof(AdjSmem<8>); }
 

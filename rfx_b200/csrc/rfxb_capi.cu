@@ -1,6 +1,8 @@
 // Host side of the C ABI declared in include/rfxb200.h: plan and batch
 // objects, device allocation, descriptor upload, launch sequencing and the
 // CUDA-graph replay of step chunks.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,8 +19,8 @@
 #include "rfxb_common.cuh"
 
 namespace rfxb {
-template <int TY>
-__global__ void fwd_step_kernel(const RfxbInst*, const RfxbWork*, int, int);
+template <int TY, bool TMA>
+__global__ void fwd_step_kernel(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
 __global__ void dft_kernel(const RfxbInst*, const RfxbDftPlane*, int, int, int);
 __global__ void pack_kernel(float*, const float*, RfxbInst);
 __global__ void unpack_kernel(float*, const float*, RfxbInst);
@@ -27,8 +29,8 @@ __global__ void coef_kernel(RfxbInst, float*, float*, float*, float*, const floa
 __global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
-template <int TY>
-__global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
+template <int TY, bool TMA>
+__global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int);
 size_t adj_step_smem_bytes();
 }  // namespace rfxb
 
@@ -94,6 +96,8 @@ struct RfxbPlan {
   int adj_fpar = 0;   // parity of the adjoint field buffers
   // single-plan group state
   RfxbBatch* self_group = nullptr;
+  // TMA descriptors (layout in rfxb_inst.h, RFXB_NMAPS)
+  CUtensorMap tmaps[RFXB_NMAPS];
 
   ~RfxbPlan() {
     for (void* p : allocs) cudaFree(p);
@@ -128,6 +132,8 @@ struct RfxbBatch {
   RfxbWork* d_work = nullptr;
   int n_work = 0;
   RfxbDftPlane* d_dft = nullptr;
+  CUtensorMap* d_maps = nullptr;   // RFXB_NMAPS per plan
+  int* d_status = nullptr;         // device status word of the group's launches
   std::vector<RfxbDftPlane> dft;
   int dft_blocks = 0;
   std::vector<void*> allocs;
@@ -176,12 +182,77 @@ int resident_ctas() {
   static int r = -1;
   if (r < 0) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fwd_step_kernel<kTY>, 32 * kTY, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fwd_step_kernel<kTY, true>, 32 * kTY, 0) != cudaSuccess ||
         per_sm < 1)
       per_sm = 4;
     r = per_sm * sm_count();
   }
   return r;
+}
+
+// TMA staging is the default; RFXB_STAGING=cpasync selects per-thread 16-byte
+// cp.async staging of the same planes.
+bool use_tma() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_STAGING");
+    v = (e && std::string(e) == "cpasync") ? 0 : 1;
+  }
+  return v == 1;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so the
+// library needs no link-time dependency on libcuda.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }
+  return fn;
+}
+
+// 4-D map over a block of `ncomp` padded per-cell arrays with component stride
+// cs: dims (zs, ny+2, nx+2, ncomp), origin at cell (i, j) = (-1, -1), k = 0.
+int encode_block_map(CUtensorMap* m, const RfxbPlan& p, float* block, int ncomp, unsigned bx, unsigned by,
+                     unsigned bc) {
+  auto fn = tensor_map_encoder();
+  if (!fn) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled is not available from the driver");
+  const RfxbInst& I = p.inst;
+  void* addr = block + (I.off0 - I.ps - I.zs);
+  cuuint64_t dims[4] = {(cuuint64_t)I.zs, (cuuint64_t)(p.ny + 2), (cuuint64_t)(p.nx + 2), (cuuint64_t)ncomp};
+  cuuint64_t strides[3] = {(cuuint64_t)I.zs * 4, (cuuint64_t)I.ps * 4, (cuuint64_t)I.cs * 4};
+  cuuint32_t box[4] = {bx, by, 1, bc};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, addr, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return 0;
+}
+
+int encode_forward_maps(RfxbPlan* p) {
+  const unsigned ty = kTY;
+  for (int s = 0; s < 2; ++s) {
+    if (int rc = encode_block_map(&p->tmaps[s], *p, p->inst.F[s][0], 6, 40, ty + 2, 3)) return rc;
+    if (int rc = encode_block_map(&p->tmaps[2 + s], *p, p->inst.F[s][0], 6, 36, ty + 1, 3)) return rc;
+  }
+  return encode_block_map(&p->tmaps[4], *p, p->ca, 3, 32, ty, 2);
+}
+
+int encode_adjoint_maps(RfxbPlan* p) {
+  const unsigned ty = kTY;
+  for (int s = 0; s < 2; ++s) {
+    if (int rc = encode_block_map(&p->tmaps[5 + s], *p, p->adj.aF[s][0], 6, 40, ty + 2, 3)) return rc;
+    if (int rc = encode_block_map(&p->tmaps[7 + s], *p, p->adj.aF[s][0], 6, 36, ty + 1, 3)) return rc;
+  }
+  if (int rc = encode_block_map(&p->tmaps[9], *p, p->ca, 3, 40, ty + 2, 1)) return rc;
+  return encode_block_map(&p->tmaps[10], *p, p->ca, 3, 32, ty, 1);
 }
 
 int upload_tables(RfxbPlan* p, const float* h, int n, const float** dst) {
@@ -241,7 +312,18 @@ int build_group(RfxbBatch* g) {
   if (!g->dft.empty()) {
     if (int rc = galloc((void**)&g->d_dft, sizeof(RfxbDftPlane) * g->dft.size())) return rc;
   }
+  if (int rc = galloc((void**)&g->d_maps, sizeof(CUtensorMap) * RFXB_NMAPS * g->plans.size())) return rc;
+  if (int rc = galloc((void**)&g->d_status, sizeof(int))) return rc;
+  RFXB_CUDA(cudaMemset(g->d_status, 0, sizeof(int)));
   RFXB_CUDA(cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking));
+  return 0;
+}
+
+int upload_maps(RfxbBatch* g, cudaStream_t st) {
+  std::vector<CUtensorMap> m(g->plans.size() * RFXB_NMAPS);
+  for (size_t q = 0; q < g->plans.size(); ++q)
+    std::memcpy(&m[q * RFXB_NMAPS], g->plans[q]->tmaps, sizeof(CUtensorMap) * RFXB_NMAPS);
+  RFXB_CUDA(cudaMemcpyAsync(g->d_maps, m.data(), sizeof(CUtensorMap) * m.size(), cudaMemcpyHostToDevice, st));
   return 0;
 }
 
@@ -269,7 +351,9 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
   for (const auto& pl : g->dft)
     if (*has_dft && pl.acc == nullptr)
       return fail(RFXB_E_INVALID, "either every DFT plane of a group gets accumulator and phase table, or none");
+  for (auto& I : insts) I.status = g->d_status;
   RFXB_CUDA(cudaMemcpyAsync(g->d_inst, insts.data(), sizeof(RfxbInst) * insts.size(), cudaMemcpyHostToDevice, st));
+  if (int rc = upload_maps(g, st)) return rc;
   if (!g->dft.empty())
     RFXB_CUDA(cudaMemcpyAsync(g->d_dft, g->dft.data(), sizeof(RfxbDftPlane) * g->dft.size(),
                               cudaMemcpyHostToDevice, st));
@@ -281,7 +365,10 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, c
   int par = par0;
   for (int s = 0; s < n_steps; ++s) {
     const int n = step0 + s;
-    fwd_step_kernel<kTY><<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_work, n, par);
+    if (use_tma())
+      fwd_step_kernel<kTY, true><<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_work, g->d_maps, n, par);
+    else
+      fwd_step_kernel<kTY, false><<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_work, g->d_maps, n, par);
     if (has_dft)
       dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, par ^ 1);
     par ^= 1;
@@ -363,6 +450,7 @@ int ensure_adjoint(RfxbPlan* p, cudaStream_t st) {
         if (int rc = p->alloc(&p->adj.aPsiE[s][a], p->psi_elems[a])) return rc;
       }
     p->adj_alloc = true;
+    if (int rc = encode_adjoint_maps(p)) return rc;
   }
   for (int s = 0; s < 2; ++s) RFXB_CUDA(cudaMemsetAsync(p->adj.aF[s][0], 0, 6 * p->elems * sizeof(float), st));
   for (int s = 0; s < 2; ++s)
@@ -405,8 +493,10 @@ int upload_adjoint(RfxbBatch* g, const RfxbAdjointIO* aios, cudaStream_t st) {
       return fail(RFXB_E_STATE, "gradient requested without a gradient region or coefficient derivatives");
     adjs[q] = p->adj;
   }
+  for (auto& I : insts) I.status = g->d_status;
   RFXB_CUDA(cudaMemcpyAsync(g->d_inst, insts.data(), sizeof(RfxbInst) * insts.size(), cudaMemcpyHostToDevice, st));
   RFXB_CUDA(cudaMemcpyAsync(g->d_adj, adjs.data(), sizeof(AdjInst) * adjs.size(), cudaMemcpyHostToDevice, st));
+  if (int rc = upload_maps(g, st)) return rc;
   return 0;
 }
 
@@ -436,7 +526,9 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
   if (!two) {
     static bool attr = false;
     if (!attr) {
-      RFXB_CUDA(cudaFuncSetAttribute(adj_step_kernel<kTY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      RFXB_CUDA(cudaFuncSetAttribute(adj_step_kernel<kTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)adj_step_smem_bytes()));
+      RFXB_CUDA(cudaFuncSetAttribute(adj_step_kernel<kTY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)adj_step_smem_bytes()));
       attr = true;
     }
@@ -448,8 +540,12 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
         adj_pass_a<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
         adj_pass_b<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
       } else {
-        adj_step_kernel<kTY><<<g->n_work, dim3(32, kTY), adj_step_smem_bytes(), cs>>>(g->d_inst, g->d_adj,
-                                                                                      g->d_work, s, par, fpar);
+        if (use_tma())
+          adj_step_kernel<kTY, true><<<g->n_work, dim3(32, kTY), adj_step_smem_bytes(), cs>>>(
+              g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar);
+        else
+          adj_step_kernel<kTY, false><<<g->n_work, dim3(32, kTY), adj_step_smem_bytes(), cs>>>(
+              g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar);
         fpar ^= 1;
       }
       par ^= 1;
@@ -541,9 +637,10 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
     if (int rc = p->alloc(&q, 6 * p->elems)) return bail(rc);
     for (int c = 0; c < 6; ++c) I.F[s][c] = q + c * p->elems;
   }
-  if (int rc = p->alloc(&p->ca, p->elems)) return bail(rc);
-  if (int rc = p->alloc(&p->cb, p->elems)) return bail(rc);
-  if (int rc = p->alloc(&p->ce, p->elems)) return bail(rc);
+  // ca, cb, ce in one block with the field component stride (one TMA map)
+  if (int rc = p->alloc(&p->ca, 3 * p->elems)) return bail(rc);
+  p->cb = p->ca + p->elems;
+  p->ce = p->ca + 2 * p->elems;
   for (float* q : {p->ca, p->cb, p->ce})
     if (cudaMemset(q, 0, p->elems * sizeof(float)) != cudaSuccess) return bail(fail(RFXB_E_LAUNCH, "cudaMemset"));
   I.ca = p->ca; I.cb = p->cb; I.ce = p->ce; I.ch = nullptr;
@@ -626,6 +723,8 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
   if (hb[0] >= hb[1]) { I.hb[0] = 0; I.hb[1] = 0; }
   p->hcells = (long long)(I.hb[1] - I.hb[0]) * (I.hb[3] - I.hb[2]) * (I.hb[5] - I.hb[4]);
   I.hist = nullptr;
+  std::memset(p->tmaps, 0, sizeof(p->tmaps));
+  if (int rc = encode_forward_maps(p)) return bail(rc);
   // own single-plan group
   RfxbBatch* g = new RfxbBatch();
   g->plans.push_back(p);
@@ -845,6 +944,26 @@ int rfxb_batch_adjoint_begin(RfxbBatch* g, const RfxbAdjointIO* aios, int n_tota
 int rfxb_batch_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, int n_steps, void* stream) {
   if (!g || !aios) return fail(RFXB_E_INVALID, "null argument");
   return group_adjoint_advance(g, aios, step_hi, n_steps, static_cast<cudaStream_t>(stream));
+}
+
+int rfxb_plan_device_status(RfxbPlan* p, void* stream) {
+  if (!p) return fail(RFXB_E_INVALID, "null plan");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  RFXB_CUDA(cudaStreamSynchronize(st));
+  int v = 0;
+  RFXB_CUDA(cudaMemcpy(&v, p->self_group->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
+  return 0;
+}
+
+int rfxb_batch_device_status(RfxbBatch* g, void* stream) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  RFXB_CUDA(cudaStreamSynchronize(st));
+  int v = 0;
+  RFXB_CUDA(cudaMemcpy(&v, g->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
+  return 0;
 }
 
 int64_t rfxb_plan_device_bytes(const RfxbPlan* p) {

@@ -23,10 +23,26 @@ namespace rfxb {
 #define RFXB_EW 40   // staged E row: z in [z0 - 4, z0 + 36)
 #define RFXB_HW 36   // staged H row: z in [z0 - 4, z0 + 32)
 
+// float counts padded so every array of a stage starts on a 128-byte boundary
+// (the alignment TMA writes into shared memory need)
+__host__ __device__ constexpr int pad128(int nfloats) { return (nfloats % 32) ? 32 - (nfloats % 32) : 0; }
+
 template <int TY>
-struct __align__(16) FwdStage {
+struct FwdStageDims {
+  static constexpr int NE = 3 * (TY + 2) * RFXB_EW;
+  static constexpr int NH = 3 * (TY + 1) * RFXB_HW;
+  static constexpr int NC = 2 * TY * RFXB_TZ;
+  static constexpr int PE = pad128(NE) ? pad128(NE) : 32;
+  static constexpr int PH = pad128(NE + PE + NH) ? pad128(NE + PE + NH) : 32;
+  static constexpr unsigned BYTES = 4u * (NE + NH + NC);   // bytes the TMA boxes deliver
+};
+
+template <int TY>
+struct __align__(128) FwdStage {
   float e[3][TY + 2][RFXB_EW];   // ex ey ez, rows y0-1 .. y0+TY
+  float pe[FwdStageDims<TY>::PE];
   float h[3][TY + 1][RFXB_HW];   // hx hy hz (H^{n-1/2}), rows y0-1 .. y0+TY-1
+  float ph[FwdStageDims<TY>::PH];
   float cab[2][TY][RFXB_TZ];     // ca cb, rows y0 .. y0+TY-1, z from z0
 };
 
@@ -35,6 +51,7 @@ struct FwdSmem {
   FwdStage<TY> st[RFXB_NSTAGE];      // plane p lives in stage (p + 1) & 3
   float h[3][TY + 1][RFXB_TZ + 1];   // H^{n+1/2} of plane i: [y - y0 + 1][z - z0 + 1]
   RfxbInst P;
+  unsigned long long mbar[RFXB_NSTAGE];
 };
 
 __device__ __forceinline__ int stage_of(int p) { return (p + 1) & (RFXB_NSTAGE - 1); }
@@ -175,15 +192,38 @@ __device__ __forceinline__ void load_stage(FwdSmem<TY>& S, const FwdCtx& C, cons
   }
 }
 
+// Issue the TMA boxes of plane ip into its stage (one thread).  Tensor maps of
+// an instance: [0|1] field block of parity 0|1 with the E box, [2|3] the same
+// with the H box, [4] the coefficient block with the ca/cb box.
 template <int TY>
+__device__ __forceinline__ void tma_stage(FwdSmem<TY>& S, const CUtensorMap* tm, int par, int y0, int z0, int ip) {
+  const int s = stage_of(ip);
+  const uint32_t mb = smem_u32(&S.mbar[s]);
+  mbar_expect_tx(mb, FwdStageDims<TY>::BYTES);
+  tma_load_4d(smem_u32(&S.st[s].e[0][0][0]), tm + par, z0 - 4, y0, ip + 1, 0, mb);
+  tma_load_4d(smem_u32(&S.st[s].h[0][0][0]), tm + 2 + par, z0 - 4, y0, ip + 1, 3, mb);
+  tma_load_4d(smem_u32(&S.st[s].cab[0][0][0]), tm + 4, z0, y0 + 1, ip + 1, 0, mb);
+}
+
+// Planes are loaded in order xa-1, xa, ...; stage (p+1)&3 completes its
+// k-th fill on mbarrier phase k, so plane p waits on parity ((p-xa+1)/4) & 1.
+__device__ __forceinline__ uint32_t stage_parity(int p, int xa) { return (uint32_t)(((p - xa + 1) >> 2) & 1); }
+
+template <int TY, bool TMA>
 __global__ void __launch_bounds__(32 * TY, 4)
-fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work, int n, int par) {
+fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work,
+                const CUtensorMap* __restrict__ maps, int n, int par) {
   __shared__ FwdSmem<TY> S;
   const int lane = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * 32 + lane;
   const RfxbWork w = work[blockIdx.x];
   load_inst(S.P, insts + w.inst, tid, 32 * TY);
+  if (TMA && tid == 0) {
+    for (int q = 0; q < RFXB_NSTAGE; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
+    mbar_fence_init();
+  }
   __syncthreads();
+  const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const RfxbInst& P = S.P;
   FwdCtx C;
   C.nx = P.nx; C.ny = P.ny; C.nz = P.nz; C.zs = P.zs; C.ncp = P.ncp; C.par = par;
@@ -232,16 +272,33 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   const bool pec_kz = ((pec & 4u) != 0) && (k == C.nz - 1);
 
   const int xa = w.xa, xb = w.xb;
-  // pipeline: planes xa-1 and xa (group 0), xa+1 (group 1), xa+2 (group 2)
-  load_stage<TY>(S, C, ca, cb, y0, z0, xa - 1, tid);
-  load_stage<TY>(S, C, ca, cb, y0, z0, xa, tid);
-  cp_async_commit();
-  load_stage<TY>(S, C, ca, cb, y0, z0, xa + 1, tid);
-  cp_async_commit();
-  if (xa + 2 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, xa + 2, tid);
-  cp_async_commit();
-  cp_async_wait<2>();
-  __syncthreads();
+  // A wait that runs out marks the launch failed and leaves the CTA after
+  // draining the boxes it issued (a stalled copy cannot be waited out forever).
+  auto bail = [&](int last_issued, int from) {
+    if (tid == 0) {
+      atomicOr(P.status, 1);
+      for (int p = from; p <= last_issued; ++p) mbar_wait_bounded(smem_u32(&S.mbar[stage_of(p)]), stage_parity(p, xa));
+    }
+  };
+  if (TMA) {
+    if (tid == 0) {
+      for (int p = xa - 1; p <= min(xa + 2, C.nx); ++p) tma_stage<TY>(S, tm, par, y0, z0, p);
+    }
+    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa - 1)]), stage_parity(xa - 1, xa)) &&
+                    mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa)]), stage_parity(xa, xa));
+    if (__syncthreads_or(!ok)) { bail(min(xa + 2, C.nx), xa - 1); return; }
+  } else {
+    // pipeline: planes xa-1 and xa (group 0), xa+1 (group 1), xa+2 (group 2)
+    load_stage<TY>(S, C, ca, cb, y0, z0, xa - 1, tid);
+    load_stage<TY>(S, C, ca, cb, y0, z0, xa, tid);
+    cp_async_commit();
+    load_stage<TY>(S, C, ca, cb, y0, z0, xa + 1, tid);
+    cp_async_commit();
+    if (xa + 2 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, xa + 2, tid);
+    cp_async_commit();
+    cp_async_wait<2>();
+    __syncthreads();
+  }
 
   // H of plane xa-1 at this column (computed, not stored: its owner stores it).
   float hy_prev = 0.f, hz_prev = 0.f;
@@ -258,10 +315,18 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   const bool has_emask = P.emask != nullptr;
 
   for (int i = xa; i < xb; ++i) {
-    cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
-    __syncthreads();      // ... for every thread; plane i-1's stage is free
-    if (i + 3 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, i + 3, tid);
-    cp_async_commit();
+    if (TMA) {
+      // plane i+1 has landed; after the barrier every thread is done with
+      // plane i-1, whose stage takes plane i+3
+      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), stage_parity(i + 1, xa));
+      if (__syncthreads_or(!ok)) { bail(min(i + 2, C.nx), i + 1); return; }
+      if (tid == 0 && i + 3 <= C.nx) tma_stage<TY>(S, tm, par, y0, z0, i + 3);
+    } else {
+      cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
+      __syncthreads();      // ... for every thread; plane i-1's stage is free
+      if (i + 3 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, i + 3, tid);
+      cp_async_commit();
+    }
     const int b0 = stage_of(i), b1 = stage_of(i + 1);
     const float xh = __ldg(P.xh + i), xe = __ldg(P.xe + i);
 
@@ -449,7 +514,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     hy_prev = hy;
     hz_prev = hz;
   }
-  cp_async_wait<0>();
+  if (!TMA) cp_async_wait<0>();
 }
 
 // Running DFT of one plane per launch entry, Kahan-compensated
@@ -539,7 +604,7 @@ __global__ void coef_kernel(RfxbInst P, float* ca, float* cb, float* ce, float* 
 }
 
 // Explicit template instantiations used by the host side.
-template __global__ void fwd_step_kernel<8>(const RfxbInst*, const RfxbWork*, int, int);
-template __global__ void fwd_step_kernel<4>(const RfxbInst*, const RfxbWork*, int, int);
+template __global__ void fwd_step_kernel<8, true>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+template __global__ void fwd_step_kernel<8, false>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
 
 }  // namespace rfxb

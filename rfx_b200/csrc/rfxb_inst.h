@@ -15,9 +15,15 @@
 // stencils carry no boundary branches.
 #pragma once
 #include <cstdint>
+#include <cuda.h>   // CUtensorMap
 
 #define RFXB_TZ 32          // tile extent along z (one warp)
 #define RFXB_MAXC 6
+// TMA descriptors per instance: [0|1] fields parity 0|1 with the E box,
+// [2|3] with the H box, [4] coefficients with the ca/cb box, [5|6] adjoint
+// fields with the E box, [7|8] with the H box, [9] cb with the E box,
+// [10] ca with the tile box.
+#define RFXB_NMAPS 16
 
 // CPML psi layout per axis (q = which of the two corrected components):
 //   x: ((side*2 + q)*n + s)*ny*zs + j*zs + k
@@ -71,6 +77,7 @@ struct RfxbInst {
   const float* dcb;        // d cb / d eps_r over the gradient region
   double* grad;            // accumulated dJ/d eps_r over the gradient region
   float* src_adj;          // dJ/d w[n, s] output [n*src_ld + s]
+  int* status;             // device status word: bit 0 = a pipeline wait ran out
 };
 
 struct AdjInst {           // adjoint state of one instance (same layouts as the forward state)

@@ -238,6 +238,10 @@ class Plan:
     def record_history(self, step0, n_steps):
         check(self._lib.rfxb_plan_record_history(self._h, int(step0), int(n_steps)), "rfxb_plan_record_history")
 
+    def check_device(self):
+        """Synchronise and raise if a bounded wait inside a kernel ran out."""
+        check(self._lib.rfxb_plan_device_status(self._h, _stream()), "rfxb_plan_device_status")
+
     def checkpoint_reserve(self, n):
         check(self._lib.rfxb_plan_checkpoint_reserve(self._h, int(n)), "rfxb_plan_checkpoint_reserve")
 
@@ -304,6 +308,9 @@ class Batch:
 
     def record_history(self, step0, n_steps):
         check(self._lib.rfxb_batch_record_history(self._h, int(step0), int(n_steps)), "rfxb_batch_record_history")
+
+    def check_device(self):
+        check(self._lib.rfxb_batch_device_status(self._h, _stream()), "rfxb_batch_device_status")
 
     def adjoint_begin(self, n_total, aios):
         arr = (RfxbAdjointIO * len(self.plans))(*[Plan.adjoint_io(**kw) for kw in aios])

@@ -208,7 +208,7 @@ def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes
             if report_every:
                 torch.cuda.current_stream().synchronize()
                 print(f"[PROGRESS] {report_label} step {done}/{n_steps}", flush=True)
-        torch.cuda.current_stream().synchronize()
+        plan.check_device()
         ts_all = probe_out.cpu().numpy() if probe_out is not None else np.zeros((n_steps, 0), np.float32)
         ts = ts_all[:, :len(probes)]
         out_planes = tuple(d._replace(accumulator=a.cpu().numpy()) for d, a in zip(dft_planes, accs))
