@@ -126,21 +126,34 @@ def test_autograd_function(cuda):
                                        (small_nonuniform, (12, 18, 12, 18, 11, 13))])
 def test_gradient_matches_oracle_adjoint(cuda, build, box):
     """dJ/d eps_r of the CUDA adjoint against the oracle's float64 transpose
-    for J = <G, ts> with a seeded G (relative L2 below 1e-4)."""
+    for J = <G, ts> with a seeded G.
+
+    Tolerance: relative L2 below max(1e-4, 2 x the error of the oracle's own
+    float32 run against its float64 run).  In the vacuum box of the uniform
+    scene the gradient is a sum over 140 steps with heavy cancellation, and
+    float32 arithmetic of the same algorithm already lands about 1e-3 from
+    float64 there; the graded scene stays near 1e-7.  The source adjoint has
+    no such cancellation and is held to 1e-4."""
     from oracle.adjoint import forward_adjoint
     from tests.scenarios import rel_l2
     sc = build(n_steps=140)
     G = np.random.default_rng(7).standard_normal((sc.n_steps, len(sc.probes)))
-    _, og, osrc = forward_adjoint(sc.ogrid, sc.materials, sc.n_steps, nonuniform=sc.lane == "nonuniform",
-                                  boundary=sc.boundary, pec_axes=sc.pec_axes, sources=sc.sources, probes=sc.probes,
-                                  pec_mask=sc.pec_mask, box=box, objective_grad=lambda ts: G)
+    res = {}
+    for dt in (np.float64, np.float32):
+        _, og, osrc = forward_adjoint(sc.ogrid, sc.materials, sc.n_steps, nonuniform=sc.lane == "nonuniform",
+                                      boundary=sc.boundary, pec_axes=sc.pec_axes, sources=sc.sources,
+                                      probes=sc.probes, pec_mask=sc.pec_mask, box=box, objective_grad=lambda ts: G,
+                                      dtype=dt)
+        res[dt] = (og, osrc)
+    og, osrc = res[np.float64]
+    e32 = rel_l2(res[np.float32][0], og)
     r = _runner(sc, box)
     r.forward()
     grad, src_adj = r.backward(torch.from_numpy(G.astype(np.float32)).cuda())
     e = rel_l2(grad.cpu().numpy(), og)
     es = rel_l2(src_adj.cpu().numpy(), osrc)
-    print(sc.name, "grad relL2 vs oracle adjoint", e, "source adjoint", es)
-    assert e < 1e-4 and es < 1e-4
+    print(sc.name, "grad relL2 vs oracle f64 adjoint", e, "(oracle f32:", e32, ") source adjoint", es)
+    assert e < max(1e-4, 2.0 * e32) and es < 1e-4
     r.close()
 
 
