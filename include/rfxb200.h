@@ -201,6 +201,24 @@ int rfxb_batch_adjoint_advance(RfxbBatch* batch, const RfxbAdjointIO* aios, int 
 int rfxb_plan_device_status(RfxbPlan* plan, void* stream);
 int rfxb_batch_device_status(RfxbBatch* batch, void* stream);
 
+/* Forward steps without any device allocation.  No counterpart in the
+ * reference: rfx leaves memory to JAX, so it never needs this.  It is for
+ * callers that cannot call cudaMalloc -- a host program whose own allocator
+ * owns all device memory, or one that cannot afford the device-wide
+ * synchronisation an allocation may bring mid-loop -- and therefore cannot
+ * create a plan.  One call loads the caller's fields (reference layout),
+ * computes the coefficients from eps_r_dev / sigma_dev (mu_r = 1, no edge
+ * mask), starts from zero CPML psi, runs n_steps steps of the fused step
+ * kernel with sources and probes from io, and writes the fields back.  All
+ * internal state lives in one fixed 64 MiB device array inside the library:
+ * grids whose state does not fit (about 0.8 M cells) get RFXB_E_NOMEM, and DFT
+ * planes or gradient regions get RFXB_E_INVALID (use a plan for those).  The
+ * first call on a device looks up the array's address (make it before any
+ * stream capture).  Calls share the array: each clears what must start at
+ * zero, and two calls whose GPU work overlaps race on it. */
+int rfxb_forward_noalloc(const RfxbDesc* desc, const float* eps_r_dev, const float* sigma_dev,
+                         float* const* fields_dev, const RfxbStepIO* io, int step0, int n_steps, void* stream);
+
 /* Bytes of device memory a plan holds (state, coefficients, psi, history,
  * checkpoints). */
 int64_t rfxb_plan_device_bytes(const RfxbPlan* plan);

@@ -54,6 +54,14 @@ int fail(int code, const std::string& msg) {
       return fail(RFXB_E_LAUNCH, std::string(#call) + ": " + cudaGetErrorString(_e));          \
   } while (0)
 
+}  // namespace
+
+namespace rfxb {
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace rfxb
+
+namespace {
+
 int sm_count() {
   static int n = -1;
   if (n < 0) {
