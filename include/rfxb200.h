@@ -223,6 +223,14 @@ int rfxb_forward_noalloc(const RfxbDesc* desc, const float* eps_r_dev, const flo
  * checkpoints). */
 int64_t rfxb_plan_device_bytes(const RfxbPlan* plan);
 
+/* Which forward step kernel the launches of a plan (or batch) use: 0 the
+ * generic one (cp.async staging, CPML psi read from global memory), 1 TMA
+ * staging without CPML, 2 TMA staging with the CPML psi staged by TMA one
+ * plane ahead; -1 for a null handle.  A diagnostic of this implementation,
+ * no counterpart in the reference. */
+int rfxb_plan_forward_variant(const RfxbPlan* plan);
+int rfxb_batch_forward_variant(const RfxbBatch* batch);
+
 #ifdef __cplusplus
 }
 #endif

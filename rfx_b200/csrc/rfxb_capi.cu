@@ -6,12 +6,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
 #include <tuple>
+#include <queue>
 #include <utility>
 #include <vector>
 
@@ -19,8 +21,9 @@
 #include "rfxb_common.cuh"
 
 namespace rfxb {
-template <int TY, bool TMA>
+template <int TY, int MODE>
 __global__ void fwd_step_kernel(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+size_t fwd_step_smem_bytes(int mode);
 __global__ void dft_kernel(const RfxbInst*, const RfxbDftPlane*, int, int, int);
 __global__ void pack_kernel(float*, const float*, RfxbInst);
 __global__ void unpack_kernel(float*, const float*, RfxbInst);
@@ -106,6 +109,7 @@ struct RfxbPlan {
   RfxbBatch* self_group = nullptr;
   // TMA descriptors (layout in rfxb_inst.h, RFXB_NMAPS)
   CUtensorMap tmaps[RFXB_NMAPS];
+  bool psi_maps_ok = false;    // the CPML psi maps encoded (staged-psi kernel usable)
 
   ~RfxbPlan() {
     for (void* p : allocs) cudaFree(p);
@@ -142,6 +146,7 @@ struct RfxbBatch {
   RfxbDftPlane* d_dft = nullptr;
   CUtensorMap* d_maps = nullptr;   // RFXB_NMAPS per plan
   int* d_status = nullptr;         // device status word of the group's launches
+  int fwd_mode = 0;                // forward step kernel variant (see rfxb_fwd.cu)
   std::vector<RfxbDftPlane> dft;
   int dft_blocks = 0;
   std::vector<void*> allocs;
@@ -186,16 +191,130 @@ void make_work(const RfxbPlan& p, int inst_index, int chunks, std::vector<RfxbWo
         out.push_back(RfxbWork{inst_index, y * kTY, z * 32, xa, std::min(p.nx, xa + xlen)});
 }
 
-int resident_ctas() {
-  static int r = -1;
-  if (r < 0) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fwd_step_kernel<kTY, true>, 32 * kTY, 0) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 4;
-    r = per_sm * sm_count();
+// Cost-balanced work list.  A CTA's time is modelled as the sum over its
+// planes of 1 (a plain Yee tile-plane) plus `slab` for every CPML slab the
+// plane and tile lie in, plus `prologue` plane-costs for its start-up (the
+// extra planes it stages and the H it recomputes at xa-1).  Each tile's x
+// line is cut into pieces of about equal cost; the piece size is chosen, over
+// one to four waves of the resident CTA capacity, by simulating the block
+// scheduler's greedy dispatch of the pieces in decreasing cost order (the
+// order the list is emitted in), so heavy CPML tiles and large instances of a
+// batch no longer set the step time.
+void make_balanced_work(const std::vector<RfxbPlan*>& plans, int resident, double slab, double prologue,
+                        std::vector<RfxbWork>& out) {
+  struct Tile { int inst, y0, z0, nx, ncpx; double c, cx; double total; };
+  std::vector<Tile> tiles;
+  double W = 0.0;
+  for (size_t q = 0; q < plans.size(); ++q) {
+    const RfxbPlan& p = *plans[q];
+    const int n = p.inst.ncp;
+    const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
+    for (int y0 = 0; y0 < p.ny; y0 += kTY)
+      for (int z0 = 0; z0 < p.nz; z0 += 32) {
+        double c = 1.0;
+        if ((ax & 2u) && (y0 - 1 < n || y0 + kTY - 1 >= p.ny - n)) c += slab;
+        if ((ax & 4u) && (z0 - 1 < n || z0 + 31 >= p.nz - n)) c += slab;
+        const int ncpx = (ax & 1u) ? n : 0;
+        const double cx = (ax & 1u) ? slab : 0.0;
+        const double total = p.nx * c + 2.0 * ncpx * cx;
+        tiles.push_back(Tile{(int)q, y0, z0, p.nx, ncpx, c, cx, total});
+        W += total;
+      }
   }
-  return r;
+  auto plane_cost = [](const Tile& t, int i) {
+    return t.c + ((i < t.ncpx || i >= t.nx - t.ncpx) ? t.cx : 0.0);
+  };
+  struct Item { RfxbWork w; double cost; int piece; };
+  auto cut = [&](double T, std::vector<Item>& items) {
+    items.clear();
+    for (const Tile& t : tiles) {
+      const int mmax = std::max(1, t.nx / 4);   // pieces of at least 4 planes
+      const int m = std::max(1, std::min(mmax, (int)std::llround(t.total / T)));
+      int xa = 0;
+      double acc = 0.0;
+      for (int piece = 1; piece <= m; ++piece) {
+        const double goal = t.total * piece / m;
+        int xb = xa;
+        double c = 0.0;
+        while (xb < t.nx && (piece == m || acc + c + 0.5 * plane_cost(t, xb) <= goal)) {
+          c += plane_cost(t, xb);
+          ++xb;
+        }
+        if (xb == xa) { c += plane_cost(t, xb); ++xb; }
+        items.push_back(Item{RfxbWork{t.inst, t.y0, t.z0, xa, xb}, c + prologue * t.c, piece});
+        acc += c;
+        xa = xb;
+        if (xa >= t.nx) break;
+      }
+    }
+    // decreasing cost in 5% buckets; within a bucket x-piece major, so tiles
+    // that neighbour in (y, z) run the same x range together and share halos
+    // through L2
+    double cmax = 0.0;
+    for (const Item& it : items) cmax = std::max(cmax, it.cost);
+    auto bucket = [&](const Item& it) { return (int)std::floor(20.0 * it.cost / cmax); };
+    std::stable_sort(items.begin(), items.end(), [&](const Item& a, const Item& b) {
+      const int ba = bucket(a), bb = bucket(b);
+      if (ba != bb) return ba > bb;
+      return a.piece < b.piece;
+    });
+  };
+  auto makespan = [&](const std::vector<Item>& items) {
+    std::priority_queue<double, std::vector<double>, std::greater<double>> slots;
+    for (int r = 0; r < resident; ++r) slots.push(0.0);
+    double end = 0.0;
+    for (const Item& it : items) {
+      const double t = slots.top() + it.cost;
+      slots.pop();
+      slots.push(t);
+      end = std::max(end, t);
+    }
+    return end;
+  };
+  std::vector<Item> best, cur;
+  double best_t = 1e300;
+  for (int waves = 1; waves <= 4; ++waves) {
+    cut(W / ((double)resident * waves), cur);
+    const double t = makespan(cur);
+    if (t < best_t * (1.0 - 0.02)) { best_t = t; best = cur; }   // more waves only for a clear gain
+  }
+  out.clear();
+  for (const Item& it : best) out.push_back(it.w);
+}
+
+// RFXB_WORK=uniform selects the plain split (one x chunk count for the group).
+bool balanced_work() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_WORK");
+    v = (e && std::string(e) == "uniform") ? 0 : 1;
+  }
+  return v == 1;
+}
+
+// Forward step kernel of a mode with its dynamic shared memory enabled.
+using FwdKernel = void (*)(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+FwdKernel fwd_kernel(int mode) {
+  static bool init[3] = {false, false, false};
+  FwdKernel k = mode == 2 ? fwd_step_kernel<kTY, 2> : mode == 1 ? fwd_step_kernel<kTY, 1> : fwd_step_kernel<kTY, 0>;
+  if (!init[mode]) {
+    init[mode] = true;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_step_smem_bytes(mode));
+  }
+  return k;
+}
+
+int resident_ctas(int mode) {
+  static int r[3] = {-1, -1, -1};
+  if (r[mode] < 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fwd_kernel(mode), 32 * kTY,
+                                                      fwd_step_smem_bytes(mode)) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = mode == 2 ? 3 : 4;
+    r[mode] = per_sm * sm_count();
+  }
+  return r[mode];
 }
 
 // TMA staging is the default; RFXB_STAGING=cpasync selects per-thread 16-byte
@@ -244,13 +363,100 @@ int encode_block_map(CUtensorMap* m, const RfxbPlan& p, float* block, int ncomp,
   return 0;
 }
 
+// 4-D map over one CPML psi array: dims (d0, d1, d2, 4 = side*2 + q), rows of
+// d0 floats, box (b0, b1, 1, 2).
+int encode_psi_map(CUtensorMap* m, float* base, long long d0, long long d1, long long d2, unsigned b0, unsigned b1) {
+  auto fn = tensor_map_encoder();
+  if (!fn) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled is not available from the driver");
+  cuuint64_t dims[4] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2, 4};
+  cuuint64_t strides[3] = {(cuuint64_t)(d0 * 4), (cuuint64_t)(d0 * d1 * 4), (cuuint64_t)(d0 * d1 * d2 * 4)};
+  cuuint32_t box[4] = {b0, b1, 1, 2};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled (psi) failed (" + std::to_string((int)r) + ")");
+  return 0;
+}
+
+int encode_psi_maps(RfxbPlan* p);
+
 int encode_forward_maps(RfxbPlan* p) {
   const unsigned ty = kTY;
   for (int s = 0; s < 2; ++s) {
     if (int rc = encode_block_map(&p->tmaps[s], *p, p->inst.F[s][0], 6, 40, ty + 2, 3)) return rc;
     if (int rc = encode_block_map(&p->tmaps[2 + s], *p, p->inst.F[s][0], 6, 36, ty + 1, 3)) return rc;
   }
-  return encode_block_map(&p->tmaps[4], *p, p->ca, 3, 32, ty, 2);
+  if (int rc = encode_block_map(&p->tmaps[4], *p, p->ca, 3, 32, ty, 2)) return rc;
+  if (int rc = encode_block_map(&p->tmaps[10], *p, p->ca, 3, 32, ty, 1)) return rc;
+  const RfxbInst& I = p->inst;
+  p->psi_maps_ok = false;
+  if (I.ncp > 0) {
+    // a psi map the driver refuses only rules out the staged-psi kernel
+    const int rc = encode_psi_maps(p);
+    p->psi_maps_ok = rc == 0;
+  }
+  return 0;
+}
+
+int encode_psi_maps(RfxbPlan* p) {
+  const unsigned ty = kTY;
+  const RfxbInst& I = p->inst;
+  {
+    const long long n = I.ncp, n4 = I.ncp4;
+    for (int s = 0; s < 2; ++s) {
+      if (I.cpml_axes & 1u) {
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + s], I.psH[s][0], I.zs, p->ny, n, 36, ty + 1)) return rc;
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + s], I.psE[s][0], I.zs, p->ny, n, 32, ty)) return rc;
+      }
+      if (I.cpml_axes & 2u) {
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + 2 + s], I.psH[s][1], I.zs, n, p->nx, 36, ty + 1)) return rc;
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + 2 + s], I.psE[s][1], I.zs, n, p->nx, 32, ty)) return rc;
+      }
+      if (I.cpml_axes & 4u) {
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + 4 + s], I.psH[s][2], n4, p->ny, p->nx, (unsigned)n4, ty + 1))
+          return rc;
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + 4 + s], I.psE[s][2], n4, p->ny, p->nx, (unsigned)n4, ty))
+          return rc;
+      }
+    }
+  }
+  return 0;
+}
+
+// Whether mode 2 (TMA-staged psi) can run a plan: the z-psi rows fit the
+// ring, no tile reaches both slabs of an axis (its rows y0-1..y0+TY-1 or
+// columns z0-1..z0+31), and psi offsets fit 32-bit arithmetic.
+bool psi_staging_ok(const RfxbPlan& p) {
+  const RfxbInst& I = p.inst;
+  if (I.ncp == 0) return true;
+  if (!p.psi_maps_ok || I.ncp4 > 16) return false;
+  for (int a = 0; a < 3; ++a)
+    if (p.psi_elems[a] >= (1LL << 31)) return false;
+  const int n = I.ncp;
+  if (I.cpml_axes & 2u)
+    for (int y0 = 0; y0 < p.ny; y0 += kTY)
+      if (y0 - 1 < n && y0 + kTY - 1 >= p.ny - n) return false;
+  if (I.cpml_axes & 4u)
+    for (int z0 = 0; z0 < p.nz; z0 += 32)
+      if (z0 - 1 < n && z0 + 31 >= p.nz - n) return false;
+  return true;
+}
+
+// Forward kernel variant of a group: 0 with RFXB_STAGING=cpasync or when a
+// plan cannot stage its psi, 1 without any CPML, else 2.
+// RFXB_FWD_MODE=2 runs CPML-free groups on the staged-psi variant too (a
+// diagnostic of that variant's own cost).
+int group_fwd_mode(const RfxbBatch* g) {
+  if (!use_tma()) return 0;
+  bool any_cpml = false;
+  for (auto* p : g->plans) {
+    if (p->inst.ncp > 0) any_cpml = true;
+    if (!psi_staging_ok(*p)) return 0;
+  }
+  const char* e = getenv("RFXB_FWD_MODE");
+  if (e && std::string(e) == "2") return 2;
+  return any_cpml ? 2 : 1;
 }
 
 int encode_adjoint_maps(RfxbPlan* p) {
@@ -282,8 +488,13 @@ int build_group(RfxbBatch* g) {
     tiles += (long long)((p->ny + kTY - 1) / kTY) * ((p->nz + 31) / 32);
     min_nx = std::min(min_nx, p->nx);
   }
-  const int chunks = pick_chunks(tiles, min_nx, resident_ctas());
-  for (size_t q = 0; q < g->plans.size(); ++q) make_work(*g->plans[q], (int)q, chunks, work);
+  g->fwd_mode = group_fwd_mode(g);
+  if (balanced_work()) {
+    make_balanced_work(g->plans, resident_ctas(g->fwd_mode), g->fwd_mode == 2 ? 0.4 : 1.0, 3.0, work);
+  } else {
+    const int chunks = pick_chunks(tiles, min_nx, resident_ctas(g->fwd_mode));
+    for (size_t q = 0; q < g->plans.size(); ++q) make_work(*g->plans[q], (int)q, chunks, work);
+  }
   g->n_work = (int)work.size();
   auto galloc = [&](void** ptr, size_t bytes) -> int {
     cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
@@ -373,10 +584,8 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, c
   int par = par0;
   for (int s = 0; s < n_steps; ++s) {
     const int n = step0 + s;
-    if (use_tma())
-      fwd_step_kernel<kTY, true><<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_work, g->d_maps, n, par);
-    else
-      fwd_step_kernel<kTY, false><<<g->n_work, dim3(32, kTY), 0, st>>>(g->d_inst, g->d_work, g->d_maps, n, par);
+    fwd_kernel(g->fwd_mode)<<<g->n_work, dim3(32, kTY), fwd_step_smem_bytes(g->fwd_mode), st>>>(
+        g->d_inst, g->d_work, g->d_maps, n, par);
     if (has_dft)
       dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, par ^ 1);
     par ^= 1;
@@ -663,6 +872,7 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
   I.ncp = ncp;
   I.cpml_axes = ncp > 0 ? (d->cpml_axes & 7u) : 0u;
   if (I.cpml_axes == 0) I.ncp = 0;
+  I.ncp4 = (I.ncp + 3) / 4 * 4;
   if (I.ncp > 0) {
     std::vector<float> tb(6 * 3 * ncp);
     for (int f = 0; f < 6; ++f)
@@ -681,9 +891,20 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
       if (!(d->cpml_cell[f] > 0.0)) return bail(fail(RFXB_E_INVALID, "CPML cell sizes must be positive"));
       I.ib[f] = (float)(1.0 / d->cpml_cell[f]);
     }
+    // (b, c / cell, (1/kappa - 1) / cell) per face and layer for the staged-psi kernel
+    std::vector<float4> t4(6 * ncp);
+    for (int f = 0; f < 6; ++f)
+      for (int s = 0; s < ncp; ++s)
+        t4[f * ncp + s] = make_float4(tb[(f * 3 + 0) * ncp + s], (float)((double)tb[(f * 3 + 1) * ncp + s] * I.ib[f]),
+                                      (float)((double)tb[(f * 3 + 2) * ncp + s] * I.ib[f]), 0.f);
+    float4* dct = nullptr;
+    if (int rc = p->alloc(&dct, t4.size())) return bail(rc);
+    if (cudaMemcpy(dct, t4.data(), t4.size() * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(RFXB_E_LAUNCH, "cudaMemcpy"));
+    I.cpt = dct;
     p->psi_elems[0] = 4LL * ncp * d->ny * I.zs;
     p->psi_elems[1] = 4LL * d->nx * ncp * I.zs;
-    p->psi_elems[2] = 4LL * d->nx * d->ny * ncp;
+    p->psi_elems[2] = 4LL * d->nx * d->ny * I.ncp4;
     for (int a = 0; a < 3; ++a) {
       if (!((I.cpml_axes >> a) & 1u)) { p->psi_elems[a] = 0; }
       for (int s = 0; s < 2; ++s) {
@@ -972,6 +1193,16 @@ int rfxb_batch_device_status(RfxbBatch* g, void* stream) {
   RFXB_CUDA(cudaMemcpy(&v, g->d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (v) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
   return 0;
+}
+
+int rfxb_plan_forward_variant(const RfxbPlan* p) {
+  if (!p || !p->self_group) return -1;
+  return p->self_group->fwd_mode;
+}
+
+int rfxb_batch_forward_variant(const RfxbBatch* g) {
+  if (!g) return -1;
+  return g->fwd_mode;
 }
 
 int64_t rfxb_plan_device_bytes(const RfxbPlan* p) {

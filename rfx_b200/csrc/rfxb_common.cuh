@@ -80,7 +80,7 @@ __device__ __forceinline__ long long psi_index_y(const RfxbInst& P, int side, in
   return ((long long)((side * 2 + q) * P.nx + i) * P.ncp + s) * P.zs + k;
 }
 __device__ __forceinline__ long long psi_index_z(const RfxbInst& P, int side, int q, int s, int i, int j) {
-  return ((long long)((side * 2 + q) * P.nx + i) * P.ny + j) * P.ncp + s;
+  return ((long long)((side * 2 + q) * P.nx + i) * P.ny + j) * P.ncp4 + s;
 }
 
 // Copy a descriptor into shared memory (word-wise, all threads help).

@@ -2,9 +2,10 @@
 //
 // One CTA owns a (TY x 32) tile of the (y, z) plane and marches along x over
 // an x range [xa, xb).  For each x plane i it
-//   1. keeps a 4-stage cp.async pipeline of the input planes i-1 .. i+2 in
-//      shared memory, 16-byte copies of: E with a one-cell halo on every side,
-//      H with the low y/z halo, and the ca/cb coefficients of the tile;
+//   1. keeps a 4-stage pipeline of the input planes i-1 .. i+2 in shared
+//      memory: E with a one-cell halo on every side, H with the low y/z halo,
+//      and the ca/cb coefficients of the tile (TMA boxes, or 16-byte cp.async
+//      copies in the generic mode);
 //   2. computes H^{n+1/2} on the tile plus the low y row / low z column halo
 //      (rfx/core/yee.py:226-291 / :411-453, then rfx/boundaries/cpml.py:804-1065);
 //   3. computes E^{n+1} on the tile from those H values and the H of plane
@@ -15,6 +16,14 @@
 // Fields and psi are ping-ponged between two buffers, so halo cells
 // recomputed by a neighbour CTA always read step-n values.  CPML work is
 // confined to CTAs whose tile touches a y/z slab and to x-slab planes.
+//
+// Modes (template MODE):
+//   0  generic: cp.async staging, psi read and written in global memory;
+//   1  TMA staging, no CPML in the launch;
+//   2  TMA staging, and the psi of every CPML plane/tile (plus ce) arrive by
+//      TMA into a two-slot ring one plane ahead, so the slab cells see no
+//      global-load latency.  The host selects it when no tile touches both
+//      slabs of an axis and the z layers fit the ring.
 #include "rfxb_common.cuh"
 
 namespace rfxb {
@@ -22,10 +31,12 @@ namespace rfxb {
 #define RFXB_NSTAGE 4
 #define RFXB_EW 40   // staged E row: z in [z0 - 4, z0 + 36)
 #define RFXB_HW 36   // staged H row: z in [z0 - 4, z0 + 32)
+#define RFXB_ZPMAX 16  // largest z-psi row (layers rounded up to 4) mode 2 stages
 
 // float counts padded so every array of a stage starts on a 128-byte boundary
 // (the alignment TMA writes into shared memory need)
 __host__ __device__ constexpr int pad128(int nfloats) { return (nfloats % 32) ? 32 - (nfloats % 32) : 0; }
+__host__ __device__ constexpr int up32(int nfloats) { return (nfloats + 31) / 32 * 32; }
 
 template <int TY>
 struct FwdStageDims {
@@ -52,7 +63,34 @@ struct FwdSmem {
   float h[3][TY + 1][RFXB_TZ + 1];   // H^{n+1/2} of plane i: [y - y0 + 1][z - z0 + 1]
   RfxbInst P;
   unsigned long long mbar[RFXB_NSTAGE];
+  unsigned long long pbar[2];        // psi ring (mode 2)
 };
+
+// One slot of the mode-2 psi ring (floats, 128-byte aligned sub-arrays):
+//   HX/HY [q][TY+1][36]  H-side psi of the x / y slab, rows y0-1.., z from z0-4
+//   HZ    [q][TY+1][n4]  H-side psi of the z slab, rows y0-1.., layer s
+//   EX/EY [q][TY][32]    E-side psi of the x / y slab on the tile
+//   EZ    [q][TY][n4]    E-side psi of the z slab
+//   CE    [TY][32]       ce of the tile
+template <int TY>
+struct PsiSlot {
+  static constexpr int HX = 0;
+  static constexpr int HY = HX + up32(2 * (TY + 1) * RFXB_HW);
+  static constexpr int HZ = HY + up32(2 * (TY + 1) * RFXB_HW);
+  static constexpr int EX = HZ + up32(2 * (TY + 1) * RFXB_ZPMAX);
+  static constexpr int EY = EX + up32(2 * TY * RFXB_TZ);
+  static constexpr int EZ = EY + up32(2 * TY * RFXB_TZ);
+  static constexpr int CE = EZ + up32(2 * TY * RFXB_ZPMAX);
+  static constexpr int FLOATS = CE + up32(TY * RFXB_TZ);
+  static constexpr unsigned BH = 4u * 2 * (TY + 1) * RFXB_HW;   // bytes of an HX / HY box
+  static constexpr unsigned BE = 4u * 2 * TY * RFXB_TZ;         // bytes of an EX / EY box
+  static constexpr unsigned BC = 4u * TY * RFXB_TZ;             // bytes of the CE box
+};
+
+template <int TY>
+__host__ __device__ constexpr size_t fwd_smem_bytes(int mode) {
+  return sizeof(FwdSmem<TY>) + (mode == 2 ? 2 * sizeof(float) * PsiSlot<TY>::FLOATS : 0);
+}
 
 __device__ __forceinline__ int stage_of(int p) { return (p + 1) & (RFXB_NSTAGE - 1); }
 
@@ -67,7 +105,8 @@ struct FwdCtx {
   bool cpx, cpy, cpz;      // CPML axis active (y/z: and this tile touches a slab)
 };
 
-// H^{n+1/2} components selected by MASK (1 hx, 2 hy, 4 hz) at (i, jj, kk).
+// H^{n+1/2} components selected by MASK (1 hx, 2 hy, 4 hz) at (i, jj, kk),
+// CPML read from global memory (mode 0).
 // (ly, lz): the cell's row and z index in the staged planes (lz = k - z0 + 4).
 template <int TY, int MASK>
 __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, const FwdCtx& C,
@@ -165,6 +204,89 @@ __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, 
   }
 }
 
+// Mode-2 CPML state of one axis at one cell: whether the cell is in the slab,
+// its profile (b, c/cell, (1/kappa-1)/cell) and the element offset of its
+// psi entry q = 0 (q = 1 is one q-stride further).
+struct CpAx {
+  bool on;
+  float4 c;
+  int off;
+};
+
+// Yee part of H^{n+1/2} at one cell plus its mode-2 CPML corrections.  The
+// staged psi are read at slot row r (0 = row y0-1), z column lz of the H
+// boxes and layer sz of the z box; new psi (WRITE) go to the other parity.
+template <int TY, int MASK, bool WRITE>
+__device__ __forceinline__ void h_cell2(const RfxbInst& P, const FwdSmem<TY>& S, const float* PS, const FwdCtx& C,
+                                        int b0, int b1, int ly, int lz, int r, int sz, float chc,
+                                        float xh, float yh, float zh, const CpAx& X, const CpAx& Y, const CpAx& Z,
+                                        float& hx, float& hy, float& hz) {
+  using L = PsiSlot<TY>;
+  const FwdStage<TY>& A = S.st[b0];
+  const FwdStage<TY>& B = S.st[b1];
+  const float Ex = A.e[0][ly][lz], Ey = A.e[1][ly][lz], Ez = A.e[2][ly][lz];
+  const float dEz_y = A.e[2][ly + 1][lz] - Ez;
+  const float dEy_z = A.e[1][ly][lz + 1] - Ey;
+  const float dEx_z = A.e[0][ly][lz + 1] - Ex;
+  const float dEz_x = B.e[2][ly][lz] - Ez;
+  const float dEy_x = B.e[1][ly][lz] - Ey;
+  const float dEx_y = A.e[0][ly + 1][lz] - Ex;
+  if (MASK & 1) hx = A.h[0][ly][lz] - chc * (dEz_y * yh - dEy_z * zh);
+  if (MASK & 2) hy = A.h[1][ly][lz] - chc * (dEx_z * zh - dEz_x * xh);
+  if (MASK & 4) hz = A.h[2][ly][lz] - chc * (dEy_x * xh - dEx_y * yh);
+  constexpr int RH = (TY + 1) * RFXB_HW;   // q stride of an H box
+  const int par = C.par;
+  if (X.on) {   // Hy += ch psi(dEz/dx) [q0], Hz -= ch psi(dEy/dx) [q1]
+    const int o = r * RFXB_HW + lz;
+    const int qs = P.ncp * P.ny * P.zs;
+    if (MASK & 2) {
+      const float p = X.c.x * PS[L::HX + o] + X.c.y * dEz_x;
+      if (WRITE) P.psH[par ^ 1][0][X.off] = p;
+      hy = hy + chc * p;
+      hy = hy + chc * (X.c.z * dEz_x);
+    }
+    if (MASK & 4) {
+      const float p = X.c.x * PS[L::HX + RH + o] + X.c.y * dEy_x;
+      if (WRITE) P.psH[par ^ 1][0][X.off + qs] = p;
+      hz = hz - chc * p;
+      hz = hz - chc * (X.c.z * dEy_x);
+    }
+  }
+  if (Y.on) {   // Hx -= ch psi(dEz/dy) [q0], Hz += ch psi(dEx/dy) [q1]
+    const int o = r * RFXB_HW + lz;
+    const int qs = P.nx * P.ncp * P.zs;
+    if (MASK & 1) {
+      const float p = Y.c.x * PS[L::HY + o] + Y.c.y * dEz_y;
+      if (WRITE) P.psH[par ^ 1][1][Y.off] = p;
+      hx = hx - chc * p;
+      hx = hx - chc * (Y.c.z * dEz_y);
+    }
+    if (MASK & 4) {
+      const float p = Y.c.x * PS[L::HY + RH + o] + Y.c.y * dEx_y;
+      if (WRITE) P.psH[par ^ 1][1][Y.off + qs] = p;
+      hz = hz + chc * p;
+      hz = hz + chc * (Y.c.z * dEx_y);
+    }
+  }
+  if (Z.on) {   // Hx += ch psi(dEy/dz) [q0], Hy -= ch psi(dEx/dz) [q1]
+    const int n4 = P.ncp4;
+    const int o = r * n4 + sz;
+    const int qs = P.nx * P.ny * n4;
+    if (MASK & 1) {
+      const float p = Z.c.x * PS[L::HZ + o] + Z.c.y * dEy_z;
+      if (WRITE) P.psH[par ^ 1][2][Z.off] = p;
+      hx = hx + chc * p;
+      hx = hx + chc * (Z.c.z * dEy_z);
+    }
+    if (MASK & 2) {
+      const float p = Z.c.x * PS[L::HZ + (TY + 1) * n4 + o] + Z.c.y * dEx_z;
+      if (WRITE) P.psH[par ^ 1][2][Z.off + qs] = p;
+      hy = hy - chc * p;
+      hy = hy - chc * (Z.c.z * dEx_z);
+    }
+  }
+}
+
 // Stage plane ip of the input state with 16-byte copies.  Every copy starts on
 // a 16-byte boundary: off0, ps, zs, cs and z0 are multiples of 32 elements.
 // Rows past the grid read the zero guard row j = ny.
@@ -209,17 +331,67 @@ __device__ __forceinline__ void tma_stage(FwdSmem<TY>& S, const CUtensorMap* tm,
 // k-th fill on mbarrier phase k, so plane p waits on parity ((p-xa+1)/4) & 1.
 __device__ __forceinline__ uint32_t stage_parity(int p, int xa) { return (uint32_t)(((p - xa + 1) >> 2) & 1); }
 
-template <int TY, bool TMA>
-__global__ void __launch_bounds__(32 * TY, 4)
+// Which CPML slab of an axis a CTA's cells (rows y0-1 .. y0+TY-1, or z
+// columns z0-1 .. z0+31) reach: the side, or -1.  The host guarantees at most
+// one side per axis for mode 2.
+__device__ __forceinline__ int tile_side(int lo, int hi, int n, int ncp) {
+  if (lo < ncp) return 0;
+  if (hi >= n - ncp) return 1;
+  return -1;
+}
+
+// Issue the mode-2 psi boxes of plane p into ring slot `slot` (one thread):
+// H and E psi of the x slab when p is in it, of the y / z slab the tile
+// reaches, and the ce tile.  Returns whether anything was issued.
+template <int TY>
+__device__ __forceinline__ void psi_issue(float* slot, uint32_t mb, const CUtensorMap* tm, const RfxbInst& P,
+                                          int par, int y0, int z0, int p, bool cpx, int ysd, int zsd) {
+  using L = PsiSlot<TY>;
+  const int ncp = P.ncp, n4 = P.ncp4;
+  int s = 0;
+  const int xsd = cpx ? cpml_side(p, P.nx, ncp, s) : -1;
+  unsigned bytes = L::BC;
+  if (xsd >= 0) bytes += L::BH + L::BE;
+  if (ysd >= 0) bytes += L::BH + L::BE;
+  if (zsd >= 0) bytes += 4u * 2 * (TY + 1) * n4 + 4u * 2 * TY * n4;
+  mbar_expect_tx(mb, bytes);
+  if (xsd >= 0) {
+    tma_load_4d(smem_u32(slot + L::HX), tm + RFXB_MAP_PSH + 0 + par, z0 - 4, y0 - 1, s, 2 * xsd, mb);
+    tma_load_4d(smem_u32(slot + L::EX), tm + RFXB_MAP_PSE + 0 + par, z0, y0, s, 2 * xsd, mb);
+  }
+  if (ysd >= 0) {
+    const int jb = ysd ? P.ny - ncp : 0;
+    tma_load_4d(smem_u32(slot + L::HY), tm + RFXB_MAP_PSH + 2 + par, z0 - 4, y0 - 1 - jb, p, 2 * ysd, mb);
+    tma_load_4d(smem_u32(slot + L::EY), tm + RFXB_MAP_PSE + 2 + par, z0, y0 - jb, p, 2 * ysd, mb);
+  }
+  if (zsd >= 0) {
+    tma_load_4d(smem_u32(slot + L::HZ), tm + RFXB_MAP_PSH + 4 + par, 0, y0 - 1, p, 2 * zsd, mb);
+    tma_load_4d(smem_u32(slot + L::EZ), tm + RFXB_MAP_PSE + 4 + par, 0, y0, p, 2 * zsd, mb);
+  }
+  tma_load_4d(smem_u32(slot + L::CE), tm + 10, z0, y0 + 1, p + 1, 2, mb);
+}
+
+template <int MODE>
+struct FwdBounds { static constexpr int MIN_CTAS = 4; };
+template <>
+struct FwdBounds<2> { static constexpr int MIN_CTAS = 3; };
+
+template <int TY, int MODE>
+__global__ void __launch_bounds__(32 * TY, FwdBounds<MODE>::MIN_CTAS)
 fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work,
                 const CUtensorMap* __restrict__ maps, int n, int par) {
-  __shared__ FwdSmem<TY> S;
+  constexpr bool TMA = MODE != 0;
+  using L = PsiSlot<TY>;
+  extern __shared__ __align__(128) unsigned char fwd_smem_raw[];
+  FwdSmem<TY>& S = *reinterpret_cast<FwdSmem<TY>*>(fwd_smem_raw);
+  float* ring = reinterpret_cast<float*>(fwd_smem_raw + sizeof(FwdSmem<TY>));   // mode 2: 2 slots
   const int lane = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * 32 + lane;
   const RfxbWork w = work[blockIdx.x];
   load_inst(S.P, insts + w.inst, tid, 32 * TY);
   if (TMA && tid == 0) {
     for (int q = 0; q < RFXB_NSTAGE; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
+    if (MODE == 2) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
     mbar_fence_init();
   }
   __syncthreads();
@@ -233,9 +405,9 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   C.ch = P.ch;
   C.ch0 = P.ch0;
   const int y0 = w.y0, z0 = w.z0;
-  C.cpx = C.ncp > 0 && (P.cpml_axes & 1u);
-  C.cpy = C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY - 1 >= C.ny - C.ncp);
-  C.cpz = C.ncp > 0 && (P.cpml_axes & 4u) && (z0 - 1 < C.ncp || z0 + 31 >= C.nz - C.ncp);
+  C.cpx = MODE != 1 && C.ncp > 0 && (P.cpml_axes & 1u);
+  C.cpy = MODE != 1 && C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY - 1 >= C.ny - C.ncp);
+  C.cpz = MODE != 1 && C.ncp > 0 && (P.cpml_axes & 4u) && (z0 - 1 < C.ncp || z0 + 31 >= C.nz - C.ncp);
   const float* ca = P.ca;
   const float* cb = P.cb;
   const int j = y0 + ty, k = z0 + lane;
@@ -250,6 +422,29 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   const bool col_halo = (ty == hcw) && (lane < TY) && (z0 >= 1) && (y0 + lane < C.ny);
   const float yh_col = col_halo ? __ldg(P.yh + y0 + lane) : 0.f;
   const float zh_col = col_halo ? __ldg(P.zh + z0 - 1) : 0.f;
+
+  // Mode-2 CPML state: the slab side this tile reaches per axis, and this
+  // thread's own-cell profile and psi offsets (y and z are fixed along the
+  // x march; x is per plane).
+  const int ysd = (MODE == 2 && C.cpy) ? tile_side(y0 - 1, y0 + TY - 1, C.ny, C.ncp) : -1;
+  const int zsd = (MODE == 2 && C.cpz) ? tile_side(z0 - 1, z0 + 31, C.nz, C.ncp) : -1;
+  const int jb = ysd == 1 ? C.ny - C.ncp : 0;
+  const int kb = zsd == 1 ? C.nz - C.ncp : 0;
+  CpAx cyo{false, make_float4(0.f, 0.f, 0.f, 0.f), 0}, czo{false, make_float4(0.f, 0.f, 0.f, 0.f), 0};
+  if (MODE == 2) {
+    const int sy = j - jb, sz = k - kb;
+    if (own && ysd >= 0 && sy >= 0 && sy < C.ncp) {
+      cyo.on = true;
+      cyo.c = __ldg(P.cpt + (2 + ysd) * C.ncp + sy);
+      cyo.off = (2 * ysd * C.nx * C.ncp + sy) * C.zs + k;   // + i * ncp * zs per plane
+    }
+    if (own && zsd >= 0 && sz >= 0 && sz < C.ncp) {
+      czo.on = true;
+      czo.c = __ldg(P.cpt + (4 + zsd) * C.ncp + sz);
+      czo.off = (2 * zsd * C.nx * C.ny + j) * P.ncp4 + sz;    // + i * ny * ncp4 per plane
+    }
+  }
+  const bool psi_tile = ysd >= 0 || zsd >= 0;   // every plane needs the psi ring
 
   // Sources and probes whose (j, k) is this thread's column.
   unsigned smask = 0u, pmask = 0u;
@@ -272,20 +467,47 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   const bool pec_kz = ((pec & 4u) != 0) && (k == C.nz - 1);
 
   const int xa = w.xa, xb = w.xb;
+  // psi ring bookkeeping (mode 2; identical in every thread): which planes
+  // need psi, the next phase parity of each slot, and fills in flight
+  auto psi_need = [&](int p) {
+    if (MODE != 2 || p < 0 || p >= C.nx) return false;
+    return psi_tile || (C.cpx && (p < C.ncp || p >= C.nx - C.ncp));
+  };
+  unsigned pph = 0u, pout = 0u;
+  auto psi_fill = [&](int p) {
+    if (!psi_need(p)) return;
+    if (tid == 0)
+      psi_issue<TY>(ring + (p & 1) * L::FLOATS, smem_u32(&S.pbar[p & 1]), tm, P, par, y0, z0, p, C.cpx, ysd, zsd);
+    pout |= 1u << (p & 1);
+  };
+  auto psi_wait = [&](int p) -> bool {
+    if (!psi_need(p)) return true;
+    const int s = p & 1;
+    const bool ok = mbar_wait_bounded(smem_u32(&S.pbar[s]), (pph >> s) & 1u);
+    if (ok) {
+      pph ^= 1u << s;
+      pout &= ~(1u << s);
+    }
+    return ok;
+  };
   // A wait that runs out marks the launch failed and leaves the CTA after
   // draining the boxes it issued (a stalled copy cannot be waited out forever).
   auto bail = [&](int last_issued, int from) {
     if (tid == 0) {
       atomicOr(P.status, 1);
       for (int p = from; p <= last_issued; ++p) mbar_wait_bounded(smem_u32(&S.mbar[stage_of(p)]), stage_parity(p, xa));
+      for (int s = 0; s < 2; ++s)
+        if (pout & (1u << s)) mbar_wait_bounded(smem_u32(&S.pbar[s]), (pph >> s) & 1u);
     }
   };
   if (TMA) {
     if (tid == 0) {
       for (int p = xa - 1; p <= min(xa + 2, C.nx); ++p) tma_stage<TY>(S, tm, par, y0, z0, p);
     }
+    psi_fill(xa - 1);
+    psi_fill(xa);
     const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa - 1)]), stage_parity(xa - 1, xa)) &&
-                    mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa)]), stage_parity(xa, xa));
+                    mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa)]), stage_parity(xa, xa)) && psi_wait(xa - 1);
     if (__syncthreads_or(!ok)) { bail(min(xa + 2, C.nx), xa - 1); return; }
   } else {
     // pipeline: planes xa-1 and xa (group 0), xa+1 (group 1), xa+2 (group 2)
@@ -300,13 +522,33 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     __syncthreads();
   }
 
+  // x-slab profile of plane p (mode 2; uniform over the CTA)
+  auto x_ax = [&](int p) {
+    CpAx a{false, make_float4(0.f, 0.f, 0.f, 0.f), 0};
+    int s = 0;
+    const int sd = C.cpx ? cpml_side(p, C.nx, C.ncp, s) : -1;
+    if (sd >= 0) {
+      a.on = true;
+      a.c = __ldg(P.cpt + sd * C.ncp + s);
+      a.off = (2 * sd * C.ncp + s) * C.ny * C.zs + j * C.zs + k;
+    }
+    return a;
+  };
+
   // H of plane xa-1 at this column (computed, not stored: its owner stores it).
   float hy_prev = 0.f, hz_prev = 0.f;
   if (xa > 0 && own) {
     float hx_, hy_, hz_;
     const float xhp = __ldg(P.xh + xa - 1);
-    h_cell<TY, 6>(P, S, C, stage_of(xa - 1), stage_of(xa), xa - 1, j, k, ly, lz, xhp, yh, zh, false,
-                  hx_, hy_, hz_);
+    if (MODE == 2) {
+      const float chc = C.ch ? C.ch[C.off0 + (long long)(xa - 1) * C.ps + (long long)j * C.zs + k] : C.ch0;
+      const CpAx cx = x_ax(xa - 1);
+      h_cell2<TY, 6, false>(P, S, ring + ((xa - 1) & 1) * L::FLOATS, C, stage_of(xa - 1), stage_of(xa), ly, lz, ly,
+                            k - kb, chc, xhp, yh, zh, cx, cyo, czo, hx_, hy_, hz_);
+    } else {
+      h_cell<TY, 6>(P, S, C, stage_of(xa - 1), stage_of(xa), xa - 1, j, k, ly, lz, xhp, yh, zh, false,
+                    hx_, hy_, hz_);
+    }
     hy_prev = hy_;
     hz_prev = hz_;
   }
@@ -316,11 +558,13 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
 
   for (int i = xa; i < xb; ++i) {
     if (TMA) {
-      // plane i+1 has landed; after the barrier every thread is done with
-      // plane i-1, whose stage takes plane i+3
-      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), stage_parity(i + 1, xa));
+      // plane i+1 has landed (and plane i's psi); after the barrier every
+      // thread is done with plane i-1, whose stage takes plane i+3 and whose
+      // psi slot takes plane i+1
+      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), stage_parity(i + 1, xa)) && psi_wait(i);
       if (__syncthreads_or(!ok)) { bail(min(i + 2, C.nx), i + 1); return; }
       if (tid == 0 && i + 3 <= C.nx) tma_stage<TY>(S, tm, par, y0, z0, i + 3);
+      if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
       __syncthreads();      // ... for every thread; plane i-1's stage is free
@@ -329,12 +573,24 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     }
     const int b0 = stage_of(i), b1 = stage_of(i + 1);
     const float xh = __ldg(P.xh + i), xe = __ldg(P.xe + i);
+    const float* PS = ring + (i & 1) * L::FLOATS;
+    CpAx cx{false, make_float4(0.f, 0.f, 0.f, 0.f), 0}, cy = cyo, cz = czo;
+    if (MODE == 2) {
+      cx = x_ax(i);
+      cy.off += i * C.ncp * C.zs;
+      cz.off += i * C.ny * P.ncp4;
+    }
 
     // ---- H phase ----
     float hx = 0.f, hy = 0.f, hz = 0.f;
     const long long e = C.off0 + (long long)i * C.ps + (long long)j * C.zs + k;
     if (own) {
-      h_cell<TY, 7>(P, S, C, b0, b1, i, j, k, ly, lz, xh, yh, zh, true, hx, hy, hz);
+      if (MODE == 2) {
+        const float chc = C.ch ? C.ch[e] : C.ch0;
+        h_cell2<TY, 7, true>(P, S, PS, C, b0, b1, ly, lz, ly, k - kb, chc, xh, yh, zh, cx, cy, cz, hx, hy, hz);
+      } else {
+        h_cell<TY, 7>(P, S, C, b0, b1, i, j, k, ly, lz, xh, yh, zh, true, hx, hy, hz);
+      }
       C.Fo[3 * C.cs + e] = hx;
       C.Fo[4 * C.cs + e] = hy;
       C.Fo[5 * C.cs + e] = hz;
@@ -344,14 +600,42 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     S.h[2][ly][lh] = hz;
     if (ty == 0) {  // halo row j = y0 - 1: hx, hz
       float a = 0.f, bq = 0.f, cq = 0.f;
-      if (row_halo) h_cell<TY, 5>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
+      if (row_halo) {
+        if (MODE == 2) {
+          const int jr = y0 - 1;
+          const float chc = C.ch ? C.ch[C.off0 + (long long)i * C.ps + (long long)jr * C.zs + k] : C.ch0;
+          CpAx ry{false, make_float4(0.f, 0.f, 0.f, 0.f), 0};
+          const int sy = jr - jb;
+          if (ysd >= 0 && sy >= 0 && sy < C.ncp) { ry.on = true; ry.c = __ldg(P.cpt + (2 + ysd) * C.ncp + sy); }
+          CpAx rz = czo;
+          if (zsd >= 0 && !rz.on && k - kb >= 0 && k - kb < C.ncp) {   // own lane past the grid edge only
+            rz.on = true;
+            rz.c = __ldg(P.cpt + (4 + zsd) * C.ncp + (k - kb));
+          }
+          h_cell2<TY, 5, false>(P, S, PS, C, b0, b1, 0, lz, 0, k - kb, chc, xh, yh_row, zh, cx, ry, rz, a, bq, cq);
+        } else {
+          h_cell<TY, 5>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
+        }
+      }
       S.h[0][0][lh] = a;
       S.h[2][0][lh] = cq;
     }
     if (ty == hcw && lane < TY) {  // halo column k = z0 - 1: hx, hy
       float a = 0.f, bq = 0.f, cq = 0.f;
-      if (col_halo) h_cell<TY, 3>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false,
-                                  a, bq, cq);
+      if (col_halo) {
+        if (MODE == 2) {
+          const int jc = y0 + lane, kc = z0 - 1;
+          const float chc = C.ch ? C.ch[C.off0 + (long long)i * C.ps + (long long)jc * C.zs + kc] : C.ch0;
+          CpAx ry{false, make_float4(0.f, 0.f, 0.f, 0.f), 0}, rz{false, make_float4(0.f, 0.f, 0.f, 0.f), 0};
+          const int sy = jc - jb, sz = kc - kb;
+          if (ysd >= 0 && sy >= 0 && sy < C.ncp) { ry.on = true; ry.c = __ldg(P.cpt + (2 + ysd) * C.ncp + sy); }
+          if (zsd >= 0 && sz >= 0 && sz < C.ncp) { rz.on = true; rz.c = __ldg(P.cpt + (4 + zsd) * C.ncp + sz); }
+          h_cell2<TY, 3, false>(P, S, PS, C, b0, b1, lane + 1, 3, lane + 1, sz, chc, xh, yh_col, zh_col, cx, ry, rz,
+                                a, bq, cq);
+        } else {
+          h_cell<TY, 3>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false, a, bq, cq);
+        }
+      }
       S.h[0][lane + 1][0] = a;
       S.h[1][lane + 1][0] = bq;
     }
@@ -367,15 +651,56 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
       const float dHz_x = hz - hz_prev;
       const float dHy_x = hy - hy_prev;
       const float dHx_y = hx - S.h[0][ly - 1][lh];
-      const float cx = dHz_y * ye - dHy_z * ze;
-      const float cy = dHx_z * ze - dHz_x * xe;
-      const float cz = dHy_x * xe - dHx_y * ye;
+      const float cx_ = dHz_y * ye - dHy_z * ze;
+      const float cy_ = dHx_z * ze - dHz_x * xe;
+      const float cz_ = dHy_x * xe - dHx_y * ye;
       const float cav = A.cab[0][ty][lane], cbv = A.cab[1][ty][lane];
-      float ex = cav * Ex + cbv * cx;
-      float ey = cav * Ey + cbv * cy;
-      float ez = cav * Ez + cbv * cz;
+      float ex = cav * Ex + cbv * cx_;
+      float ey = cav * Ey + cbv * cy_;
+      float ez = cav * Ez + cbv * cz_;
       const int ncp = C.ncp;
-      if (C.cpx || C.cpy || C.cpz) {
+      if (MODE == 2) {
+        if (cx.on || cy.on || cz.on) {
+          const float ce = PS[L::CE + ty * RFXB_TZ + lane];
+          constexpr int RE = TY * RFXB_TZ;   // q stride of an E box
+          const int o = ty * RFXB_TZ + lane;
+          if (cx.on) {   // Ey -= ce psi(dHz/dx) [q0], Ez += ce psi(dHy/dx) [q1]
+            const int qs = ncp * C.ny * C.zs;
+            const float p0 = cx.c.x * PS[L::EX + o] + cx.c.y * dHz_x;
+            const float p1 = cx.c.x * PS[L::EX + RE + o] + cx.c.y * dHy_x;
+            P.psE[par ^ 1][0][cx.off] = p0;
+            P.psE[par ^ 1][0][cx.off + qs] = p1;
+            ey = ey - ce * p0;
+            ey = ey - ce * (cx.c.z * dHz_x);
+            ez = ez + ce * p1;
+            ez = ez + ce * (cx.c.z * dHy_x);
+          }
+          if (cy.on) {   // Ex += ce psi(dHz/dy) [q0], Ez -= ce psi(dHx/dy) [q1]
+            const int qs = C.nx * ncp * C.zs;
+            const float p0 = cy.c.x * PS[L::EY + o] + cy.c.y * dHz_y;
+            const float p1 = cy.c.x * PS[L::EY + RE + o] + cy.c.y * dHx_y;
+            P.psE[par ^ 1][1][cy.off] = p0;
+            P.psE[par ^ 1][1][cy.off + qs] = p1;
+            ex = ex + ce * p0;
+            ex = ex + ce * (cy.c.z * dHz_y);
+            ez = ez - ce * p1;
+            ez = ez - ce * (cy.c.z * dHx_y);
+          }
+          if (cz.on) {   // Ex -= ce psi(dHy/dz) [q0], Ey += ce psi(dHx/dz) [q1]
+            const int n4 = P.ncp4;
+            const int qs = C.nx * C.ny * n4;
+            const int oz = ty * n4 + (k - kb);
+            const float p0 = cz.c.x * PS[L::EZ + oz] + cz.c.y * dHy_z;
+            const float p1 = cz.c.x * PS[L::EZ + TY * n4 + oz] + cz.c.y * dHx_z;
+            P.psE[par ^ 1][2][cz.off] = p0;
+            P.psE[par ^ 1][2][cz.off + qs] = p1;
+            ex = ex - ce * p0;
+            ex = ex - ce * (cz.c.z * dHy_z);
+            ey = ey + ce * p1;
+            ey = ey + ce * (cz.c.z * dHx_z);
+          }
+        }
+      } else if (C.cpx || C.cpy || C.cpz) {
         int s, sd;
         float ce = 0.f;
         bool ce_loaded = false;
@@ -476,7 +801,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
           const int ci = ((i - P.hb[0]) * sy + (j - P.hb[2])) * sz + (k - P.hb[4]);
           float* hp = P.hist + (long long)(n - P.hist_step0) * P.hist_ld + ci;
           hp[0] = Ex; hp[hc] = Ey; hp[2 * hc] = Ez;
-          hp[3 * hc] = cx; hp[4 * hc] = cy; hp[5 * hc] = cz;
+          hp[3 * hc] = cx_; hp[4 * hc] = cy_; hp[5 * hc] = cz_;
         }
       }
       if (pmask | smask | (unsigned)src_tail | (unsigned)prb_tail) {
@@ -604,7 +929,10 @@ __global__ void coef_kernel(RfxbInst P, float* ca, float* cb, float* ce, float* 
 }
 
 // Explicit template instantiations used by the host side.
-template __global__ void fwd_step_kernel<8, true>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
-template __global__ void fwd_step_kernel<8, false>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+template __global__ void fwd_step_kernel<8, 0>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+template __global__ void fwd_step_kernel<8, 1>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+template __global__ void fwd_step_kernel<8, 2>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+
+size_t fwd_step_smem_bytes(int mode) { return fwd_smem_bytes<8>(mode); }
 
 }  // namespace rfxb

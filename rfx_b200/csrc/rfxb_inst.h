@@ -22,13 +22,20 @@
 // TMA descriptors per instance: [0|1] fields parity 0|1 with the E box,
 // [2|3] with the H box, [4] coefficients with the ca/cb box, [5|6] adjoint
 // fields with the E box, [7|8] with the H box, [9] cb with the E box,
-// [10] ca with the tile box.
-#define RFXB_NMAPS 16
+// [10] one coefficient with the tile box, then the CPML psi of parity 0|1:
+// [11|12] H-side x, [13|14] H-side y, [15|16] H-side z (H boxes), [17|18]
+// E-side x, [19|20] E-side y, [21|22] E-side z (tile boxes).
+#define RFXB_NMAPS 24
+#define RFXB_MAP_PSH 11
+#define RFXB_MAP_PSE 17
 
-// CPML psi layout per axis (q = which of the two corrected components):
+// CPML psi layout per axis (q = which of the two corrected components,
+// n = layers, n4 = n rounded up to a multiple of 4):
 //   x: ((side*2 + q)*n + s)*ny*zs + j*zs + k
 //   y: ((side*2 + q)*nx + i)*n*zs + s*zs + k
-//   z: ((side*2 + q)*nx + i)*ny*n + j*n + s
+//   z: ((side*2 + q)*nx + i)*ny*n4 + j*n4 + s
+// Every row is a multiple of 16 bytes, so each axis is a TMA-tileable 4-D
+// array (rows along k for x and y, along s for z).
 struct RfxbInst {
   int nx, ny, nz, zs;
   long long ps;            // plane stride (elements)
@@ -46,8 +53,10 @@ struct RfxbInst {
   const float* ze; const float* zh;
   // CPML
   int ncp;                 // layers per face (0 = none)
+  int ncp4;                // ncp rounded up to a multiple of 4 (z psi row length)
   unsigned cpml_axes;      // bit a set -> axis a absorbs
   const float* cpb;        // [face][3][ncp]: b, c, (1/kappa - 1); face = 2*axis + side
+  const float4* cpt;       // [face][ncp]: (b, c / cell, (1/kappa - 1) / cell, 0)
   float ib[6];             // 1 / boundary cell size per face
   float* psH[2][3];        // H-side psi per axis, ping-pong
   float* psE[2][3];        // E-side psi per axis, ping-pong

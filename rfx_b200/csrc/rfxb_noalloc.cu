@@ -34,8 +34,9 @@
 #include "rfxb_common.cuh"
 
 namespace rfxb {
-template <int TY, bool TMA>
+template <int TY, int MODE>
 __global__ void fwd_step_kernel(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+size_t fwd_step_smem_bytes(int mode);
 __global__ void pack_kernel(float*, const float*, RfxbInst);
 __global__ void unpack_kernel(float*, const float*, RfxbInst);
 __global__ void coef_kernel(RfxbInst, float*, float*, float*, float*, const float*, const float*, const float*,
@@ -101,6 +102,7 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
       !d->inv_zh_host)
     return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: inverse spacing tables are required");
   const int ncp = d->cpml_axes ? d->cpml_layers : 0;
+  const int ncp4 = (ncp + 3) / 4 * 4;
   if (ncp < 0 || ncp > 64) return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: cpml_layers must be 0..64");
   if (ncp > 0 && (!d->cpml_b_host || !d->cpml_c_host || !d->cpml_kappa_host))
     return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: CPML profiles are required");
@@ -135,7 +137,7 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   if (ncp > 0) {
     if (d->cpml_axes & 1u) psi_elems[0] = 4LL * ncp * d->ny * I.zs;
     if (d->cpml_axes & 2u) psi_elems[1] = 4LL * d->nx * ncp * I.zs;
-    if (d->cpml_axes & 4u) psi_elems[2] = 4LL * d->nx * d->ny * ncp;
+    if (d->cpml_axes & 4u) psi_elems[2] = 4LL * d->nx * d->ny * ncp4;
   }
   const int ty_tiles = (d->ny + TY - 1) / TY, tz_tiles = (d->nz + 31) / 32;
   const long long tiles = (long long)ty_tiles * tz_tiles;
@@ -186,6 +188,7 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   const float* htabs[6] = {d->inv_xe_host, d->inv_xh_host, d->inv_ye_host, d->inv_yh_host, d->inv_ze_host,
                            d->inv_zh_host};
   I.ncp = ncp;
+  I.ncp4 = ncp4;
   I.cpml_axes = ncp > 0 ? (d->cpml_axes & 7u) : 0u;
   I.cpb = reinterpret_cast<const float*>(base + o_cpb);
   for (int s = 0; s < 2; ++s)
@@ -275,7 +278,8 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   const RfxbWork* dW = reinterpret_cast<const RfxbWork*>(base + o_work);
   int par = 0;
   for (int s = 0; s < n_steps; ++s) {
-    fwd_step_kernel<TY, false><<<(unsigned)n_work, dim3(32, TY), 0, st>>>(dI, dW, nullptr, step0 + s, par);
+    fwd_step_kernel<TY, 0><<<(unsigned)n_work, dim3(32, TY), fwd_step_smem_bytes(0), st>>>(dI, dW, nullptr, step0 + s,
+                                                                                           par);
     par ^= 1;
   }
   for (int c = 0; c < 6; ++c) unpack_kernel<<<blocks, 256, 0, st>>>(fields_dev[c], I.F[par][c], I);

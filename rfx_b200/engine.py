@@ -176,8 +176,25 @@ class Plan:
         nx, ny, nz = self.shape
         return 56 * nx * ny * nz + 8 * self.psi_entries()
 
+    def adjoint_algorithmic_bytes_per_step(self) -> int:
+        """Bytes one reverse step must move at minimum: the forward's (six
+        adjoint fields read and written, ca/cb, adjoint psi read and written)
+        plus, over the gradient region, the recorded history (6 floats) read
+        and the float64 gradient read and written."""
+        gb = self.spec.grad_box
+        box = 0
+        if gb:
+            i0, i1, j0, j1, k0, k1 = gb
+            box = max(0, i1 - i0) * max(0, j1 - j0) * max(0, k1 - k0)
+        return self.algorithmic_bytes_per_step() + (24 + 16) * box
+
     def device_bytes(self) -> int:
         return int(self._lib.rfxb_plan_device_bytes(self._h))
+
+    def forward_variant(self) -> int:
+        """0 generic step kernel, 1 TMA staging without CPML, 2 TMA staging
+        with TMA-staged CPML psi."""
+        return int(self._lib.rfxb_plan_forward_variant(self._h))
 
     # -- state ---------------------------------------------------------------
     def _dev(self, a, dtype=torch.float32):

@@ -26,8 +26,8 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 def main(ref_root):
     src = os.path.join(ref_root, "tests", "fixtures", "golden_forward_no_rlc_s11.npy")
     shutil.copyfile(src, os.path.join(HERE, "forward_no_rlc_s11.npy"))
-    from tests.scenarios import c1_readme, small_nonuniform, small_uniform
-    for build in (small_uniform, small_nonuniform, c1_readme):
+    from tests.scenarios import c1_readme, medium_uniform, small_nonuniform, small_uniform
+    for build in (small_uniform, small_nonuniform, c1_readme, medium_uniform):
         sc = build()
         out = {}
         for tag, dt in (("f32", np.float32), ("f64", np.float64)):

@@ -134,6 +134,31 @@ def small_uniform(n_steps=240, seed=1):
                     dft, pec_mask=pec, domain=domain, dx=dx)
 
 
+def medium_uniform(n_steps=200, seed=3):
+    """small_uniform's feature set on a grid long enough in y and z (44 x 76
+    cells across, CPML 6) that no 8 x 32 tile reaches both slabs of an axis,
+    so the forward step stages its CPML psi by TMA."""
+    rng = np.random.default_rng(seed)
+    dx = 1e-3
+    domain = (0.028, 0.032, 0.064)
+    g = oracle.make_uniform_grid(domain, dx, cpml_layers=6)
+    shape = g.shape
+    eps, sig = _boxes(rng, shape, 4, 6.0, 0.05, 6, 3, 10)
+    mu = np.ones(shape, np.float32)
+    pec = np.zeros(shape, bool)
+    pec[18:24, 14:22, 40] = True
+    mats = (eps, sig, mu)
+    s1 = (12, 13, 30)
+    s2 = (24, 30, 50)
+    w1 = oracle.j_source_waveform(g, s1, mats, n_steps, f0=12e9, bandwidth=0.8)
+    w2 = oracle.j_source_waveform(g, s2, mats, n_steps, f0=20e9, bandwidth=0.5, amplitude=0.5)
+    probes = [(30, 16, 60, "ez"), (22, 41, 48, "hy"), (25, 10, 70, "ex"), (18, 40, 33, "hz")]
+    freqs = np.linspace(8e9, 20e9, 3).astype(np.float32)
+    dft = [(2, 66, "ez", freqs), (1, 5, "hx", freqs[:2])]
+    return Scenario("medium_uniform", "uniform", g, mats, n_steps, [(*s1, "ez", w1), (*s2, "ey", w2)], probes,
+                    dft, pec_mask=pec, domain=domain, dx=dx)
+
+
 def graded_dz(rng, n, lo=1e-4, hi=5e-4, max_ratio=1.2):
     """Seeded smooth grading within [lo, hi] with adjacent ratio <= max_ratio."""
     d = [float(rng.uniform(lo, hi))]
