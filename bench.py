@@ -155,10 +155,10 @@ def cpu_baseline_port(args, n_workers=1, n_time=60):
 # our arm
 # ---------------------------------------------------------------------------
 
-def _traffic_per_cell():
-    """DRAM bytes per cell and launch of fwd_step_kernel from the committed
-    ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "fwd_step_kernel.md")
+def _traffic_per_cell(kernel):
+    """DRAM bytes per cell and launch of a step kernel from its committed ncu
+    summary (profiles/<kernel>.md), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"dram_bytes_per_cell_per_launch:\s*([0-9.eE+-]+)", open(path).read())
@@ -195,13 +195,15 @@ def run_ours(args, rank, world, local_rank):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         sw.forward()
         e1.record(stream)
         _, gs = sw.objectives()
-        sw.backward(gs)
         e2.record(stream)
-        return e0, e1, e2
+        sw.backward(gs)
+        e3.record(stream)
+        return e0, e1, e2, e3
 
     for _ in range(args.warmup):
         one_step()
@@ -219,26 +221,33 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    total_ms = sum(a.elapsed_time(c) for a, b, c in events)
-    fwd_ms = sum(a.elapsed_time(b) for a, b, c in events)
-    t = torch.tensor([total_ms, fwd_ms], device=dev, dtype=torch.float64)
+    total_ms = sum(a.elapsed_time(d) for a, b, c, d in events)
+    fwd_ms = sum(a.elapsed_time(b) for a, b, c, d in events)
+    adj_ms = sum(c.elapsed_time(d) for a, b, c, d in events)
+    t = torch.tensor([total_ms, fwd_ms, adj_ms], device=dev, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, fwd_ms = float(t[0]), float(t[1])
+    total_ms, fwd_ms, adj_ms = float(t[0]), float(t[1]), float(t[2])
     value = cells * N * args.steps * world / (total_ms / 1e3) / 1e6
 
-    # roofline of the forward step kernel: algorithmic bytes per launch over
-    # its average launch time (forward phase = one launch per time step)
-    alg_bytes = sum(p.algorithmic_bytes_per_step() for p in sw.plans)
-    fwd_launch_s = fwd_ms / 1e3 / (N * args.steps)
-    achieved = alg_bytes / fwd_launch_s / 1e9
-    tpc = _traffic_per_cell()
-    roofline = {"kernel": "fwd_step_kernel<8>", "bound": "hbm", "achieved": round(achieved, 1),
-                "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+    # rooflines of the two step kernels: algorithmic bytes per launch over the
+    # average launch time (one launch per time step in each phase; the
+    # backward phase also holds one adjoint-init launch per bench step)
+    def roof(kernel, alg, ms, what):
+        launch_s = ms / 1e3 / (N * args.steps)
+        achieved = alg / launch_s / 1e9
+        tpc = _traffic_per_cell(kernel)
+        return {"kernel": kernel, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4),
                 "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
-                "traffic": (round(tpc * cells) if tpc else None),
-                "algorithmic_bytes_per_launch": int(alg_bytes),
-                "fwd_share_of_step": round(fwd_ms / total_ms, 3)}
+                "traffic": (round(tpc * cells) if tpc else None), "algorithmic_bytes_per_launch": int(alg),
+                "share_of_step": round(ms / total_ms, 3), "what": what}
+
+    roof_adj = roof("adj_step_kernel", sum(p.adjoint_algorithmic_bytes_per_step() for p in sw.plans), adj_ms,
+                    "fused reverse step, batched over all instances")
+    roof_fwd = roof("fwd_step_kernel", sum(p.algorithmic_bytes_per_step() for p in sw.plans), fwd_ms,
+                    "fused forward step, batched over all instances")
+    roofline, roofline_other = (roof_adj, roof_fwd) if adj_ms >= fwd_ms else (roof_fwd, roof_adj)
 
     # single-instance comparison (each simulation launched on its own)
     single = None
@@ -296,12 +305,14 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_port(args, n_workers=1, n_time=args.cpu_time_steps)
 
-    launches = args.steps * (N + 2 * N + 1)
+    # our kernels per bench step: N forward steps, one adjoint init, N fused reverse steps
+    launches = args.steps * (2 * N + 1)
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 2), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-                "config": _workload_config(args, cells, world), "roofline": roofline, "cpu_baseline": cpu,
+                "config": _workload_config(args, cells, world), "roofline": roofline,
+                "roofline_other_kernel": roofline_other, "cpu_baseline": cpu,
                 "e2e": e2e, "single": single, "gpu_launches": launches,
                 "clocks": clk.summary(), "host_wall_s_timed": round(t_host, 3)}
         print(json.dumps(line), flush=True)

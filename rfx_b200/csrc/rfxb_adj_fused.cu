@@ -51,6 +51,10 @@ template <int TY>
 struct AdjSmem {
   AdjStage<TY> st[RFXB_ANSTAGE];
   float p[3][TY + 1][RFXB_TZ + 1];   // ch * aH1 of plane i, [y - y0 + 1][z - z0 + 1]
+  // CPML terms of the y / z relations exchanged between neighbouring cells:
+  // phase A r_E of (y q0, y q1, z q0, z q1) at rows y0-1 .. y0+TY, columns
+  // z0-1 .. z0+32; then phase B r_H at rows y0-1 .. y0+TY-1, columns z0-1 .. z0+31
+  float rx[4][TY + 2][RFXB_TZ + 2];
   RfxbInst P;
   AdjInst A;
   unsigned long long mbar[RFXB_ANSTAGE];
@@ -86,14 +90,12 @@ __device__ __forceinline__ float r_e(const RfxbInst& P, const AdjInst& A, const 
   int s;
   const int sd = cpml_side(coord, nax, C.ncp, s);
   if (sd < 0) return 0.f;
-  const int face = 2 * axis + sd;
-  const float* tb = P.cpb + (size_t)face * 3 * C.ncp;
-  const float b = __ldg(tb + s), c = __ldg(tb + C.ncp + s), km = __ldg(tb + 2 * C.ncp + s);
+  const float4 cf = __ldg(P.cpt + (2 * axis + sd) * C.ncp + s);
   const float ce = P.ce[cell_index(C, i, j, k)];
   const long long qi = psi_q(P, axis, sd, q, s, i, j, k);
   const float nu = A.aPsiE[C.par][axis][qi] + sgn * ce * at;
-  if (write) A.aPsiE[C.par ^ 1][axis][qi] = b * nu;
-  return P.ib[face] * (c * nu + sgn * ce * km * at);
+  if (write) A.aPsiE[C.par ^ 1][axis][qi] = cf.x * nu;
+  return cf.y * nu + sgn * ce * (cf.z * at);
 }
 
 // r_H of one CPML-H relation at cell (i, j, k) with p_t = ch aH1_t there.
@@ -105,17 +107,55 @@ __device__ __forceinline__ float r_h(const RfxbInst& P, const AdjInst& A, const 
   int s;
   const int sd = cpml_side(coord, nax, C.ncp, s);
   if (sd < 0) return 0.f;
-  const int face = 2 * axis + sd;
-  const float* tb = P.cpb + (size_t)face * 3 * C.ncp;
-  const float b = __ldg(tb + s), c = __ldg(tb + C.ncp + s), km = __ldg(tb + 2 * C.ncp + s);
+  const float4 cf = __ldg(P.cpt + (2 * axis + sd) * C.ncp + s);
   const long long qi = psi_q(P, axis, sd, q, s, i, j, k);
   const float nu = A.aPsiH[C.par][axis][qi] + sgn * pt;
-  if (write) A.aPsiH[C.par ^ 1][axis][qi] = b * nu;
-  return P.ib[face] * (c * nu + sgn * km * pt);
+  if (write) A.aPsiH[C.par ^ 1][axis][qi] = cf.x * nu;
+  return cf.y * nu + sgn * (cf.z * pt);
+}
+
+// r_E / r_H with the folded profile (b, c/cell, (1/kappa-1)/cell) of the
+// staged-psi forward: c' nu + s ce k' a_t and c' nu + s k' p_t.  Zero outside
+// the grid and outside the slab.
+__device__ __forceinline__ float re_eval(const RfxbInst& P, const AdjInst& A, const AdjCtx& C, int axis, int q,
+                                         float sgn, int i, int j, int k, float at, float ce, bool write) {
+  const int coord = axis == 0 ? i : axis == 1 ? j : k;
+  const int nax = axis == 0 ? C.nx : axis == 1 ? C.ny : C.nz;
+  if (coord < 0 || coord >= nax) return 0.f;
+  int s;
+  const int sd = cpml_side(coord, nax, C.ncp, s);
+  if (sd < 0) return 0.f;
+  const float4 cf = __ldg(P.cpt + (2 * axis + sd) * C.ncp + s);
+  const long long qi = psi_q(P, axis, sd, q, s, i, j, k);
+  const float nu = __ldg(A.aPsiE[C.par][axis] + qi) + sgn * ce * at;
+  if (write) A.aPsiE[C.par ^ 1][axis][qi] = cf.x * nu;
+  return cf.y * nu + sgn * ce * (cf.z * at);
+}
+
+__device__ __forceinline__ float rh_eval(const RfxbInst& P, const AdjInst& A, const AdjCtx& C, int axis, int q,
+                                         float sgn, int i, int j, int k, float pt, bool write) {
+  const int coord = axis == 0 ? i : axis == 1 ? j : k;
+  const int nax = axis == 0 ? C.nx : axis == 1 ? C.ny : C.nz;
+  if (coord < 0 || coord >= nax) return 0.f;
+  int s;
+  const int sd = cpml_side(coord, nax, C.ncp, s);
+  if (sd < 0) return 0.f;
+  const float4 cf = __ldg(P.cpt + (2 * axis + sd) * C.ncp + s);
+  const long long qi = psi_q(P, axis, sd, q, s, i, j, k);
+  const float nu = __ldg(A.aPsiH[C.par][axis] + qi) + sgn * pt;
+  if (write) A.aPsiH[C.par ^ 1][axis][qi] = cf.x * nu;
+  return cf.y * nu + sgn * (cf.z * pt);
+}
+
+// Whether a cell lies in a CPML slab of an active axis other than x.
+__device__ __forceinline__ bool in_yz_slab(const AdjCtx& C, int j, int k) {
+  return (C.cpy && (j < C.ncp || j >= C.ny - C.ncp)) || (C.cpz && (k < C.ncp || k >= C.nz - C.ncp));
 }
 
 // Phase A at (i, jj, kk): aH1 components selected by MASK (1 hx, 2 hy, 4 hz).
-template <int TY, int MASK>
+// With CP, the CPML-E^T terms are evaluated here at the cell and its +1
+// neighbours (the prologue plane); without, the caller adds them.
+template <int TY, int MASK, bool CP = true>
 __device__ __forceinline__ void adj_a_cell(const RfxbInst& P, const AdjInst& A, const AdjSmem<TY>& S,
                                            const AdjCtx& C, int b0, int b1, int i, int jj, int kk, int ly, int lz,
                                            float xe0, float xe1, float ye0, float ye1, float ze0, float ze1,
@@ -135,6 +175,7 @@ __device__ __forceinline__ void adj_a_cell(const RfxbInst& P, const AdjInst& A, 
   if (MASK & 2) ahy = X.ah[1][ly][lz] + ((xe0 * qz - xe1 * (cbx * az_x1)) - (ze0 * qx - ze1 * (cbz * ax_z1)));
   if (MASK & 4) ahz = X.ah[2][ly][lz] + ((ye0 * qx - ye1 * (cby * ax_y1)) - (xe0 * qy - xe1 * (cbx * ay_x1)));
   // CPML-E^T: aH_h(x) += r_E(x) - r_E(x + 1 along the axis); own cells write aPsiE'
+  if (!CP) return;
   if (C.cpx) {
     if (own || (MASK & 4)) ahz += r_e(P, A, C, 0, 0, -1.f, i, jj, kk, ay0, own) -
                                   r_e(P, A, C, 0, 0, -1.f, i + 1, jj, kk, ay_x1, false);   // (ey <- hz)
@@ -326,6 +367,26 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     }
   }
 
+  // The x relations of CPML-E^T are carried along the march: r_E of plane i
+  // at this column (q0: ey <- hz, q1: ez <- hy) and at this thread's halo
+  // cell (row y0-1: q0; column z0-1: q1) is evaluated one plane ahead; the
+  // CTA owning a plane writes its psi when it evaluates it.
+  float rx0 = 0.f, rx1 = 0.f, rxh = 0.f;
+  if (C.cpx) {
+    const AdjStage<TY>& X0 = S.st[astage_of(xa)];
+    if (own) {
+      const float ce = P.ce[cell_index(C, xa, j, k)];
+      rx0 = re_eval(P, A, C, 0, 0, -1.f, xa, j, k, X0.ae[1][ly][lz], ce, true);
+      rx1 = re_eval(P, A, C, 0, 1, +1.f, xa, j, k, X0.ae[2][ly][lz], ce, true);
+    }
+    if (row_halo)
+      rxh = re_eval(P, A, C, 0, 0, -1.f, xa, y0 - 1, k, X0.ae[1][0][lz], P.ce[cell_index(C, xa, y0 - 1, k)], false);
+    if (col_halo)
+      rxh = re_eval(P, A, C, 0, 1, +1.f, xa, y0 + lane, z0 - 1, X0.ae[2][lane + 1][3],
+                    P.ce[cell_index(C, xa, y0 + lane, z0 - 1)], false);
+  }
+  const bool yz_tile = C.cpy || C.cpz;
+
   for (int i = xa; i < xb; ++i) {
     if (TMA) {
       const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of(i + 1)]), astage_parity(i + 1, xa));
@@ -342,10 +403,73 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     const float xh0 = __ldg(P.xh + i), xhm = __ldg(P.xh + i - 1);
     const long long e = cell_index(C, i, j, k);
 
+    // x relations of plane i+1 (written by this CTA when it owns that plane)
+    float nx0 = 0.f, nx1 = 0.f, nxh = 0.f;
+    if (C.cpx && i + 1 < C.nx) {
+      const AdjStage<TY>& Y1 = S.st[b1];
+      const bool wr = i + 1 < xb;
+      if (own) {
+        const float ce = P.ce[e + C.ps];
+        nx0 = re_eval(P, A, C, 0, 0, -1.f, i + 1, j, k, Y1.ae[1][ly][lz], ce, wr);
+        nx1 = re_eval(P, A, C, 0, 1, +1.f, i + 1, j, k, Y1.ae[2][ly][lz], ce, wr);
+      }
+      if (row_halo)
+        nxh = re_eval(P, A, C, 0, 0, -1.f, i + 1, y0 - 1, k, Y1.ae[1][0][lz],
+                      P.ce[cell_index(C, i + 1, y0 - 1, k)], false);
+      if (col_halo)
+        nxh = re_eval(P, A, C, 0, 1, +1.f, i + 1, y0 + lane, z0 - 1, Y1.ae[2][lane + 1][3],
+                      P.ce[cell_index(C, i + 1, y0 + lane, z0 - 1)], false);
+    }
+
+    // r_E of the y / z relations at the tile, its +1 row / column and the
+    // halo cells, once per cell (own cells write their psi)
+    if (yz_tile) {
+      const AdjStage<TY>& X = S.st[b0];
+      auto re_fill = [&](int r, int c, bool write) {
+        const int jj = y0 - 1 + r, kk = z0 - 1 + c;
+        float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+        if (jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+          const float ce = P.ce[cell_index(C, i, jj, kk)];
+          const float ax = X.ae[0][r][c + 3], ay = X.ae[1][r][c + 3], az = X.ae[2][r][c + 3];
+          if (C.cpy) {
+            v0 = re_eval(P, A, C, 1, 0, +1.f, i, jj, kk, ax, ce, write);   // ex <- hz
+            v1 = re_eval(P, A, C, 1, 1, -1.f, i, jj, kk, az, ce, write);   // ez <- hx
+          }
+          if (C.cpz) {
+            v2 = re_eval(P, A, C, 2, 0, -1.f, i, jj, kk, ax, ce, write);   // ex <- hy
+            v3 = re_eval(P, A, C, 2, 1, +1.f, i, jj, kk, ay, ce, write);   // ey <- hx
+          }
+        }
+        S.rx[0][r][c] = v0;
+        S.rx[1][r][c] = v1;
+        S.rx[2][r][c] = v2;
+        S.rx[3][r][c] = v3;
+      };
+      re_fill(ly, lh, own);
+      constexpr int W = RFXB_TZ + 2;
+      if (tid < 2 * W + 2 * TY) {
+        if (tid < W) re_fill(0, tid, false);
+        else if (tid < 2 * W) re_fill(TY + 1, tid - W, false);
+        else if (tid < 2 * W + TY) re_fill(tid - 2 * W + 1, 0, false);
+        else re_fill(tid - 2 * W - TY + 1, W - 1, false);
+      }
+      __syncthreads();
+    }
+
     // ---- phase A ----
     float ahx = 0.f, ahy = 0.f, ahz = 0.f;
     if (own) {
-      adj_a_cell<TY, 7>(P, A, S, C, b0, b1, i, j, k, ly, lz, xe0, xe1, ye0, ye1, ze0, ze1, true, ahx, ahy, ahz);
+      adj_a_cell<TY, 7, false>(P, A, S, C, b0, b1, i, j, k, ly, lz, xe0, xe1, ye0, ye1, ze0, ze1, true, ahx, ahy,
+                               ahz);
+      if (C.cpx) { ahz += rx0 - nx0; ahy += rx1 - nx1; }
+      if (C.cpy) {
+        ahz += S.rx[0][ly][lh] - S.rx[0][ly + 1][lh];
+        ahx += S.rx[1][ly][lh] - S.rx[1][ly + 1][lh];
+      }
+      if (C.cpz) {
+        ahy += S.rx[2][ly][lh] - S.rx[2][ly][lh + 1];
+        ahx += S.rx[3][ly][lh] - S.rx[3][ly][lh + 1];
+      }
       if (P.g && (pmask || prb_tail)) {   // H-probe cotangent of y_n
         for (unsigned m = pmask; m; m &= m - 1) {
           const int q = __ffs(m) - 1;
@@ -388,8 +512,14 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       float a1 = 0.f, a2 = 0.f, a3 = 0.f;
       float chr = 0.f;
       if (row_halo) {
-        adj_a_cell<TY, 5>(P, A, S, C, b0, b1, i, y0 - 1, k, 0, lz, xe0, xe1, ye0_r, ye1_r, ze0_r, ze1_r, false,
-                          a1, a2, a3);
+        adj_a_cell<TY, 5, false>(P, A, S, C, b0, b1, i, y0 - 1, k, 0, lz, xe0, xe1, ye0_r, ye1_r, ze0_r, ze1_r,
+                                 false, a1, a2, a3);
+        if (C.cpx) a3 += rxh - nxh;
+        if (C.cpy) {
+          a3 += S.rx[0][0][lh] - S.rx[0][1][lh];
+          a1 += S.rx[1][0][lh] - S.rx[1][1][lh];
+        }
+        if (C.cpz) a1 += S.rx[3][0][lh] - S.rx[3][0][lh + 1];
         chr = chat(i, y0 - 1, k);
         if (P.g) {
           for (int q = 0; q < P.nprb; ++q) {
@@ -408,8 +538,15 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       float a1 = 0.f, a2 = 0.f, a3 = 0.f;
       float chz = 0.f;
       if (col_halo) {
-        adj_a_cell<TY, 3>(P, A, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xe0, xe1, ye0_c, ye1_c, ze0_c, ze1_c,
-                          false, a1, a2, a3);
+        adj_a_cell<TY, 3, false>(P, A, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xe0, xe1, ye0_c, ye1_c,
+                                 ze0_c, ze1_c, false, a1, a2, a3);
+        const int r = lane + 1;
+        if (C.cpx) a2 += rxh - nxh;
+        if (C.cpy) a1 += S.rx[1][r][0] - S.rx[1][r + 1][0];
+        if (C.cpz) {
+          a2 += S.rx[2][r][0] - S.rx[2][r][1];
+          a1 += S.rx[3][r][0] - S.rx[3][r][1];
+        }
         chz = chat(i, y0 + lane, z0 - 1);
         if (P.g) {
           for (int q = 0; q < P.nprb; ++q) {
@@ -426,6 +563,33 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     }
     __syncthreads();
 
+    // r_H of the y / z relations at the tile and the low halo row / column
+    // (rows y0-1 .. y0+TY-1, columns z0-1 .. z0+31), once per cell
+    if (yz_tile) {
+      auto rh_fill = [&](int r, int c, bool write, bool ny_, bool nz_) {
+        const int jj = y0 - 1 + r, kk = z0 - 1 + c;
+        float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+        if (jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+          if (C.cpy && ny_) {
+            v0 = rh_eval(P, A, C, 1, 0, -1.f, i, jj, kk, S.p[0][r][c], write);   // hx <- ez
+            v1 = rh_eval(P, A, C, 1, 1, +1.f, i, jj, kk, S.p[2][r][c], write);   // hz <- ex
+          }
+          if (C.cpz && nz_) {
+            v2 = rh_eval(P, A, C, 2, 0, +1.f, i, jj, kk, S.p[0][r][c], write);   // hx <- ey
+            v3 = rh_eval(P, A, C, 2, 1, -1.f, i, jj, kk, S.p[1][r][c], write);   // hy <- ex
+          }
+        }
+        S.rx[0][r][c] = v0;
+        S.rx[1][r][c] = v1;
+        S.rx[2][r][c] = v2;
+        S.rx[3][r][c] = v3;
+      };
+      rh_fill(ly, lh, own, true, true);
+      if (tid < RFXB_TZ) rh_fill(0, tid + 1, false, true, false);                          // row y0-1: y relations
+      else if (tid < RFXB_TZ + TY) rh_fill(tid - RFXB_TZ + 1, 0, false, false, true);      // column z0-1: z relations
+      __syncthreads();
+    }
+
     // ---- phase B ----
     float py = 0.f, pz = 0.f;
     float rhy = 0.f, rhz = 0.f;
@@ -441,18 +605,18 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       float ay = cav * X.ae[1][ly][lz] + ((xh0 * pz - xhm * pz_prev) - (zh0 * px - zhm * px_zm));
       float az = cav * X.ae[2][ly][lz] + ((yh0 * px - yhm * px_ym) - (xh0 * py - xhm * py_prev));
       if (C.cpx) {   // (hy <- ez, +1, q0), (hz <- ey, -1, q1): aE(x) += r(x-1) - r(x)
-        rhy = r_h(P, A, C, 0, 0, +1.f, i, j, k, py, true);
-        rhz = r_h(P, A, C, 0, 1, -1.f, i, j, k, pz, true);
+        rhy = rh_eval(P, A, C, 0, 0, +1.f, i, j, k, py, true);
+        rhz = rh_eval(P, A, C, 0, 1, -1.f, i, j, k, pz, true);
         az += rhy_prev - rhy;
         ay += rhz_prev - rhz;
       }
       if (C.cpy) {   // (hx <- ez, -1, q0), (hz <- ex, +1, q1)
-        az += r_h(P, A, C, 1, 0, -1.f, i, j - 1, k, px_ym, false) - r_h(P, A, C, 1, 0, -1.f, i, j, k, px, true);
-        ax += r_h(P, A, C, 1, 1, +1.f, i, j - 1, k, pz_ym, false) - r_h(P, A, C, 1, 1, +1.f, i, j, k, pz, true);
+        az += S.rx[0][ly - 1][lh] - S.rx[0][ly][lh];
+        ax += S.rx[1][ly - 1][lh] - S.rx[1][ly][lh];
       }
       if (C.cpz) {   // (hx <- ey, +1, q0), (hy <- ex, -1, q1)
-        ay += r_h(P, A, C, 2, 0, +1.f, i, j, k - 1, px_zm, false) - r_h(P, A, C, 2, 0, +1.f, i, j, k, px, true);
-        ax += r_h(P, A, C, 2, 1, -1.f, i, j, k - 1, py_zm, false) - r_h(P, A, C, 2, 1, -1.f, i, j, k, py, true);
+        ay += S.rx[2][ly][lh - 1] - S.rx[2][ly][lh];
+        ax += S.rx[3][ly][lh - 1] - S.rx[3][ly][lh];
       }
       if (n >= 1 && (pmask | smask | (unsigned)prb_tail | (unsigned)src_tail)) {
         if (P.g) {   // E-probe cotangent of y_{n-1}
@@ -505,6 +669,9 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     pz_prev = pz;
     rhy_prev = rhy;
     rhz_prev = rhz;
+    rx0 = nx0;
+    rx1 = nx1;
+    rxh = nxh;
   }
   if (!TMA) cp_async_wait<0>();
 }
