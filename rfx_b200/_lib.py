@@ -89,6 +89,8 @@ SIGNATURES = {
     "rfxb_batch_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rfxb_plan_forward_variant": (C.c_int, [C.c_void_p]),
     "rfxb_batch_forward_variant": (C.c_int, [C.c_void_p]),
+    "rfxb_plan_adjoint_variant": (C.c_int, [C.c_void_p]),
+    "rfxb_batch_adjoint_variant": (C.c_int, [C.c_void_p]),
     "rfxb_forward_noalloc": (C.c_int, [C.POINTER(RfxbDesc), C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
                                        C.POINTER(RfxbStepIO), C.c_int, C.c_int, C.c_void_p]),
 }

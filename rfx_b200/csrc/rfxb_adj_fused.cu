@@ -1,5 +1,5 @@
-// Fused reverse step of the adjoint: the same tiling, x-march, 4-stage
-// cp.async pipeline and halo recomputation as the forward step kernel.
+// Fused reverse step of the adjoint: the same tiling, x-march, staged plane
+// pipeline and halo recomputation as the forward step kernel.
 //
 // The transpose of one forward step (see rfxb_adj.cu for the derivation)
 // has the forward's dependency shape with the roles swapped:
@@ -14,6 +14,16 @@
 // state, so halo cells recomputed by a neighbour CTA read step-consistent
 // values.  The eps_r gradient over the recorded region is accumulated in
 // phase A from the forward history.
+//
+// The CPML terms of each relation are evaluated once per cell: the y / z
+// relations are exchanged between neighbouring cells through shared memory,
+// the x relations are carried along the march.  Modes (template MODE):
+//   0  cp.async staging (4 planes), psi and ce read from global memory;
+//   1  TMA staging (4 planes), psi and ce read from global memory;
+//   2  TMA staging (3 planes) plus a two-slot ring that brings, one plane
+//      ahead, every adjoint psi and ce value the plane's CPML terms read, so
+//      no slab cell waits on a global load.  The host selects it when no
+//      tile reaches both slabs of an axis.
 #include "rfxb_common.cuh"
 
 namespace rfxb {
@@ -23,6 +33,7 @@ namespace rfxb {
 #define RFXB_AHW 36
 
 __host__ __device__ constexpr int apad128(int nfloats) { return (nfloats % 32) ? 32 - (nfloats % 32) : 32; }
+__host__ __device__ constexpr int up32(int nfloats) { return (nfloats + 31) / 32 * 32; }
 
 template <int TY>
 struct AdjDims {
@@ -47,9 +58,10 @@ struct __align__(128) AdjStage {
   float ca[TY][RFXB_TZ];           // ca of the tile
 };
 
+// The plane stages come last so that a kernel using fewer of them (mode 2)
+// allocates only those, followed by its psi ring.
 template <int TY>
 struct AdjSmem {
-  AdjStage<TY> st[RFXB_ANSTAGE];
   float p[3][TY + 1][RFXB_TZ + 1];   // ch * aH1 of plane i, [y - y0 + 1][z - z0 + 1]
   // CPML terms of the y / z relations exchanged between neighbouring cells:
   // phase A r_E of (y q0, y q1, z q0, z q1) at rows y0-1 .. y0+TY, columns
@@ -58,9 +70,40 @@ struct AdjSmem {
   RfxbInst P;
   AdjInst A;
   unsigned long long mbar[RFXB_ANSTAGE];
+  unsigned long long pbar[2];        // psi ring (mode 2)
+  AdjStage<TY> st[RFXB_ANSTAGE];
 };
 
-__device__ __forceinline__ int astage_of(int p) { return (p + 1) & (RFXB_ANSTAGE - 1); }
+// Plane p lives in stage (p + 1) mod NST.
+template <int NST>
+__device__ __forceinline__ int astage_of(int p) { return (p + 1) % NST; }
+// Planes are loaded in order xa-1, xa, ...; a stage completes its k-th fill on
+// mbarrier phase k.
+template <int NST>
+__device__ __forceinline__ uint32_t astage_parity(int p, int xa) { return (uint32_t)(((p - xa + 1) / NST) & 1); }
+
+// One slot of the mode-2 psi ring: everything the CPML terms of plane p read
+// (floats, 128-byte aligned sub-arrays; zp = the launch's largest z-psi row):
+//   EY  [q][TY+2][40]  adjoint E-side psi of the y slab, rows y0-1.., z from z0-4
+//   HY  [q][TY+1][36]  adjoint H-side psi of the y slab, rows y0-1.., z from z0-4
+//   EXN [q][TY+1][36]  adjoint E-side psi of the x slab at plane p+1
+//   HX  [q][TY][32]    adjoint H-side psi of the x slab on the tile
+//   CE  [TY+2][40]     ce of plane p on the E footprint
+//   CEN [TY+1][36]     ce of plane p+1 on the H footprint
+//   EZ  [q][TY+2][n4]  adjoint E-side psi of the z slab, layer s
+//   HZ  [q][TY+1][n4]  adjoint H-side psi of the z slab
+template <int TY>
+struct APsiSlot {
+  static constexpr int EY = 0;
+  static constexpr int HY = EY + up32(2 * (TY + 2) * RFXB_AEW);
+  static constexpr int EXN = HY + up32(2 * (TY + 1) * RFXB_AHW);
+  static constexpr int HX = EXN + up32(2 * (TY + 1) * RFXB_AHW);
+  static constexpr int CE = HX + up32(2 * TY * RFXB_TZ);
+  static constexpr int CEN = CE + up32((TY + 2) * RFXB_AEW);
+  static constexpr int EZ = CEN + up32((TY + 1) * RFXB_AHW);
+  __host__ __device__ static constexpr int HZ(int zp) { return EZ + up32(2 * (TY + 2) * zp); }
+  __host__ __device__ static constexpr int FLOATS(int zp) { return HZ(zp) + up32(2 * (TY + 1) * zp); }
+};
 
 struct AdjCtx {
   int nx, ny, nz, zs, ncp, par, apar;
@@ -199,7 +242,7 @@ __device__ __forceinline__ void adj_a_cell(const RfxbInst& P, const AdjInst& A, 
 template <int TY>
 __device__ __forceinline__ void adj_load_stage(AdjSmem<TY>& S, const AdjCtx& C, const float* aF0, const float* ca,
                                                const float* cb, int y0, int z0, int ip, int tid) {
-  AdjStage<TY>& D = S.st[astage_of(ip)];
+  AdjStage<TY>& D = S.st[astage_of<RFXB_ANSTAGE>(ip)];
   const long long pb = C.off0 + (long long)ip * C.ps;
   constexpr int RE = (TY + 2) * 10, RH = (TY + 1) * 9, RC = TY * 8;
   constexpr int NE = 4 * RE, NH = 3 * RH, NC = RC;
@@ -224,10 +267,10 @@ __device__ __forceinline__ void adj_load_stage(AdjSmem<TY>& S, const AdjCtx& C, 
 
 // TMA boxes of plane ip (one thread): adjoint E and H of parity apar, cb with
 // the E footprint, ca of the tile.
-template <int TY>
+template <int TY, int NST>
 __device__ __forceinline__ void adj_tma_stage(AdjSmem<TY>& S, const CUtensorMap* tm, int apar, int y0, int z0,
                                               int ip) {
-  const int s = astage_of(ip);
+  const int s = astage_of<NST>(ip);
   const uint32_t mb = smem_u32(&S.mbar[s]);
   mbar_expect_tx(mb, AdjDims<TY>::BYTES);
   tma_load_4d(smem_u32(&S.st[s].ae[0][0][0]), tm + 5 + apar, z0 - 4, y0, ip + 1, 0, mb);
@@ -236,14 +279,78 @@ __device__ __forceinline__ void adj_tma_stage(AdjSmem<TY>& S, const CUtensorMap*
   tma_load_4d(smem_u32(&S.st[s].ca[0][0]), tm + 10, z0, y0 + 1, ip + 1, 0, mb);
 }
 
-__device__ __forceinline__ uint32_t astage_parity(int p, int xa) { return (uint32_t)(((p - xa + 1) >> 2) & 1); }
+// r_E / r_H of one relation from a given old psi (mode 2: staged); the new
+// psi goes to the other parity at index qi.
+__device__ __forceinline__ float re_core(const AdjInst& A, const AdjCtx& C, int axis, const float4& cf, long long qi,
+                                         float psi, float sgn, float ce, float at, bool write) {
+  const float nu = psi + sgn * ce * at;
+  if (write) A.aPsiE[C.par ^ 1][axis][qi] = cf.x * nu;
+  return cf.y * nu + sgn * ce * (cf.z * at);
+}
+__device__ __forceinline__ float rh_core(const AdjInst& A, const AdjCtx& C, int axis, const float4& cf, long long qi,
+                                         float psi, float sgn, float pt, bool write) {
+  const float nu = psi + sgn * pt;
+  if (write) A.aPsiH[C.par ^ 1][axis][qi] = cf.x * nu;
+  return cf.y * nu + sgn * (cf.z * pt);
+}
 
-template <int TY, bool TMA>
-__global__ void __launch_bounds__(32 * TY, 4)
+// Which CPML slab of an axis the cells lo..hi of a CTA reach: side or -1
+// (mode 2 guarantees at most one side per axis).
+__device__ __forceinline__ int atile_side(int lo, int hi, int n, int ncp) {
+  if (lo < ncp) return 0;
+  if (hi >= n - ncp) return 1;
+  return -1;
+}
+
+// Issue the mode-2 ring boxes of plane p (one thread).
+template <int TY>
+__device__ __forceinline__ void apsi_issue(float* slot, uint32_t mb, const CUtensorMap* tm, const AdjCtx& C, int zp4,
+                                           int y0, int z0, int p, bool yz_tile, int ysd, int zsd, int n4) {
+  using L = APsiSlot<TY>;
+  const int par = C.par;
+  int sx = 0, sn = 0;
+  const int xsd = C.cpx ? cpml_side(p, C.nx, C.ncp, sx) : -1;
+  const int xnd = (C.cpx && p + 1 < C.nx) ? cpml_side(p + 1, C.nx, C.ncp, sn) : -1;
+  unsigned bytes = 0;
+  if (yz_tile) bytes += 4u * (TY + 2) * RFXB_AEW;
+  if (ysd >= 0) bytes += 4u * 2 * (TY + 2) * RFXB_AEW + 4u * 2 * (TY + 1) * RFXB_AHW;
+  if (zsd >= 0) bytes += 4u * 2 * (TY + 2) * n4 + 4u * 2 * (TY + 1) * n4;
+  if (xnd >= 0) bytes += 4u * 2 * (TY + 1) * RFXB_AHW + 4u * (TY + 1) * RFXB_AHW;
+  if (xsd >= 0) bytes += 4u * 2 * TY * RFXB_TZ;
+  mbar_expect_tx(mb, bytes);
+  if (yz_tile) tma_load_4d(smem_u32(slot + L::CE), tm + 9, z0 - 4, y0, p + 1, 2, mb);
+  if (ysd >= 0) {
+    const int jb = ysd ? C.ny - C.ncp : 0;
+    tma_load_4d(smem_u32(slot + L::EY), tm + RFXB_MAP_APE + 2 + par, z0 - 4, y0 - 1 - jb, p, 2 * ysd, mb);
+    tma_load_4d(smem_u32(slot + L::HY), tm + RFXB_MAP_APH + 2 + par, z0 - 4, y0 - 1 - jb, p, 2 * ysd, mb);
+  }
+  if (zsd >= 0) {
+    tma_load_4d(smem_u32(slot + L::EZ), tm + RFXB_MAP_APE + 4 + par, 0, y0 - 1, p, 2 * zsd, mb);
+    tma_load_4d(smem_u32(slot + L::HZ(zp4)), tm + RFXB_MAP_APH + 4 + par, 0, y0 - 1, p, 2 * zsd, mb);
+  }
+  if (xnd >= 0) {
+    tma_load_4d(smem_u32(slot + L::EXN), tm + RFXB_MAP_APE + 0 + par, z0 - 4, y0 - 1, sn, 2 * xnd, mb);
+    tma_load_4d(smem_u32(slot + L::CEN), tm + 23, z0 - 4, y0, p + 2, 2, mb);
+  }
+  if (xsd >= 0) tma_load_4d(smem_u32(slot + L::HX), tm + RFXB_MAP_APH + 0 + par, z0, y0, sx, 2 * xsd, mb);
+}
+
+template <int MODE>
+struct AdjBounds { static constexpr int MIN_CTAS = 4; };
+template <>
+struct AdjBounds<2> { static constexpr int MIN_CTAS = 3; };
+
+template <int TY, int MODE>
+__global__ void __launch_bounds__(32 * TY, AdjBounds<MODE>::MIN_CTAS)
 adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
-                const RfxbWork* __restrict__ work, const CUtensorMap* __restrict__ maps, int n, int par, int apar) {
+                const RfxbWork* __restrict__ work, const CUtensorMap* __restrict__ maps, int n, int par, int apar,
+                int zp) {
+  constexpr bool TMA = MODE != 0;
+  constexpr int NST = MODE == 2 ? 3 : RFXB_ANSTAGE;   // plane stages
+  using L = APsiSlot<TY>;
   extern __shared__ __align__(128) unsigned char adj_smem_raw[];
   AdjSmem<TY>& S = *reinterpret_cast<AdjSmem<TY>*>(adj_smem_raw);
+  float* ring = reinterpret_cast<float*>(&S.st[NST]);   // mode 2: two psi slots after the stages
   const int lane = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * 32 + lane;
   const RfxbWork w = work[blockIdx.x];
@@ -255,7 +362,8 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     for (int t = tid; t < nw; t += 32 * TY) d[t] = __ldg(s + t);
   }
   if (TMA && tid == 0) {
-    for (int q = 0; q < RFXB_ANSTAGE; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
+    for (int q = 0; q < NST; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
+    if (MODE == 2) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
     mbar_fence_init();
   }
   __syncthreads();
@@ -308,19 +416,51 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   const int xa = w.xa, xb = w.xb;
   const float* ca = P.ca;
   const float* cb = P.cb;
+  // mode-2 psi ring: the slab side this tile reaches per axis, and the
+  // bookkeeping of the two slots (identical in every thread)
+  const bool yz_tile = C.cpy || C.cpz;
+  const int ysd = (MODE == 2 && C.cpy) ? atile_side(y0 - 1, y0 + TY, C.ny, C.ncp) : -1;
+  const int zsd = (MODE == 2 && C.cpz) ? atile_side(z0 - 1, z0 + 32, C.nz, C.ncp) : -1;
+  const int n4 = P.ncp4;
+  auto xslab = [&](int p) { return C.cpx && p >= 0 && p < C.nx && (p < C.ncp || p >= C.nx - C.ncp); };
+  auto psi_need = [&](int p) {
+    if (MODE != 2 || p < 0 || p >= C.nx) return false;
+    return yz_tile || xslab(p) || xslab(p + 1);
+  };
+  unsigned pph = 0u, pout = 0u;
+  auto psi_fill = [&](int p) {
+    if (!psi_need(p)) return;
+    if (tid == 0)
+      apsi_issue<TY>(ring + (p & 1) * L::FLOATS(zp), smem_u32(&S.pbar[p & 1]), tm, C, zp, y0, z0, p, yz_tile, ysd,
+                     zsd, n4);
+    pout |= 1u << (p & 1);
+  };
+  auto psi_wait = [&](int p) -> bool {
+    if (!psi_need(p)) return true;
+    const int sl = p & 1;
+    const bool ok = mbar_wait_bounded(smem_u32(&S.pbar[sl]), (pph >> sl) & 1u);
+    if (ok) {
+      pph ^= 1u << sl;
+      pout &= ~(1u << sl);
+    }
+    return ok;
+  };
   auto bail = [&](int last_issued, int from) {
     if (tid == 0) {
       atomicOr(P.status, 1);
       for (int p = from; p <= last_issued; ++p)
-        mbar_wait_bounded(smem_u32(&S.mbar[astage_of(p)]), astage_parity(p, xa));
+        mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(p)]), astage_parity<NST>(p, xa));
+      for (int sl = 0; sl < 2; ++sl)
+        if (pout & (1u << sl)) mbar_wait_bounded(smem_u32(&S.pbar[sl]), (pph >> sl) & 1u);
     }
   };
   if (TMA) {
     if (tid == 0)
-      for (int p = xa - 1; p <= min(xa + 2, C.nx); ++p) adj_tma_stage<TY>(S, tm, apar, y0, z0, p);
-    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of(xa - 1)]), astage_parity(xa - 1, xa)) &&
-                    mbar_wait_bounded(smem_u32(&S.mbar[astage_of(xa)]), astage_parity(xa, xa));
-    if (__syncthreads_or(!ok)) { bail(min(xa + 2, C.nx), xa - 1); return; }
+      for (int p = xa - 1; p <= min(xa + NST - 2, C.nx); ++p) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, p);
+    psi_fill(xa);
+    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa - 1)]), astage_parity<NST>(xa - 1, xa)) &&
+                    mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa)]), astage_parity<NST>(xa, xa));
+    if (__syncthreads_or(!ok)) { bail(min(xa + NST - 2, C.nx), xa - 1); return; }
   } else {
     adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa - 1, tid);
     adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa, tid);
@@ -338,7 +478,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   if (xa > 0 && own) {
     float a1, a2, a3;
     const int im = xa - 1;
-    adj_a_cell<TY, 6>(P, A, S, C, astage_of(im), astage_of(xa), im, j, k, ly, lz, __ldg(P.xe + im),
+    adj_a_cell<TY, 6>(P, A, S, C, astage_of<NST>(im), astage_of<NST>(xa), im, j, k, ly, lz, __ldg(P.xe + im),
                       __ldg(P.xe + xa), ye0, ye1, ze0, ze1, false, a1, a2, a3);
     if (P.g) {   // H-probe cotangent of y_n at plane xa-1
       for (unsigned m = pmask; m; m &= m - 1) {
@@ -373,7 +513,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   // CTA owning a plane writes its psi when it evaluates it.
   float rx0 = 0.f, rx1 = 0.f, rxh = 0.f;
   if (C.cpx) {
-    const AdjStage<TY>& X0 = S.st[astage_of(xa)];
+    const AdjStage<TY>& X0 = S.st[astage_of<NST>(xa)];
     if (own) {
       const float ce = P.ce[cell_index(C, xa, j, k)];
       rx0 = re_eval(P, A, C, 0, 0, -1.f, xa, j, k, X0.ae[1][ly][lz], ce, true);
@@ -385,27 +525,52 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       rxh = re_eval(P, A, C, 0, 1, +1.f, xa, y0 + lane, z0 - 1, X0.ae[2][lane + 1][3],
                     P.ce[cell_index(C, xa, y0 + lane, z0 - 1)], false);
   }
-  const bool yz_tile = C.cpy || C.cpz;
 
   for (int i = xa; i < xb; ++i) {
     if (TMA) {
-      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of(i + 1)]), astage_parity(i + 1, xa));
-      if (__syncthreads_or(!ok)) { bail(min(i + 2, C.nx), i + 1); return; }
-      if (tid == 0 && i + 3 <= C.nx) adj_tma_stage<TY>(S, tm, apar, y0, z0, i + 3);
+      // plane i+1 (and plane i's psi) have landed; after the barrier plane
+      // i-1's stage takes plane i+NST-1 and its psi slot plane i+1
+      const bool ok =
+          mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(i + 1)]), astage_parity<NST>(i + 1, xa)) && psi_wait(i);
+      if (__syncthreads_or(!ok)) { bail(min(i + NST - 2, C.nx), i + 1); return; }
+      if (tid == 0 && i + NST - 1 <= C.nx) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, i + NST - 1);
+      if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();
       __syncthreads();
       if (i + 3 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, i + 3, tid);
       cp_async_commit();
     }
-    const int b0 = astage_of(i), b1 = astage_of(i + 1);
+    const int b0 = astage_of<NST>(i), b1 = astage_of<NST>(i + 1);
+    const float* PS = ring + (i & 1) * L::FLOATS(zp);
     const float xe0 = __ldg(P.xe + i), xe1 = __ldg(P.xe + i + 1);
     const float xh0 = __ldg(P.xh + i), xhm = __ldg(P.xh + i - 1);
     const long long e = cell_index(C, i, j, k);
 
     // x relations of plane i+1 (written by this CTA when it owns that plane)
     float nx0 = 0.f, nx1 = 0.f, nxh = 0.f;
-    if (C.cpx && i + 1 < C.nx) {
+    if (MODE == 2 && xslab(i + 1)) {   // psi and ce of plane i+1 from the ring
+      const AdjStage<TY>& Y1 = S.st[b1];
+      const bool wr = i + 1 < xb;
+      int sx;
+      const int sd = cpml_side(i + 1, C.nx, C.ncp, sx);
+      const float4 cf = __ldg(P.cpt + sd * C.ncp + sx);
+      constexpr int RQ = (TY + 1) * RFXB_AHW;
+      auto xnext = [&](int r, int zc, int jj, int kk, float at0, float at1, bool write, float& v0, float& v1) {
+        const float ce = PS[L::CEN + r * RFXB_AHW + zc];
+        v0 = re_core(A, C, 0, cf, psi_q(P, 0, sd, 0, sx, i + 1, jj, kk), PS[L::EXN + r * RFXB_AHW + zc], -1.f, ce,
+                     at0, write);
+        v1 = re_core(A, C, 0, cf, psi_q(P, 0, sd, 1, sx, i + 1, jj, kk), PS[L::EXN + RQ + r * RFXB_AHW + zc], +1.f,
+                     ce, at1, write);
+      };
+      if (own) xnext(ly, lz, j, k, Y1.ae[1][ly][lz], Y1.ae[2][ly][lz], wr, nx0, nx1);
+      float d0 = 0.f, d1 = 0.f;
+      if (row_halo) { xnext(0, lz, y0 - 1, k, Y1.ae[1][0][lz], 0.f, false, d0, d1); nxh = d0; }
+      if (col_halo) {
+        xnext(lane + 1, 3, y0 + lane, z0 - 1, 0.f, Y1.ae[2][lane + 1][3], false, d0, d1);
+        nxh = d1;
+      }
+    } else if (MODE != 2 && C.cpx && i + 1 < C.nx) {
       const AdjStage<TY>& Y1 = S.st[b1];
       const bool wr = i + 1 < xb;
       if (own) {
@@ -428,7 +593,31 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       auto re_fill = [&](int r, int c, bool write) {
         const int jj = y0 - 1 + r, kk = z0 - 1 + c;
         float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-        if (jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+        if (MODE == 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+          const float ce = PS[L::CE + r * RFXB_AEW + c + 3];
+          const float ax = X.ae[0][r][c + 3], ay = X.ae[1][r][c + 3], az = X.ae[2][r][c + 3];
+          int sl;
+          if (C.cpy) {
+            const int sd = cpml_side(jj, C.ny, C.ncp, sl);
+            if (sd >= 0) {
+              const float4 cf = __ldg(P.cpt + (2 + sd) * C.ncp + sl);
+              const int o = r * RFXB_AEW + c + 3;
+              v0 = re_core(A, C, 1, cf, psi_q(P, 1, sd, 0, sl, i, jj, kk), PS[L::EY + o], +1.f, ce, ax, write);
+              v1 = re_core(A, C, 1, cf, psi_q(P, 1, sd, 1, sl, i, jj, kk), PS[L::EY + (TY + 2) * RFXB_AEW + o], -1.f,
+                           ce, az, write);
+            }
+          }
+          if (C.cpz) {
+            const int sd = cpml_side(kk, C.nz, C.ncp, sl);
+            if (sd >= 0) {
+              const float4 cf = __ldg(P.cpt + (4 + sd) * C.ncp + sl);
+              const int o = r * n4 + sl;
+              v2 = re_core(A, C, 2, cf, psi_q(P, 2, sd, 0, sl, i, jj, kk), PS[L::EZ + o], -1.f, ce, ax, write);
+              v3 = re_core(A, C, 2, cf, psi_q(P, 2, sd, 1, sl, i, jj, kk), PS[L::EZ + (TY + 2) * n4 + o], +1.f, ce,
+                           ay, write);
+            }
+          }
+        } else if (MODE != 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
           const float ce = P.ce[cell_index(C, i, jj, kk)];
           const float ax = X.ae[0][r][c + 3], ay = X.ae[1][r][c + 3], az = X.ae[2][r][c + 3];
           if (C.cpy) {
@@ -569,7 +758,29 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       auto rh_fill = [&](int r, int c, bool write, bool ny_, bool nz_) {
         const int jj = y0 - 1 + r, kk = z0 - 1 + c;
         float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-        if (jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+        if (MODE == 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+          int sl;
+          if (C.cpy && ny_) {
+            const int sd = cpml_side(jj, C.ny, C.ncp, sl);
+            if (sd >= 0) {
+              const float4 cf = __ldg(P.cpt + (2 + sd) * C.ncp + sl);
+              const int o = r * RFXB_AHW + c + 3;
+              v0 = rh_core(A, C, 1, cf, psi_q(P, 1, sd, 0, sl, i, jj, kk), PS[L::HY + o], -1.f, S.p[0][r][c], write);
+              v1 = rh_core(A, C, 1, cf, psi_q(P, 1, sd, 1, sl, i, jj, kk), PS[L::HY + (TY + 1) * RFXB_AHW + o], +1.f,
+                           S.p[2][r][c], write);
+            }
+          }
+          if (C.cpz && nz_) {
+            const int sd = cpml_side(kk, C.nz, C.ncp, sl);
+            if (sd >= 0) {
+              const float4 cf = __ldg(P.cpt + (4 + sd) * C.ncp + sl);
+              const int hz = L::HZ(zp), o = r * n4 + sl;
+              v2 = rh_core(A, C, 2, cf, psi_q(P, 2, sd, 0, sl, i, jj, kk), PS[hz + o], +1.f, S.p[0][r][c], write);
+              v3 = rh_core(A, C, 2, cf, psi_q(P, 2, sd, 1, sl, i, jj, kk), PS[hz + (TY + 1) * n4 + o], -1.f,
+                           S.p[1][r][c], write);
+            }
+          }
+        } else if (MODE != 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
           if (C.cpy && ny_) {
             v0 = rh_eval(P, A, C, 1, 0, -1.f, i, jj, kk, S.p[0][r][c], write);   // hx <- ez
             v1 = rh_eval(P, A, C, 1, 1, +1.f, i, jj, kk, S.p[2][r][c], write);   // hz <- ex
@@ -605,8 +816,19 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       float ay = cav * X.ae[1][ly][lz] + ((xh0 * pz - xhm * pz_prev) - (zh0 * px - zhm * px_zm));
       float az = cav * X.ae[2][ly][lz] + ((yh0 * px - yhm * px_ym) - (xh0 * py - xhm * py_prev));
       if (C.cpx) {   // (hy <- ez, +1, q0), (hz <- ey, -1, q1): aE(x) += r(x-1) - r(x)
-        rhy = rh_eval(P, A, C, 0, 0, +1.f, i, j, k, py, true);
-        rhz = rh_eval(P, A, C, 0, 1, -1.f, i, j, k, pz, true);
+        if (MODE == 2) {
+          if (xslab(i)) {
+            int sx;
+            const int sd = cpml_side(i, C.nx, C.ncp, sx);
+            const float4 cf = __ldg(P.cpt + sd * C.ncp + sx);
+            const int o = ty * RFXB_TZ + lane;
+            rhy = rh_core(A, C, 0, cf, psi_q(P, 0, sd, 0, sx, i, j, k), PS[L::HX + o], +1.f, py, true);
+            rhz = rh_core(A, C, 0, cf, psi_q(P, 0, sd, 1, sx, i, j, k), PS[L::HX + TY * RFXB_TZ + o], -1.f, pz, true);
+          }
+        } else {
+          rhy = rh_eval(P, A, C, 0, 0, +1.f, i, j, k, py, true);
+          rhz = rh_eval(P, A, C, 0, 1, -1.f, i, j, k, pz, true);
+        }
         az += rhy_prev - rhy;
         ay += rhz_prev - rhz;
       }
@@ -676,11 +898,19 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   if (!TMA) cp_async_wait<0>();
 }
 
-template __global__ void adj_step_kernel<8, true>(const RfxbInst*, const AdjInst*, const RfxbWork*,
-                                                  const CUtensorMap*, int, int, int);
-template __global__ void adj_step_kernel<8, false>(const RfxbInst*, const AdjInst*, const RfxbWork*,
-                                                   const CUtensorMap*, int, int, int);
+template __global__ void adj_step_kernel<8, 0>(const RfxbInst*, const AdjInst*, const RfxbWork*,
+                                               const CUtensorMap*, int, int, int, int);
+template __global__ void adj_step_kernel<8, 1>(const RfxbInst*, const AdjInst*, const RfxbWork*,
+                                               const CUtensorMap*, int, int, int, int);
+template __global__ void adj_step_kernel<8, 2>(const RfxbInst*, const AdjInst*, const RfxbWork*,
+                                               const CUtensorMap*, int, int, int, int);
 
-size_t adj_step_smem_bytes() { return sizeof(AdjSmem<8>); }
+// Dynamic shared memory of a mode: the fixed part, the plane stages it uses
+// and (mode 2) the two ring slots sized for z-psi rows of zp floats.
+size_t adj_step_smem_bytes(int mode, int zp) {
+  const size_t fixed = offsetof(AdjSmem<8>, st);
+  if (mode != 2) return fixed + RFXB_ANSTAGE * sizeof(AdjStage<8>);
+  return fixed + 3 * sizeof(AdjStage<8>) + 2 * sizeof(float) * (size_t)APsiSlot<8>::FLOATS(zp);
+}
 
 }  // namespace rfxb

@@ -32,9 +32,10 @@ __global__ void coef_kernel(RfxbInst, float*, float*, float*, float*, const floa
 __global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
-template <int TY, bool TMA>
-__global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int);
-size_t adj_step_smem_bytes();
+template <int TY, int MODE>
+__global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int,
+                                int);
+size_t adj_step_smem_bytes(int mode, int zp);
 }  // namespace rfxb
 
 using namespace rfxb;
@@ -110,6 +111,7 @@ struct RfxbPlan {
   // TMA descriptors (layout in rfxb_inst.h, RFXB_NMAPS)
   CUtensorMap tmaps[RFXB_NMAPS];
   bool psi_maps_ok = false;    // the CPML psi maps encoded (staged-psi kernel usable)
+  bool adj_psi_maps_ok = false;  // the same for the adjoint psi
 
   ~RfxbPlan() {
     for (void* p : allocs) cudaFree(p);
@@ -147,6 +149,8 @@ struct RfxbBatch {
   CUtensorMap* d_maps = nullptr;   // RFXB_NMAPS per plan
   int* d_status = nullptr;         // device status word of the group's launches
   int fwd_mode = 0;                // forward step kernel variant (see rfxb_fwd.cu)
+  int adj_mode = -1;               // reverse step kernel variant (see rfxb_adj_fused.cu), -1 not chosen yet
+  int adj_zp = 4;                  // z-psi row capacity of the mode-2 reverse ring
   std::vector<RfxbDftPlane> dft;
   int dft_blocks = 0;
   std::vector<void*> allocs;
@@ -466,7 +470,84 @@ int encode_adjoint_maps(RfxbPlan* p) {
     if (int rc = encode_block_map(&p->tmaps[7 + s], *p, p->adj.aF[s][0], 6, 36, ty + 1, 3)) return rc;
   }
   if (int rc = encode_block_map(&p->tmaps[9], *p, p->ca, 3, 40, ty + 2, 1)) return rc;
-  return encode_block_map(&p->tmaps[10], *p, p->ca, 3, 32, ty, 1);
+  if (int rc = encode_block_map(&p->tmaps[10], *p, p->ca, 3, 32, ty, 1)) return rc;
+  if (int rc = encode_block_map(&p->tmaps[23], *p, p->ca, 3, 36, ty + 1, 1)) return rc;
+  p->adj_psi_maps_ok = false;
+  const RfxbInst& I = p->inst;
+  if (I.ncp > 0) {
+    // a psi map the driver refuses only rules out the staged-psi reverse kernel
+    auto enc = [&]() -> int {
+      const long long n = I.ncp, n4 = I.ncp4;
+      for (int s = 0; s < 2; ++s) {
+        if (I.cpml_axes & 1u) {
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + s], p->adj.aPsiE[s][0], I.zs, p->ny, n, 36, ty + 1))
+            return rc;
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + s], p->adj.aPsiH[s][0], I.zs, p->ny, n, 32, ty))
+            return rc;
+        }
+        if (I.cpml_axes & 2u) {
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + 2 + s], p->adj.aPsiE[s][1], I.zs, n, p->nx, 40, ty + 2))
+            return rc;
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + 2 + s], p->adj.aPsiH[s][1], I.zs, n, p->nx, 36, ty + 1))
+            return rc;
+        }
+        if (I.cpml_axes & 4u) {
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + 4 + s], p->adj.aPsiE[s][2], n4, p->ny, p->nx,
+                                      (unsigned)n4, ty + 2))
+            return rc;
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + 4 + s], p->adj.aPsiH[s][2], n4, p->ny, p->nx,
+                                      (unsigned)n4, ty + 1))
+            return rc;
+        }
+      }
+      return 0;
+    };
+    p->adj_psi_maps_ok = enc() == 0;
+  }
+  return 0;
+}
+
+// Whether the staged-psi reverse kernel can run a plan: like the forward's
+// test, over the cells its CPML terms touch (rows y0-1 .. y0+TY, columns
+// z0-1 .. z0+32).
+bool adj_psi_staging_ok(const RfxbPlan& p) {
+  const RfxbInst& I = p.inst;
+  if (I.ncp == 0) return true;
+  if (!p.adj_psi_maps_ok || I.ncp4 > 16) return false;
+  for (int a = 0; a < 3; ++a)
+    if (p.psi_elems[a] >= (1LL << 31)) return false;
+  const int n = I.ncp;
+  if (I.cpml_axes & 2u)
+    for (int y0 = 0; y0 < p.ny; y0 += kTY)
+      if (y0 - 1 < n && y0 + kTY >= p.ny - n) return false;
+  if (I.cpml_axes & 4u)
+    for (int z0 = 0; z0 < p.nz; z0 += 32)
+      if (z0 - 1 < n && z0 + 32 >= p.nz - n) return false;
+  return true;
+}
+
+// Reverse kernel variant of a group: 0 with RFXB_STAGING=cpasync, 2 when
+// every plan can stage its psi, else 1; and the ring's z-row capacity.
+void group_adj_mode(RfxbBatch* g) {
+  g->adj_zp = 4;
+  if (!use_tma()) { g->adj_mode = 0; return; }
+  int mode = 2;
+  for (auto* p : g->plans) {
+    if (!adj_psi_staging_ok(*p)) mode = 1;
+    g->adj_zp = std::max(g->adj_zp, p->inst.ncp4);
+  }
+  g->adj_mode = mode;
+}
+
+using AdjKernel = void (*)(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int, int);
+AdjKernel adj_kernel(int mode) {
+  static bool init[3] = {false, false, false};
+  AdjKernel k = mode == 2 ? adj_step_kernel<kTY, 2> : mode == 1 ? adj_step_kernel<kTY, 1> : adj_step_kernel<kTY, 0>;
+  if (!init[mode]) {
+    init[mode] = true;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_step_smem_bytes(mode, 16));
+  }
+  return k;
 }
 
 int upload_tables(RfxbPlan* p, const float* h, int n, const float** dst) {
@@ -740,16 +821,10 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
   }
   if (int rc = upload_adjoint(g, aios, st)) return rc;
   const bool two = use_twopass();
-  if (!two) {
-    static bool attr = false;
-    if (!attr) {
-      RFXB_CUDA(cudaFuncSetAttribute(adj_step_kernel<kTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)adj_step_smem_bytes()));
-      RFXB_CUDA(cudaFuncSetAttribute(adj_step_kernel<kTY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)adj_step_smem_bytes()));
-      attr = true;
-    }
-  }
+  if (g->adj_mode < 0) group_adj_mode(g);
+  const int amode = g->adj_mode, zp = g->adj_zp;
+  AdjKernel akern = two ? nullptr : adj_kernel(amode);
+  const size_t asmem = adj_step_smem_bytes(amode, zp);
   auto launch = [&](cudaStream_t cs) -> int {
     int par = par0, fpar = fpar0;
     for (int s = step_hi - 1; s >= step_hi - n_steps; --s) {
@@ -757,12 +832,7 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
         adj_pass_a<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
         adj_pass_b<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
       } else {
-        if (use_tma())
-          adj_step_kernel<kTY, true><<<g->n_work, dim3(32, kTY), adj_step_smem_bytes(), cs>>>(
-              g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar);
-        else
-          adj_step_kernel<kTY, false><<<g->n_work, dim3(32, kTY), adj_step_smem_bytes(), cs>>>(
-              g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar);
+        akern<<<g->n_work, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar, zp);
         fpar ^= 1;
       }
       par ^= 1;
@@ -1203,6 +1273,16 @@ int rfxb_plan_forward_variant(const RfxbPlan* p) {
 int rfxb_batch_forward_variant(const RfxbBatch* g) {
   if (!g) return -1;
   return g->fwd_mode;
+}
+
+int rfxb_plan_adjoint_variant(const RfxbPlan* p) {
+  if (!p || !p->self_group) return -1;
+  return p->self_group->adj_mode;
+}
+
+int rfxb_batch_adjoint_variant(const RfxbBatch* g) {
+  if (!g) return -1;
+  return g->adj_mode;
 }
 
 int64_t rfxb_plan_device_bytes(const RfxbPlan* p) {

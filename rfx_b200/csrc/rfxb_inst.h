@@ -24,10 +24,16 @@
 // fields with the E box, [7|8] with the H box, [9] cb with the E box,
 // [10] one coefficient with the tile box, then the CPML psi of parity 0|1:
 // [11|12] H-side x, [13|14] H-side y, [15|16] H-side z (H boxes), [17|18]
-// E-side x, [19|20] E-side y, [21|22] E-side z (tile boxes).
-#define RFXB_NMAPS 24
+// E-side x, [19|20] E-side y, [21|22] E-side z (tile boxes); [23] one
+// coefficient with the H box; then the adjoint psi of parity 0|1: [24|25]
+// E-side x (H box), [26|27] E-side y (E box), [28|29] E-side z (E rows),
+// [30|31] H-side x (tile box), [32|33] H-side y (H box), [34|35] H-side z
+// (H rows).
+#define RFXB_NMAPS 36
 #define RFXB_MAP_PSH 11
 #define RFXB_MAP_PSE 17
+#define RFXB_MAP_APE 24
+#define RFXB_MAP_APH 30
 
 // CPML psi layout per axis (q = which of the two corrected components,
 // n = layers, n4 = n rounded up to a multiple of 4):

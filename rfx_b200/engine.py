@@ -196,6 +196,11 @@ class Plan:
         with TMA-staged CPML psi."""
         return int(self._lib.rfxb_plan_forward_variant(self._h))
 
+    def adjoint_variant(self) -> int:
+        """0 cp.async staging, 1 TMA staging, 2 TMA staging with TMA-staged
+        adjoint psi; -1 before the first adjoint advance."""
+        return int(self._lib.rfxb_plan_adjoint_variant(self._h))
+
     # -- state ---------------------------------------------------------------
     def _dev(self, a, dtype=torch.float32):
         t = torch.as_tensor(np.asarray(a) if not isinstance(a, torch.Tensor) else a)
