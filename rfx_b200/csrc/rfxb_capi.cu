@@ -143,8 +143,17 @@ struct RfxbBatch {
   std::vector<RfxbPlan*> plans;
   RfxbInst* d_inst = nullptr;
   AdjInst* d_adj = nullptr;
-  RfxbWork* d_work = nullptr;
+  RfxbWork* d_work = nullptr;     // every tile (reverse steps; forward steps when not split)
   int n_work = 0;
+  // forward steps split between the CPML-free kernel (list 1) and the
+  // staged-psi kernel (list 2), launched side by side on two streams
+  bool fwd_split = false;
+  RfxbWork* d_wf1 = nullptr;
+  int n_wf1 = 0;
+  RfxbWork* d_wf2 = nullptr;
+  int n_wf2 = 0;
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   RfxbDftPlane* d_dft = nullptr;
   CUtensorMap* d_maps = nullptr;   // RFXB_NMAPS per plan
   int* d_status = nullptr;         // device status word of the group's launches
@@ -159,6 +168,9 @@ struct RfxbBatch {
   ~RfxbBatch() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (side_stream) cudaStreamDestroy(side_stream);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     for (void* p : allocs) cudaFree(p);
   }
 };
@@ -204,43 +216,42 @@ void make_work(const RfxbPlan& p, int inst_index, int chunks, std::vector<RfxbWo
 // scheduler's greedy dispatch of the pieces in decreasing cost order (the
 // order the list is emitted in), so heavy CPML tiles and large instances of a
 // batch no longer set the step time.
-void make_balanced_work(const std::vector<RfxbPlan*>& plans, int resident, double slab, double prologue,
-                        std::vector<RfxbWork>& out) {
-  struct Tile { int inst, y0, z0, nx, ncpx; double c, cx; double total; };
-  std::vector<Tile> tiles;
-  double W = 0.0;
-  for (size_t q = 0; q < plans.size(); ++q) {
-    const RfxbPlan& p = *plans[q];
-    const int n = p.inst.ncp;
-    const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
-    for (int y0 = 0; y0 < p.ny; y0 += kTY)
-      for (int z0 = 0; z0 < p.nz; z0 += 32) {
-        double c = 1.0;
-        if ((ax & 2u) && (y0 - 1 < n || y0 + kTY - 1 >= p.ny - n)) c += slab;
-        if ((ax & 4u) && (z0 - 1 < n || z0 + 31 >= p.nz - n)) c += slab;
-        const int ncpx = (ax & 1u) ? n : 0;
-        const double cx = (ax & 1u) ? slab : 0.0;
-        const double total = p.nx * c + 2.0 * ncpx * cx;
-        tiles.push_back(Tile{(int)q, y0, z0, p.nx, ncpx, c, cx, total});
-        W += total;
-      }
-  }
-  auto plane_cost = [](const Tile& t, int i) {
+// A run of planes [xa, xb) of one tile with its modelled per-plane cost:
+// c, plus cx on the planes of the x slabs (i < ncpx or i >= nx - ncpx).
+struct WorkSeg {
+  int inst, y0, z0, xa, xb, nx, ncpx;
+  double c, cx;
+};
+
+void balance_segments(const std::vector<WorkSeg>& segs, int resident, double prologue, std::vector<RfxbWork>& out) {
+  out.clear();
+  if (segs.empty()) return;
+  auto plane_cost = [](const WorkSeg& t, int i) {
     return t.c + ((i < t.ncpx || i >= t.nx - t.ncpx) ? t.cx : 0.0);
   };
+  std::vector<double> total(segs.size());
+  double W = 0.0;
+  for (size_t q = 0; q < segs.size(); ++q) {
+    double t = 0.0;
+    for (int i = segs[q].xa; i < segs[q].xb; ++i) t += plane_cost(segs[q], i);
+    total[q] = t;
+    W += t;
+  }
   struct Item { RfxbWork w; double cost; int piece; };
   auto cut = [&](double T, std::vector<Item>& items) {
     items.clear();
-    for (const Tile& t : tiles) {
-      const int mmax = std::max(1, t.nx / 4);   // pieces of at least 4 planes
-      const int m = std::max(1, std::min(mmax, (int)std::llround(t.total / T)));
-      int xa = 0;
+    for (size_t q = 0; q < segs.size(); ++q) {
+      const WorkSeg& t = segs[q];
+      const int len = t.xb - t.xa;
+      const int mmax = std::max(1, len / 4);   // pieces of at least 4 planes
+      const int m = std::max(1, std::min(mmax, (int)std::llround(total[q] / T)));
+      int xa = t.xa;
       double acc = 0.0;
       for (int piece = 1; piece <= m; ++piece) {
-        const double goal = t.total * piece / m;
+        const double goal = total[q] * piece / m;
         int xb = xa;
         double c = 0.0;
-        while (xb < t.nx && (piece == m || acc + c + 0.5 * plane_cost(t, xb) <= goal)) {
+        while (xb < t.xb && (piece == m || acc + c + 0.5 * plane_cost(t, xb) <= goal)) {
           c += plane_cost(t, xb);
           ++xb;
         }
@@ -248,7 +259,7 @@ void make_balanced_work(const std::vector<RfxbPlan*>& plans, int resident, doubl
         items.push_back(Item{RfxbWork{t.inst, t.y0, t.z0, xa, xb}, c + prologue * t.c, piece});
         acc += c;
         xa = xb;
-        if (xa >= t.nx) break;
+        if (xa >= t.xb) break;
       }
     }
     // decreasing cost in 5% buckets; within a bucket x-piece major, so tiles
@@ -282,18 +293,131 @@ void make_balanced_work(const std::vector<RfxbPlan*>& plans, int resident, doubl
     const double t = makespan(cur);
     if (t < best_t * (1.0 - 0.02)) { best_t = t; best = cur; }   // more waves only for a clear gain
   }
-  out.clear();
   for (const Item& it : best) out.push_back(it.w);
 }
 
+// Whether a forward tile's cells (rows y0-1 .. y0+TY-1, columns z0-1 ..
+// z0+31) reach a y or z CPML slab.
+bool tile_reaches_yz(const RfxbPlan& p, int y0, int z0) {
+  const int n = p.inst.ncp;
+  const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
+  return ((ax & 2u) && (y0 - 1 < n || y0 + kTY - 1 >= p.ny - n)) ||
+         ((ax & 4u) && (z0 - 1 < n || z0 + 31 >= p.nz - n));
+}
+
+// Segments of every tile's full x line (cost model of the staged kernels).
+void all_segments(const std::vector<RfxbPlan*>& plans, double slab, std::vector<WorkSeg>& segs) {
+  for (size_t q = 0; q < plans.size(); ++q) {
+    const RfxbPlan& p = *plans[q];
+    const int n = p.inst.ncp;
+    const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
+    for (int y0 = 0; y0 < p.ny; y0 += kTY)
+      for (int z0 = 0; z0 < p.nz; z0 += 32) {
+        double c = 1.0;
+        if ((ax & 2u) && (y0 - 1 < n || y0 + kTY - 1 >= p.ny - n)) c += slab;
+        if ((ax & 4u) && (z0 - 1 < n || z0 + 31 >= p.nz - n)) c += slab;
+        const int ncpx = (ax & 1u) ? n : 0;
+        segs.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, c, (ax & 1u) ? slab : 0.0});
+      }
+  }
+}
+
+// Split of the forward work between the CPML-free kernel (variant 1) and the
+// staged-psi kernel (variant 2): a tile that reaches no y/z slab runs planes
+// ncp+1 .. nx-ncp-1 (whose x-1 prologue plane is outside the x slab too) on
+// variant 1, everything else on variant 2.
+void split_segments(const std::vector<RfxbPlan*>& plans, double slab, std::vector<WorkSeg>& plain,
+                    std::vector<WorkSeg>& cpml) {
+  for (size_t q = 0; q < plans.size(); ++q) {
+    const RfxbPlan& p = *plans[q];
+    const int n = p.inst.ncp;
+    const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
+    for (int y0 = 0; y0 < p.ny; y0 += kTY)
+      for (int z0 = 0; z0 < p.nz; z0 += 32) {
+        if (ax == 0u) {
+          plain.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, 0, 1.0, 0.0});
+          continue;
+        }
+        const int ncpx = (ax & 1u) ? n : 0;
+        const double cx = (ax & 1u) ? slab : 0.0;
+        if (tile_reaches_yz(p, y0, z0)) {
+          double c = 1.0;
+          if ((ax & 2u) && (y0 - 1 < n || y0 + kTY - 1 >= p.ny - n)) c += slab;
+          if ((ax & 4u) && (z0 - 1 < n || z0 + 31 >= p.nz - n)) c += slab;
+          cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, c, cx});
+          continue;
+        }
+        const int lo = ncpx > 0 ? ncpx + 1 : 0, hi = ncpx > 0 ? p.nx - ncpx : p.nx;
+        if (hi - lo < 4) {
+          cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, 1.0, cx});
+          continue;
+        }
+        plain.push_back(WorkSeg{(int)q, y0, z0, lo, hi, p.nx, 0, 1.0, 0.0});
+        if (lo > 0) cpml.push_back(WorkSeg{(int)q, y0, z0, 0, lo, p.nx, ncpx, 1.0, cx});
+        if (hi < p.nx) cpml.push_back(WorkSeg{(int)q, y0, z0, hi, p.nx, p.nx, ncpx, 1.0, cx});
+      }
+  }
+}
+
+void make_balanced_work(const std::vector<RfxbPlan*>& plans, int resident, double slab, double prologue,
+                        std::vector<RfxbWork>& out) {
+  std::vector<WorkSeg> segs;
+  all_segments(plans, slab, segs);
+  balance_segments(segs, resident, prologue, out);
+}
+
 // RFXB_WORK=uniform selects the plain split (one x chunk count for the group).
-bool balanced_work() {
+// RFXB_FWD_SPLIT=0 runs all forward tiles of a staged-psi group on one kernel.
+bool fwd_split_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_FWD_SPLIT");
+    v = (e && std::string(e) == "0") ? 0 : 1;
+  }
+  return v == 1;
+}
+
+// Work-list builder: 1 cost-balanced (default), 0 RFXB_WORK=uniform (one x
+// chunk count for the group), 2 RFXB_WORK=stream (x pieces of at most
+// RFXB_WORK_PLANES planes, default 24, listed piece-major and then in raster
+// order of instance, y, z, so that tiles which share halo rows are dispatched
+// together and stay within a few planes of each other: their halo reads then
+// come from L2).
+int work_mode() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("RFXB_WORK");
-    v = (e && std::string(e) == "uniform") ? 0 : 1;
+    v = (e && std::string(e) == "uniform") ? 0 : (e && std::string(e) == "stream") ? 2 : 1;
   }
-  return v == 1;
+  return v;
+}
+
+int stream_planes() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_WORK_PLANES");
+    v = e ? std::max(4, atoi(e)) : 24;
+  }
+  return v;
+}
+
+void make_stream_work(const std::vector<RfxbPlan*>& plans, int planes, std::vector<RfxbWork>& out) {
+  out.clear();
+  std::vector<int> pieces(plans.size());
+  int max_m = 0;
+  for (size_t q = 0; q < plans.size(); ++q) {
+    pieces[q] = std::max(1, (plans[q]->nx + planes / 2) / planes);
+    max_m = std::max(max_m, pieces[q]);
+  }
+  for (int m = 0; m < max_m; ++m)
+    for (size_t q = 0; q < plans.size(); ++q) {
+      const RfxbPlan& p = *plans[q];
+      if (m >= pieces[q]) continue;
+      const int xa = (int)((long long)p.nx * m / pieces[q]);
+      const int xb = (int)((long long)p.nx * (m + 1) / pieces[q]);
+      for (int y0 = 0; y0 < p.ny; y0 += kTY)
+        for (int z0 = 0; z0 < p.nz; z0 += 32) out.push_back(RfxbWork{(int)q, y0, z0, xa, xb});
+    }
 }
 
 // Forward step kernel of a mode with its dynamic shared memory enabled.
@@ -332,6 +456,22 @@ bool use_tma() {
   return v == 1;
 }
 
+// L2 sector promotion of the TMA boxes (RFXB_L2PROMO = none | 64 | 128 |
+// 256; default 128).  The boxes' halo columns cover only part of a line, so
+// promotion decides how much of the neighbour's line a halo miss drags in.
+CUtensorMapL2promotion l2_promotion() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_L2PROMO");
+    const std::string m = e ? e : "128";
+    v = m == "none" ? 0 : m == "64" ? 1 : m == "256" ? 3 : 2;
+  }
+  return v == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE
+         : v == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+         : v == 3 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+                  : CU_TENSOR_MAP_L2_PROMOTION_L2_128B;
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point, so the
 // library needs no link-time dependency on libcuda.
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -361,7 +501,7 @@ int encode_block_map(CUtensorMap* m, const RfxbPlan& p, float* block, int ncomp,
   cuuint32_t box[4] = {bx, by, 1, bc};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, addr, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return 0;
@@ -377,7 +517,7 @@ int encode_psi_map(CUtensorMap* m, float* base, long long d0, long long d1, long
   cuuint32_t box[4] = {b0, b1, 1, 2};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled (psi) failed (" + std::to_string((int)r) + ")");
   return 0;
@@ -570,8 +710,10 @@ int build_group(RfxbBatch* g) {
     min_nx = std::min(min_nx, p->nx);
   }
   g->fwd_mode = group_fwd_mode(g);
-  if (balanced_work()) {
+  if (work_mode() == 1) {
     make_balanced_work(g->plans, resident_ctas(g->fwd_mode), g->fwd_mode == 2 ? 0.4 : 1.0, 3.0, work);
+  } else if (work_mode() == 2) {
+    make_stream_work(g->plans, stream_planes(), work);
   } else {
     const int chunks = pick_chunks(tiles, min_nx, resident_ctas(g->fwd_mode));
     for (size_t q = 0; q < g->plans.size(); ++q) make_work(*g->plans[q], (int)q, chunks, work);
@@ -583,6 +725,27 @@ int build_group(RfxbBatch* g) {
     g->allocs.push_back(*ptr);
     return 0;
   };
+  // forward split (variant 2 groups, balanced lists; RFXB_FWD_SPLIT=0 keeps one list)
+  g->fwd_split = false;
+  if (g->fwd_mode == 2 && work_mode() == 1 && fwd_split_enabled()) {
+    std::vector<WorkSeg> plain, cpml;
+    split_segments(g->plans, 0.4, plain, cpml);
+    std::vector<RfxbWork> w1, w2;
+    balance_segments(plain, resident_ctas(1), 3.0, w1);
+    balance_segments(cpml, resident_ctas(2), 3.0, w2);
+    if (!w1.empty() && !w2.empty()) {
+      if (int rc = galloc((void**)&g->d_wf1, sizeof(RfxbWork) * w1.size())) return rc;
+      if (int rc = galloc((void**)&g->d_wf2, sizeof(RfxbWork) * w2.size())) return rc;
+      RFXB_CUDA(cudaMemcpy(g->d_wf1, w1.data(), sizeof(RfxbWork) * w1.size(), cudaMemcpyHostToDevice));
+      RFXB_CUDA(cudaMemcpy(g->d_wf2, w2.data(), sizeof(RfxbWork) * w2.size(), cudaMemcpyHostToDevice));
+      g->n_wf1 = (int)w1.size();
+      g->n_wf2 = (int)w2.size();
+      RFXB_CUDA(cudaStreamCreateWithFlags(&g->side_stream, cudaStreamNonBlocking));
+      RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
+      RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
+      g->fwd_split = true;
+    }
+  }
   if (int rc = galloc((void**)&g->d_inst, sizeof(RfxbInst) * g->plans.size())) return rc;
   if (int rc = galloc((void**)&g->d_adj, sizeof(AdjInst) * g->plans.size())) return rc;
   if (int rc = galloc((void**)&g->d_work, sizeof(RfxbWork) * work.size())) return rc;
@@ -665,8 +828,20 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, c
   int par = par0;
   for (int s = 0; s < n_steps; ++s) {
     const int n = step0 + s;
-    fwd_kernel(g->fwd_mode)<<<g->n_work, dim3(32, kTY), fwd_step_smem_bytes(g->fwd_mode), st>>>(
-        g->d_inst, g->d_work, g->d_maps, n, par);
+    if (g->fwd_split) {
+      // staged-psi tiles on the caller's stream, CPML-free tiles beside them
+      RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
+      RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
+      fwd_kernel(2)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps, n,
+                                                                              par);
+      fwd_kernel(1)<<<g->n_wf1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(g->d_inst, g->d_wf1,
+                                                                                          g->d_maps, n, par);
+      RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
+      RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0));
+    } else {
+      fwd_kernel(g->fwd_mode)<<<g->n_work, dim3(32, kTY), fwd_step_smem_bytes(g->fwd_mode), st>>>(
+          g->d_inst, g->d_work, g->d_maps, n, par);
+    }
     if (has_dft)
       dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, par ^ 1);
     par ^= 1;
