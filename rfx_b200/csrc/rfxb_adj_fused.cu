@@ -23,7 +23,10 @@
 //   2  TMA staging (3 planes) plus a two-slot ring that brings, one plane
 //      ahead, every adjoint psi and ce value the plane's CPML terms read, so
 //      no slab cell waits on a global load.  The host selects it when no
-//      tile reaches both slabs of an axis.
+//      tile reaches both slabs of an axis;
+//   3  TMA staging (4 planes) with the CPML code compiled out, for the
+//      tiles and x ranges whose reverse step touches no slab (the host runs
+//      them beside variant 2 or 1 on a second stream).
 #include "rfxb_common.cuh"
 
 namespace rfxb {
@@ -377,9 +380,9 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   C.ch0 = P.ch0;
   const int y0 = w.y0, z0 = w.z0;
   // the +1 neighbours of the tile (row y0+TY, column z0+32) also read CPML terms
-  C.cpx = C.ncp > 0 && (P.cpml_axes & 1u);
-  C.cpy = C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY >= C.ny - C.ncp);
-  C.cpz = C.ncp > 0 && (P.cpml_axes & 4u) && (z0 - 1 < C.ncp || z0 + 32 >= C.nz - C.ncp);
+  C.cpx = MODE != 3 && C.ncp > 0 && (P.cpml_axes & 1u);
+  C.cpy = MODE != 3 && C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY >= C.ny - C.ncp);
+  C.cpz = MODE != 3 && C.ncp > 0 && (P.cpml_axes & 4u) && (z0 - 1 < C.ncp || z0 + 32 >= C.nz - C.ncp);
   const float* aF0 = A.aF[apar][0];
   float* aFo = A.aF[apar ^ 1][0];
   const int j = y0 + ty, k = z0 + lane;
@@ -903,6 +906,8 @@ template __global__ void adj_step_kernel<8, 0>(const RfxbInst*, const AdjInst*, 
 template __global__ void adj_step_kernel<8, 1>(const RfxbInst*, const AdjInst*, const RfxbWork*,
                                                const CUtensorMap*, int, int, int, int);
 template __global__ void adj_step_kernel<8, 2>(const RfxbInst*, const AdjInst*, const RfxbWork*,
+                                               const CUtensorMap*, int, int, int, int);
+template __global__ void adj_step_kernel<8, 3>(const RfxbInst*, const AdjInst*, const RfxbWork*,
                                                const CUtensorMap*, int, int, int, int);
 
 // Dynamic shared memory of a mode: the fixed part, the plane stages it uses

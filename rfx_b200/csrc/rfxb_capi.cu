@@ -152,6 +152,12 @@ struct RfxbBatch {
   int n_wf1 = 0;
   RfxbWork* d_wf2 = nullptr;
   int n_wf2 = 0;
+  // reverse steps split the same way (list 1 on the CPML-free variant 3)
+  bool adj_split = false;
+  RfxbWork* d_wa1 = nullptr;
+  int n_wa1 = 0;
+  RfxbWork* d_wa2 = nullptr;
+  int n_wa2 = 0;
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   RfxbDftPlane* d_dft = nullptr;
@@ -348,6 +354,44 @@ void split_segments(const std::vector<RfxbPlan*>& plans, double slab, std::vecto
           continue;
         }
         const int lo = ncpx > 0 ? ncpx + 1 : 0, hi = ncpx > 0 ? p.nx - ncpx : p.nx;
+        if (hi - lo < 4) {
+          cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, 1.0, cx});
+          continue;
+        }
+        plain.push_back(WorkSeg{(int)q, y0, z0, lo, hi, p.nx, 0, 1.0, 0.0});
+        if (lo > 0) cpml.push_back(WorkSeg{(int)q, y0, z0, 0, lo, p.nx, ncpx, 1.0, cx});
+        if (hi < p.nx) cpml.push_back(WorkSeg{(int)q, y0, z0, hi, p.nx, p.nx, ncpx, 1.0, cx});
+      }
+  }
+}
+
+// The reverse step's split: its CPML terms reach rows y0-1 .. y0+TY, columns
+// z0-1 .. z0+32 and planes xa-1 .. xb, so the CPML-free range of a tile that
+// reaches no y/z slab is ncp+1 .. nx-ncp-2.
+void split_adj_segments(const std::vector<RfxbPlan*>& plans, double slab, std::vector<WorkSeg>& plain,
+                        std::vector<WorkSeg>& cpml) {
+  for (size_t q = 0; q < plans.size(); ++q) {
+    const RfxbPlan& p = *plans[q];
+    const int n = p.inst.ncp;
+    const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
+    for (int y0 = 0; y0 < p.ny; y0 += kTY)
+      for (int z0 = 0; z0 < p.nz; z0 += 32) {
+        if (ax == 0u) {
+          plain.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, 0, 1.0, 0.0});
+          continue;
+        }
+        const int ncpx = (ax & 1u) ? n : 0;
+        const double cx = (ax & 1u) ? slab : 0.0;
+        const bool yz = ((ax & 2u) && (y0 - 1 < n || y0 + kTY >= p.ny - n)) ||
+                        ((ax & 4u) && (z0 - 1 < n || z0 + 32 >= p.nz - n));
+        if (yz) {
+          double c = 1.0;
+          if ((ax & 2u) && (y0 - 1 < n || y0 + kTY >= p.ny - n)) c += slab;
+          if ((ax & 4u) && (z0 - 1 < n || z0 + 32 >= p.nz - n)) c += slab;
+          cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, c, cx});
+          continue;
+        }
+        const int lo = ncpx > 0 ? ncpx + 1 : 0, hi = ncpx > 0 ? p.nx - ncpx - 1 : p.nx;
         if (hi - lo < 4) {
           cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, 1.0, cx});
           continue;
@@ -666,23 +710,29 @@ bool adj_psi_staging_ok(const RfxbPlan& p) {
   return true;
 }
 
-// Reverse kernel variant of a group: 0 with RFXB_STAGING=cpasync, 2 when
-// every plan can stage its psi, else 1; and the ring's z-row capacity.
+// Reverse kernel variant of a group: 0 with RFXB_STAGING=cpasync, 3 without
+// any CPML, 2 when every plan can stage its psi, else 1; and the ring's
+// z-row capacity.
 void group_adj_mode(RfxbBatch* g) {
   g->adj_zp = 4;
   if (!use_tma()) { g->adj_mode = 0; return; }
   int mode = 2;
+  bool any_cpml = false;
   for (auto* p : g->plans) {
     if (!adj_psi_staging_ok(*p)) mode = 1;
+    if (p->inst.ncp > 0) any_cpml = true;
     g->adj_zp = std::max(g->adj_zp, p->inst.ncp4);
   }
-  g->adj_mode = mode;
+  g->adj_mode = any_cpml ? mode : 3;   // no CPML anywhere: the lean variant
 }
 
 using AdjKernel = void (*)(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int, int);
 AdjKernel adj_kernel(int mode) {
-  static bool init[3] = {false, false, false};
-  AdjKernel k = mode == 2 ? adj_step_kernel<kTY, 2> : mode == 1 ? adj_step_kernel<kTY, 1> : adj_step_kernel<kTY, 0>;
+  static bool init[4] = {false, false, false, false};
+  AdjKernel k = mode == 3   ? adj_step_kernel<kTY, 3>
+                : mode == 2 ? adj_step_kernel<kTY, 2>
+                : mode == 1 ? adj_step_kernel<kTY, 1>
+                            : adj_step_kernel<kTY, 0>;
   if (!init[mode]) {
     init[mode] = true;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_step_smem_bytes(mode, 16));
@@ -744,6 +794,26 @@ int build_group(RfxbBatch* g) {
       RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
       RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
       g->fwd_split = true;
+    }
+    // reverse split (used when the reverse kernel is variant 1 or 2)
+    std::vector<WorkSeg> aplain, acpml;
+    split_adj_segments(g->plans, 0.4, aplain, acpml);
+    std::vector<RfxbWork> a1, a2;
+    balance_segments(aplain, 4 * sm_count(), 3.0, a1);
+    balance_segments(acpml, 3 * sm_count(), 3.0, a2);
+    if (!a1.empty() && !a2.empty()) {
+      if (int rc = galloc((void**)&g->d_wa1, sizeof(RfxbWork) * a1.size())) return rc;
+      if (int rc = galloc((void**)&g->d_wa2, sizeof(RfxbWork) * a2.size())) return rc;
+      RFXB_CUDA(cudaMemcpy(g->d_wa1, a1.data(), sizeof(RfxbWork) * a1.size(), cudaMemcpyHostToDevice));
+      RFXB_CUDA(cudaMemcpy(g->d_wa2, a2.data(), sizeof(RfxbWork) * a2.size(), cudaMemcpyHostToDevice));
+      g->n_wa1 = (int)a1.size();
+      g->n_wa2 = (int)a2.size();
+      if (!g->side_stream) {
+        RFXB_CUDA(cudaStreamCreateWithFlags(&g->side_stream, cudaStreamNonBlocking));
+        RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
+        RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
+      }
+      g->adj_split = true;
     }
   }
   if (int rc = galloc((void**)&g->d_inst, sizeof(RfxbInst) * g->plans.size())) return rc;
@@ -1007,7 +1077,18 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
         adj_pass_a<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
         adj_pass_b<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
       } else {
-        akern<<<g->n_work, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar, zp);
+        if (g->adj_split && amode != 0) {
+          RFXB_CUDA(cudaEventRecord(g->ev_fork, cs));
+          RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
+          akern<<<g->n_wa2, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2, g->d_maps, s, par, fpar, zp);
+          adj_kernel(3)<<<g->n_wa1, dim3(32, kTY), adj_step_smem_bytes(3, zp), g->side_stream>>>(
+              g->d_inst, g->d_adj, g->d_wa1, g->d_maps, s, par, fpar, zp);
+          RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
+          RFXB_CUDA(cudaStreamWaitEvent(cs, g->ev_join, 0));
+        } else {
+          akern<<<g->n_work, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar,
+                                                         zp);
+        }
         fpar ^= 1;
       }
       par ^= 1;

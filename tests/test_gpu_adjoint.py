@@ -36,7 +36,14 @@ def _runner(sc, box, mode="history", K=None):
                          mode=mode, checkpoint_every=K)
 
 
-@pytest.mark.parametrize("build", [small_uniform, small_nonuniform, medium_uniform])
+def _small_uniform_pec(n_steps=150):
+    """small_uniform with PEC faces instead of CPML (the CPML-free reverse
+    kernel)."""
+    import dataclasses
+    return dataclasses.replace(small_uniform(n_steps=n_steps), boundary="pec")
+
+
+@pytest.mark.parametrize("build", [small_uniform, small_nonuniform, medium_uniform, _small_uniform_pec])
 def test_adjoint_is_exact_transpose(cuda, build):
     sc = build(n_steps=150)
     box = (14, 18, 14, 18, 12, 14) if sc.lane == "uniform" else (12, 16, 12, 16, 11, 13)
@@ -47,8 +54,10 @@ def test_adjoint_is_exact_transpose(cuda, build):
     J = float((g.double() * ts.double()).sum())
     _, src_adj = r.backward(g)
     J_adj = float((src_adj.double() * r.src_table.double()).sum())
-    print(sc.name, "J", J, "via adjoint", J_adj)
+    print(sc.name, sc.boundary, "J", J, "via adjoint", J_adj, "reverse variant", r.plan.adjoint_variant())
     assert abs(J - J_adj) <= 2e-5 * abs(J)
+    if sc.boundary == "pec":
+        assert r.plan.adjoint_variant() == 3
     r.close()
 
 
