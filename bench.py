@@ -343,6 +343,105 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# secondary workloads (the other configurations, on request)
+# ---------------------------------------------------------------------------
+
+def run_secondary(args, which):
+    """One device-timed line for the large uniform, graded or adjoint
+    configuration: each bench step runs the configuration's full step count."""
+    import torch
+
+    from rfx_b200 import workloads
+    from rfx_b200.grid import face_pads
+    from rfx_b200.simulation import MaterialArrays, init_dft_plane_probe, prepare_device_run
+
+    torch.cuda.set_device(0)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    N = args.time_steps
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    if which in ("large_uniform", "graded"):
+        if which == "large_uniform":
+            g, eps, sig, src, probes, dft = workloads.large_uniform(n_steps=N)
+            pec, axes, offset = None, "xyz", 1
+            desc = ("large_uniform: 256^3 interior dx 1 mm + CPML 10 -> 277^3, 32 seeded boxes, Ez pulse 10 GHz, "
+                    "8 probes, z-plane DFT at 16 frequencies")
+        else:
+            g, eps, sig, pec, src, probes, dft = workloads.graded(n_steps=N)
+            pads = face_pads(g)
+            axes = "".join(a for a, (lo, hi) in zip("xyz", (pads[0:2], pads[2:4], pads[4:6])) if lo + hi > 0)
+            offset = 0
+            desc = ("graded: 192 x 192 x 96 cells, z graded 0.1-0.5 mm, CPML 12 -> 217 x 217 x 121, PEC sheet, "
+                    "substrate, Ex pulse 20 GHz, 4 probes, DFT plane at 8 frequencies")
+        planes = [init_dft_plane_probe(a, ix, c, f, g.shape) for (a, ix, c, f) in dft]
+        mats = MaterialArrays(eps, sig, np.ones_like(eps))
+        r = prepare_device_run(g, mats, N, cpml_axes=axes, pec_axes="xyz", sources=src,
+                               probes=[p[:4] for p in probes], dft_planes=planes, pec_mask=pec,
+                               dft_time_offset=offset)
+        plan = r.plan
+        cells = int(np.prod(g.shape))
+
+        def one():
+            plan.reset()
+            for a in r.dft_accs:
+                a.zero_()
+            plan.advance(0, N, r.src_table, r.probe_out, r.dft_accs, r.dft_phases)
+
+        dft_bytes = sum(32 * len(d.freqs) * int(np.prod(a.shape[1:])) for d, a in zip(planes, r.dft_accs))
+        alg = plan.algorithmic_bytes_per_step() + dft_bytes
+        metric = "Mcell-steps/s forward, 1 B200"
+        kernel = "fwd_step_kernel + dft_kernel (whole step)"
+    else:
+        from rfx_b200.adjoint import AdjointRunner, probe_dft_objective
+        g, eps, sig, src, probes, box, freqs = workloads.adjoint_region(n_steps=N)
+        runner = AdjointRunner(g, MaterialArrays(eps, sig, np.ones_like(eps)), N, sources=src, probes=probes, box=box,
+                               boundary="cpml", cpml_axes="xyz", pec_axes="xyz", mode="segments",
+                               checkpoint_every=64)
+        plan = runner.plan
+        cells = int(np.prod(g.shape))
+        desc = ("adjoint_region: 200 x 120 x 48 at 0.5 mm + CPML 10 -> 221 x 141 x 69, design 64 x 64 x 2, "
+                "Ez pulse 15 GHz, 4 probes, objective over 5 frequencies, checkpoint every 64 steps")
+
+        def one():
+            ts = runner.forward()
+            t = ts.detach().clone().requires_grad_(True)
+            probe_dft_objective(t, freqs, float(g.dt)).backward()
+            runner.backward(t.grad.to(torch.float32).contiguous())
+
+        # forward + segment recompute + reverse step, each ~ one forward's bytes
+        alg = 3 * plan.algorithmic_bytes_per_step()
+        metric = "Mcell-steps/s fwd+adjoint grad (checkpoint every 64), 1 B200"
+        kernel = "fwd_step_kernel x2 + adj_step_kernel (whole step)"
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        ev[0].record()
+        for _ in range(args.steps):
+            one()
+        ev[1].record()
+        torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1])
+    variant = {"forward": plan.forward_variant(), "reverse": plan.adjoint_variant()}
+    step_s = ms / 1e3 / (args.steps * N)
+    achieved = alg / step_s / 1e9
+    line = {"metric": metric, "value": round(cells * N * args.steps / (ms / 1e3) / 1e6, 1), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": desc, "time_steps": N, "cells": cells, "kernel_variants": variant,
+                       "l2": "inputs larger than L2"},
+            "roofline": {"kernel": kernel, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                         "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "peak_source": peak_src,
+                         "traffic": None, "algorithmic_bytes_per_step": int(alg)},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    plan.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -356,11 +455,21 @@ def main():
     ap.add_argument("--no-single", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="batched_sweep",
+                    choices=["batched_sweep", "large_uniform", "graded", "adjoint_region"],
+                    help="batched_sweep is the headline line; the others print a secondary forward (or "
+                         "forward+adjoint) line for the other configurations")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
-    if args.impl == "reference":
+    if args.workload != "batched_sweep":
+        if args.impl == "reference" or world > 1:
+            raise SystemExit("secondary workloads run on our arm at one GPU only")
+        if "--time-steps" not in sys.argv:
+            args.time_steps = {"large_uniform": 4000, "graded": 6000, "adjoint_region": 3000}[args.workload]
+        run_secondary(args, args.workload)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_ours(args, rank, world, local_rank)

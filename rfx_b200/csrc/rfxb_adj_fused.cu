@@ -639,11 +639,14 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       };
       re_fill(ly, lh, own);
       constexpr int W = RFXB_TZ + 2;
-      if (tid < 2 * W + 2 * TY) {
-        if (tid < W) re_fill(0, tid, false);
-        else if (tid < 2 * W) re_fill(TY + 1, tid - W, false);
-        else if (tid < 2 * W + TY) re_fill(tid - 2 * W + 1, 0, false);
-        else re_fill(tid - 2 * W - TY + 1, W - 1, false);
+      // the extra cells go to the last warps (warps 0 and 1 carry the phase-A
+      // halo row and column, the middle warps the phase-B extras)
+      const int t = tid - (32 * TY - (2 * W + 2 * TY));
+      if (t >= 0) {
+        if (t < W) re_fill(0, t, false);
+        else if (t < 2 * W) re_fill(TY + 1, t - W, false);
+        else if (t < 2 * W + TY) re_fill(t - 2 * W + 1, 0, false);
+        else re_fill(t - 2 * W - TY + 1, W - 1, false);
       }
       __syncthreads();
     }
@@ -799,8 +802,9 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         S.rx[3][r][c] = v3;
       };
       rh_fill(ly, lh, own, true, true);
-      if (tid < RFXB_TZ) rh_fill(0, tid + 1, false, true, false);                          // row y0-1: y relations
-      else if (tid < RFXB_TZ + TY) rh_fill(tid - RFXB_TZ + 1, 0, false, false, true);      // column z0-1: z relations
+      const int t = tid - 64;   // warps 2 and 3
+      if (t >= 0 && t < RFXB_TZ) rh_fill(0, t + 1, false, true, false);                     // row y0-1: y relations
+      else if (t >= RFXB_TZ && t < RFXB_TZ + TY) rh_fill(t - RFXB_TZ + 1, 0, false, false, true);   // column z0-1
       __syncthreads();
     }
 

@@ -162,10 +162,22 @@ def _to_np(a, dtype=np.float32):
     return np.asarray(a, dtype=dtype)
 
 
-def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
-               dft_time_offset, lumped_specs=(), return_state=True, report_every=None, report_label="",
-               kappa_max=None, noop_faces=(), device=None):
-    """Shared driver of the uniform and graded lanes."""
+class DeviceRun(NamedTuple):
+    """A prepared device run: the plan with materials set and state reset,
+    and the device tables its steps read and write."""
+    plan: object
+    src_table: object          # (n_steps, n_src) float32 or None
+    probe_out: object          # (n_steps, n_probe) float32 or None
+    dft_accs: list             # complex64 accumulators per DFT plane
+    dft_phases: list           # (n_steps, n_f) phase tables per plane
+    probes: list               # probe tuples (user probes first, then port V/I probes)
+    vi_rows: list              # per lumped port: [(probe row, sign), ...]
+
+
+def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
+                       dft_time_offset, lumped_specs=(), kappa_max=None, noop_faces=(), device=None) -> DeviceRun:
+    """Build the plan of one simulation and upload its inputs (the set-up half
+    of ``run_device``); the caller owns the plan and closes it."""
     dev = require_cuda(device)
     shape = tuple(int(v) for v in grid.shape)
     n_steps = int(n_steps)
@@ -199,11 +211,27 @@ def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes
         for d in dft_planes:
             accs.append(torch.from_numpy(np.ascontiguousarray(np.asarray(d.accumulator, np.complex64))).to(dev))
             phases.append(torch.from_numpy(dft_phase_table(d.freqs, n_steps, grid.dt, dft_time_offset)).to(dev))
+    except BaseException:
+        plan.close()
+        raise
+    return DeviceRun(plan, src_table, probe_out, accs, phases, prb, vi_rows)
+
+
+def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
+               dft_time_offset, lumped_specs=(), return_state=True, report_every=None, report_label="",
+               kappa_max=None, noop_faces=(), device=None):
+    """Shared driver of the uniform and graded lanes."""
+    n_steps = int(n_steps)
+    r = prepare_device_run(grid, materials, n_steps, cpml_axes=cpml_axes, pec_axes=pec_axes, sources=sources,
+                           probes=probes, dft_planes=dft_planes, pec_mask=pec_mask, dft_time_offset=dft_time_offset,
+                           lumped_specs=lumped_specs, kappa_max=kappa_max, noop_faces=noop_faces, device=device)
+    plan, probe_out, accs = r.plan, r.probe_out, r.dft_accs
+    try:
         chunk = int(report_every) if report_every else n_steps
         done = 0
         while done < n_steps:
             k = min(chunk, n_steps - done)
-            plan.advance(done, k, src_table, probe_out, accs, phases)
+            plan.advance(done, k, r.src_table, probe_out, accs, r.dft_phases)
             done += k
             if report_every:
                 torch.cuda.current_stream().synchronize()
@@ -215,10 +243,10 @@ def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes
         lumped = None
         if lumped_specs:
             lumped = []
-            for spec, rows in zip(lumped_specs, vi_rows):
+            for spec, rows in zip(lumped_specs, r.vi_rows):
                 dx = float(grid.dx)
                 v = ts_all[:, rows[0][0]].astype(np.float64) * rows[0][1] * dx
-                iv = sum(ts_all[:, r].astype(np.float64) * s for r, s in rows[1:]) * dx
+                iv = sum(ts_all[:, q].astype(np.float64) * sg for q, sg in rows[1:]) * dx
                 lumped.append((spec, _vi_dft(v, iv, spec.freqs, float(grid.dt))))
             lumped = tuple(lumped)
         state = None
