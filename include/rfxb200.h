@@ -219,6 +219,12 @@ int rfxb_batch_device_status(RfxbBatch* batch, void* stream);
 int rfxb_forward_noalloc(const RfxbDesc* desc, const float* eps_r_dev, const float* sigma_dev,
                          float* const* fields_dev, const RfxbStepIO* io, int step0, int n_steps, void* stream);
 
+/* Sum of E^2 + H^2 over the cells box[0] <= i < box[1], box[2] <= j < box[3],
+ * box[4] <= k < box[5] of the plan's current state, written (float64,
+ * overwritten) to *energy_dev in stream order: the interior-energy check of
+ * run_until_decay (rfx/simulation.py:2493-2505). */
+int rfxb_plan_box_energy(RfxbPlan* plan, const int* box, double* energy_dev, void* stream);
+
 /* Bytes of device memory a plan holds (state, coefficients, psi, history,
  * checkpoints). */
 int64_t rfxb_plan_device_bytes(const RfxbPlan* plan);

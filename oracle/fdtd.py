@@ -509,7 +509,7 @@ def _plane(a, axis, index):
 
 
 def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
-         probes_before_dft, dx_vi):
+         probes_before_dft, dx_vi, stop=None):
     f = st.f
     cdt = np.complex64 if f == np.float32 else np.complex128
     ts = np.zeros((n_steps, len(probes)), f)
@@ -563,6 +563,10 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
         else:
             _dft()
             _probes()
+        if stop is not None and stop(n, F):
+            ts = ts[:n + 1]
+            vi = vi[:n + 1] if vi is not None else None
+            break
     return OracleResult(ts, accs, {c: st.F[c].copy() for c in COMPONENTS}, vi, st.psi)
 
 
@@ -598,3 +602,50 @@ def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_plane
                   exact_materials=exact_materials)
     return _run(st, n_steps, sources, probes, dft_planes, (), 0,
                 probes_before_dft=False, dx_vi=grid.dx)
+
+
+def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100,
+                            max_steps=50_000, decay_energy_consecutive=2, monitor=None, boundary="pec",
+                            cpml_axes="xyz", pec_axes=None, sources=(), probes=(), pec_mask=None,
+                            dtype=np.float32):
+    """``rfx.simulation.run_until_decay`` (rfx/simulation.py:2198-2700), energy
+    and point-field stops only.  Absorbing boundary: at step n with n+1 >=
+    min_steps and n % check_interval == 0 the interior energy
+    U = sum(E^2 + H^2) over the non-CPML slice (:2493-2505, summed here in
+    float64) updates its running peak, and ``decay_energy_consecutive``
+    consecutive checks with U < decay_by * peak stop the run (:2603-2622).
+    Closed boundary: the squared field at ``monitor`` = (i, j, k, comp)
+    (after the step's source injection) keeps a running peak every step, and a
+    check step with value^2 < decay_by * peak stops (:2623-2633).
+    Returns (OracleResult, steps run)."""
+    if pec_axes is None:
+        pec_axes = "xyz"
+    absorbing = boundary == "cpml"
+    st = _Stepper(grid, materials, dtype=dtype, nonuniform=False,
+                  cpml_axes=cpml_axes if absorbing else "",
+                  pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=1.0)
+    p = grid.pads
+    sl = (slice(p[0], grid.nx - p[1]), slice(p[2], grid.ny - p[3]), slice(p[4], grid.nz - p[5]))
+    state = {"peak_U": 0.0, "below": 0, "peak_sq": 0.0, "steps": 0}
+
+    def stop(n, F):
+        state["steps"] = n + 1
+        if absorbing:
+            if n + 1 >= min_steps and n % check_interval == 0:
+                U = float(sum(np.sum(np.asarray(F[c][sl], np.float64) ** 2) for c in COMPONENTS))
+                state["peak_U"] = max(state["peak_U"], U)
+                if U < decay_by * state["peak_U"]:
+                    state["below"] += 1
+                    if state["below"] >= decay_energy_consecutive:
+                        return True
+                else:
+                    state["below"] = 0
+            return False
+        i, j, k, comp = monitor
+        v2 = float(F[comp][i, j, k]) ** 2
+        state["peak_sq"] = max(state["peak_sq"], v2)
+        return (n + 1 >= min_steps and n % check_interval == 0 and state["peak_sq"] > 0.0
+                and v2 < decay_by * state["peak_sq"])
+
+    res = _run(st, max_steps, sources, probes, (), (), 1, probes_before_dft=True, dx_vi=grid.dx, stop=stop)
+    return res, state["steps"]

@@ -11,7 +11,7 @@ reverse-time adjoint and the batched sweep.
 from .grid import Grid, NonUniformGrid, make_nonuniform_grid  # noqa: F401
 from .simulation import (  # noqa: F401
     DFTPlaneProbe, FDTDState, LumpedPortSParamSpec, MaterialArrays, ProbeSpec, SimResult,
-    extract_lumped_s11, init_dft_plane_probe, run,
+    extract_lumped_s11, init_dft_plane_probe, run, run_until_decay,
 )
 from .sources import (  # noqa: F401
     GaussianPulse, LumpedPort, SourceSpec, make_current_source, make_j_source, make_port_source,

@@ -59,6 +59,7 @@ struct __align__(128) AdjStage {
   float ah[3][TY + 1][RFXB_AHW];   // adjoint H, rows y0-1 .. y0+TY-1, z from z0-4
   float p2[AdjDims<TY>::P2];
   float ca[TY][RFXB_TZ];           // ca of the tile
+  unsigned char em[TY][RFXB_TZ];   // PEC edge-mask bits of the tile (staged only when the plan has a mask)
 };
 
 // The plane stages come last so that a kernel using fewer of them (mode 2)
@@ -275,7 +276,9 @@ __device__ __forceinline__ void adj_tma_stage(AdjSmem<TY>& S, const CUtensorMap*
                                               int ip) {
   const int s = astage_of<NST>(ip);
   const uint32_t mb = smem_u32(&S.mbar[s]);
-  mbar_expect_tx(mb, AdjDims<TY>::BYTES);
+  const bool em = S.P.emask != nullptr;
+  mbar_expect_tx(mb, AdjDims<TY>::BYTES + (em ? (unsigned)(TY * RFXB_TZ) : 0u));
+  if (em) tma_load_4d(smem_u32(&S.st[s].em[0][0]), tm + RFXB_MAP_EMASK, z0, y0 + 1, ip + 1, 0, mb);
   tma_load_4d(smem_u32(&S.st[s].ae[0][0][0]), tm + 5 + apar, z0 - 4, y0, ip + 1, 0, mb);
   tma_load_4d(smem_u32(&S.st[s].cbp[0][0]), tm + 9, z0 - 4, y0, ip + 1, 1, mb);
   tma_load_4d(smem_u32(&S.st[s].ah[0][0][0]), tm + 7 + apar, z0 - 4, y0, ip + 1, 3, mb);
@@ -885,7 +888,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       if (pec_k0) { ax = 0.f; ay = 0.f; }
       if (pec_kz) az = 0.f;
       if (P.emask) {
-        const unsigned m = P.emask[e];
+        const unsigned m = TMA ? (unsigned)X.em[ty][lane] : (unsigned)P.emask[e];
         if (m & 1u) ax = 0.f;
         if (m & 2u) ay = 0.f;
         if (m & 4u) az = 0.f;

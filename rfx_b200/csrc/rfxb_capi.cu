@@ -21,7 +21,7 @@
 #include "rfxb_common.cuh"
 
 namespace rfxb {
-template <int TY, int MODE>
+template <int TY, int MODE, bool EM>
 __global__ void fwd_step_kernel(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
 size_t fwd_step_smem_bytes(int mode);
 __global__ void dft_kernel(const RfxbInst*, const RfxbDftPlane*, int, int, int);
@@ -32,6 +32,7 @@ __global__ void coef_kernel(RfxbInst, float*, float*, float*, float*, const floa
 __global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
+__global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
 template <int TY, int MODE>
 __global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int,
                                 int);
@@ -466,11 +467,14 @@ void make_stream_work(const std::vector<RfxbPlan*>& plans, int planes, std::vect
 
 // Forward step kernel of a mode with its dynamic shared memory enabled.
 using FwdKernel = void (*)(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
-FwdKernel fwd_kernel(int mode) {
-  static bool init[3] = {false, false, false};
-  FwdKernel k = mode == 2 ? fwd_step_kernel<kTY, 2> : mode == 1 ? fwd_step_kernel<kTY, 1> : fwd_step_kernel<kTY, 0>;
-  if (!init[mode]) {
-    init[mode] = true;
+FwdKernel fwd_kernel(int mode, bool em = false) {
+  static bool init[3][2] = {{false, false}, {false, false}, {false, false}};
+  em = em && mode != 0;
+  FwdKernel k = mode == 2 ? (em ? fwd_step_kernel<kTY, 2, true> : fwd_step_kernel<kTY, 2, false>)
+                : mode == 1 ? (em ? fwd_step_kernel<kTY, 1, true> : fwd_step_kernel<kTY, 1, false>)
+                            : fwd_step_kernel<kTY, 0, false>;
+  if (!init[mode][em]) {
+    init[mode][em] = true;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_step_smem_bytes(mode));
   }
   return k;
@@ -548,6 +552,24 @@ int encode_block_map(CUtensorMap* m, const RfxbPlan& p, float* block, int ncomp,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return 0;
+}
+
+// Map over the padded PEC edge-mask bytes: dims (zs, ny+2, nx+2, 1) with the
+// origin at cell (-1, -1, 0), the tile box (32, TY, 1, 1).
+int encode_emask_map(RfxbPlan* p) {
+  auto fn = tensor_map_encoder();
+  if (!fn) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled is not available from the driver");
+  const RfxbInst& I = p->inst;
+  void* addr = p->emask + (I.off0 - I.ps - I.zs);
+  cuuint64_t dims[4] = {(cuuint64_t)I.zs, (cuuint64_t)(p->ny + 2), (cuuint64_t)(p->nx + 2), 1};
+  cuuint64_t strides[3] = {(cuuint64_t)I.zs, (cuuint64_t)I.ps, (cuuint64_t)I.ps * (cuuint64_t)(p->nx + 2)};
+  cuuint32_t box[4] = {32, (cuuint32_t)kTY, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = fn(&p->tmaps[RFXB_MAP_EMASK], CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, addr, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled (edge mask) failed (" + std::to_string((int)r) + ")");
   return 0;
 }
 
@@ -896,20 +918,22 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
 
 int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, cudaStream_t st) {
   int par = par0;
+  bool em = false;   // stage the PEC edge masks when a plan of the group has one
+  for (auto* p : g->plans) em = em || p->inst.emask != nullptr;
   for (int s = 0; s < n_steps; ++s) {
     const int n = step0 + s;
     if (g->fwd_split) {
       // staged-psi tiles on the caller's stream, CPML-free tiles beside them
       RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
       RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
-      fwd_kernel(2)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps, n,
+      fwd_kernel(2, em)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps, n,
                                                                               par);
-      fwd_kernel(1)<<<g->n_wf1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(g->d_inst, g->d_wf1,
+      fwd_kernel(1, em)<<<g->n_wf1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(g->d_inst, g->d_wf1,
                                                                                           g->d_maps, n, par);
       RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
       RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0));
     } else {
-      fwd_kernel(g->fwd_mode)<<<g->n_work, dim3(32, kTY), fwd_step_smem_bytes(g->fwd_mode), st>>>(
+      fwd_kernel(g->fwd_mode, em)<<<g->n_work, dim3(32, kTY), fwd_step_smem_bytes(g->fwd_mode), st>>>(
           g->d_inst, g->d_work, g->d_maps, n, par);
     }
     if (has_dft)
@@ -1311,6 +1335,7 @@ int rfxb_plan_set_materials(RfxbPlan* p, const float* eps_r, const float* sigma,
   if (edge_mask && !p->emask) {
     if (int rc = p->alloc(&p->emask, p->elems)) return rc;
     RFXB_CUDA(cudaMemsetAsync(p->emask, 0, p->elems, st));
+    if (int rc = encode_emask_map(p)) return rc;
   }
   p->inst.emask = edge_mask ? p->emask : nullptr;
   const long long cells = (long long)p->nx * p->ny * p->nz;
@@ -1518,6 +1543,20 @@ int rfxb_batch_device_status(RfxbBatch* g, void* stream) {
   int v = 0;
   RFXB_CUDA(cudaMemcpy(&v, g->d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (v) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
+  return 0;
+}
+
+int rfxb_plan_box_energy(RfxbPlan* p, const int* b, double* out, void* stream) {
+  if (!p || !b || !out) return fail(RFXB_E_INVALID, "plan, box and output are required");
+  if (b[0] < 0 || b[1] > p->nx || b[2] < 0 || b[3] > p->ny || b[4] < 0 || b[5] > p->nz || b[0] >= b[1] ||
+      b[2] >= b[3] || b[4] >= b[5])
+    return fail(RFXB_E_INVALID, "energy box out of range or empty");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  RFXB_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+  const long long cells = (long long)(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]);
+  const int blocks = (int)std::max<long long>(1, std::min<long long>((cells + 255) / 256, 8LL * sm_count()));
+  box_energy_kernel<<<blocks, 256, 0, st>>>(p->inst, p->par, b[0], b[1], b[2], b[3], b[4], b[5], out);
+  RFXB_CUDA(cudaGetLastError());
   return 0;
 }
 

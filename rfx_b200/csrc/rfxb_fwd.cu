@@ -55,6 +55,7 @@ struct __align__(128) FwdStage {
   float h[3][TY + 1][RFXB_HW];   // hx hy hz (H^{n-1/2}), rows y0-1 .. y0+TY-1
   float ph[FwdStageDims<TY>::PH];
   float cab[2][TY][RFXB_TZ];     // ca cb, rows y0 .. y0+TY-1, z from z0
+  unsigned char em[TY][RFXB_TZ]; // PEC edge-mask bits of the tile (staged only when the plan has a mask)
 };
 
 template <int TY>
@@ -317,11 +318,12 @@ __device__ __forceinline__ void load_stage(FwdSmem<TY>& S, const FwdCtx& C, cons
 // Issue the TMA boxes of plane ip into its stage (one thread).  Tensor maps of
 // an instance: [0|1] field block of parity 0|1 with the E box, [2|3] the same
 // with the H box, [4] the coefficient block with the ca/cb box.
-template <int TY>
+template <int TY, bool EM>
 __device__ __forceinline__ void tma_stage(FwdSmem<TY>& S, const CUtensorMap* tm, int par, int y0, int z0, int ip) {
   const int s = stage_of(ip);
   const uint32_t mb = smem_u32(&S.mbar[s]);
-  mbar_expect_tx(mb, FwdStageDims<TY>::BYTES);
+  mbar_expect_tx(mb, FwdStageDims<TY>::BYTES + (EM ? (unsigned)(TY * RFXB_TZ) : 0u));
+  if (EM) tma_load_4d(smem_u32(&S.st[s].em[0][0]), tm + RFXB_MAP_EMASK, z0, y0 + 1, ip + 1, 0, mb);
   tma_load_4d(smem_u32(&S.st[s].e[0][0][0]), tm + par, z0 - 4, y0, ip + 1, 0, mb);
   tma_load_4d(smem_u32(&S.st[s].h[0][0][0]), tm + 2 + par, z0 - 4, y0, ip + 1, 3, mb);
   tma_load_4d(smem_u32(&S.st[s].cab[0][0][0]), tm + 4, z0, y0 + 1, ip + 1, 0, mb);
@@ -376,7 +378,9 @@ struct FwdBounds { static constexpr int MIN_CTAS = 4; };
 template <>
 struct FwdBounds<2> { static constexpr int MIN_CTAS = 3; };
 
-template <int TY, int MODE>
+// EM: the launch's plans have PEC edge masks, staged by TMA with the planes
+// (TMA modes); without EM the mask (if any) is read from global memory.
+template <int TY, int MODE, bool EM>
 __global__ void __launch_bounds__(32 * TY, FwdBounds<MODE>::MIN_CTAS)
 fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work,
                 const CUtensorMap* __restrict__ maps, int n, int par) {
@@ -502,7 +506,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   };
   if (TMA) {
     if (tid == 0) {
-      for (int p = xa - 1; p <= min(xa + 2, C.nx); ++p) tma_stage<TY>(S, tm, par, y0, z0, p);
+      for (int p = xa - 1; p <= min(xa + 2, C.nx); ++p) tma_stage<TY, EM>(S, tm, par, y0, z0, p);
     }
     psi_fill(xa - 1);
     psi_fill(xa);
@@ -563,7 +567,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
       // psi slot takes plane i+1
       const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), stage_parity(i + 1, xa)) && psi_wait(i);
       if (__syncthreads_or(!ok)) { bail(min(i + 2, C.nx), i + 1); return; }
-      if (tid == 0 && i + 3 <= C.nx) tma_stage<TY>(S, tm, par, y0, z0, i + 3);
+      if (tid == 0 && i + 3 <= C.nx) tma_stage<TY, EM>(S, tm, par, y0, z0, i + 3);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
@@ -787,7 +791,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
       if (pec_k0) { ex = 0.f; ey = 0.f; }
       if (pec_kz) ez = 0.f;
       if (has_emask) {
-        const unsigned m = P.emask[e];
+        const unsigned m = (TMA && EM) ? (unsigned)A.em[ty][lane] : (unsigned)P.emask[e];
         if (m) {
           ex = ex * (1.f - (float)(m & 1u));
           ey = ey * (1.f - (float)((m >> 1) & 1u));
@@ -929,9 +933,14 @@ __global__ void coef_kernel(RfxbInst P, float* ca, float* cb, float* ce, float* 
 }
 
 // Explicit template instantiations used by the host side.
-template __global__ void fwd_step_kernel<8, 0>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
-template __global__ void fwd_step_kernel<8, 1>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
-template __global__ void fwd_step_kernel<8, 2>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+template __global__ void fwd_step_kernel<8, 0, false>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int,
+                                                      int);
+template __global__ void fwd_step_kernel<8, 1, false>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int,
+                                                      int);
+template __global__ void fwd_step_kernel<8, 1, true>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+template __global__ void fwd_step_kernel<8, 2, false>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int,
+                                                      int);
+template __global__ void fwd_step_kernel<8, 2, true>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
 
 size_t fwd_step_smem_bytes(int mode) { return fwd_smem_bytes<8>(mode); }
 

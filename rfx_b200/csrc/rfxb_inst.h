@@ -28,8 +28,9 @@
 // coefficient with the H box; then the adjoint psi of parity 0|1: [24|25]
 // E-side x (H box), [26|27] E-side y (E box), [28|29] E-side z (E rows),
 // [30|31] H-side x (tile box), [32|33] H-side y (H box), [34|35] H-side z
-// (H rows).
-#define RFXB_NMAPS 36
+// (H rows); [36] the PEC edge-mask bytes with the tile box.
+#define RFXB_NMAPS 37
+#define RFXB_MAP_EMASK 36   // PEC edge mask bytes with the tile box
 #define RFXB_MAP_PSH 11
 #define RFXB_MAP_PSE 17
 #define RFXB_MAP_APE 24

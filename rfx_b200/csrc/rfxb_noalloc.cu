@@ -34,7 +34,7 @@
 #include "rfxb_common.cuh"
 
 namespace rfxb {
-template <int TY, int MODE>
+template <int TY, int MODE, bool EM>
 __global__ void fwd_step_kernel(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
 size_t fwd_step_smem_bytes(int mode);
 __global__ void pack_kernel(float*, const float*, RfxbInst);
@@ -278,7 +278,7 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   const RfxbWork* dW = reinterpret_cast<const RfxbWork*>(base + o_work);
   int par = 0;
   for (int s = 0; s < n_steps; ++s) {
-    fwd_step_kernel<TY, 0><<<(unsigned)n_work, dim3(32, TY), fwd_step_smem_bytes(0), st>>>(dI, dW, nullptr, step0 + s,
+    fwd_step_kernel<TY, 0, false><<<(unsigned)n_work, dim3(32, TY), fwd_step_smem_bytes(0), st>>>(dI, dW, nullptr, step0 + s,
                                                                                            par);
     par ^= 1;
   }

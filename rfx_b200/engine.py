@@ -191,6 +191,16 @@ class Plan:
     def device_bytes(self) -> int:
         return int(self._lib.rfxb_plan_device_bytes(self._h))
 
+    def box_energy(self, box, out=None):
+        """Device scalar (float64 tensor) of sum(E^2 + H^2) over ``box`` =
+        (i0, i1, j0, j1, k0, k1) of the current state, in stream order."""
+        if out is None:
+            out = torch.empty((), device=self.device, dtype=torch.float64)
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        check(self._lib.rfxb_plan_box_energy(self._h, b, C.c_void_p(out.data_ptr()), _stream()),
+              "rfxb_plan_box_energy")
+        return out
+
     def forward_variant(self) -> int:
         """0 generic step kernel, 1 TMA staging without CPML, 2 TMA staging
         with TMA-staged CPML psi."""

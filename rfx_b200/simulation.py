@@ -312,6 +312,109 @@ def run(grid, materials, n_steps, *, boundary="pec", cpml_axes="xyz", pec_axes=N
                      lumped_port_sparams=lumped, grid=grid)
 
 
+def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100, max_steps=50_000,
+                    decay_energy_consecutive=2, radiated_flux_box=None, flux_env_checks=4, monitor_component="ez",
+                    monitor_position=None, boundary="pec", cpml_axes="xyz", pec_axes=None, periodic=None,
+                    debye=None, lorentz=None, tfsf=None, sources=None, probes=None, dft_planes=None,
+                    flux_monitors=None, waveguide_ports=None, ntff=None, snapshot=None, checkpoint=False,
+                    aniso_eps=None, aniso_inv_eps=None, aniso_inv_eps_smooth=False, pec_mask=None,
+                    pec_occupancy=None, conformal_weights=None, wire_port_sparams=None, lumped_port_sparams=None,
+                    lumped_rlc=None, kerr_chi3=None, field_dtype=None, return_state=True, mag_sources=None,
+                    checkpoint_segments=None, stencil_order=2, report_every=None, report_label="",
+                    sheet_impedance=None, device=None) -> SimResult:
+    """Run until the field energy decays (rfx/simulation.py:2198-2700).
+
+    Absorbing boundary: every ``check_interval`` steps (once ``min_steps`` are
+    done) the interior energy U = sum(E^2 + H^2) over the non-CPML slice is
+    reduced on the device (float64 accumulation); the run stops after
+    ``decay_energy_consecutive`` consecutive checks with U < decay_by * peak U.
+    Closed boundary: the squared field ``monitor_component`` at
+    ``monitor_position`` (default: the domain centre) keeps a running peak
+    over every step, and a check step with value^2 < decay_by * peak stops.
+    The steps run between checks are replayed as one captured chunk."""
+    _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf, flux_monitors=flux_monitors,
+                 waveguide_ports=waveguide_ports, ntff=ntff, aniso_eps=aniso_eps, aniso_inv_eps=aniso_inv_eps,
+                 pec_occupancy=pec_occupancy, conformal_weights=conformal_weights,
+                 wire_port_sparams=wire_port_sparams, lumped_port_sparams=lumped_port_sparams,
+                 lumped_rlc=lumped_rlc, kerr_chi3=kerr_chi3, mag_sources=mag_sources,
+                 sheet_impedance=sheet_impedance, radiated_flux_box=radiated_flux_box)
+    if checkpoint_segments is not None:
+        raise NotImplementedError("checkpoint_segments is not supported by run_until_decay "
+                                  "(rfx/simulation.py:2289-2294)")
+    if periodic is not None and any(periodic):
+        raise NotImplementedError("periodic axes are outside this path")
+    if stencil_order != 2:
+        raise NotImplementedError("only the (2,2) Yee stencil is on this path")
+    if boundary not in ("pec", "cpml"):
+        raise NotImplementedError(f"boundary={boundary!r} is outside this path")
+    if check_interval < 1 or max_steps < 1:
+        raise ValueError("check_interval and max_steps must be >= 1")
+    if pec_axes is None:
+        pec_axes = "xyz"
+    absorbing = boundary == "cpml"
+    use_cpml = absorbing and int(grid.cpml_layers) > 0
+    srcs = [(s.i, s.j, s.k, s.component, s.waveform) for s in (sources or [])]
+    for s in srcs:
+        if np.asarray(s[4]).shape[0] < max_steps:
+            raise ValueError("source waveforms must cover max_steps")
+    prbs = [(p.i, p.j, p.k, p.component) for p in (probes or [])]
+    n_user = len(prbs)
+    if not absorbing:
+        if monitor_position is None:
+            mon = (grid.nx // 2, grid.ny // 2, grid.nz // 2)
+        else:
+            mon = tuple(grid.position_to_index(monitor_position))
+        prbs.append((*mon, monitor_component))
+    planes = list(dft_planes or [])
+    r = prepare_device_run(grid, materials, max_steps, cpml_axes=cpml_axes if use_cpml else "", pec_axes=pec_axes,
+                           sources=srcs, probes=prbs, dft_planes=planes, pec_mask=pec_mask, dft_time_offset=1,
+                           noop_faces=set(getattr(grid, "pec_faces", None) or ()), device=device)
+    plan = r.plan
+    try:
+        box = (grid.pad_x_lo, grid.nx - grid.pad_x_hi, grid.pad_y_lo, grid.ny - grid.pad_y_hi,
+               grid.pad_z_lo, grid.nz - grid.pad_z_hi)
+        energy = torch.empty((), device=plan.device, dtype=torch.float64)
+        peak_u, below, peak_sq = 0.0, 0, 0.0
+        n_check = -(-(max(min_steps, 1) - 1) // check_interval) * check_interval   # first eligible check step
+        done = 0
+        while done < max_steps:
+            target = min(n_check + 1, max_steps)
+            # steps done .. target-1, relative to the tables' row `done` (the
+            # captured chunk is then reused for every later check interval)
+            plan.advance(0, target - done,
+                         r.src_table[done:] if r.src_table is not None else None,
+                         r.probe_out[done:] if r.probe_out is not None else None,
+                         r.dft_accs, [ph[done:] for ph in r.dft_phases])
+            first, done = done, target
+            if done - 1 != n_check:
+                break
+            if absorbing:
+                u = float(plan.box_energy(box, energy).item())
+                peak_u = max(peak_u, u)
+                if u < decay_by * peak_u:
+                    below += 1
+                    if below >= decay_energy_consecutive:
+                        break
+                else:
+                    below = 0
+            else:
+                v = r.probe_out[first:done, -1].double().cpu().numpy()
+                peak_sq = max(peak_sq, float(np.max(v * v)))
+                if peak_sq > 0.0 and float(v[-1]) ** 2 < decay_by * peak_sq:
+                    break
+            n_check += check_interval
+        plan.check_device()
+        ts = r.probe_out[:done, :n_user].cpu().numpy() if r.probe_out is not None else np.zeros((done, 0),
+                                                                                               np.float32)
+        out_planes = tuple(d._replace(accumulator=a.cpu().numpy()) for d, a in zip(planes, r.dft_accs))
+        state = None
+        if return_state:
+            state = FDTDState(*[t.cpu().numpy() for t in plan.store_fields()], step=done)
+        return SimResult(state=state, time_series=ts, dft_planes=out_planes if planes else None, grid=grid)
+    finally:
+        plan.close()
+
+
 def extract_lumped_s11(v_dft, i_dft, z0=50.0):
     """rfx/probes/probes.py:1240-1274."""
     denom = v_dft - z0 * i_dft
