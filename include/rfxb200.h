@@ -70,6 +70,18 @@ typedef struct {
   int n_freqs;
 } RfxbDftDesc;
 
+/* One Poynting-flux monitor (rfx/probes/probes.py:476-580, accumulated as in
+ * rfx/simulation.py:1590-1642): the two tangential E components on plane
+ * `index` of the normal axis and the two tangential H components averaged
+ * over planes index-1 and index (index 0: plane 0 twice), on the region
+ * [lo1, hi1) x [lo2, hi2) of the plane's tangential axes (x-normal: y, z;
+ * y-normal: x, z; z-normal: x, y). */
+typedef struct {
+  int axis, index;
+  int lo1, hi1, lo2, hi2;
+  int n_freqs;
+} RfxbFluxDesc;
+
 /* Static description of one simulation (grid, boundaries, monitors).
  * Replaces the trace-time setup of _build_step_setup (rfx/simulation.py:626)
  * and _build_nu_scan (rfx/nonuniform.py:998). */
@@ -106,6 +118,9 @@ typedef struct {
   /* gradient region [i0,i1) x [j0,j1) x [k0,k1) whose forward history the
    * adjoint needs; i0 >= i1 means none */
   int grad_box[6];
+  /* Poynting-flux monitors */
+  int n_flux;
+  const RfxbFluxDesc* flux_host;
 } RfxbDesc;
 
 /* Per-call device buffers of the forward path. */
@@ -114,6 +129,11 @@ typedef struct {
   float* probe_out_dev;        /* [n_total_steps][n_probe], may be NULL */
   void* const* dft_acc_dev;    /* n_dft complex64 arrays (n_freqs, n1, n2), accumulated */
   const void* const* dft_phase_dev; /* n_dft float2 arrays [n_total_steps][n_freqs]: (cos, sin)*dt */
+  /* n_flux complex128 accumulators [4][n_freqs][n1][n2] (E1, E2, H1, H2),
+   * accumulated, and n_flux complex128 kernels [n_total_steps][2][n_freqs]:
+   * the E and H phase factors times dt and the window weight of each step */
+  void* const* flux_acc_dev;
+  const void* const* flux_kernel_dev;
 } RfxbStepIO;
 
 /* Per-call device buffers of the adjoint path. */

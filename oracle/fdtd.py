@@ -498,6 +498,7 @@ class OracleResult(NamedTuple):
     state: dict                       # final fields
     vi: np.ndarray | None             # (n_steps, n_ports, 2) pre-source V, I
     psi: dict
+    flux: list | None = None          # per flux monitor: complex128 (4, n_freqs, n1, n2)
 
 
 def _plane(a, axis, index):
@@ -508,8 +509,56 @@ def _plane(a, axis, index):
     return a[:, :, index]
 
 
+_FLUX_COMPONENTS = {0: ("ey", "ez", "hy", "hz"), 1: ("ez", "ex", "hz", "hx"), 2: ("ex", "ey", "hx", "hy")}
+
+
+def flux_window_weight(step, total_steps, window, alpha):
+    """rfx/core/dft_utils.py:8-50 (float32)."""
+    if total_steps <= 1 or window == "rect":
+        return np.float32(1.0)
+    x = np.float32(step) / np.float32(max(total_steps - 1, 1))
+    if window == "hann" or (window == "tukey" and alpha >= 1.0):
+        return np.float32(0.5) * (np.float32(1.0) - np.cos(np.float32(2.0 * np.pi) * x))
+    a = float(alpha)
+    if a <= 0.0:
+        return np.float32(1.0)
+    if x < a / 2.0:
+        return np.float32(0.5) * (np.float32(1.0) + np.cos(np.float32(np.pi) * (np.float32(2.0) * x / np.float32(a)
+                                                                                - np.float32(1.0))))
+    if x <= 1.0 - a / 2.0:
+        return np.float32(1.0)
+    return np.float32(0.5) * (np.float32(1.0) + np.cos(np.float32(np.pi) * (
+        np.float32(2.0) * x / np.float32(a) - np.float32(2.0 / a) + np.float32(1.0))))
+
+
+def _flux_step(F, mon, acc, step, dt):
+    """rfx/simulation.py:1590-1642: E at plane index, H averaged over index-1
+    and index (float32), times exp(-j 2 pi f t) dt w (E, t = step dt) and
+    exp(-j 2 pi f (t - dt/2)) dt w (H), accumulated in complex128."""
+    axis, index, lo1, hi1, lo2, hi2, freqs, total, window, alpha = mon
+    c = _FLUX_COMPONENTS[axis]
+    im1 = max(index - 1, 0)
+
+    def cut(a, plane):
+        s = [slice(None)] * 3
+        s[axis] = plane
+        t = a[tuple(s)]
+        return t[lo1:hi1, lo2:hi2]
+
+    e1, e2 = cut(F[c[0]], index), cut(F[c[1]], index)
+    h1 = (cut(F[c[2]], im1) + cut(F[c[2]], index)) * np.float32(0.5)
+    h2 = (cut(F[c[3]], im1) + cut(F[c[3]], index)) * np.float32(0.5)
+    f = np.asarray(freqs, np.float64)
+    t = float(step) * dt
+    w = float(flux_window_weight(step, total, window, alpha))
+    ke = np.exp(-1j * 2.0 * np.pi * f * t) * dt * w
+    kh = np.exp(-1j * 2.0 * np.pi * f * (t - dt * 0.5)) * dt * w
+    for q, (v, k) in enumerate(((e1, ke), (e2, ke), (h1, kh), (h2, kh))):
+        acc[q] += np.asarray(v, np.float64)[None, :, :] * k[:, None, None]
+
+
 def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
-         probes_before_dft, dx_vi, stop=None):
+         probes_before_dft, dx_vi, stop=None, flux_monitors=()):
     f = st.f
     cdt = np.complex64 if f == np.float32 else np.complex128
     ts = np.zeros((n_steps, len(probes)), f)
@@ -520,6 +569,7 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
         accs.append(np.zeros([len(freqs)] + shp, cdt))
     vi = np.zeros((n_steps, len(vi_ports), 2), f) if vi_ports else None
     dt = st.g.dt
+    flux_accs = [np.zeros((4, len(m[6]), m[3] - m[2], m[5] - m[4]), np.complex128) for m in flux_monitors]
     for n in range(n_steps):
         st.update_h()
         st.cpml_h()
@@ -563,16 +613,19 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
         else:
             _dft()
             _probes()
+        for m, acc in zip(flux_monitors, flux_accs):
+            _flux_step(F, m, acc, n + 1, dt)
         if stop is not None and stop(n, F):
             ts = ts[:n + 1]
             vi = vi[:n + 1] if vi is not None else None
             break
-    return OracleResult(ts, accs, {c: st.F[c].copy() for c in COMPONENTS}, vi, st.psi)
+    return OracleResult(ts, accs, {c: st.F[c].copy() for c in COMPONENTS}, vi, st.psi,
+                        flux_accs if flux_monitors else None)
 
 
 def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
                 pec_axes=None, sources=(), probes=(), dft_planes=(), pec_mask=None,
-                vi_ports=(), kappa_max=1.0, dtype=np.float32, exact_materials=False):
+                vi_ports=(), kappa_max=1.0, dtype=np.float32, exact_materials=False, flux_monitors=()):
     """``rfx.simulation.run`` (rfx/simulation.py:1686-2138), scan body order of
     rfx/simulation.py:1255-1685.  ``pec_axes=None`` means all axes
     (rfx/simulation.py:684-691).  ``sources`` are ``(i, j, k, comp, waveform)``,
@@ -585,7 +638,7 @@ def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
                   pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=kappa_max,
                   exact_materials=exact_materials)
     return _run(st, n_steps, sources, probes, dft_planes, vi_ports, 1,
-                probes_before_dft=True, dx_vi=grid.dx)
+                probes_before_dft=True, dx_vi=grid.dx, flux_monitors=flux_monitors)
 
 
 def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_planes=(),

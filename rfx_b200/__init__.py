@@ -10,8 +10,8 @@ reverse-time adjoint and the batched sweep.
 
 from .grid import Grid, NonUniformGrid, make_nonuniform_grid  # noqa: F401
 from .simulation import (  # noqa: F401
-    DFTPlaneProbe, FDTDState, LumpedPortSParamSpec, MaterialArrays, ProbeSpec, SimResult,
-    extract_lumped_s11, init_dft_plane_probe, run, run_until_decay,
+    DFTPlaneProbe, FDTDState, FluxMonitor, LumpedPortSParamSpec, MaterialArrays, ProbeSpec, SimResult,
+    extract_lumped_s11, flux_spectrum, init_dft_plane_probe, init_flux_monitor, run, run_until_decay,
 )
 from .sources import (  # noqa: F401
     GaussianPulse, LumpedPort, SourceSpec, make_current_source, make_j_source, make_port_source,

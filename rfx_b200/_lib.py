@@ -21,6 +21,11 @@ class RfxbDftDesc(C.Structure):
     _fields_ = [("axis", C.c_int), ("index", C.c_int), ("component", C.c_int), ("n_freqs", C.c_int)]
 
 
+class RfxbFluxDesc(C.Structure):
+    _fields_ = [("axis", C.c_int), ("index", C.c_int), ("lo1", C.c_int), ("hi1", C.c_int), ("lo2", C.c_int),
+                ("hi2", C.c_int), ("n_freqs", C.c_int)]
+
+
 class RfxbDesc(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
@@ -37,6 +42,7 @@ class RfxbDesc(C.Structure):
         ("n_probe", C.c_int), ("probe_cells_host", c_int32_p),
         ("n_dft", C.c_int), ("dft_host", C.POINTER(RfxbDftDesc)),
         ("grad_box", C.c_int * 6),
+        ("n_flux", C.c_int), ("flux_host", C.POINTER(RfxbFluxDesc)),
     ]
 
 
@@ -46,6 +52,8 @@ class RfxbStepIO(C.Structure):
         ("probe_out_dev", C.c_void_p),
         ("dft_acc_dev", C.POINTER(C.c_void_p)),
         ("dft_phase_dev", C.POINTER(C.c_void_p)),
+        ("flux_acc_dev", C.POINTER(C.c_void_p)),
+        ("flux_kernel_dev", C.POINTER(C.c_void_p)),
     ]
 
 

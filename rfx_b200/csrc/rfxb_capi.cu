@@ -33,6 +33,7 @@ __global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int
 __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
 __global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
+__global__ void flux_kernel(const RfxbInst*, const RfxbFluxPlane*, int, int, int);
 template <int TY, int MODE>
 __global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int,
                                 int);
@@ -94,6 +95,7 @@ struct RfxbPlan {
   std::vector<RfxbDftDesc> dft;
   std::vector<float2*> dft_cmp;
   std::vector<long long> dft_cells;
+  std::vector<RfxbFluxDesc> flux;
   long long psi_elems[3] = {0, 0, 0};
   // history
   float* hist = nullptr;
@@ -162,6 +164,9 @@ struct RfxbBatch {
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   RfxbDftPlane* d_dft = nullptr;
+  RfxbFluxPlane* d_flux = nullptr;
+  std::vector<RfxbFluxPlane> flux;
+  int flux_blocks = 0;
   CUtensorMap* d_maps = nullptr;   // RFXB_NMAPS per plan
   int* d_status = nullptr;         // device status word of the group's launches
   int fwd_mode = 0;                // forward step kernel variant (see rfxb_fwd.cu)
@@ -864,6 +869,35 @@ int build_group(RfxbBatch* g) {
     }
   }
   g->dft_blocks = blocks;
+  // flux monitors (tangential components per normal axis, rfx/probes/probes.py:508-512)
+  static const int kFluxComp[3][4] = {{RFXB_EY, RFXB_EZ, RFXB_HY, RFXB_HZ},
+                                      {RFXB_EZ, RFXB_EX, RFXB_HZ, RFXB_HX},
+                                      {RFXB_EX, RFXB_EY, RFXB_HX, RFXB_HY}};
+  g->flux.clear();
+  int fblocks = 0;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    RfxbPlan* p = g->plans[q];
+    for (const RfxbFluxDesc& fd : p->flux) {
+      RfxbFluxPlane pl{};
+      pl.inst = (int)q;
+      pl.axis = fd.axis;
+      pl.index = fd.index;
+      pl.im1 = std::max(fd.index - 1, 0);
+      pl.lo1 = fd.lo1;
+      pl.n1 = fd.hi1 - fd.lo1;
+      pl.lo2 = fd.lo2;
+      pl.n2 = fd.hi2 - fd.lo2;
+      pl.nf = fd.n_freqs;
+      for (int t = 0; t < 4; ++t) pl.comp[t] = kFluxComp[fd.axis][t];
+      pl.block0 = fblocks;
+      fblocks += (pl.n1 * pl.n2 + 255) / 256;
+      g->flux.push_back(pl);
+    }
+  }
+  g->flux_blocks = fblocks;
+  if (!g->flux.empty()) {
+    if (int rc = galloc((void**)&g->d_flux, sizeof(RfxbFluxPlane) * g->flux.size())) return rc;
+  }
   if (!g->dft.empty()) {
     if (int rc = galloc((void**)&g->d_dft, sizeof(RfxbDftPlane) * g->dft.size())) return rc;
   }
@@ -883,7 +917,8 @@ int upload_maps(RfxbBatch* g, cudaStream_t st) {
 }
 
 // Upload descriptors with this call's IO pointers.
-int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_prb, cudaStream_t st) {
+int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_prb, bool* has_flux,
+                 cudaStream_t st) {
   std::vector<RfxbInst> insts(g->plans.size());
   *has_dft = false;
   *has_prb = false;
@@ -903,6 +938,23 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
       if (on) *has_dft = true;
     }
   }
+  *has_flux = false;
+  size_t fi = 0;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    const RfxbStepIO* io = ios ? &ios[q] : nullptr;
+    for (size_t d = 0; d < g->plans[q]->flux.size(); ++d, ++fi) {
+      const bool on = io && io->flux_acc_dev && io->flux_kernel_dev && io->flux_acc_dev[d] && io->flux_kernel_dev[d];
+      g->flux[fi].acc = on ? static_cast<double2*>(io->flux_acc_dev[d]) : nullptr;
+      g->flux[fi].kern = on ? static_cast<const double2*>(io->flux_kernel_dev[d]) : nullptr;
+      if (on) *has_flux = true;
+    }
+  }
+  for (const auto& pl : g->flux)
+    if (*has_flux && pl.acc == nullptr)
+      return fail(RFXB_E_INVALID, "either every flux monitor of a group gets accumulator and kernel, or none");
+  if (!g->flux.empty())
+    RFXB_CUDA(cudaMemcpyAsync(g->d_flux, g->flux.data(), sizeof(RfxbFluxPlane) * g->flux.size(),
+                              cudaMemcpyHostToDevice, st));
   for (const auto& pl : g->dft)
     if (*has_dft && pl.acc == nullptr)
       return fail(RFXB_E_INVALID, "either every DFT plane of a group gets accumulator and phase table, or none");
@@ -916,7 +968,7 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
   return 0;
 }
 
-int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, cudaStream_t st) {
+int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, bool has_flux, cudaStream_t st) {
   int par = par0;
   bool em = false;   // stage the PEC edge masks when a plan of the group has one
   for (auto* p : g->plans) em = em || p->inst.emask != nullptr;
@@ -938,6 +990,8 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, c
     }
     if (has_dft)
       dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, par ^ 1);
+    if (has_flux)
+      flux_kernel<<<g->flux_blocks, 256, 0, st>>>(g->d_inst, g->d_flux, (int)g->flux.size(), n, par ^ 1);
     par ^= 1;
   }
   RFXB_CUDA(cudaGetLastError());
@@ -989,16 +1043,16 @@ int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, c
   const int par0 = g->plans[0]->par;
   for (auto* p : g->plans)
     if (p->par != par0) return fail(RFXB_E_STATE, "plans of a batch must share the step parity");
-  bool has_dft = false, has_prb = false;
-  if (int rc = upload_group(g, ios, &has_dft, &has_prb, st)) return rc;
+  bool has_dft = false, has_prb = false, has_flux = false;
+  if (int rc = upload_group(g, ios, &has_dft, &has_prb, &has_flux, st)) return rc;
   if (graphs_enabled() && n_steps >= 4) {
-    const GraphKey key{0, step0, n_steps, par0, 0, has_dft ? 1 : 0};
+    const GraphKey key{0, step0, n_steps, par0, 0, (has_dft ? 1 : 0) | (has_flux ? 2 : 0)};
     if (int rc = run_graph(g, key, st, [&](cudaStream_t cs) {
-          return launch_steps(g, step0, n_steps, par0, has_dft, cs);
+          return launch_steps(g, step0, n_steps, par0, has_dft, has_flux, cs);
         }))
       return rc;
   } else {
-    if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, st)) return rc;
+    if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, has_flux, st)) return rc;
   }
   for (auto* p : g->plans) p->par = (par0 + n_steps) & 1;
   return 0;
@@ -1180,6 +1234,16 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
         dd.component > 5 || dd.n_freqs < 1)
       return fail(RFXB_E_INVALID, "DFT plane descriptor out of range");
   }
+  for (int q = 0; q < d->n_flux; ++q) {
+    const RfxbFluxDesc& fd = d->flux_host[q];
+    const int dims[3] = {d->nx, d->ny, d->nz};
+    if (fd.axis < 0 || fd.axis > 2 || fd.index < 0 || fd.index >= dims[fd.axis] || fd.n_freqs < 1)
+      return fail(RFXB_E_INVALID, "flux monitor descriptor out of range");
+    const int t1 = fd.axis == 0 ? d->ny : d->nx, t2 = fd.axis == 2 ? d->ny : d->nz;
+    if (fd.lo1 < 0 || fd.hi1 > t1 || fd.lo1 >= fd.hi1 || fd.lo2 < 0 || fd.hi2 > t2 || fd.lo2 >= fd.hi2)
+      return fail(RFXB_E_INVALID, "flux monitor region out of range or empty");
+  }
+  if (d->n_flux > 0 && !d->flux_host) return fail(RFXB_E_INVALID, "flux monitors need descriptors");
   const int* hb = d->grad_box;
   if (hb[0] < hb[1]) {
     if (hb[0] < 0 || hb[1] > d->nx || hb[2] < 0 || hb[3] > d->ny || hb[4] < 0 || hb[5] > d->nz || hb[2] >= hb[3] ||
@@ -1298,6 +1362,7 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
     p->dft_cmp.push_back(c);
     p->dft_cells.push_back(n1 * n2);
   }
+  for (int q = 0; q < d->n_flux; ++q) p->flux.push_back(d->flux_host[q]);
   for (int k = 0; k < 6; ++k) I.hb[k] = hb[k];
   if (hb[0] >= hb[1]) { I.hb[0] = 0; I.hb[1] = 0; }
   p->hcells = (long long)(I.hb[1] - I.hb[0]) * (I.hb[3] - I.hb[2]) * (I.hb[5] - I.hb[4]);

@@ -108,6 +108,17 @@ struct RfxbWork {          // one CTA: a (y, z) tile over an x range
   int xa, xb;
 };
 
+struct RfxbFluxPlane {     // one Poynting-flux monitor of one instance
+  int inst;
+  int axis, index, im1;    // normal axis, E plane, the other H plane (index-1, or 0)
+  int lo1, n1, lo2, n2;    // region on the tangential axes (reference order)
+  int nf;
+  int comp[4];             // E1 E2 H1 H2 component codes
+  double2* acc;            // caller accumulator [4][nf][n1][n2] complex128
+  const double2* kern;     // [n][2][nf]: E and H factors (phase * dt * window)
+  int block0;              // first CTA of this monitor in the launch
+};
+
 struct RfxbDftPlane {      // one running-DFT plane of one instance
   int inst;
   int axis, index, comp;

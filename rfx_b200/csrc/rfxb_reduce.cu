@@ -41,4 +41,48 @@ __global__ void __launch_bounds__(256) box_energy_kernel(RfxbInst P, int par, in
   }
 }
 
+// Poynting-flux monitor accumulation for one step (rfx/simulation.py:1590-
+// 1642): E1, E2 at the plane, H1, H2 averaged over the plane and the one
+// before it in float32, each multiplied by its complex128 step factor and
+// added to the complex128 accumulators.  One thread per region cell.
+__global__ void flux_kernel(const RfxbInst* __restrict__ insts, const RfxbFluxPlane* __restrict__ planes,
+                            int nplanes, int n, int par) {
+  int q = 0;
+  while (q + 1 < nplanes && planes[q + 1].block0 <= (int)blockIdx.x) ++q;
+  const RfxbFluxPlane& M = planes[q];
+  const RfxbInst& P = insts[M.inst];
+  const int c = (blockIdx.x - M.block0) * blockDim.x + threadIdx.x;
+  const int cells = M.n1 * M.n2;
+  if (c >= cells) return;
+  const int a = M.lo1 + c / M.n2, b = M.lo2 + c % M.n2;
+  long long e, em1;
+  auto at = [&](int plane) {
+    int i, j, k;
+    if (M.axis == 0) { i = plane; j = a; k = b; }
+    else if (M.axis == 1) { i = a; j = plane; k = b; }
+    else { i = a; j = b; k = plane; }
+    return P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
+  };
+  e = at(M.index);
+  em1 = at(M.im1);
+  float v[4];
+  v[0] = P.F[par][M.comp[0]][e];
+  v[1] = P.F[par][M.comp[1]][e];
+  v[2] = (P.F[par][M.comp[2]][em1] + P.F[par][M.comp[2]][e]) * 0.5f;
+  v[3] = (P.F[par][M.comp[3]][em1] + P.F[par][M.comp[3]][e]) * 0.5f;
+  const double2* kn = M.kern + (long long)n * 2 * M.nf;
+  for (int f = 0; f < M.nf; ++f) {
+    const double2 ke = kn[f], kh = kn[M.nf + f];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const double2 k2 = t < 2 ? ke : kh;
+      double2* acc = M.acc + ((long long)t * M.nf + f) * cells + c;
+      double2 s = *acc;
+      s.x += (double)v[t] * k2.x;
+      s.y += (double)v[t] * k2.y;
+      *acc = s;
+    }
+  }
+}
+
 }  // namespace rfxb

@@ -73,6 +73,7 @@ class PlanSpec:
     probes: list = field(default_factory=list)    # (i, j, k, comp, presource)
     dft: list = field(default_factory=list)       # (axis, index, comp, n_freqs)
     grad_box: tuple | None = None                 # (i0, i1, j0, j1, k0, k1)
+    flux: list = field(default_factory=list)      # (axis, index, lo1, hi1, lo2, hi2, n_freqs)
 
 
 class Plan:
@@ -136,6 +137,13 @@ class Plan:
         gb = spec.grad_box or (0, 0, 0, 0, 0, 0)
         for q in range(6):
             d.grad_box[q] = int(gb[q])
+        flux_arr = (_lib.RfxbFluxDesc * max(1, len(spec.flux)))()
+        for q, fdesc in enumerate(spec.flux):
+            for name, v in zip(("axis", "index", "lo1", "hi1", "lo2", "hi2", "n_freqs"), fdesc):
+                setattr(flux_arr[q], name, int(v))
+        self._keep.append(flux_arr)
+        d.n_flux = len(spec.flux)
+        d.flux_host = C.cast(flux_arr, C.POINTER(_lib.RfxbFluxDesc))
         self.n_src = len(src)
         self.n_probe = len(prb)
         self.dft = list(spec.dft)
@@ -248,7 +256,7 @@ class Plan:
 
     # -- stepping ------------------------------------------------------------
     @staticmethod
-    def step_io(src_table=None, probe_out=None, dft_accs=None, dft_phases=None):
+    def step_io(src_table=None, probe_out=None, dft_accs=None, dft_phases=None, flux_accs=None, flux_kernels=None):
         io = RfxbStepIO()
         io.src_wave_dev = src_table.data_ptr() if src_table is not None else None
         io.probe_out_dev = probe_out.data_ptr() if probe_out is not None else None
@@ -259,10 +267,17 @@ class Plan:
             io.dft_acc_dev = C.cast(acc, C.POINTER(C.c_void_p))
             io.dft_phase_dev = C.cast(ph, C.POINTER(C.c_void_p))
             keep += [acc, ph]
+        if flux_accs:
+            acc = (C.c_void_p * len(flux_accs))(*[a.data_ptr() for a in flux_accs])
+            kn = (C.c_void_p * len(flux_kernels))(*[k.data_ptr() for k in flux_kernels])
+            io.flux_acc_dev = C.cast(acc, C.POINTER(C.c_void_p))
+            io.flux_kernel_dev = C.cast(kn, C.POINTER(C.c_void_p))
+            keep += [acc, kn]
         return io, keep
 
-    def advance(self, step0, n_steps, src_table=None, probe_out=None, dft_accs=None, dft_phases=None):
-        io, keep = self.step_io(src_table, probe_out, dft_accs, dft_phases)
+    def advance(self, step0, n_steps, src_table=None, probe_out=None, dft_accs=None, dft_phases=None,
+                flux_accs=None, flux_kernels=None):
+        io, keep = self.step_io(src_table, probe_out, dft_accs, dft_phases, flux_accs, flux_kernels)
         check(self._lib.rfxb_plan_advance(self._h, C.byref(io), int(step0), int(n_steps), _stream()),
               "rfxb_plan_advance")
         del keep

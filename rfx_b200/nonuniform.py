@@ -30,7 +30,7 @@ def run_nonuniform(grid, materials, n_steps, *, pec_mask=None, pec_occupancy=Non
     use_cpml = int(grid.cpml_layers) > 0
     srcs = [tuple(s) for s in (sources or [])]
     prbs = [tuple(p) for p in (probes or [])]
-    ts, planes, _, state = run_device(
+    ts, planes, _, state, _ = run_device(
         grid, materials, n_steps, cpml_axes=axes if use_cpml else "", pec_axes="xyz", sources=srcs,
         probes=prbs, dft_planes=list(dft_planes or []), pec_mask=pec_mask, dft_time_offset=0,
         return_state=True, noop_faces=set(pec_faces or ()), device=device)

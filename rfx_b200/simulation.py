@@ -70,6 +70,93 @@ class DFTPlaneProbe(NamedTuple):
     window_alpha: float = 0.25
 
 
+class FluxMonitor(NamedTuple):
+    """Poynting-flux DFT accumulators of a plane region
+    (rfx/probes/probes.py:476-506); accumulators are complex128."""
+    e1_dft: np.ndarray
+    e2_dft: np.ndarray
+    h1_dft: np.ndarray
+    h2_dft: np.ndarray
+    freqs: np.ndarray
+    axis: int
+    index: int
+    dA: np.ndarray
+    total_steps: int
+    window: str
+    window_alpha: float
+    lo1: int = 0
+    hi1: int = -1
+    lo2: int = 0
+    hi2: int = -1
+
+
+def init_flux_monitor(axis, index, freqs, grid_shape, d1, d2, dft_total_steps=0, dft_window="rect",
+                      dft_window_alpha=0.25, lo1=0, hi1=-1, lo2=0, hi2=-1) -> FluxMonitor:
+    """rfx/probes/probes.py:515-579: a flux monitor on plane ``index`` of
+    ``axis`` over [lo1, hi1) x [lo2, hi2) of the tangential axes (-1: full
+    extent), area weight dA = d1 d2 (scalars or per-cell arrays)."""
+    full1 = grid_shape[1] if axis == 0 else grid_shape[0]
+    full2 = grid_shape[1] if axis == 2 else grid_shape[2]
+    hi1 = full1 if hi1 < 0 else hi1
+    hi2 = full2 if hi2 < 0 else hi2
+    n1, n2, nf = hi1 - lo1, hi2 - lo2, len(freqs)
+    zeros = np.zeros((nf, n1, n2), np.complex128)
+    w1 = np.asarray(d1, np.float32)
+    w2 = np.asarray(d2, np.float32)
+    if w1.ndim > 0:
+        w1 = w1[lo1:hi1]
+    if w2.ndim > 0:
+        w2 = w2[lo2:hi2]
+    dA = np.reshape(w1, (-1, 1)) * np.reshape(w2, (1, -1))
+    return FluxMonitor(zeros, zeros.copy(), zeros.copy(), zeros.copy(), np.asarray(freqs), int(axis), int(index),
+                       dA, int(dft_total_steps), dft_window, float(dft_window_alpha), lo1, hi1, lo2, hi2)
+
+
+def flux_spectrum(mon: FluxMonitor, *, exact_f64: bool = False) -> np.ndarray:
+    """rfx/probes/probes.py:613-680: the integral of Re(E x H*) . n dA per
+    frequency (positive: power flowing towards +axis).  The accumulators are
+    complex128 here, so both paths evaluate in float64."""
+    e1, e2 = np.asarray(mon.e1_dft, np.complex128), np.asarray(mon.e2_dft, np.complex128)
+    h1, h2 = np.asarray(mon.h1_dft, np.complex128), np.asarray(mon.h2_dft, np.complex128)
+    integrand = e1 * np.conj(h2) - e2 * np.conj(h1)
+    return np.real(np.sum(integrand * np.asarray(mon.dA, np.float64), axis=(-2, -1)))
+
+
+def dft_window_weight(step, total_steps, window, alpha):
+    """rfx/core/dft_utils.py:8-50, float32 arithmetic."""
+    if total_steps <= 1 or window == "rect":
+        return np.float32(1.0)
+    x = np.float32(step) / np.float32(max(total_steps - 1, 1))
+    if window == "hann" or (window == "tukey" and alpha >= 1.0):
+        return np.float32(0.5) * (np.float32(1.0) - np.cos(np.float32(2.0 * np.pi) * x))
+    if window == "tukey":
+        a = float(alpha)
+        if a <= 0.0:
+            return np.float32(1.0)
+        if x < a / 2.0:
+            return np.float32(0.5) * (np.float32(1.0) + np.cos(np.float32(np.pi) * (np.float32(2.0) * x / np.float32(a)
+                                                                                    - np.float32(1.0))))
+        if x <= 1.0 - a / 2.0:
+            return np.float32(1.0)
+        return np.float32(0.5) * (np.float32(1.0) + np.cos(np.float32(np.pi) * (
+            np.float32(2.0) * x / np.float32(a) - np.float32(2.0 / a) + np.float32(1.0))))
+    raise ValueError(f"unknown DFT window {window!r}")
+
+
+def flux_kernel_table(mon: FluxMonitor, n_steps, dt):
+    """(n_steps, 2, n_freqs) complex128 step factors of a flux monitor
+    (rfx/simulation.py:1590-1642): E sampled at t = (n+1) dt, H at t - dt/2,
+    times dt and the window weight of step n+1."""
+    f = np.asarray(mon.freqs, np.float64)
+    t = np.arange(1, n_steps + 1, dtype=np.float64) * float(dt)
+    w = np.array([dft_window_weight(n, mon.total_steps, mon.window, mon.window_alpha)
+                  for n in range(1, n_steps + 1)], np.float64)
+    out = np.empty((n_steps, 2, len(f)), np.complex128)
+    out[:, 0, :] = np.exp(-1j * 2.0 * np.pi * f[None, :] * t[:, None]) * float(dt) * w[:, None]
+    out[:, 1, :] = np.exp(-1j * 2.0 * np.pi * f[None, :] * (t[:, None] - float(dt) * 0.5)) * float(dt) * w[:, None]
+    return out
+
+
 class SimResult(NamedTuple):
     """rfx/simulation.py:135-178 (fields on this path)."""
     state: FDTDState | None
@@ -172,10 +259,13 @@ class DeviceRun(NamedTuple):
     dft_phases: list           # (n_steps, n_f) phase tables per plane
     probes: list               # probe tuples (user probes first, then port V/I probes)
     vi_rows: list              # per lumped port: [(probe row, sign), ...]
+    flux_accs: tuple = ()      # complex128 (4, n_f, n1, n2) per flux monitor
+    flux_kernels: tuple = ()   # complex128 (n_steps, 2, n_f) per flux monitor
 
 
 def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
-                       dft_time_offset, lumped_specs=(), kappa_max=None, noop_faces=(), device=None) -> DeviceRun:
+                       dft_time_offset, lumped_specs=(), kappa_max=None, noop_faces=(), flux_monitors=(),
+                       device=None) -> DeviceRun:
     """Build the plan of one simulation and upload its inputs (the set-up half
     of ``run_device``); the caller owns the plan and closes it."""
     dev = require_cuda(device)
@@ -193,7 +283,9 @@ def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources
     cp = build_cpml(grid, cpml_axes, kappa_max=kappa_max, noop_faces=noop_faces) if cpml_axes else None
     plan = Plan(PlanSpec(shape=shape, dt=float(grid.dt), tables=spacing_tables(grid), cpml=cp,
                          pec_axes=pec_axes, sources=[s[:4] for s in srcs], probes=prb,
-                         dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in dft_planes]), dev)
+                         dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in dft_planes],
+                         flux=[(m.axis, m.index, m.lo1, m.hi1, m.lo2, m.hi2, len(m.freqs)) for m in flux_monitors]),
+                dev)
     try:
         em = tangential_edge_masks(_to_np(pec_mask, bool)) if pec_mask is not None else None
         mu = getattr(materials, "mu_r", None)
@@ -211,27 +303,35 @@ def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources
         for d in dft_planes:
             accs.append(torch.from_numpy(np.ascontiguousarray(np.asarray(d.accumulator, np.complex64))).to(dev))
             phases.append(torch.from_numpy(dft_phase_table(d.freqs, n_steps, grid.dt, dft_time_offset)).to(dev))
+        faccs, fkerns = [], []
+        for m in flux_monitors:
+            faccs.append(torch.from_numpy(np.stack([np.asarray(a, np.complex128) for a in
+                                                    (m.e1_dft, m.e2_dft, m.h1_dft, m.h2_dft)])).to(dev).contiguous())
+            fkerns.append(torch.from_numpy(flux_kernel_table(m, n_steps, grid.dt)).to(dev))
     except BaseException:
         plan.close()
         raise
-    return DeviceRun(plan, src_table, probe_out, accs, phases, prb, vi_rows)
+    return DeviceRun(plan, src_table, probe_out, accs, phases, prb, vi_rows, faccs, fkerns)
 
 
 def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
                dft_time_offset, lumped_specs=(), return_state=True, report_every=None, report_label="",
-               kappa_max=None, noop_faces=(), device=None):
-    """Shared driver of the uniform and graded lanes."""
+               kappa_max=None, noop_faces=(), flux_monitors=(), device=None):
+    """Shared driver of the uniform and graded lanes.  Returns (time series,
+    DFT planes, lumped-port results, state, flux monitors)."""
     n_steps = int(n_steps)
+    flux_monitors = list(flux_monitors)
     r = prepare_device_run(grid, materials, n_steps, cpml_axes=cpml_axes, pec_axes=pec_axes, sources=sources,
                            probes=probes, dft_planes=dft_planes, pec_mask=pec_mask, dft_time_offset=dft_time_offset,
-                           lumped_specs=lumped_specs, kappa_max=kappa_max, noop_faces=noop_faces, device=device)
+                           lumped_specs=lumped_specs, kappa_max=kappa_max, noop_faces=noop_faces,
+                           flux_monitors=flux_monitors, device=device)
     plan, probe_out, accs = r.plan, r.probe_out, r.dft_accs
     try:
         chunk = int(report_every) if report_every else n_steps
         done = 0
         while done < n_steps:
             k = min(chunk, n_steps - done)
-            plan.advance(done, k, r.src_table, probe_out, accs, r.dft_phases)
+            plan.advance(done, k, r.src_table, probe_out, accs, r.dft_phases, r.flux_accs, r.flux_kernels)
             done += k
             if report_every:
                 torch.cuda.current_stream().synchronize()
@@ -253,7 +353,11 @@ def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes
         if return_state:
             f = [t.cpu().numpy() for t in plan.store_fields()]
             state = FDTDState(*f, step=n_steps)
-        return ts, out_planes, lumped, state
+        out_flux = []
+        for m, a in zip(flux_monitors, r.flux_accs):
+            a = a.cpu().numpy()
+            out_flux.append(m._replace(e1_dft=a[0], e2_dft=a[1], h1_dft=a[2], h2_dft=a[3]))
+        return ts, out_planes, lumped, state, tuple(out_flux)
     finally:
         plan.close()
 
@@ -276,7 +380,7 @@ def run(grid, materials, n_steps, *, boundary="pec", cpml_axes="xyz", pec_axes=N
     """Uniform-grid scan (rfx/simulation.py:1686).  Step order per
     rfx/simulation.py:1255-1685: H, CPML-H, E, CPML-E, PEC faces, PEC mask,
     soft sources, probes, DFT planes at ``t = (n+1) dt``."""
-    _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf, flux_monitors=flux_monitors,
+    _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf,
                  waveguide_ports=waveguide_ports, ntff=ntff, snapshot=snapshot, aniso_eps=aniso_eps,
                  aniso_inv_eps=aniso_inv_eps, pec_occupancy=pec_occupancy, conformal_weights=conformal_weights,
                  wire_port_sparams=wire_port_sparams, wire_refplane_sparams=wire_refplane_sparams,
@@ -303,13 +407,14 @@ def run(grid, materials, n_steps, *, boundary="pec", cpml_axes="xyz", pec_axes=N
         raise NotImplementedError(f"boundary={boundary!r} is outside this path")
     srcs = [(s.i, s.j, s.k, s.component, s.waveform) for s in (sources or [])]
     prbs = [(p.i, p.j, p.k, p.component) for p in (probes or [])]
-    ts, planes, lumped, state = run_device(
+    ts, planes, lumped, state, flux = run_device(
         grid, materials, n_steps, cpml_axes=cpml_axes if use_cpml else "", pec_axes=pec_axes, sources=srcs,
         probes=prbs, dft_planes=list(dft_planes or []), pec_mask=pec_mask, dft_time_offset=1,
         lumped_specs=list(lumped_port_sparams or []), return_state=return_state, report_every=report_every,
-        report_label=report_label, noop_faces=set(getattr(grid, "pec_faces", None) or ()), device=device)
+        report_label=report_label, noop_faces=set(getattr(grid, "pec_faces", None) or ()),
+        flux_monitors=list(flux_monitors or []), device=device)
     return SimResult(state=state, time_series=ts, dft_planes=planes if dft_planes else None,
-                     lumped_port_sparams=lumped, grid=grid)
+                     flux_monitors=flux if flux_monitors else None, lumped_port_sparams=lumped, grid=grid)
 
 
 def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100, max_steps=50_000,

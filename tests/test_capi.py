@@ -14,6 +14,7 @@ from rfx_b200.cpml import build_cpml
 from rfx_b200.grid import spacing_tables
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "rfxb200.h")
 
 
 def _declared_symbols():
@@ -31,13 +32,33 @@ def test_library_exports_every_declared_symbol():
     assert lib.rfxb_version() >= 10000
 
 
-def test_struct_layout_matches_header():
-    """ctypes mirrors of the header structs have the C sizes (x86-64 ABI)."""
-    assert C.sizeof(_lib.RfxbDftDesc) == 16
-    assert C.sizeof(_lib.RfxbStepIO) == 32
-    assert C.sizeof(_lib.RfxbAdjointIO) == 40
-    # 3 ints + pad, double, 6 ptrs, int, uint, 3 ptrs, 6 doubles, uint, (int,ptr)x2, int+pad, ptr, 6 ints
-    assert C.sizeof(_lib.RfxbDesc) == 16 + 48 + 8 + 24 + 48 + 8 + 16 + 16 + 16 + 24
+def test_struct_layout_matches_header(tmp_path):
+    """ctypes mirrors of the header structs have the sizes and field offsets
+    the C compiler gives them (the header compiled with gcc here)."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    structs = {
+        "RfxbDftDesc": _lib.RfxbDftDesc, "RfxbFluxDesc": _lib.RfxbFluxDesc, "RfxbDesc": _lib.RfxbDesc,
+        "RfxbStepIO": _lib.RfxbStepIO, "RfxbAdjointIO": _lib.RfxbAdjointIO,
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                                text=True).stdout.split("\n") if line)
+    for name, cls in structs.items():
+        assert int(out[name]) == C.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert int(out[f"{name}.{fname}"]) == getattr(cls, fname).offset, f"{name}.{fname}"
 
 
 def _desc(shape=(10, 10, 10), **over):
