@@ -417,6 +417,17 @@ void make_balanced_work(const std::vector<RfxbPlan*>& plans, int resident, doubl
 }
 
 // RFXB_WORK=uniform selects the plain split (one x chunk count for the group).
+// Modelled extra cost of a tile-plane per CPML slab it lies in, relative to
+// a plain tile-plane (RFXB_SLAB_WEIGHT, default 0.4).
+double slab_weight() {
+  static double v = -1.0;
+  if (v < 0.0) {
+    const char* e = getenv("RFXB_SLAB_WEIGHT");
+    v = e ? std::max(0.0, atof(e)) : 0.4;
+  }
+  return v;
+}
+
 // RFXB_FWD_SPLIT=0 runs all forward tiles of a staged-psi group on one kernel.
 bool fwd_split_enabled() {
   static int v = -1;
@@ -788,7 +799,7 @@ int build_group(RfxbBatch* g) {
   }
   g->fwd_mode = group_fwd_mode(g);
   if (work_mode() == 1) {
-    make_balanced_work(g->plans, resident_ctas(g->fwd_mode), g->fwd_mode == 2 ? 0.4 : 1.0, 3.0, work);
+    make_balanced_work(g->plans, resident_ctas(g->fwd_mode), g->fwd_mode == 2 ? slab_weight() : 1.0, 3.0, work);
   } else if (work_mode() == 2) {
     make_stream_work(g->plans, stream_planes(), work);
   } else {
@@ -806,7 +817,7 @@ int build_group(RfxbBatch* g) {
   g->fwd_split = false;
   if (g->fwd_mode == 2 && work_mode() == 1 && fwd_split_enabled()) {
     std::vector<WorkSeg> plain, cpml;
-    split_segments(g->plans, 0.4, plain, cpml);
+    split_segments(g->plans, slab_weight(), plain, cpml);
     std::vector<RfxbWork> w1, w2;
     balance_segments(plain, resident_ctas(1), 3.0, w1);
     balance_segments(cpml, resident_ctas(2), 3.0, w2);
@@ -824,7 +835,7 @@ int build_group(RfxbBatch* g) {
     }
     // reverse split (used when the reverse kernel is variant 1 or 2)
     std::vector<WorkSeg> aplain, acpml;
-    split_adj_segments(g->plans, 0.4, aplain, acpml);
+    split_adj_segments(g->plans, slab_weight(), aplain, acpml);
     std::vector<RfxbWork> a1, a2;
     balance_segments(aplain, 4 * sm_count(), 3.0, a1);
     balance_segments(acpml, 3 * sm_count(), 3.0, a2);
