@@ -82,6 +82,16 @@ typedef struct {
   int n_freqs;
 } RfxbFluxDesc;
 
+/* The near-to-far-field Huygens box (rfx/farfield.py:32-79 NTFFBox): six
+ * faces at i_lo, i_hi (x), j_lo, j_hi (y) and k_lo, k_hi (z), each covering
+ * the half-open ranges [lo, hi) of its two tangential axes.  Accumulated as
+ * rfx/farfield.py:208-313 accumulate_ntff does, once per step after the E
+ * update and source injection. */
+typedef struct {
+  int i_lo, i_hi, j_lo, j_hi, k_lo, k_hi;
+  int n_freqs;
+} RfxbNtffDesc;
+
 /* Static description of one simulation (grid, boundaries, monitors).
  * Replaces the trace-time setup of _build_step_setup (rfx/simulation.py:626)
  * and _build_nu_scan (rfx/nonuniform.py:998). */
@@ -121,6 +131,8 @@ typedef struct {
   /* Poynting-flux monitors */
   int n_flux;
   const RfxbFluxDesc* flux_host;
+  /* NTFF Huygens box, NULL for none */
+  const RfxbNtffDesc* ntff_host;
 } RfxbDesc;
 
 /* Per-call device buffers of the forward path. */
@@ -134,6 +146,15 @@ typedef struct {
    * the E and H phase factors times dt and the window weight of each step */
   void* const* flux_acc_dev;
   const void* const* flux_kernel_dev;
+  /* NTFF box: complex64 running sums and Kahan residuals, each the six faces
+   * x_lo, x_hi, y_lo, y_hi, z_lo, z_hi back to back, face f an array
+   * (n_freqs, n1, n2, 4) of the tangential components (x faces: ey ez hy hz;
+   * y faces: ex ez hx hz; z faces: ex ey hx hy), and the complex64 phase
+   * table [n_total_steps][2][n_freqs] (E factor, H factor, both times dt).
+   * All three NULL: no accumulation. */
+  void* ntff_acc_dev;
+  void* ntff_cmp_dev;
+  const void* ntff_phase_dev;
 } RfxbStepIO;
 
 /* Per-call device buffers of the adjoint path. */

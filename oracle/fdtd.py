@@ -499,6 +499,7 @@ class OracleResult(NamedTuple):
     vi: np.ndarray | None             # (n_steps, n_ports, 2) pre-source V, I
     psi: dict
     flux: list | None = None          # per flux monitor: complex128 (4, n_freqs, n1, n2)
+    ntff: dict | None = None          # NTFF faces: {"x_lo": ..., "c_x_lo": ...} complex64 (n_f, n1, n2, 4)
 
 
 def _plane(a, axis, index):
@@ -557,8 +558,73 @@ def _flux_step(F, mon, acc, step, dt):
         acc[q] += np.asarray(v, np.float64)[None, :, :] * k[:, None, None]
 
 
+NTFF_FACES = ("x_lo", "x_hi", "y_lo", "y_hi", "z_lo", "z_hi")
+_NTFF_COMPONENTS = {0: ("ey", "ez", "hy", "hz"), 1: ("ex", "ez", "hx", "hz"), 2: ("ex", "ey", "hx", "hy")}
+
+
+def ntff_init(box):
+    """Zeroed NTFF running sums and Kahan residuals (rfx/farfield.py:164-205):
+    ``box`` = (i_lo, i_hi, j_lo, j_hi, k_lo, k_hi, freqs); x faces are
+    (n_f, nj, nk, 4), y faces (n_f, ni, nk, 4), z faces (n_f, ni, nj, 4)."""
+    i0, i1, j0, j1, k0, k1, freqs = box
+    nf = len(freqs)
+    dims = {0: (j1 - j0, k1 - k0), 1: (i1 - i0, k1 - k0), 2: (i1 - i0, j1 - j0)}
+    out = {}
+    for q, name in enumerate(NTFF_FACES):
+        out[name] = np.zeros((nf,) + dims[q // 2] + (4,), np.complex64)
+        out["c_" + name] = np.zeros_like(out[name])
+    return out
+
+
+def ntff_phases(freqs, step, dt):
+    """E and H step factors of rfx/farfield.py:230-244 in float32 / complex64:
+    t = f32(step) * f32(dt), omega = f32(2 pi) * f32(f), E factor
+    exp(-1j omega t) dt, H factor exp(-1j omega (t + dt/2)) dt."""
+    d = np.float32(dt)
+    t = np.float32(step) * d
+    om = np.float32(2 * np.pi) * np.asarray(freqs, np.float32)
+    th = np.float32(t + d * np.float32(0.5))
+    out = []
+    for tt in (t, th):
+        a = (om * tt).astype(np.float32).astype(np.float64)
+        c = np.cos(a).astype(np.float32) * d
+        sn = -np.sin(a).astype(np.float32) * d
+        out.append((c.astype(np.float32), sn.astype(np.float32)))
+    return out
+
+
+def ntff_step(F, box, acc, step, dt):
+    """One step of rfx/farfield.py:208-313: on each face the four tangential
+    components times the step's factor (E factor for the E pair, H factor for
+    the H pair), Kahan-added per real and imaginary part in float32."""
+    i0, i1, j0, j1, k0, k1, freqs = box
+    (ce, se), (chh, sh) = ntff_phases(freqs, step, dt)
+    lo = (i0, j0, k0)
+    hi = (i1, j1, k1)
+    for q, name in enumerate(NTFF_FACES):
+        ax = q // 2
+        idx = hi[ax] if q & 1 else lo[ax]
+        sl = [slice(i0, i1), slice(j0, j1), slice(k0, k1)]
+        sl[ax] = idx
+        vals = np.stack([np.asarray(F[c][tuple(sl)], np.float32) for c in _NTFF_COMPONENTS[ax]], axis=-1)
+        wr = np.stack([ce, ce, chh, chh], axis=-1)[:, None, None, :]
+        wi = np.stack([se, se, sh, sh], axis=-1)[:, None, None, :]
+        s, c = acc[name], acc["c_" + name]
+        for part, w in (("real", wr), ("imag", wi)):
+            sv = getattr(s, part).astype(np.float32)
+            cv = getattr(c, part).astype(np.float32)
+            val = (vals[None] * w).astype(np.float32)
+            y = (val - cv).astype(np.float32)
+            t = (sv + y).astype(np.float32)
+            cv = ((t - sv).astype(np.float32) - y).astype(np.float32)
+            if part == "real":
+                s.real, c.real = t, cv
+            else:
+                s.imag, c.imag = t, cv
+
+
 def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
-         probes_before_dft, dx_vi, stop=None, flux_monitors=()):
+         probes_before_dft, dx_vi, stop=None, flux_monitors=(), ntff=None):
     f = st.f
     cdt = np.complex64 if f == np.float32 else np.complex128
     ts = np.zeros((n_steps, len(probes)), f)
@@ -570,6 +636,7 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
     vi = np.zeros((n_steps, len(vi_ports), 2), f) if vi_ports else None
     dt = st.g.dt
     flux_accs = [np.zeros((4, len(m[6]), m[3] - m[2], m[5] - m[4]), np.complex128) for m in flux_monitors]
+    ntff_acc = ntff_init(ntff) if ntff is not None else None
     for n in range(n_steps):
         st.update_h()
         st.cpml_h()
@@ -615,22 +682,27 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
             _probes()
         for m, acc in zip(flux_monitors, flux_accs):
             _flux_step(F, m, acc, n + 1, dt)
+        if ntff is not None:
+            ntff_step(F, ntff, ntff_acc, n, dt)
         if stop is not None and stop(n, F):
             ts = ts[:n + 1]
             vi = vi[:n + 1] if vi is not None else None
             break
     return OracleResult(ts, accs, {c: st.F[c].copy() for c in COMPONENTS}, vi, st.psi,
-                        flux_accs if flux_monitors else None)
+                        flux_accs if flux_monitors else None, ntff_acc)
 
 
 def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
                 pec_axes=None, sources=(), probes=(), dft_planes=(), pec_mask=None,
-                vi_ports=(), kappa_max=1.0, dtype=np.float32, exact_materials=False, flux_monitors=()):
+                vi_ports=(), kappa_max=1.0, dtype=np.float32, exact_materials=False, flux_monitors=(),
+                ntff=None):
     """``rfx.simulation.run`` (rfx/simulation.py:1686-2138), scan body order of
     rfx/simulation.py:1255-1685.  ``pec_axes=None`` means all axes
     (rfx/simulation.py:684-691).  ``sources`` are ``(i, j, k, comp, waveform)``,
     ``probes`` ``(i, j, k, comp)``, ``dft_planes`` ``(axis, index, comp, freqs)``.
-    The uniform DFT time stamp is ``(n+1) dt`` (rfx/simulation.py:1574)."""
+    The uniform DFT time stamp is ``(n+1) dt`` (rfx/simulation.py:1574).
+    ``ntff`` = (i_lo, i_hi, j_lo, j_hi, k_lo, k_hi, freqs) accumulates the
+    Huygens box after the step's probes (rfx/simulation.py:1570-1572)."""
     if pec_axes is None:
         pec_axes = "xyz"
     st = _Stepper(grid, materials, dtype=dtype, nonuniform=False,
@@ -638,11 +710,11 @@ def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
                   pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=kappa_max,
                   exact_materials=exact_materials)
     return _run(st, n_steps, sources, probes, dft_planes, vi_ports, 1,
-                probes_before_dft=True, dx_vi=grid.dx, flux_monitors=flux_monitors)
+                probes_before_dft=True, dx_vi=grid.dx, flux_monitors=flux_monitors, ntff=ntff)
 
 
 def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_planes=(),
-                   pec_mask=None, kappa_max=1.0, dtype=np.float32, exact_materials=False):
+                   pec_mask=None, kappa_max=1.0, dtype=np.float32, exact_materials=False, ntff=None):
     """``rfx.nonuniform.run_nonuniform`` (rfx/nonuniform.py:1589-1804), scan body
     of rfx/nonuniform.py:1256-1568: PEC on every axis, DFT time stamp ``n dt``
     (rfx/nonuniform.py:1461), DFT before probes."""
@@ -654,7 +726,7 @@ def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_plane
                   pec_axes="xyz", pec_mask=pec_mask, kappa_max=kappa_max,
                   exact_materials=exact_materials)
     return _run(st, n_steps, sources, probes, dft_planes, (), 0,
-                probes_before_dft=False, dx_vi=grid.dx)
+                probes_before_dft=False, dx_vi=grid.dx, ntff=ntff)
 
 
 def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100,

@@ -1,7 +1,8 @@
 """rfx_b200: B200-native time-stepping hot path of the rfx FDTD solver.
 
 The Yee E/H leapfrog on uniform and graded grids, CPML, PEC faces and edge
-masks, soft sources, point probes and running-DFT planes run as hand-written
+masks, soft sources, point probes, running-DFT planes, Poynting-flux monitors
+and the NTFF Huygens box run as hand-written
 sm_100a CUDA kernels behind the C ABI of ``include/rfxb200.h``; the modules
 here are the host-side mirror of the reference's Python interface for that
 path (``rfx.simulation.run``, ``rfx.nonuniform.run_nonuniform``), plus the
@@ -18,5 +19,9 @@ from .sources import (  # noqa: F401
     make_source, setup_lumped_port,
 )
 from .nonuniform import run_nonuniform  # noqa: F401
+from .farfield import (  # noqa: F401
+    FarFieldResult, NTFFBox, NTFFData, compute_far_field, directivity, init_ntff_data, make_ntff_box,
+    radiation_pattern,
+)
 
 __version__ = "0.1.0"

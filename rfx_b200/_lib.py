@@ -26,6 +26,11 @@ class RfxbFluxDesc(C.Structure):
                 ("hi2", C.c_int), ("n_freqs", C.c_int)]
 
 
+class RfxbNtffDesc(C.Structure):
+    _fields_ = [("i_lo", C.c_int), ("i_hi", C.c_int), ("j_lo", C.c_int), ("j_hi", C.c_int), ("k_lo", C.c_int),
+                ("k_hi", C.c_int), ("n_freqs", C.c_int)]
+
+
 class RfxbDesc(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
@@ -43,6 +48,7 @@ class RfxbDesc(C.Structure):
         ("n_dft", C.c_int), ("dft_host", C.POINTER(RfxbDftDesc)),
         ("grad_box", C.c_int * 6),
         ("n_flux", C.c_int), ("flux_host", C.POINTER(RfxbFluxDesc)),
+        ("ntff_host", C.POINTER(RfxbNtffDesc)),
     ]
 
 
@@ -54,6 +60,9 @@ class RfxbStepIO(C.Structure):
         ("dft_phase_dev", C.POINTER(C.c_void_p)),
         ("flux_acc_dev", C.POINTER(C.c_void_p)),
         ("flux_kernel_dev", C.POINTER(C.c_void_p)),
+        ("ntff_acc_dev", C.c_void_p),
+        ("ntff_cmp_dev", C.c_void_p),
+        ("ntff_phase_dev", C.c_void_p),
     ]
 
 

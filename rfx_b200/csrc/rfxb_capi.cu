@@ -34,6 +34,7 @@ __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
 __global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
 __global__ void flux_kernel(const RfxbInst*, const RfxbFluxPlane*, int, int, int);
+__global__ void ntff_kernel(const RfxbInst*, const RfxbNtffFace*, int, int, int);
 template <int TY, int MODE>
 __global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int,
                                 int);
@@ -96,6 +97,8 @@ struct RfxbPlan {
   std::vector<float2*> dft_cmp;
   std::vector<long long> dft_cells;
   std::vector<RfxbFluxDesc> flux;
+  bool has_ntff = false;
+  RfxbNtffDesc ntff{};
   long long psi_elems[3] = {0, 0, 0};
   // history
   float* hist = nullptr;
@@ -167,6 +170,10 @@ struct RfxbBatch {
   RfxbFluxPlane* d_flux = nullptr;
   std::vector<RfxbFluxPlane> flux;
   int flux_blocks = 0;
+  RfxbNtffFace* d_ntff = nullptr;
+  std::vector<RfxbNtffFace> ntff;   // six faces per plan with a box
+  std::vector<long long> ntff_off;  // float2 offset of each face in its plan's buffers
+  int ntff_blocks = 0;
   CUtensorMap* d_maps = nullptr;   // RFXB_NMAPS per plan
   int* d_status = nullptr;         // device status word of the group's launches
   int fwd_mode = 0;                // forward step kernel variant (see rfxb_fwd.cu)
@@ -909,6 +916,43 @@ int build_group(RfxbBatch* g) {
   if (!g->flux.empty()) {
     if (int rc = galloc((void**)&g->d_flux, sizeof(RfxbFluxPlane) * g->flux.size())) return rc;
   }
+  // NTFF boxes: faces x_lo, x_hi, y_lo, y_hi, z_lo, z_hi with the tangential
+  // components of rfx/farfield.py:247-269
+  static const int kNtffComp[3][4] = {{RFXB_EY, RFXB_EZ, RFXB_HY, RFXB_HZ},
+                                      {RFXB_EX, RFXB_EZ, RFXB_HX, RFXB_HZ},
+                                      {RFXB_EX, RFXB_EY, RFXB_HX, RFXB_HY}};
+  g->ntff.clear();
+  g->ntff_off.clear();
+  int nblocks = 0;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    RfxbPlan* p = g->plans[q];
+    if (!p->has_ntff) continue;
+    const RfxbNtffDesc& b = p->ntff;
+    const int lo[3] = {b.i_lo, b.j_lo, b.k_lo}, hi[3] = {b.i_hi, b.j_hi, b.k_hi};
+    long long off = 0;
+    for (int f = 0; f < 6; ++f) {
+      const int ax = f / 2, t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+      RfxbNtffFace A{};
+      A.inst = (int)q;
+      A.axis = ax;
+      A.index = (f & 1) ? hi[ax] : lo[ax];
+      A.lo1 = lo[t1];
+      A.n1 = hi[t1] - lo[t1];
+      A.lo2 = lo[t2];
+      A.n2 = hi[t2] - lo[t2];
+      A.nf = b.n_freqs;
+      for (int t = 0; t < 4; ++t) A.comp[t] = kNtffComp[ax][t];
+      A.block0 = nblocks;
+      nblocks += (A.n1 * A.n2 + 255) / 256;
+      g->ntff.push_back(A);
+      g->ntff_off.push_back(off);
+      off += (long long)A.nf * A.n1 * A.n2 * 4;
+    }
+  }
+  g->ntff_blocks = nblocks;
+  if (!g->ntff.empty()) {
+    if (int rc = galloc((void**)&g->d_ntff, sizeof(RfxbNtffFace) * g->ntff.size())) return rc;
+  }
   if (!g->dft.empty()) {
     if (int rc = galloc((void**)&g->d_dft, sizeof(RfxbDftPlane) * g->dft.size())) return rc;
   }
@@ -929,7 +973,7 @@ int upload_maps(RfxbBatch* g, cudaStream_t st) {
 
 // Upload descriptors with this call's IO pointers.
 int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_prb, bool* has_flux,
-                 cudaStream_t st) {
+                 bool* has_ntff, cudaStream_t st) {
   std::vector<RfxbInst> insts(g->plans.size());
   *has_dft = false;
   *has_prb = false;
@@ -960,6 +1004,22 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
       if (on) *has_flux = true;
     }
   }
+  *has_ntff = false;
+  for (size_t f = 0; f < g->ntff.size(); ++f) {
+    RfxbNtffFace& A = g->ntff[f];
+    const RfxbStepIO* io = ios ? &ios[A.inst] : nullptr;
+    const bool on = io && io->ntff_acc_dev && io->ntff_cmp_dev && io->ntff_phase_dev;
+    A.acc = on ? static_cast<float2*>(io->ntff_acc_dev) + g->ntff_off[f] : nullptr;
+    A.cmp = on ? static_cast<float2*>(io->ntff_cmp_dev) + g->ntff_off[f] : nullptr;
+    A.phase = on ? static_cast<const float2*>(io->ntff_phase_dev) : nullptr;
+    if (on) *has_ntff = true;
+  }
+  for (const auto& A : g->ntff)
+    if (*has_ntff && A.acc == nullptr)
+      return fail(RFXB_E_INVALID, "either every NTFF box of a group gets accumulators and phase table, or none");
+  if (!g->ntff.empty())
+    RFXB_CUDA(cudaMemcpyAsync(g->d_ntff, g->ntff.data(), sizeof(RfxbNtffFace) * g->ntff.size(),
+                              cudaMemcpyHostToDevice, st));
   for (const auto& pl : g->flux)
     if (*has_flux && pl.acc == nullptr)
       return fail(RFXB_E_INVALID, "either every flux monitor of a group gets accumulator and kernel, or none");
@@ -979,7 +1039,8 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
   return 0;
 }
 
-int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, bool has_flux, cudaStream_t st) {
+int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, bool has_flux, bool has_ntff,
+                 cudaStream_t st) {
   int par = par0;
   bool em = false;   // stage the PEC edge masks when a plan of the group has one
   for (auto* p : g->plans) em = em || p->inst.emask != nullptr;
@@ -1003,6 +1064,8 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, b
       dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, par ^ 1);
     if (has_flux)
       flux_kernel<<<g->flux_blocks, 256, 0, st>>>(g->d_inst, g->d_flux, (int)g->flux.size(), n, par ^ 1);
+    if (has_ntff)
+      ntff_kernel<<<g->ntff_blocks, 256, 0, st>>>(g->d_inst, g->d_ntff, (int)g->ntff.size(), n, par ^ 1);
     par ^= 1;
   }
   RFXB_CUDA(cudaGetLastError());
@@ -1054,16 +1117,16 @@ int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, c
   const int par0 = g->plans[0]->par;
   for (auto* p : g->plans)
     if (p->par != par0) return fail(RFXB_E_STATE, "plans of a batch must share the step parity");
-  bool has_dft = false, has_prb = false, has_flux = false;
-  if (int rc = upload_group(g, ios, &has_dft, &has_prb, &has_flux, st)) return rc;
+  bool has_dft = false, has_prb = false, has_flux = false, has_ntff = false;
+  if (int rc = upload_group(g, ios, &has_dft, &has_prb, &has_flux, &has_ntff, st)) return rc;
   if (graphs_enabled() && n_steps >= 4) {
-    const GraphKey key{0, step0, n_steps, par0, 0, (has_dft ? 1 : 0) | (has_flux ? 2 : 0)};
+    const GraphKey key{0, step0, n_steps, par0, 0, (has_dft ? 1 : 0) | (has_flux ? 2 : 0) | (has_ntff ? 4 : 0)};
     if (int rc = run_graph(g, key, st, [&](cudaStream_t cs) {
-          return launch_steps(g, step0, n_steps, par0, has_dft, has_flux, cs);
+          return launch_steps(g, step0, n_steps, par0, has_dft, has_flux, has_ntff, cs);
         }))
       return rc;
   } else {
-    if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, has_flux, st)) return rc;
+    if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, has_flux, has_ntff, st)) return rc;
   }
   for (auto* p : g->plans) p->par = (par0 + n_steps) & 1;
   return 0;
@@ -1255,6 +1318,11 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
       return fail(RFXB_E_INVALID, "flux monitor region out of range or empty");
   }
   if (d->n_flux > 0 && !d->flux_host) return fail(RFXB_E_INVALID, "flux monitors need descriptors");
+  if (const RfxbNtffDesc* b = d->ntff_host) {
+    if (b->i_lo < 0 || b->i_lo >= b->i_hi || b->i_hi >= d->nx || b->j_lo < 0 || b->j_lo >= b->j_hi ||
+        b->j_hi >= d->ny || b->k_lo < 0 || b->k_lo >= b->k_hi || b->k_hi >= d->nz || b->n_freqs < 1)
+      return fail(RFXB_E_INVALID, "NTFF box out of range or empty");
+  }
   const int* hb = d->grad_box;
   if (hb[0] < hb[1]) {
     if (hb[0] < 0 || hb[1] > d->nx || hb[2] < 0 || hb[3] > d->ny || hb[4] < 0 || hb[5] > d->nz || hb[2] >= hb[3] ||
@@ -1374,6 +1442,10 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
     p->dft_cells.push_back(n1 * n2);
   }
   for (int q = 0; q < d->n_flux; ++q) p->flux.push_back(d->flux_host[q]);
+  if (d->ntff_host) {
+    p->has_ntff = true;
+    p->ntff = *d->ntff_host;
+  }
   for (int k = 0; k < 6; ++k) I.hb[k] = hb[k];
   if (hb[0] >= hb[1]) { I.hb[0] = 0; I.hb[1] = 0; }
   p->hcells = (long long)(I.hb[1] - I.hb[0]) * (I.hb[3] - I.hb[2]) * (I.hb[5] - I.hb[4]);

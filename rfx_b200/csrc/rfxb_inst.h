@@ -108,6 +108,18 @@ struct RfxbWork {          // one CTA: a (y, z) tile over an x range
   int xa, xb;
 };
 
+struct RfxbNtffFace {      // one face of one instance's NTFF box
+  int inst;
+  int axis, index;         // normal axis and face plane
+  int lo1, n1, lo2, n2;    // tangential ranges (x face: j, k; y face: i, k; z face: i, j)
+  int nf;
+  int comp[4];             // tangential E E H H component codes
+  float2* acc;             // running sums (nf, n1, n2, 4) complex64
+  float2* cmp;             // Kahan residuals, same layout
+  const float2* phase;     // [n][2][nf]: E and H factors times dt
+  int block0;              // first CTA of this face in the launch
+};
+
 struct RfxbFluxPlane {     // one Poynting-flux monitor of one instance
   int inst;
   int axis, index, im1;    // normal axis, E plane, the other H plane (index-1, or 0)

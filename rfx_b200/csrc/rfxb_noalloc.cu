@@ -97,6 +97,7 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   if (step0 < 0 || n_steps < 0) return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: negative step range");
   if (d->n_dft > 0) return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: DFT planes need a plan");
   if (d->n_flux > 0) return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: flux monitors need a plan");
+  if (d->ntff_host) return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: an NTFF box needs a plan");
   if (d->grad_box[0] < d->grad_box[1])
     return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: gradient regions need a plan");
   if (!d->inv_xe_host || !d->inv_xh_host || !d->inv_ye_host || !d->inv_yh_host || !d->inv_ze_host ||

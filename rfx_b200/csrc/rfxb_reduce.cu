@@ -85,4 +85,54 @@ __global__ void flux_kernel(const RfxbInst* __restrict__ insts, const RfxbFluxPl
   }
 }
 
+// NTFF Huygens-box accumulation for one step (rfx/farfield.py:208-313): on
+// each face the four tangential components times the step's complex64 factor
+// (E factor for the two E components, H factor, half a step later, for the
+// two H components), Kahan-added to the complex64 running sums per real and
+// imaginary part.  One thread per face cell; a thread's 4 components are
+// adjacent (32 B), so a warp reads and writes 1 KB runs per frequency.
+__global__ void __launch_bounds__(256) ntff_kernel(const RfxbInst* __restrict__ insts,
+                                                   const RfxbNtffFace* __restrict__ faces, int nfaces, int n,
+                                                   int par) {
+  int q = 0;
+  while (q + 1 < nfaces && faces[q + 1].block0 <= (int)blockIdx.x) ++q;
+  const RfxbNtffFace& A = faces[q];
+  const RfxbInst& P = insts[A.inst];
+  const int c = (blockIdx.x - A.block0) * blockDim.x + threadIdx.x;
+  const int cells = A.n1 * A.n2;
+  if (c >= cells) return;
+  const int a = A.lo1 + c / A.n2, b = A.lo2 + c % A.n2;
+  int i, j, k;
+  if (A.axis == 0) { i = A.index; j = a; k = b; }
+  else if (A.axis == 1) { i = a; j = A.index; k = b; }
+  else { i = a; j = b; k = A.index; }
+  const long long e = P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
+  float v[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) v[t] = P.F[par][A.comp[t]][e];
+  const float2* ph = A.phase + (long long)n * 2 * A.nf;
+  for (int f = 0; f < A.nf; ++f) {
+    const float2 we = __ldg(ph + f), wh = __ldg(ph + A.nf + f);
+    float4* sp = reinterpret_cast<float4*>(A.acc + ((long long)f * cells + c) * 4);
+    float4* rp = reinterpret_cast<float4*>(A.cmp + ((long long)f * cells + c) * 4);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {    // h = 0: the E pair, h = 1: the H pair
+      const float2 w = h == 0 ? we : wh;
+      float4 s = sp[h], r = rp[h];
+      float* sv = reinterpret_cast<float*>(&s);
+      float* rv = reinterpret_cast<float*>(&r);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {  // (re, im) of the two components
+        const float val = __fmul_rn(v[2 * h + (u >> 1)], (u & 1) ? w.y : w.x);
+        const float y = val - rv[u];
+        const float t = sv[u] + y;
+        rv[u] = (t - sv[u]) - y;
+        sv[u] = t;
+      }
+      sp[h] = s;
+      rp[h] = r;
+    }
+  }
+}
+
 }  // namespace rfxb

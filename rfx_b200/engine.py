@@ -74,6 +74,7 @@ class PlanSpec:
     dft: list = field(default_factory=list)       # (axis, index, comp, n_freqs)
     grad_box: tuple | None = None                 # (i0, i1, j0, j1, k0, k1)
     flux: list = field(default_factory=list)      # (axis, index, lo1, hi1, lo2, hi2, n_freqs)
+    ntff: tuple | None = None                     # (i_lo, i_hi, j_lo, j_hi, k_lo, k_hi, n_freqs)
 
 
 class Plan:
@@ -144,6 +145,10 @@ class Plan:
         self._keep.append(flux_arr)
         d.n_flux = len(spec.flux)
         d.flux_host = C.cast(flux_arr, C.POINTER(_lib.RfxbFluxDesc))
+        if spec.ntff is not None:
+            box = _lib.RfxbNtffDesc(*(int(v) for v in spec.ntff))
+            self._keep.append(box)
+            d.ntff_host = C.pointer(box)
         self.n_src = len(src)
         self.n_probe = len(prb)
         self.dft = list(spec.dft)
@@ -256,7 +261,10 @@ class Plan:
 
     # -- stepping ------------------------------------------------------------
     @staticmethod
-    def step_io(src_table=None, probe_out=None, dft_accs=None, dft_phases=None, flux_accs=None, flux_kernels=None):
+    def step_io(src_table=None, probe_out=None, dft_accs=None, dft_phases=None, flux_accs=None, flux_kernels=None,
+                ntff=None):
+        """``ntff``: (running sums, Kahan residuals, phase table) device
+        tensors of the NTFF box (layout in ``rfx_b200.simulation.NTFFData``)."""
         io = RfxbStepIO()
         io.src_wave_dev = src_table.data_ptr() if src_table is not None else None
         io.probe_out_dev = probe_out.data_ptr() if probe_out is not None else None
@@ -273,11 +281,14 @@ class Plan:
             io.flux_acc_dev = C.cast(acc, C.POINTER(C.c_void_p))
             io.flux_kernel_dev = C.cast(kn, C.POINTER(C.c_void_p))
             keep += [acc, kn]
+        if ntff is not None:
+            acc, cmp, ph = ntff
+            io.ntff_acc_dev, io.ntff_cmp_dev, io.ntff_phase_dev = acc.data_ptr(), cmp.data_ptr(), ph.data_ptr()
         return io, keep
 
     def advance(self, step0, n_steps, src_table=None, probe_out=None, dft_accs=None, dft_phases=None,
-                flux_accs=None, flux_kernels=None):
-        io, keep = self.step_io(src_table, probe_out, dft_accs, dft_phases, flux_accs, flux_kernels)
+                flux_accs=None, flux_kernels=None, ntff=None):
+        io, keep = self.step_io(src_table, probe_out, dft_accs, dft_phases, flux_accs, flux_kernels, ntff)
         check(self._lib.rfxb_plan_advance(self._h, C.byref(io), int(step0), int(n_steps), _stream()),
               "rfxb_plan_advance")
         del keep

@@ -18,6 +18,7 @@ import torch
 
 from .cpml import build_cpml
 from .engine import Plan, PlanSpec, require_cuda
+from .farfield import init_ntff_data, ntff_descriptor, ntff_phase_table, pack_ntff, unpack_ntff
 from .grid import face_pads, spacing_tables
 from .sources import SourceSpec  # noqa: F401  (re-export: the reference's spec type)
 
@@ -261,11 +262,12 @@ class DeviceRun(NamedTuple):
     vi_rows: list              # per lumped port: [(probe row, sign), ...]
     flux_accs: tuple = ()      # complex128 (4, n_f, n1, n2) per flux monitor
     flux_kernels: tuple = ()   # complex128 (n_steps, 2, n_f) per flux monitor
+    ntff: tuple | None = None  # NTFF box: (sums, Kahan residuals, (n_steps, 2, n_f) phase table)
 
 
 def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
                        dft_time_offset, lumped_specs=(), kappa_max=None, noop_faces=(), flux_monitors=(),
-                       device=None) -> DeviceRun:
+                       ntff_box=None, ntff_data=None, device=None) -> DeviceRun:
     """Build the plan of one simulation and upload its inputs (the set-up half
     of ``run_device``); the caller owns the plan and closes it."""
     dev = require_cuda(device)
@@ -284,7 +286,8 @@ def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources
     plan = Plan(PlanSpec(shape=shape, dt=float(grid.dt), tables=spacing_tables(grid), cpml=cp,
                          pec_axes=pec_axes, sources=[s[:4] for s in srcs], probes=prb,
                          dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in dft_planes],
-                         flux=[(m.axis, m.index, m.lo1, m.hi1, m.lo2, m.hi2, len(m.freqs)) for m in flux_monitors]),
+                         flux=[(m.axis, m.index, m.lo1, m.hi1, m.lo2, m.hi2, len(m.freqs)) for m in flux_monitors],
+                         ntff=ntff_descriptor(ntff_box) if ntff_box is not None else None),
                 dev)
     try:
         em = tangential_edge_masks(_to_np(pec_mask, bool)) if pec_mask is not None else None
@@ -308,30 +311,34 @@ def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources
             faccs.append(torch.from_numpy(np.stack([np.asarray(a, np.complex128) for a in
                                                     (m.e1_dft, m.e2_dft, m.h1_dft, m.h2_dft)])).to(dev).contiguous())
             fkerns.append(torch.from_numpy(flux_kernel_table(m, n_steps, grid.dt)).to(dev))
+        ntff = None
+        if ntff_box is not None:
+            acc, cmp = pack_ntff(ntff_data if ntff_data is not None else init_ntff_data(ntff_box), dev)
+            ntff = (acc, cmp, torch.from_numpy(ntff_phase_table(ntff_box.freqs, n_steps, grid.dt)).to(dev))
     except BaseException:
         plan.close()
         raise
-    return DeviceRun(plan, src_table, probe_out, accs, phases, prb, vi_rows, faccs, fkerns)
+    return DeviceRun(plan, src_table, probe_out, accs, phases, prb, vi_rows, faccs, fkerns, ntff)
 
 
 def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
                dft_time_offset, lumped_specs=(), return_state=True, report_every=None, report_label="",
-               kappa_max=None, noop_faces=(), flux_monitors=(), device=None):
+               kappa_max=None, noop_faces=(), flux_monitors=(), ntff_box=None, ntff_data=None, device=None):
     """Shared driver of the uniform and graded lanes.  Returns (time series,
-    DFT planes, lumped-port results, state, flux monitors)."""
+    DFT planes, lumped-port results, state, flux monitors, NTFF data or None)."""
     n_steps = int(n_steps)
     flux_monitors = list(flux_monitors)
     r = prepare_device_run(grid, materials, n_steps, cpml_axes=cpml_axes, pec_axes=pec_axes, sources=sources,
                            probes=probes, dft_planes=dft_planes, pec_mask=pec_mask, dft_time_offset=dft_time_offset,
                            lumped_specs=lumped_specs, kappa_max=kappa_max, noop_faces=noop_faces,
-                           flux_monitors=flux_monitors, device=device)
+                           flux_monitors=flux_monitors, ntff_box=ntff_box, ntff_data=ntff_data, device=device)
     plan, probe_out, accs = r.plan, r.probe_out, r.dft_accs
     try:
         chunk = int(report_every) if report_every else n_steps
         done = 0
         while done < n_steps:
             k = min(chunk, n_steps - done)
-            plan.advance(done, k, r.src_table, probe_out, accs, r.dft_phases, r.flux_accs, r.flux_kernels)
+            plan.advance(done, k, r.src_table, probe_out, accs, r.dft_phases, r.flux_accs, r.flux_kernels, r.ntff)
             done += k
             if report_every:
                 torch.cuda.current_stream().synchronize()
@@ -357,7 +364,8 @@ def run_device(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes
         for m, a in zip(flux_monitors, r.flux_accs):
             a = a.cpu().numpy()
             out_flux.append(m._replace(e1_dft=a[0], e2_dft=a[1], h1_dft=a[2], h2_dft=a[3]))
-        return ts, out_planes, lumped, state, tuple(out_flux)
+        ntff_out = unpack_ntff(ntff_box, r.ntff[0], r.ntff[1]) if ntff_box is not None else None
+        return ts, out_planes, lumped, state, tuple(out_flux), ntff_out
     finally:
         plan.close()
 
@@ -379,9 +387,10 @@ def run(grid, materials, n_steps, *, boundary="pec", cpml_axes="xyz", pec_axes=N
         stencil_order=2, report_every=None, report_label="", sheet_impedance=None, device=None) -> SimResult:
     """Uniform-grid scan (rfx/simulation.py:1686).  Step order per
     rfx/simulation.py:1255-1685: H, CPML-H, E, CPML-E, PEC faces, PEC mask,
-    soft sources, probes, DFT planes at ``t = (n+1) dt``."""
+    soft sources, probes, NTFF box (an ``NTFFBox``), DFT planes at
+    ``t = (n+1) dt``, flux monitors."""
     _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf,
-                 waveguide_ports=waveguide_ports, ntff=ntff, snapshot=snapshot, aniso_eps=aniso_eps,
+                 waveguide_ports=waveguide_ports, snapshot=snapshot, aniso_eps=aniso_eps,
                  aniso_inv_eps=aniso_inv_eps, pec_occupancy=pec_occupancy, conformal_weights=conformal_weights,
                  wire_port_sparams=wire_port_sparams, wire_refplane_sparams=wire_refplane_sparams,
                  lumped_rlc=lumped_rlc, kerr_chi3=kerr_chi3, mag_sources=mag_sources,
@@ -407,14 +416,15 @@ def run(grid, materials, n_steps, *, boundary="pec", cpml_axes="xyz", pec_axes=N
         raise NotImplementedError(f"boundary={boundary!r} is outside this path")
     srcs = [(s.i, s.j, s.k, s.component, s.waveform) for s in (sources or [])]
     prbs = [(p.i, p.j, p.k, p.component) for p in (probes or [])]
-    ts, planes, lumped, state, flux = run_device(
+    ts, planes, lumped, state, flux, ntff_data = run_device(
         grid, materials, n_steps, cpml_axes=cpml_axes if use_cpml else "", pec_axes=pec_axes, sources=srcs,
         probes=prbs, dft_planes=list(dft_planes or []), pec_mask=pec_mask, dft_time_offset=1,
         lumped_specs=list(lumped_port_sparams or []), return_state=return_state, report_every=report_every,
         report_label=report_label, noop_faces=set(getattr(grid, "pec_faces", None) or ()),
-        flux_monitors=list(flux_monitors or []), device=device)
-    return SimResult(state=state, time_series=ts, dft_planes=planes if dft_planes else None,
-                     flux_monitors=flux if flux_monitors else None, lumped_port_sparams=lumped, grid=grid)
+        flux_monitors=list(flux_monitors or []), ntff_box=ntff, device=device)
+    return SimResult(state=state, time_series=ts, ntff_data=ntff_data, dft_planes=planes if dft_planes else None,
+                     flux_monitors=flux if flux_monitors else None, lumped_port_sparams=lumped, ntff_box=ntff,
+                     grid=grid)
 
 
 def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100, max_steps=50_000,
@@ -438,7 +448,7 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
     over every step, and a check step with value^2 < decay_by * peak stops.
     The steps run between checks are replayed as one captured chunk."""
     _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf, flux_monitors=flux_monitors,
-                 waveguide_ports=waveguide_ports, ntff=ntff, aniso_eps=aniso_eps, aniso_inv_eps=aniso_inv_eps,
+                 waveguide_ports=waveguide_ports, aniso_eps=aniso_eps, aniso_inv_eps=aniso_inv_eps,
                  pec_occupancy=pec_occupancy, conformal_weights=conformal_weights,
                  wire_port_sparams=wire_port_sparams, lumped_port_sparams=lumped_port_sparams,
                  lumped_rlc=lumped_rlc, kerr_chi3=kerr_chi3, mag_sources=mag_sources,
@@ -473,7 +483,7 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
     planes = list(dft_planes or [])
     r = prepare_device_run(grid, materials, max_steps, cpml_axes=cpml_axes if use_cpml else "", pec_axes=pec_axes,
                            sources=srcs, probes=prbs, dft_planes=planes, pec_mask=pec_mask, dft_time_offset=1,
-                           noop_faces=set(getattr(grid, "pec_faces", None) or ()), device=device)
+                           noop_faces=set(getattr(grid, "pec_faces", None) or ()), ntff_box=ntff, device=device)
     plan = r.plan
     try:
         box = (grid.pad_x_lo, grid.nx - grid.pad_x_hi, grid.pad_y_lo, grid.ny - grid.pad_y_hi,
@@ -489,7 +499,8 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
             plan.advance(0, target - done,
                          r.src_table[done:] if r.src_table is not None else None,
                          r.probe_out[done:] if r.probe_out is not None else None,
-                         r.dft_accs, [ph[done:] for ph in r.dft_phases])
+                         r.dft_accs, [ph[done:] for ph in r.dft_phases],
+                         ntff=(r.ntff[0], r.ntff[1], r.ntff[2][done:]) if r.ntff is not None else None)
             first, done = done, target
             if done - 1 != n_check:
                 break
@@ -515,7 +526,9 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
         state = None
         if return_state:
             state = FDTDState(*[t.cpu().numpy() for t in plan.store_fields()], step=done)
-        return SimResult(state=state, time_series=ts, dft_planes=out_planes if planes else None, grid=grid)
+        ntff_data = unpack_ntff(ntff, r.ntff[0], r.ntff[1]) if ntff is not None else None
+        return SimResult(state=state, time_series=ts, ntff_data=ntff_data,
+                         dft_planes=out_planes if planes else None, ntff_box=ntff, grid=grid)
     finally:
         plan.close()
 

@@ -40,7 +40,8 @@ def test_struct_layout_matches_header(tmp_path):
     if shutil.which("gcc") is None:
         pytest.skip("gcc not available")
     structs = {
-        "RfxbDftDesc": _lib.RfxbDftDesc, "RfxbFluxDesc": _lib.RfxbFluxDesc, "RfxbDesc": _lib.RfxbDesc,
+        "RfxbDftDesc": _lib.RfxbDftDesc, "RfxbFluxDesc": _lib.RfxbFluxDesc, "RfxbNtffDesc": _lib.RfxbNtffDesc,
+        "RfxbDesc": _lib.RfxbDesc,
         "RfxbStepIO": _lib.RfxbStepIO, "RfxbAdjointIO": _lib.RfxbAdjointIO,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
@@ -99,6 +100,13 @@ def test_plan_create_rejects_out_of_range_monitors():
     d, keep = _desc(n_probe=1, probe_cells_host=prb.ctypes.data_as(_lib.c_int32_p))
     assert lib.rfxb_plan_create(C.byref(d), C.byref(h)) == -1
     assert "probe" in lib.rfxb_last_error().decode()
+    # an NTFF face plane must lie inside the grid (i_hi is a plane index)
+    for box in ((2, 10, 2, 8, 2, 8, 1), (5, 5, 2, 8, 2, 8, 1), (2, 8, 2, 8, 2, 8, 0)):
+        nb = _lib.RfxbNtffDesc(*box)
+        d, keep = _desc(ntff_host=C.pointer(nb))
+        assert lib.rfxb_plan_create(C.byref(d), C.byref(h)) == -1
+        assert "NTFF" in lib.rfxb_last_error().decode()
+        assert h.value is None
 
 
 def test_cpml_overlap_rejected():
