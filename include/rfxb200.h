@@ -214,6 +214,19 @@ int rfxb_plan_checkpoint_reserve(RfxbPlan* plan, int n_slots);
 int rfxb_plan_checkpoint_save(RfxbPlan* plan, int slot, void* stream);
 int rfxb_plan_checkpoint_load(RfxbPlan* plan, int slot, void* stream);
 
+/* Resumable state of a plan as one byte blob (restart of long runs and
+ * sweeps).  rfx's save_state (rfx/checkpoint.py:33-62) writes the six fields
+ * and the step to HDF5; a resumed CPML run also needs its psi, and a resumed
+ * DFT its Kahan residuals, so the blob holds a header (magic "RFXBST01",
+ * shape, CPML layers and axes, section sizes) followed by the current
+ * fields, psi and DFT residuals in the plan's own layout.  dst / src may be
+ * device or host memory; save_state is asynchronous on `stream`,
+ * restore_state reads the header synchronously and rejects a blob of another
+ * shape or CPML set-up with RFXB_E_SHAPE. */
+long long rfxb_plan_state_bytes(const RfxbPlan* plan);
+int rfxb_plan_save_state(RfxbPlan* plan, void* dst, void* stream);
+int rfxb_plan_restore_state(RfxbPlan* plan, const void* src, void* stream);
+
 /* Reverse-time adjoint: the transpose of the forward step, replacing
  * jax.grad through the scan.  adjoint_begin zeroes the adjoint state and
  * injects the probe cotangent of the last step n_total-1; adjoint_advance

@@ -19,6 +19,9 @@ from .sources import (  # noqa: F401
     make_source, setup_lumped_port,
 )
 from .nonuniform import run_nonuniform  # noqa: F401
+from .checkpoint import (  # noqa: F401
+    load_plan_state, load_snapshots, load_state, save_plan_state, save_snapshots, save_state,
+)
 from .farfield import (  # noqa: F401
     FarFieldResult, NTFFBox, NTFFData, compute_far_field, directivity, init_ntff_data, make_ntff_box,
     radiation_pattern,

@@ -1622,6 +1622,92 @@ int rfxb_plan_checkpoint_load(RfxbPlan* p, int slot, void* stream) {
   return 0;
 }
 
+namespace {
+struct StateHeader {          // leading 128 bytes of a state blob
+  char magic[8];
+  int nx, ny, nz, ncp;
+  unsigned cpml_axes, n_dft;
+  long long elems, psi_elems[3], dft_bytes, total;
+  char pad[128 - 8 - 6 * 4 - 6 * 8];
+};
+static_assert(sizeof(StateHeader) == 128, "state header is 128 bytes");
+const char kStateMagic[8] = {'R', 'F', 'X', 'B', 'S', 'T', '0', '1'};
+
+StateHeader state_header(const RfxbPlan* p) {
+  StateHeader h{};
+  std::memcpy(h.magic, kStateMagic, 8);
+  h.nx = p->nx; h.ny = p->ny; h.nz = p->nz;
+  h.ncp = p->inst.ncp;
+  h.cpml_axes = p->inst.cpml_axes;
+  h.n_dft = (unsigned)p->dft.size();
+  h.elems = p->elems;
+  for (int a = 0; a < 3; ++a) h.psi_elems[a] = p->psi_elems[a];
+  h.dft_bytes = 0;
+  for (size_t q = 0; q < p->dft.size(); ++q) h.dft_bytes += p->dft[q].n_freqs * p->dft_cells[q] * (long long)sizeof(float2);
+  long long n = (long long)sizeof(StateHeader) + 6 * p->elems * (long long)sizeof(float);
+  for (int a = 0; a < 3; ++a) n += 2 * p->psi_elems[a] * (long long)sizeof(float);
+  h.total = n + h.dft_bytes;
+  return h;
+}
+
+// Sections of the blob after the header, in order: (plan buffer, bytes).
+std::vector<std::pair<void*, long long>> state_sections(RfxbPlan* p) {
+  std::vector<std::pair<void*, long long>> v;
+  for (int c = 0; c < 6; ++c) v.emplace_back(p->inst.F[p->par][c], p->elems * (long long)sizeof(float));
+  for (int a = 0; a < 3; ++a) {
+    if (p->psi_elems[a] == 0) continue;
+    v.emplace_back(p->inst.psH[p->par][a], p->psi_elems[a] * (long long)sizeof(float));
+    v.emplace_back(p->inst.psE[p->par][a], p->psi_elems[a] * (long long)sizeof(float));
+  }
+  for (size_t q = 0; q < p->dft_cmp.size(); ++q)
+    v.emplace_back(p->dft_cmp[q], p->dft[q].n_freqs * p->dft_cells[q] * (long long)sizeof(float2));
+  return v;
+}
+}  // namespace
+
+long long rfxb_plan_state_bytes(const RfxbPlan* p) {
+  if (!p) return fail(RFXB_E_INVALID, "null plan");
+  return state_header(p).total;
+}
+
+int rfxb_plan_save_state(RfxbPlan* p, void* dst, void* stream) {
+  if (!p || !dst) return fail(RFXB_E_INVALID, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const StateHeader h = state_header(p);
+  char* out = static_cast<char*>(dst);
+  // pageable source: the copy stages the header before returning
+  RFXB_CUDA(cudaMemcpyAsync(out, &h, sizeof(h), cudaMemcpyDefault, st));
+  RFXB_CUDA(cudaStreamSynchronize(st));
+  long long o = sizeof(h);
+  for (auto& sec : state_sections(p)) {
+    RFXB_CUDA(cudaMemcpyAsync(out + o, sec.first, sec.second, cudaMemcpyDefault, st));
+    o += sec.second;
+  }
+  return 0;
+}
+
+int rfxb_plan_restore_state(RfxbPlan* p, const void* src, void* stream) {
+  if (!p || !src) return fail(RFXB_E_INVALID, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  StateHeader h{};
+  RFXB_CUDA(cudaMemcpyAsync(&h, src, sizeof(h), cudaMemcpyDefault, st));
+  RFXB_CUDA(cudaStreamSynchronize(st));
+  if (std::memcmp(h.magic, kStateMagic, 8) != 0) return fail(RFXB_E_INVALID, "not a plan state blob");
+  const StateHeader mine = state_header(p);
+  if (h.nx != mine.nx || h.ny != mine.ny || h.nz != mine.nz || h.ncp != mine.ncp ||
+      h.cpml_axes != mine.cpml_axes || h.n_dft != mine.n_dft || h.elems != mine.elems ||
+      h.psi_elems[0] != mine.psi_elems[0] || h.psi_elems[1] != mine.psi_elems[1] ||
+      h.psi_elems[2] != mine.psi_elems[2] || h.dft_bytes != mine.dft_bytes || h.total != mine.total)
+    return fail(RFXB_E_SHAPE, "state blob was saved from a plan of another shape, CPML or DFT set-up");
+  const char* in = static_cast<const char*>(src);
+  long long o = sizeof(h);
+  for (auto& sec : state_sections(p)) {
+    RFXB_CUDA(cudaMemcpyAsync(sec.first, in + o, sec.second, cudaMemcpyDefault, st));
+    o += sec.second;
+  }
+  return 0;
+}
+
 int rfxb_plan_adjoint_begin(RfxbPlan* p, const RfxbAdjointIO* aio, int n_total, void* stream) {
   if (!p || !aio) return fail(RFXB_E_INVALID, "null argument");
   return group_adjoint_begin(p->self_group, aio, n_total, static_cast<cudaStream_t>(stream));

@@ -300,6 +300,23 @@ class Plan:
         """Synchronise and raise if a bounded wait inside a kernel ran out."""
         check(self._lib.rfxb_plan_device_status(self._h, _stream()), "rfxb_plan_device_status")
 
+    def save_state(self):
+        """The plan's resumable state (fields, psi, DFT Kahan residuals) as a
+        host uint8 array (``rfxb_plan_save_state``)."""
+        n = int(self._lib.rfxb_plan_state_bytes(self._h))
+        if n < 0:
+            check(n, "rfxb_plan_state_bytes")
+        out = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        check(self._lib.rfxb_plan_save_state(self._h, out.data_ptr(), _stream()), "rfxb_plan_save_state")
+        torch.cuda.current_stream().synchronize()
+        return out.numpy().copy()
+
+    def restore_state(self, blob):
+        """Load a blob of :meth:`save_state` (same shape and set-up)."""
+        src = torch.from_numpy(np.ascontiguousarray(blob, np.uint8)).pin_memory()
+        check(self._lib.rfxb_plan_restore_state(self._h, src.data_ptr(), _stream()), "rfxb_plan_restore_state")
+        torch.cuda.current_stream().synchronize()
+
     def checkpoint_reserve(self, n):
         check(self._lib.rfxb_plan_checkpoint_reserve(self._h, int(n)), "rfxb_plan_checkpoint_reserve")
 
