@@ -549,6 +549,67 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     }
     const int b0 = astage_of<NST>(i), b1 = astage_of<NST>(i + 1);
     const float* PS = ring + (i & 1) * L::FLOATS(zp);
+    // Mode 2: r_E / r_H of the y (axes bit 1) and z (bit 2) relations at
+    // footprint position (r, c) = (jj - y0 + 1, kk - z0 + 1), evaluated from
+    // the staged plane and the psi ring; .x .y: y relations q0 q1, .z .w: z
+    // relations q0 q1; zero outside the grid and the slabs.  Each cell reads
+    // its neighbours' relations this way, so no exchange barrier is needed.
+    auto re_at = [&](int r, int c, int axes, bool write) -> float4 {
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      const int jj = y0 - 1 + r, kk = z0 - 1 + c;
+      if (jj < 0 || jj >= C.ny || kk < 0 || kk >= C.nz) return v;
+      int sy = 0, sz = 0;
+      const int dy = ((axes & 1) && C.cpy) ? cpml_side(jj, C.ny, C.ncp, sy) : -1;
+      const int dz = ((axes & 2) && C.cpz) ? cpml_side(kk, C.nz, C.ncp, sz) : -1;
+      if (dy < 0 && dz < 0) return v;
+      const AdjStage<TY>& X = S.st[b0];
+      const float ce = PS[L::CE + r * RFXB_AEW + c + 3];
+      const float ax = X.ae[0][r][c + 3];
+      if (dy >= 0) {
+        const float4 cf = __ldg(P.cpt + (2 + dy) * C.ncp + sy);
+        const int o = r * RFXB_AEW + c + 3;
+        v.x = re_core(A, C, 1, cf, write ? psi_q(P, 1, dy, 0, sy, i, jj, kk) : 0, PS[L::EY + o], +1.f, ce, ax,
+                      write);                                                           // ex <- hz
+        v.y = re_core(A, C, 1, cf, write ? psi_q(P, 1, dy, 1, sy, i, jj, kk) : 0,
+                      PS[L::EY + (TY + 2) * RFXB_AEW + o], -1.f, ce, X.ae[2][r][c + 3], write);   // ez <- hx
+      }
+      if (dz >= 0) {
+        const float4 cf = __ldg(P.cpt + (4 + dz) * C.ncp + sz);
+        const int o = r * n4 + sz;
+        v.z = re_core(A, C, 2, cf, write ? psi_q(P, 2, dz, 0, sz, i, jj, kk) : 0, PS[L::EZ + o], -1.f, ce, ax,
+                      write);                                                           // ex <- hy
+        v.w = re_core(A, C, 2, cf, write ? psi_q(P, 2, dz, 1, sz, i, jj, kk) : 0, PS[L::EZ + (TY + 2) * n4 + o],
+                      +1.f, ce, X.ae[1][r][c + 3], write);                              // ey <- hx
+      }
+      return v;
+    };
+    auto rh_at = [&](int r, int c, int axes, bool write) -> float4 {
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      const int jj = y0 - 1 + r, kk = z0 - 1 + c;
+      if (jj < 0 || jj >= C.ny || kk < 0 || kk >= C.nz) return v;
+      int sy = 0, sz = 0;
+      const int dy = ((axes & 1) && C.cpy) ? cpml_side(jj, C.ny, C.ncp, sy) : -1;
+      const int dz = ((axes & 2) && C.cpz) ? cpml_side(kk, C.nz, C.ncp, sz) : -1;
+      if (dy < 0 && dz < 0) return v;
+      const float p0 = S.p[0][r][c];
+      if (dy >= 0) {
+        const float4 cf = __ldg(P.cpt + (2 + dy) * C.ncp + sy);
+        const int o = r * RFXB_AHW + c + 3;
+        v.x = rh_core(A, C, 1, cf, write ? psi_q(P, 1, dy, 0, sy, i, jj, kk) : 0, PS[L::HY + o], -1.f, p0,
+                      write);                                                           // hx <- ez
+        v.y = rh_core(A, C, 1, cf, write ? psi_q(P, 1, dy, 1, sy, i, jj, kk) : 0,
+                      PS[L::HY + (TY + 1) * RFXB_AHW + o], +1.f, S.p[2][r][c], write);  // hz <- ex
+      }
+      if (dz >= 0) {
+        const float4 cf = __ldg(P.cpt + (4 + dz) * C.ncp + sz);
+        const int hz = L::HZ(zp), o = r * n4 + sz;
+        v.z = rh_core(A, C, 2, cf, write ? psi_q(P, 2, dz, 0, sz, i, jj, kk) : 0, PS[hz + o], +1.f, p0,
+                      write);                                                           // hx <- ey
+        v.w = rh_core(A, C, 2, cf, write ? psi_q(P, 2, dz, 1, sz, i, jj, kk) : 0, PS[hz + (TY + 1) * n4 + o],
+                      -1.f, S.p[1][r][c], write);                                       // hy <- ex
+      }
+      return v;
+    };
     const float xe0 = __ldg(P.xe + i), xe1 = __ldg(P.xe + i + 1);
     const float xh0 = __ldg(P.xh + i), xhm = __ldg(P.xh + i - 1);
     const long long e = cell_index(C, i, j, k);
@@ -592,38 +653,15 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
                       P.ce[cell_index(C, i + 1, y0 + lane, z0 - 1)], false);
     }
 
-    // r_E of the y / z relations at the tile, its +1 row / column and the
-    // halo cells, once per cell (own cells write their psi)
-    if (yz_tile) {
+    // Modes 0 / 1: r_E of the y / z relations at the tile, its +1 row /
+    // column and the halo cells, once per cell into the exchange array (own
+    // cells write their psi)
+    if (MODE != 2 && yz_tile) {
       const AdjStage<TY>& X = S.st[b0];
       auto re_fill = [&](int r, int c, bool write) {
         const int jj = y0 - 1 + r, kk = z0 - 1 + c;
         float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-        if (MODE == 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
-          const float ce = PS[L::CE + r * RFXB_AEW + c + 3];
-          const float ax = X.ae[0][r][c + 3], ay = X.ae[1][r][c + 3], az = X.ae[2][r][c + 3];
-          int sl;
-          if (C.cpy) {
-            const int sd = cpml_side(jj, C.ny, C.ncp, sl);
-            if (sd >= 0) {
-              const float4 cf = __ldg(P.cpt + (2 + sd) * C.ncp + sl);
-              const int o = r * RFXB_AEW + c + 3;
-              v0 = re_core(A, C, 1, cf, psi_q(P, 1, sd, 0, sl, i, jj, kk), PS[L::EY + o], +1.f, ce, ax, write);
-              v1 = re_core(A, C, 1, cf, psi_q(P, 1, sd, 1, sl, i, jj, kk), PS[L::EY + (TY + 2) * RFXB_AEW + o], -1.f,
-                           ce, az, write);
-            }
-          }
-          if (C.cpz) {
-            const int sd = cpml_side(kk, C.nz, C.ncp, sl);
-            if (sd >= 0) {
-              const float4 cf = __ldg(P.cpt + (4 + sd) * C.ncp + sl);
-              const int o = r * n4 + sl;
-              v2 = re_core(A, C, 2, cf, psi_q(P, 2, sd, 0, sl, i, jj, kk), PS[L::EZ + o], -1.f, ce, ax, write);
-              v3 = re_core(A, C, 2, cf, psi_q(P, 2, sd, 1, sl, i, jj, kk), PS[L::EZ + (TY + 2) * n4 + o], +1.f, ce,
-                           ay, write);
-            }
-          }
-        } else if (MODE != 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+        if (jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
           const float ce = P.ce[cell_index(C, i, jj, kk)];
           const float ax = X.ae[0][r][c + 3], ay = X.ae[1][r][c + 3], az = X.ae[2][r][c + 3];
           if (C.cpy) {
@@ -656,17 +694,34 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
 
     // ---- phase A ----
     float ahx = 0.f, ahy = 0.f, ahz = 0.f;
+    float4 rown = make_float4(0.f, 0.f, 0.f, 0.f);   // mode 2: this cell's y / z r_E
     if (own) {
       adj_a_cell<TY, 7, false>(P, A, S, C, b0, b1, i, j, k, ly, lz, xe0, xe1, ye0, ye1, ze0, ze1, true, ahx, ahy,
                                ahz);
       if (C.cpx) { ahz += rx0 - nx0; ahy += rx1 - nx1; }
-      if (C.cpy) {
-        ahz += S.rx[0][ly][lh] - S.rx[0][ly + 1][lh];
-        ahx += S.rx[1][ly][lh] - S.rx[1][ly + 1][lh];
-      }
-      if (C.cpz) {
-        ahy += S.rx[2][ly][lh] - S.rx[2][ly][lh + 1];
-        ahx += S.rx[3][ly][lh] - S.rx[3][ly][lh + 1];
+      if (MODE == 2) {
+        if (yz_tile) {
+          rown = re_at(ly, lh, 3, true);
+          if (C.cpy) {
+            const float4 ry = re_at(ly + 1, lh, 1, false);
+            ahz += rown.x - ry.x;
+            ahx += rown.y - ry.y;
+          }
+          if (C.cpz) {
+            const float4 rz = re_at(ly, lh + 1, 2, false);
+            ahy += rown.z - rz.z;
+            ahx += rown.w - rz.w;
+          }
+        }
+      } else {
+        if (C.cpy) {
+          ahz += S.rx[0][ly][lh] - S.rx[0][ly + 1][lh];
+          ahx += S.rx[1][ly][lh] - S.rx[1][ly + 1][lh];
+        }
+        if (C.cpz) {
+          ahy += S.rx[2][ly][lh] - S.rx[2][ly][lh + 1];
+          ahx += S.rx[3][ly][lh] - S.rx[3][ly][lh + 1];
+        }
       }
       if (P.g && (pmask || prb_tail)) {   // H-probe cotangent of y_n
         for (unsigned m = pmask; m; m &= m - 1) {
@@ -713,11 +768,20 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         adj_a_cell<TY, 5, false>(P, A, S, C, b0, b1, i, y0 - 1, k, 0, lz, xe0, xe1, ye0_r, ye1_r, ze0_r, ze1_r,
                                  false, a1, a2, a3);
         if (C.cpx) a3 += rxh - nxh;
-        if (C.cpy) {
-          a3 += S.rx[0][0][lh] - S.rx[0][1][lh];
-          a1 += S.rx[1][0][lh] - S.rx[1][1][lh];
+        if (MODE == 2) {   // row y0 is this thread's own row: its r_E is rown
+          if (C.cpy) {
+            const float4 r0 = re_at(0, lh, 1, false);
+            a3 += r0.x - rown.x;
+            a1 += r0.y - rown.y;
+          }
+          if (C.cpz) a1 += re_at(0, lh, 2, false).w - re_at(0, lh + 1, 2, false).w;
+        } else {
+          if (C.cpy) {
+            a3 += S.rx[0][0][lh] - S.rx[0][1][lh];
+            a1 += S.rx[1][0][lh] - S.rx[1][1][lh];
+          }
+          if (C.cpz) a1 += S.rx[3][0][lh] - S.rx[3][0][lh + 1];
         }
-        if (C.cpz) a1 += S.rx[3][0][lh] - S.rx[3][0][lh + 1];
         chr = chat(i, y0 - 1, k);
         if (P.g) {
           for (int q = 0; q < P.nprb; ++q) {
@@ -740,10 +804,19 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
                                  ze0_c, ze1_c, false, a1, a2, a3);
         const int r = lane + 1;
         if (C.cpx) a2 += rxh - nxh;
-        if (C.cpy) a1 += S.rx[1][r][0] - S.rx[1][r + 1][0];
-        if (C.cpz) {
-          a2 += S.rx[2][r][0] - S.rx[2][r][1];
-          a1 += S.rx[3][r][0] - S.rx[3][r][1];
+        if (MODE == 2) {
+          if (C.cpy) a1 += re_at(r, 0, 1, false).y - re_at(r + 1, 0, 1, false).y;
+          if (C.cpz) {
+            const float4 z0v = re_at(r, 0, 2, false), z1v = re_at(r, 1, 2, false);
+            a2 += z0v.z - z1v.z;
+            a1 += z0v.w - z1v.w;
+          }
+        } else {
+          if (C.cpy) a1 += S.rx[1][r][0] - S.rx[1][r + 1][0];
+          if (C.cpz) {
+            a2 += S.rx[2][r][0] - S.rx[2][r][1];
+            a1 += S.rx[3][r][0] - S.rx[3][r][1];
+          }
         }
         chz = chat(i, y0 + lane, z0 - 1);
         if (P.g) {
@@ -761,35 +834,14 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     }
     __syncthreads();
 
-    // r_H of the y / z relations at the tile and the low halo row / column
-    // (rows y0-1 .. y0+TY-1, columns z0-1 .. z0+31), once per cell
-    if (yz_tile) {
+    // Modes 0 / 1: r_H of the y / z relations at the tile and the low halo
+    // row / column (rows y0-1 .. y0+TY-1, columns z0-1 .. z0+31), once per
+    // cell into the exchange array
+    if (MODE != 2 && yz_tile) {
       auto rh_fill = [&](int r, int c, bool write, bool ny_, bool nz_) {
         const int jj = y0 - 1 + r, kk = z0 - 1 + c;
         float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-        if (MODE == 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
-          int sl;
-          if (C.cpy && ny_) {
-            const int sd = cpml_side(jj, C.ny, C.ncp, sl);
-            if (sd >= 0) {
-              const float4 cf = __ldg(P.cpt + (2 + sd) * C.ncp + sl);
-              const int o = r * RFXB_AHW + c + 3;
-              v0 = rh_core(A, C, 1, cf, psi_q(P, 1, sd, 0, sl, i, jj, kk), PS[L::HY + o], -1.f, S.p[0][r][c], write);
-              v1 = rh_core(A, C, 1, cf, psi_q(P, 1, sd, 1, sl, i, jj, kk), PS[L::HY + (TY + 1) * RFXB_AHW + o], +1.f,
-                           S.p[2][r][c], write);
-            }
-          }
-          if (C.cpz && nz_) {
-            const int sd = cpml_side(kk, C.nz, C.ncp, sl);
-            if (sd >= 0) {
-              const float4 cf = __ldg(P.cpt + (4 + sd) * C.ncp + sl);
-              const int hz = L::HZ(zp), o = r * n4 + sl;
-              v2 = rh_core(A, C, 2, cf, psi_q(P, 2, sd, 0, sl, i, jj, kk), PS[hz + o], +1.f, S.p[0][r][c], write);
-              v3 = rh_core(A, C, 2, cf, psi_q(P, 2, sd, 1, sl, i, jj, kk), PS[hz + (TY + 1) * n4 + o], -1.f,
-                           S.p[1][r][c], write);
-            }
-          }
-        } else if (MODE != 2 && jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
+        if (jj >= 0 && jj < C.ny && kk >= 0 && kk < C.nz && in_yz_slab(C, jj, kk)) {
           if (C.cpy && ny_) {
             v0 = rh_eval(P, A, C, 1, 0, -1.f, i, jj, kk, S.p[0][r][c], write);   // hx <- ez
             v1 = rh_eval(P, A, C, 1, 1, +1.f, i, jj, kk, S.p[2][r][c], write);   // hz <- ex
@@ -842,13 +894,29 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         az += rhy_prev - rhy;
         ay += rhz_prev - rhz;
       }
-      if (C.cpy) {   // (hx <- ez, -1, q0), (hz <- ex, +1, q1)
-        az += S.rx[0][ly - 1][lh] - S.rx[0][ly][lh];
-        ax += S.rx[1][ly - 1][lh] - S.rx[1][ly][lh];
-      }
-      if (C.cpz) {   // (hx <- ey, +1, q0), (hy <- ex, -1, q1)
-        ay += S.rx[2][ly][lh - 1] - S.rx[2][ly][lh];
-        ax += S.rx[3][ly][lh - 1] - S.rx[3][ly][lh];
+      if (MODE == 2) {
+        if (yz_tile) {
+          const float4 rh = rh_at(ly, lh, 3, true);
+          if (C.cpy) {   // (hx <- ez, -1, q0), (hz <- ex, +1, q1)
+            const float4 ry = rh_at(ly - 1, lh, 1, false);
+            az += ry.x - rh.x;
+            ax += ry.y - rh.y;
+          }
+          if (C.cpz) {   // (hx <- ey, +1, q0), (hy <- ex, -1, q1)
+            const float4 rz = rh_at(ly, lh - 1, 2, false);
+            ay += rz.z - rh.z;
+            ax += rz.w - rh.w;
+          }
+        }
+      } else {
+        if (C.cpy) {   // (hx <- ez, -1, q0), (hz <- ex, +1, q1)
+          az += S.rx[0][ly - 1][lh] - S.rx[0][ly][lh];
+          ax += S.rx[1][ly - 1][lh] - S.rx[1][ly][lh];
+        }
+        if (C.cpz) {   // (hx <- ey, +1, q0), (hy <- ex, -1, q1)
+          ay += S.rx[2][ly][lh - 1] - S.rx[2][ly][lh];
+          ax += S.rx[3][ly][lh - 1] - S.rx[3][ly][lh];
+        }
       }
       if (n >= 1 && (pmask | smask | (unsigned)prb_tail | (unsigned)src_tail)) {
         if (P.g) {   // E-probe cotangent of y_{n-1}
