@@ -156,12 +156,13 @@ def cpu_baseline_port(args, n_workers=1, n_time=60):
 # ---------------------------------------------------------------------------
 
 def _traffic_per_cell(kernel):
-    """DRAM bytes per cell and launch of a step kernel from its committed ncu
-    summary (profiles/<kernel>.md), or None."""
+    """DRAM bytes per cell and time step of a step kernel (all its launches
+    of one step) from its committed ncu summary (profiles/<kernel>.md), or
+    None."""
     path = os.path.join(ROOT, "profiles", f"{kernel}.md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"dram_bytes_per_cell_per_launch:\s*([0-9.eE+-]+)", open(path).read())
+    m = re.search(r"dram_bytes_per_cell_per_step:\s*([0-9.eE+-]+)", open(path).read())
     return float(m.group(1)) if m else None
 
 
@@ -234,19 +235,21 @@ def run_ours(args, rank, world, local_rank):
     # average launch time (one launch per time step in each phase; the
     # backward phase also holds one adjoint-init launch per bench step)
     def roof(kernel, alg, ms, what):
-        launch_s = ms / 1e3 / (N * args.steps)
-        achieved = alg / launch_s / 1e9
+        step_s = ms / 1e3 / (N * args.steps)
+        achieved = alg / step_s / 1e9
         tpc = _traffic_per_cell(kernel)
         return {"kernel": kernel, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4),
                 "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
-                "traffic": (round(tpc * cells) if tpc else None), "algorithmic_bytes_per_launch": int(alg),
+                "traffic": (round(tpc * cells) if tpc else None), "algorithmic_bytes_per_step": int(alg),
                 "share_of_step": round(ms / total_ms, 3), "what": what}
 
     roof_adj = roof("adj_step_kernel", sum(p.adjoint_algorithmic_bytes_per_step() for p in sw.plans), adj_ms,
-                    "fused reverse step, batched over all instances")
+                    "fused reverse step, batched over all instances: variant 2 on the CPML tiles and variant 3 "
+                    "on the plain tiles, two streams; one step = both launches")
     roof_fwd = roof("fwd_step_kernel", sum(p.algorithmic_bytes_per_step() for p in sw.plans), fwd_ms,
-                    "fused forward step, batched over all instances")
+                    "fused forward step, batched over all instances: variant 2 on the CPML tiles and variant 1 "
+                    "on the plain tiles, two streams; one step = both launches")
     roofline, roofline_other = (roof_adj, roof_fwd) if adj_ms >= fwd_ms else (roof_fwd, roof_adj)
 
     # single-instance comparison (each simulation launched on its own)
