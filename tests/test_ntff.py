@@ -212,3 +212,66 @@ def test_run_until_decay_ntff_matches_a_plain_run(cuda):
     for name in oracle.NTFF_FACES:
         a, b = getattr(r1.ntff_data, name), getattr(r2.ntff_data, name)
         assert rel_l2(a, b) < 1e-6, name
+
+
+@pytest.mark.gpu
+def test_monitors_in_a_batch_match_single_plans(cuda):
+    """Two plans of different shapes, each with a DFT plane, a flux monitor and
+    an NTFF box, advanced as one batch (one launch per step and kernel for
+    both): every accumulator matches the plan advanced on its own."""
+    import torch
+    import rfx_b200
+    from rfx_b200.engine import Batch
+    from rfx_b200.simulation import prepare_device_run
+
+    def scene(domain, seed, box, ff, fflux):
+        g = rfx_b200.Grid(freq_max=20e9, domain=domain, dx=1e-3, cpml_layers=4)
+        n = 90
+        t = np.arange(n, dtype=np.float32) * np.float32(g.dt)
+        w = rfx_b200.GaussianPulse(f0=28e9, bandwidth=0.5)(t).astype(np.float32)
+        c = (g.nx // 2, g.ny // 2, g.nz // 2)
+        eps = (1.0 + np.random.default_rng(seed).random(g.shape)).astype(np.float32)
+        mats = rfx_b200.MaterialArrays(eps, np.zeros(g.shape, np.float32), np.ones(g.shape, np.float32))
+        planes = [rfx_b200.init_dft_plane_probe(1, c[1] - 2, "ex", ff, g.shape)]
+        mons = [rfx_b200.init_flux_monitor(2, c[2] + 3, fflux, g.shape, g.dx, g.dx, lo1=3, hi1=g.nx - 3)]
+        kw = dict(cpml_axes="xyz", pec_axes="", sources=[(*c, "ez", w)], probes=[(c[0], c[1] + 1, c[2], "ey")],
+                  dft_planes=planes, pec_mask=None, dft_time_offset=1, flux_monitors=mons,
+                  ntff_box=rfx_b200.NTFFBox(*box))
+        return g, mats, n, kw
+
+    scenes = [scene((0.012, 0.014, 0.011), 1, (4, 9, 5, 11, 4, 10, np.array([25e9, 30e9], np.float32)),
+                    [24e9, 29e9, 33e9], [26e9]),
+              scene((0.016, 0.010, 0.013), 2, (5, 13, 4, 8, 5, 11, np.array([27e9], np.float32)),
+                    [26e9], [24e9, 31e9])]
+
+    def outputs(r):
+        return ([a.cpu().numpy() for a in r.dft_accs] + [a.cpu().numpy() for a in r.flux_accs] +
+                [r.ntff[0].cpu().numpy(), r.probe_out.cpu().numpy()] + [f.cpu().numpy() for f in r.plan.store_fields()])
+
+    single = []
+    for g, mats, n, kw in scenes:
+        r = prepare_device_run(g, mats, n, **kw)
+        try:
+            r.plan.advance(0, n, r.src_table, r.probe_out, r.dft_accs, r.dft_phases, r.flux_accs, r.flux_kernels,
+                           r.ntff)
+            single.append(outputs(r))
+        finally:
+            r.plan.close()
+    runs = [prepare_device_run(g, mats, n, **kw) for g, mats, n, kw in scenes]
+    try:
+        b = Batch([r.plan for r in runs])
+        try:
+            b.advance(0, scenes[0][2], [dict(src_table=r.src_table, probe_out=r.probe_out, dft_accs=r.dft_accs,
+                                             dft_phases=r.dft_phases, flux_accs=r.flux_accs,
+                                             flux_kernels=r.flux_kernels, ntff=r.ntff) for r in runs])
+            b.check_device()
+        finally:
+            b.close()
+        for r, ref in zip(runs, single):
+            for q, (x, y) in enumerate(zip(outputs(r), ref)):
+                assert np.linalg.norm(y) > 0, q
+                assert rel_l2(x, y) < 1e-5, q
+    finally:
+        for r in runs:
+            r.plan.close()
+    torch.cuda.synchronize()
