@@ -38,6 +38,12 @@ METRIC = "Mcell-steps/s fwd+adjoint grad, batched vs single, 1 B200; % HBM roofl
 UNIT = "Mcell-steps/s"
 
 
+def _sweep_cells(args):
+    """Cells of rank 0's sweep (the reference arm runs on rank 0 alone)."""
+    from rfx_b200.workloads import batched_sweep_cells
+    return batched_sweep_cells(seed=0, n_inst=args.instances)
+
+
 def _workload_config(args, cells, world):
     return {"workload": f"batched_sweep: {args.instances} instances (n+17)^3, n~U{{64..160}} seed {{rank}}, "
                         f"CPML 8, {args.time_steps} time steps, forward + probe-DFT objective + adjoint "
@@ -339,7 +345,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": _workload_config(args, 0, world), "cpu_baseline": cb,
+            "config": _workload_config(args, _sweep_cells(args), world), "cpu_baseline": cb,
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference = NumPy float32 restatement of rfx's scan body and its transpose (oracle port); "
                     "rfx itself needs JAX, which is not installable offline here"}

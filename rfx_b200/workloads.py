@@ -107,6 +107,18 @@ def adjoint_region(seed=0, n_steps=3000):
     return g, eps, sig, src, probes, box, freqs
 
 
+def batched_sweep_cells(seed=0, n_inst=64, n_lo=64, n_hi=160):
+    """Total cell count of ``batched_sweep(seed, n_inst, ...)`` without
+    building its material arrays (same size draw, same grids)."""
+    sizes = np.random.default_rng(seed).integers(n_lo, n_hi + 1, n_inst)
+    dx = 0.5e-3
+    total = 0
+    for n in sizes:
+        g = Grid(freq_max=20e9, domain=(int(n) * dx,) * 3, dx=dx, cpml_layers=8)
+        total += g.nx * g.ny * g.nz
+    return int(total)
+
+
 def batched_sweep(seed=0, n_inst=64, n_steps=2000, n_lo=64, n_hi=160):
     rng = np.random.default_rng(seed)
     dx = 0.5e-3
