@@ -26,7 +26,11 @@
 //      tile reaches both slabs of an axis;
 //   3  TMA staging (4 planes) with the CPML code compiled out, for the
 //      tiles and x ranges whose reverse step touches no slab (the host runs
-//      them beside variant 2 or 1 on a second stream).
+//      them beside variant 2 or 1 on a second stream);
+//   4  variant 2 for tiles that reach no y slab: the y relations and the
+//      edge-mask staging compiled out and the ring without its y-slab
+//      arrays, so the shared memory (57 KB) and 64 registers allow four
+//      CTAs per SM instead of three (the host runs it on a third stream).
 #include "rfxb_common.cuh"
 
 namespace rfxb {
@@ -50,7 +54,9 @@ struct AdjDims {
   static constexpr unsigned BYTES = 4u * (NE + NB + NH + NC);
 };
 
-template <int TY>
+// One plane stage; EMS: with the tile's PEC edge-mask bits (staged only when
+// the plan has a mask; variant 4 has no room for them).
+template <int TY, bool EMS>
 struct __align__(128) AdjStage {
   float ae[3][TY + 2][RFXB_AEW];   // masked adjoint E, rows y0-1 .. y0+TY, z from z0-4
   float p0[AdjDims<TY>::P0];
@@ -59,23 +65,35 @@ struct __align__(128) AdjStage {
   float ah[3][TY + 1][RFXB_AHW];   // adjoint H, rows y0-1 .. y0+TY-1, z from z0-4
   float p2[AdjDims<TY>::P2];
   float ca[TY][RFXB_TZ];           // ca of the tile
-  unsigned char em[TY][RFXB_TZ];   // PEC edge-mask bits of the tile (staged only when the plan has a mask)
+  unsigned char em[TY][RFXB_TZ];   // PEC edge-mask bits of the tile
+};
+template <int TY>
+struct __align__(128) AdjStage<TY, false> {
+  float ae[3][TY + 2][RFXB_AEW];
+  float p0[AdjDims<TY>::P0];
+  float cbp[TY + 2][RFXB_AEW];
+  float p1[AdjDims<TY>::P1];
+  float ah[3][TY + 1][RFXB_AHW];
+  float p2[AdjDims<TY>::P2];
+  float ca[TY][RFXB_TZ];
 };
 
-// The plane stages come last so that a kernel using fewer of them (mode 2)
-// allocates only those, followed by its psi ring.
+// The plane stages come last so that a kernel using fewer of them (modes 2
+// and 4) allocates only those, followed by its psi ring (modes 2, 4) or the
+// exchange array of the CPML terms (modes 0, 1): r_E / r_H of the y and z
+// relations (y q0, y q1, z q0, z q1) at rows y0-1 .. y0+TY, columns
+// z0-1 .. z0+32.
 template <int TY>
+using AdjExchange = float[4][TY + 2][RFXB_TZ + 2];
+
+template <int TY, bool EMS>
 struct AdjSmem {
   float p[3][TY + 1][RFXB_TZ + 1];   // ch * aH1 of plane i, [y - y0 + 1][z - z0 + 1]
-  // CPML terms of the y / z relations exchanged between neighbouring cells:
-  // phase A r_E of (y q0, y q1, z q0, z q1) at rows y0-1 .. y0+TY, columns
-  // z0-1 .. z0+32; then phase B r_H at rows y0-1 .. y0+TY-1, columns z0-1 .. z0+31
-  float rx[4][TY + 2][RFXB_TZ + 2];
   RfxbInst P;
   AdjInst A;
   unsigned long long mbar[RFXB_ANSTAGE];
-  unsigned long long pbar[2];        // psi ring (mode 2)
-  AdjStage<TY> st[RFXB_ANSTAGE];
+  unsigned long long pbar[2];        // psi ring (modes 2, 4)
+  AdjStage<TY, EMS> st[RFXB_ANSTAGE];
 };
 
 // Plane p lives in stage (p + 1) mod NST.
@@ -96,11 +114,12 @@ __device__ __forceinline__ uint32_t astage_parity(int p, int xa) { return (uint3
 //   CEN [TY+1][36]     ce of plane p+1 on the H footprint
 //   EZ  [q][TY+2][n4]  adjoint E-side psi of the z slab, layer s
 //   HZ  [q][TY+1][n4]  adjoint H-side psi of the z slab
-template <int TY>
+// (YS false, variant 4: no EY / HY arrays.)
+template <int TY, bool YS>
 struct APsiSlot {
   static constexpr int EY = 0;
-  static constexpr int HY = EY + up32(2 * (TY + 2) * RFXB_AEW);
-  static constexpr int EXN = HY + up32(2 * (TY + 1) * RFXB_AHW);
+  static constexpr int HY = EY + (YS ? up32(2 * (TY + 2) * RFXB_AEW) : 0);
+  static constexpr int EXN = HY + (YS ? up32(2 * (TY + 1) * RFXB_AHW) : 0);
   static constexpr int HX = EXN + up32(2 * (TY + 1) * RFXB_AHW);
   static constexpr int CE = HX + up32(2 * TY * RFXB_TZ);
   static constexpr int CEN = CE + up32((TY + 2) * RFXB_AEW);
@@ -202,13 +221,13 @@ __device__ __forceinline__ bool in_yz_slab(const AdjCtx& C, int j, int k) {
 // Phase A at (i, jj, kk): aH1 components selected by MASK (1 hx, 2 hy, 4 hz).
 // With CP, the CPML-E^T terms are evaluated here at the cell and its +1
 // neighbours (the prologue plane); without, the caller adds them.
-template <int TY, int MASK, bool CP = true>
-__device__ __forceinline__ void adj_a_cell(const RfxbInst& P, const AdjInst& A, const AdjSmem<TY>& S,
+template <int TY, int MASK, bool CP = true, class SM>
+__device__ __forceinline__ void adj_a_cell(const RfxbInst& P, const AdjInst& A, const SM& S,
                                            const AdjCtx& C, int b0, int b1, int i, int jj, int kk, int ly, int lz,
                                            float xe0, float xe1, float ye0, float ye1, float ze0, float ze1,
                                            bool own, float& ahx, float& ahy, float& ahz) {
-  const AdjStage<TY>& X = S.st[b0];
-  const AdjStage<TY>& Y = S.st[b1];
+  const auto& X = S.st[b0];
+  const auto& Y = S.st[b1];
   const float cb0 = X.cbp[ly][lz];
   const float ax0 = X.ae[0][ly][lz], ay0 = X.ae[1][ly][lz], az0 = X.ae[2][ly][lz];
   const float qx = cb0 * ax0, qy = cb0 * ay0, qz = cb0 * az0;
@@ -243,10 +262,10 @@ __device__ __forceinline__ void adj_a_cell(const RfxbInst& P, const AdjInst& A, 
   }
 }
 
-template <int TY>
-__device__ __forceinline__ void adj_load_stage(AdjSmem<TY>& S, const AdjCtx& C, const float* aF0, const float* ca,
+template <int TY, class SM>
+__device__ __forceinline__ void adj_load_stage(SM& S, const AdjCtx& C, const float* aF0, const float* ca,
                                                const float* cb, int y0, int z0, int ip, int tid) {
-  AdjStage<TY>& D = S.st[astage_of<RFXB_ANSTAGE>(ip)];
+  auto& D = S.st[astage_of<RFXB_ANSTAGE>(ip)];
   const long long pb = C.off0 + (long long)ip * C.ps;
   constexpr int RE = (TY + 2) * 10, RH = (TY + 1) * 9, RC = TY * 8;
   constexpr int NE = 4 * RE, NH = 3 * RH, NC = RC;
@@ -271,14 +290,16 @@ __device__ __forceinline__ void adj_load_stage(AdjSmem<TY>& S, const AdjCtx& C, 
 
 // TMA boxes of plane ip (one thread): adjoint E and H of parity apar, cb with
 // the E footprint, ca of the tile.
-template <int TY, int NST>
-__device__ __forceinline__ void adj_tma_stage(AdjSmem<TY>& S, const CUtensorMap* tm, int apar, int y0, int z0,
+template <int TY, int NST, bool EMS>
+__device__ __forceinline__ void adj_tma_stage(AdjSmem<TY, EMS>& S, const CUtensorMap* tm, int apar, int y0, int z0,
                                               int ip) {
   const int s = astage_of<NST>(ip);
   const uint32_t mb = smem_u32(&S.mbar[s]);
-  const bool em = S.P.emask != nullptr;
+  const bool em = EMS && S.P.emask != nullptr;
   mbar_expect_tx(mb, AdjDims<TY>::BYTES + (em ? (unsigned)(TY * RFXB_TZ) : 0u));
-  if (em) tma_load_4d(smem_u32(&S.st[s].em[0][0]), tm + RFXB_MAP_EMASK, z0, y0 + 1, ip + 1, 0, mb);
+  if constexpr (EMS) {
+    if (em) tma_load_4d(smem_u32(&S.st[s].em[0][0]), tm + RFXB_MAP_EMASK, z0, y0 + 1, ip + 1, 0, mb);
+  }
   tma_load_4d(smem_u32(&S.st[s].ae[0][0][0]), tm + 5 + apar, z0 - 4, y0, ip + 1, 0, mb);
   tma_load_4d(smem_u32(&S.st[s].cbp[0][0]), tm + 9, z0 - 4, y0, ip + 1, 1, mb);
   tma_load_4d(smem_u32(&S.st[s].ah[0][0][0]), tm + 7 + apar, z0 - 4, y0, ip + 1, 3, mb);
@@ -309,10 +330,10 @@ __device__ __forceinline__ int atile_side(int lo, int hi, int n, int ncp) {
 }
 
 // Issue the mode-2 ring boxes of plane p (one thread).
-template <int TY>
+template <int TY, bool YS>
 __device__ __forceinline__ void apsi_issue(float* slot, uint32_t mb, const CUtensorMap* tm, const AdjCtx& C, int zp4,
                                            int y0, int z0, int p, bool yz_tile, int ysd, int zsd, int n4) {
-  using L = APsiSlot<TY>;
+  using L = APsiSlot<TY, YS>;
   const int par = C.par;
   int sx = 0, sn = 0;
   const int xsd = C.cpx ? cpml_side(p, C.nx, C.ncp, sx) : -1;
@@ -345,6 +366,8 @@ template <int MODE>
 struct AdjBounds { static constexpr int MIN_CTAS = 4; };
 template <>
 struct AdjBounds<2> { static constexpr int MIN_CTAS = 3; };
+template <>
+struct AdjBounds<4> { static constexpr int MIN_CTAS = 4; };
 
 template <int TY, int MODE>
 __global__ void __launch_bounds__(32 * TY, AdjBounds<MODE>::MIN_CTAS)
@@ -352,11 +375,15 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
                 const RfxbWork* __restrict__ work, const CUtensorMap* __restrict__ maps, int n, int par, int apar,
                 int zp) {
   constexpr bool TMA = MODE != 0;
-  constexpr int NST = MODE == 2 ? 3 : RFXB_ANSTAGE;   // plane stages
-  using L = APsiSlot<TY>;
+  constexpr bool RING = MODE == 2 || MODE == 4;       // psi ring
+  constexpr bool YS = MODE != 4;                      // y-slab relations compiled in
+  constexpr int NST = RING ? 3 : RFXB_ANSTAGE;        // plane stages
+  using L = APsiSlot<TY, YS>;
+  using SM = AdjSmem<TY, MODE != 4>;
   extern __shared__ __align__(128) unsigned char adj_smem_raw[];
-  AdjSmem<TY>& S = *reinterpret_cast<AdjSmem<TY>*>(adj_smem_raw);
-  float* ring = reinterpret_cast<float*>(&S.st[NST]);   // mode 2: two psi slots after the stages
+  SM& S = *reinterpret_cast<SM*>(adj_smem_raw);
+  float* ring = reinterpret_cast<float*>(&S.st[NST]);   // modes 2, 4: two psi slots after the stages
+  auto& rx = *reinterpret_cast<AdjExchange<TY>*>(&S.st[NST]);   // modes 0, 1: the exchange array
   const int lane = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * 32 + lane;
   const RfxbWork w = work[blockIdx.x];
@@ -369,7 +396,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   }
   if (TMA && tid == 0) {
     for (int q = 0; q < NST; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
-    if (MODE == 2) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
+    if (RING) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
     mbar_fence_init();
   }
   __syncthreads();
@@ -384,7 +411,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   const int y0 = w.y0, z0 = w.z0;
   // the +1 neighbours of the tile (row y0+TY, column z0+32) also read CPML terms
   C.cpx = MODE != 3 && C.ncp > 0 && (P.cpml_axes & 1u);
-  C.cpy = MODE != 3 && C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY >= C.ny - C.ncp);
+  C.cpy = MODE != 3 && YS && C.ncp > 0 && (P.cpml_axes & 2u) && (y0 - 1 < C.ncp || y0 + TY >= C.ny - C.ncp);
   C.cpz = MODE != 3 && C.ncp > 0 && (P.cpml_axes & 4u) && (z0 - 1 < C.ncp || z0 + 32 >= C.nz - C.ncp);
   const float* aF0 = A.aF[apar][0];
   float* aFo = A.aF[apar ^ 1][0];
@@ -425,19 +452,19 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   // mode-2 psi ring: the slab side this tile reaches per axis, and the
   // bookkeeping of the two slots (identical in every thread)
   const bool yz_tile = C.cpy || C.cpz;
-  const int ysd = (MODE == 2 && C.cpy) ? atile_side(y0 - 1, y0 + TY, C.ny, C.ncp) : -1;
-  const int zsd = (MODE == 2 && C.cpz) ? atile_side(z0 - 1, z0 + 32, C.nz, C.ncp) : -1;
+  const int ysd = (RING && C.cpy) ? atile_side(y0 - 1, y0 + TY, C.ny, C.ncp) : -1;
+  const int zsd = (RING && C.cpz) ? atile_side(z0 - 1, z0 + 32, C.nz, C.ncp) : -1;
   const int n4 = P.ncp4;
   auto xslab = [&](int p) { return C.cpx && p >= 0 && p < C.nx && (p < C.ncp || p >= C.nx - C.ncp); };
   auto psi_need = [&](int p) {
-    if (MODE != 2 || p < 0 || p >= C.nx) return false;
+    if (!RING || p < 0 || p >= C.nx) return false;
     return yz_tile || xslab(p) || xslab(p + 1);
   };
   unsigned pph = 0u, pout = 0u;
   auto psi_fill = [&](int p) {
     if (!psi_need(p)) return;
     if (tid == 0)
-      apsi_issue<TY>(ring + (p & 1) * L::FLOATS(zp), smem_u32(&S.pbar[p & 1]), tm, C, zp, y0, z0, p, yz_tile, ysd,
+      apsi_issue<TY, YS>(ring + (p & 1) * L::FLOATS(zp), smem_u32(&S.pbar[p & 1]), tm, C, zp, y0, z0, p, yz_tile, ysd,
                      zsd, n4);
     pout |= 1u << (p & 1);
   };
@@ -519,7 +546,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   // CTA owning a plane writes its psi when it evaluates it.
   float rx0 = 0.f, rx1 = 0.f, rxh = 0.f;
   if (C.cpx) {
-    const AdjStage<TY>& X0 = S.st[astage_of<NST>(xa)];
+    const auto& X0 = S.st[astage_of<NST>(xa)];
     if (own) {
       const float ce = P.ce[cell_index(C, xa, j, k)];
       rx0 = re_eval(P, A, C, 0, 0, -1.f, xa, j, k, X0.ae[1][ly][lz], ce, true);
@@ -562,7 +589,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       const int dy = ((axes & 1) && C.cpy) ? cpml_side(jj, C.ny, C.ncp, sy) : -1;
       const int dz = ((axes & 2) && C.cpz) ? cpml_side(kk, C.nz, C.ncp, sz) : -1;
       if (dy < 0 && dz < 0) return v;
-      const AdjStage<TY>& X = S.st[b0];
+      const auto& X = S.st[b0];
       const float ce = PS[L::CE + r * RFXB_AEW + c + 3];
       const float ax = X.ae[0][r][c + 3];
       if (dy >= 0) {
@@ -616,8 +643,8 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
 
     // x relations of plane i+1 (written by this CTA when it owns that plane)
     float nx0 = 0.f, nx1 = 0.f, nxh = 0.f;
-    if (MODE == 2 && xslab(i + 1)) {   // psi and ce of plane i+1 from the ring
-      const AdjStage<TY>& Y1 = S.st[b1];
+    if (RING && xslab(i + 1)) {   // psi and ce of plane i+1 from the ring
+      const auto& Y1 = S.st[b1];
       const bool wr = i + 1 < xb;
       int sx;
       const int sd = cpml_side(i + 1, C.nx, C.ncp, sx);
@@ -637,8 +664,8 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         xnext(lane + 1, 3, y0 + lane, z0 - 1, 0.f, Y1.ae[2][lane + 1][3], false, d0, d1);
         nxh = d1;
       }
-    } else if (MODE != 2 && C.cpx && i + 1 < C.nx) {
-      const AdjStage<TY>& Y1 = S.st[b1];
+    } else if (!RING && C.cpx && i + 1 < C.nx) {
+      const auto& Y1 = S.st[b1];
       const bool wr = i + 1 < xb;
       if (own) {
         const float ce = P.ce[e + C.ps];
@@ -656,8 +683,8 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     // Modes 0 / 1: r_E of the y / z relations at the tile, its +1 row /
     // column and the halo cells, once per cell into the exchange array (own
     // cells write their psi)
-    if (MODE != 2 && yz_tile) {
-      const AdjStage<TY>& X = S.st[b0];
+    if (!RING && yz_tile) {
+      const auto& X = S.st[b0];
       auto re_fill = [&](int r, int c, bool write) {
         const int jj = y0 - 1 + r, kk = z0 - 1 + c;
         float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
@@ -673,10 +700,10 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
             v3 = re_eval(P, A, C, 2, 1, +1.f, i, jj, kk, ay, ce, write);   // ey <- hx
           }
         }
-        S.rx[0][r][c] = v0;
-        S.rx[1][r][c] = v1;
-        S.rx[2][r][c] = v2;
-        S.rx[3][r][c] = v3;
+        rx[0][r][c] = v0;
+        rx[1][r][c] = v1;
+        rx[2][r][c] = v2;
+        rx[3][r][c] = v3;
       };
       re_fill(ly, lh, own);
       constexpr int W = RFXB_TZ + 2;
@@ -699,7 +726,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       adj_a_cell<TY, 7, false>(P, A, S, C, b0, b1, i, j, k, ly, lz, xe0, xe1, ye0, ye1, ze0, ze1, true, ahx, ahy,
                                ahz);
       if (C.cpx) { ahz += rx0 - nx0; ahy += rx1 - nx1; }
-      if (MODE == 2) {
+      if (RING) {
         if (yz_tile) {
           rown = re_at(ly, lh, 3, true);
           if (C.cpy) {
@@ -715,12 +742,12 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         }
       } else {
         if (C.cpy) {
-          ahz += S.rx[0][ly][lh] - S.rx[0][ly + 1][lh];
-          ahx += S.rx[1][ly][lh] - S.rx[1][ly + 1][lh];
+          ahz += rx[0][ly][lh] - rx[0][ly + 1][lh];
+          ahx += rx[1][ly][lh] - rx[1][ly + 1][lh];
         }
         if (C.cpz) {
-          ahy += S.rx[2][ly][lh] - S.rx[2][ly][lh + 1];
-          ahx += S.rx[3][ly][lh] - S.rx[3][ly][lh + 1];
+          ahy += rx[2][ly][lh] - rx[2][ly][lh + 1];
+          ahx += rx[3][ly][lh] - rx[3][ly][lh + 1];
         }
       }
       if (P.g && (pmask || prb_tail)) {   // H-probe cotangent of y_n
@@ -750,7 +777,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         const int ci = ((i - P.hb[0]) * sy + (j - P.hb[2])) * sz + (k - P.hb[4]);
         const float* hp = P.hist + (long long)(n - P.hist_step0) * P.hist_ld + ci;
         const float dca = P.dca[ci], dcb = P.dcb[ci];
-        const AdjStage<TY>& X = S.st[b0];
+        const auto& X = S.st[b0];
         const double acc = (double)X.ae[0][ly][lz] * ((double)dca * hp[0] + (double)dcb * hp[3 * hc]) +
                            (double)X.ae[1][ly][lz] * ((double)dca * hp[hc] + (double)dcb * hp[4 * hc]) +
                            (double)X.ae[2][ly][lz] * ((double)dca * hp[2 * hc] + (double)dcb * hp[5 * hc]);
@@ -768,7 +795,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         adj_a_cell<TY, 5, false>(P, A, S, C, b0, b1, i, y0 - 1, k, 0, lz, xe0, xe1, ye0_r, ye1_r, ze0_r, ze1_r,
                                  false, a1, a2, a3);
         if (C.cpx) a3 += rxh - nxh;
-        if (MODE == 2) {   // row y0 is this thread's own row: its r_E is rown
+        if (RING) {   // row y0 is this thread's own row: its r_E is rown
           if (C.cpy) {
             const float4 r0 = re_at(0, lh, 1, false);
             a3 += r0.x - rown.x;
@@ -777,10 +804,10 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
           if (C.cpz) a1 += re_at(0, lh, 2, false).w - re_at(0, lh + 1, 2, false).w;
         } else {
           if (C.cpy) {
-            a3 += S.rx[0][0][lh] - S.rx[0][1][lh];
-            a1 += S.rx[1][0][lh] - S.rx[1][1][lh];
+            a3 += rx[0][0][lh] - rx[0][1][lh];
+            a1 += rx[1][0][lh] - rx[1][1][lh];
           }
-          if (C.cpz) a1 += S.rx[3][0][lh] - S.rx[3][0][lh + 1];
+          if (C.cpz) a1 += rx[3][0][lh] - rx[3][0][lh + 1];
         }
         chr = chat(i, y0 - 1, k);
         if (P.g) {
@@ -804,7 +831,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
                                  ze0_c, ze1_c, false, a1, a2, a3);
         const int r = lane + 1;
         if (C.cpx) a2 += rxh - nxh;
-        if (MODE == 2) {
+        if (RING) {
           if (C.cpy) a1 += re_at(r, 0, 1, false).y - re_at(r + 1, 0, 1, false).y;
           if (C.cpz) {
             const float4 z0v = re_at(r, 0, 2, false), z1v = re_at(r, 1, 2, false);
@@ -812,10 +839,10 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
             a1 += z0v.w - z1v.w;
           }
         } else {
-          if (C.cpy) a1 += S.rx[1][r][0] - S.rx[1][r + 1][0];
+          if (C.cpy) a1 += rx[1][r][0] - rx[1][r + 1][0];
           if (C.cpz) {
-            a2 += S.rx[2][r][0] - S.rx[2][r][1];
-            a1 += S.rx[3][r][0] - S.rx[3][r][1];
+            a2 += rx[2][r][0] - rx[2][r][1];
+            a1 += rx[3][r][0] - rx[3][r][1];
           }
         }
         chz = chat(i, y0 + lane, z0 - 1);
@@ -837,7 +864,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     // Modes 0 / 1: r_H of the y / z relations at the tile and the low halo
     // row / column (rows y0-1 .. y0+TY-1, columns z0-1 .. z0+31), once per
     // cell into the exchange array
-    if (MODE != 2 && yz_tile) {
+    if (!RING && yz_tile) {
       auto rh_fill = [&](int r, int c, bool write, bool ny_, bool nz_) {
         const int jj = y0 - 1 + r, kk = z0 - 1 + c;
         float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
@@ -851,10 +878,10 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
             v3 = rh_eval(P, A, C, 2, 1, -1.f, i, jj, kk, S.p[1][r][c], write);   // hy <- ex
           }
         }
-        S.rx[0][r][c] = v0;
-        S.rx[1][r][c] = v1;
-        S.rx[2][r][c] = v2;
-        S.rx[3][r][c] = v3;
+        rx[0][r][c] = v0;
+        rx[1][r][c] = v1;
+        rx[2][r][c] = v2;
+        rx[3][r][c] = v3;
       };
       rh_fill(ly, lh, own, true, true);
       const int t = tid - 64;   // warps 2 and 3
@@ -867,7 +894,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     float py = 0.f, pz = 0.f;
     float rhy = 0.f, rhz = 0.f;
     if (own) {
-      const AdjStage<TY>& X = S.st[b0];
+      const auto& X = S.st[b0];
       const float px = S.p[0][ly][lh];
       py = S.p[1][ly][lh];
       pz = S.p[2][ly][lh];
@@ -878,7 +905,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       float ay = cav * X.ae[1][ly][lz] + ((xh0 * pz - xhm * pz_prev) - (zh0 * px - zhm * px_zm));
       float az = cav * X.ae[2][ly][lz] + ((yh0 * px - yhm * px_ym) - (xh0 * py - xhm * py_prev));
       if (C.cpx) {   // (hy <- ez, +1, q0), (hz <- ey, -1, q1): aE(x) += r(x-1) - r(x)
-        if (MODE == 2) {
+        if (RING) {
           if (xslab(i)) {
             int sx;
             const int sd = cpml_side(i, C.nx, C.ncp, sx);
@@ -894,7 +921,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         az += rhy_prev - rhy;
         ay += rhz_prev - rhz;
       }
-      if (MODE == 2) {
+      if (RING) {
         if (yz_tile) {
           const float4 rh = rh_at(ly, lh, 3, true);
           if (C.cpy) {   // (hx <- ez, -1, q0), (hz <- ex, +1, q1)
@@ -910,12 +937,12 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
         }
       } else {
         if (C.cpy) {   // (hx <- ez, -1, q0), (hz <- ex, +1, q1)
-          az += S.rx[0][ly - 1][lh] - S.rx[0][ly][lh];
-          ax += S.rx[1][ly - 1][lh] - S.rx[1][ly][lh];
+          az += rx[0][ly - 1][lh] - rx[0][ly][lh];
+          ax += rx[1][ly - 1][lh] - rx[1][ly][lh];
         }
         if (C.cpz) {   // (hx <- ey, +1, q0), (hy <- ex, -1, q1)
-          ay += S.rx[2][ly][lh - 1] - S.rx[2][ly][lh];
-          ax += S.rx[3][ly][lh - 1] - S.rx[3][ly][lh];
+          ay += rx[2][ly][lh - 1] - rx[2][ly][lh];
+          ax += rx[3][ly][lh - 1] - rx[3][ly][lh];
         }
       }
       if (n >= 1 && (pmask | smask | (unsigned)prb_tail | (unsigned)src_tail)) {
@@ -956,7 +983,9 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       if (pec_k0) { ax = 0.f; ay = 0.f; }
       if (pec_kz) az = 0.f;
       if (P.emask) {
-        const unsigned m = TMA ? (unsigned)X.em[ty][lane] : (unsigned)P.emask[e];
+        unsigned m;
+        if constexpr (MODE == 4) m = (unsigned)P.emask[e];   // not staged on this variant
+        else m = TMA ? (unsigned)X.em[ty][lane] : (unsigned)P.emask[e];
         if (m & 1u) ax = 0.f;
         if (m & 2u) ay = 0.f;
         if (m & 4u) az = 0.f;
@@ -984,13 +1013,22 @@ template __global__ void adj_step_kernel<8, 2>(const RfxbInst*, const AdjInst*, 
                                                const CUtensorMap*, int, int, int, int);
 template __global__ void adj_step_kernel<8, 3>(const RfxbInst*, const AdjInst*, const RfxbWork*,
                                                const CUtensorMap*, int, int, int, int);
+template __global__ void adj_step_kernel<8, 4>(const RfxbInst*, const AdjInst*, const RfxbWork*,
+                                               const CUtensorMap*, int, int, int, int);
 
 // Dynamic shared memory of a mode: the fixed part, the plane stages it uses
-// and (mode 2) the two ring slots sized for z-psi rows of zp floats.
+// and (modes 2, 4) the two ring slots sized for z-psi rows of zp floats, or
+// (modes 0, 1) the exchange array.
 size_t adj_step_smem_bytes(int mode, int zp) {
-  const size_t fixed = offsetof(AdjSmem<8>, st);
-  if (mode != 2) return fixed + RFXB_ANSTAGE * sizeof(AdjStage<8>);
-  return fixed + 3 * sizeof(AdjStage<8>) + 2 * sizeof(float) * (size_t)APsiSlot<8>::FLOATS(zp);
+  using Lite = AdjSmem<8, false>;
+  using Full = AdjSmem<8, true>;
+  if (mode == 4)
+    return offsetof(Lite, st) + 3 * sizeof(AdjStage<8, false>) +
+           2 * sizeof(float) * (size_t)APsiSlot<8, false>::FLOATS(zp);
+  const size_t fixed = offsetof(Full, st);
+  if (mode == 2) return fixed + 3 * sizeof(AdjStage<8, true>) + 2 * sizeof(float) * (size_t)APsiSlot<8, true>::FLOATS(zp);
+  if (mode == 3) return fixed + RFXB_ANSTAGE * sizeof(AdjStage<8, true>);
+  return fixed + RFXB_ANSTAGE * sizeof(AdjStage<8, true>) + sizeof(AdjExchange<8>);
 }
 
 }  // namespace rfxb

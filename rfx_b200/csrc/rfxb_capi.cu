@@ -79,6 +79,17 @@ int sm_count() {
   return n;
 }
 
+// Shared memory of one SM (228 KB on B200).
+int smem_per_sm() {
+  static int n = -1;
+  if (n < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) n = 233472;
+  }
+  return n;
+}
+
 }  // namespace
 
 struct RfxbPlan {
@@ -166,6 +177,14 @@ struct RfxbBatch {
   int n_wa2 = 0;
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // reverse variant 4 (CPML work that reaches no y slab) on a third stream
+  bool adj_lite = false;
+  RfxbWork* d_wa2y = nullptr;   // variant 2 list when variant 4 takes the rest
+  int n_wa2y = 0;
+  RfxbWork* d_wa4 = nullptr;
+  int n_wa4 = 0;
+  cudaStream_t side2 = nullptr;
+  cudaEvent_t ev_join2 = nullptr;
   RfxbDftPlane* d_dft = nullptr;
   RfxbFluxPlane* d_flux = nullptr;
   std::vector<RfxbFluxPlane> flux;
@@ -188,8 +207,10 @@ struct RfxbBatch {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     if (side_stream) cudaStreamDestroy(side_stream);
+    if (side2) cudaStreamDestroy(side2);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_join2) cudaEventDestroy(ev_join2);
     for (void* p : allocs) cudaFree(p);
   }
 };
@@ -382,7 +403,7 @@ void split_segments(const std::vector<RfxbPlan*>& plans, double slab, std::vecto
 // z0-1 .. z0+32 and planes xa-1 .. xb, so the CPML-free range of a tile that
 // reaches no y/z slab is ncp+1 .. nx-ncp-2.
 void split_adj_segments(const std::vector<RfxbPlan*>& plans, double slab, std::vector<WorkSeg>& plain,
-                        std::vector<WorkSeg>& cpml) {
+                        std::vector<WorkSeg>& cpml, std::vector<WorkSeg>* cpml_noy = nullptr) {
   for (size_t q = 0; q < plans.size(); ++q) {
     const RfxbPlan& p = *plans[q];
     const int n = p.inst.ncp;
@@ -397,21 +418,24 @@ void split_adj_segments(const std::vector<RfxbPlan*>& plans, double slab, std::v
         const double cx = (ax & 1u) ? slab : 0.0;
         const bool yz = ((ax & 2u) && (y0 - 1 < n || y0 + kTY >= p.ny - n)) ||
                         ((ax & 4u) && (z0 - 1 < n || z0 + 32 >= p.nz - n));
+        const bool ys = (ax & 2u) && (y0 - 1 < n || y0 + kTY >= p.ny - n);
+        // CPML work whose tile reaches no y slab goes to cpml_noy when given
+        std::vector<WorkSeg>& dst = (cpml_noy && !ys) ? *cpml_noy : cpml;
         if (yz) {
           double c = 1.0;
-          if ((ax & 2u) && (y0 - 1 < n || y0 + kTY >= p.ny - n)) c += slab;
+          if (ys) c += slab;
           if ((ax & 4u) && (z0 - 1 < n || z0 + 32 >= p.nz - n)) c += slab;
-          cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, c, cx});
+          dst.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, c, cx});
           continue;
         }
         const int lo = ncpx > 0 ? ncpx + 1 : 0, hi = ncpx > 0 ? p.nx - ncpx - 1 : p.nx;
         if (hi - lo < 4) {
-          cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, 1.0, cx});
+          dst.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, 1.0, cx});
           continue;
         }
         plain.push_back(WorkSeg{(int)q, y0, z0, lo, hi, p.nx, 0, 1.0, 0.0});
-        if (lo > 0) cpml.push_back(WorkSeg{(int)q, y0, z0, 0, lo, p.nx, ncpx, 1.0, cx});
-        if (hi < p.nx) cpml.push_back(WorkSeg{(int)q, y0, z0, hi, p.nx, p.nx, ncpx, 1.0, cx});
+        if (lo > 0) dst.push_back(WorkSeg{(int)q, y0, z0, 0, lo, p.nx, ncpx, 1.0, cx});
+        if (hi < p.nx) dst.push_back(WorkSeg{(int)q, y0, z0, hi, p.nx, p.nx, ncpx, 1.0, cx});
       }
   }
 }
@@ -440,6 +464,17 @@ bool fwd_split_enabled() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("RFXB_FWD_SPLIT");
+    v = (e && std::string(e) == "0") ? 0 : 1;
+  }
+  return v == 1;
+}
+
+// RFXB_ADJ_LITE=0 keeps the reverse CPML work of tiles without a y slab on
+// variant 2 instead of variant 4.
+bool adj_lite_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("RFXB_ADJ_LITE");
     v = (e && std::string(e) == "0") ? 0 : 1;
   }
   return v == 1;
@@ -773,8 +808,9 @@ void group_adj_mode(RfxbBatch* g) {
 
 using AdjKernel = void (*)(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int, int);
 AdjKernel adj_kernel(int mode) {
-  static bool init[4] = {false, false, false, false};
-  AdjKernel k = mode == 3   ? adj_step_kernel<kTY, 3>
+  static bool init[5] = {false, false, false, false, false};
+  AdjKernel k = mode == 4   ? adj_step_kernel<kTY, 4>
+                : mode == 3 ? adj_step_kernel<kTY, 3>
                 : mode == 2 ? adj_step_kernel<kTY, 2>
                 : mode == 1 ? adj_step_kernel<kTY, 1>
                             : adj_step_kernel<kTY, 0>;
@@ -840,9 +876,12 @@ int build_group(RfxbBatch* g) {
       RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
       g->fwd_split = true;
     }
-    // reverse split (used when the reverse kernel is variant 1 or 2)
-    std::vector<WorkSeg> aplain, acpml;
+    // reverse split (used when the reverse kernel is variant 1 or 2); with
+    // variant 2, the CPML work of tiles that reach no y slab can go to
+    // variant 4 on a third stream
+    std::vector<WorkSeg> aplain, acpml, aplain_b, ay, anoy;
     split_adj_segments(g->plans, slab_weight(), aplain, acpml);
+    split_adj_segments(g->plans, slab_weight(), aplain_b, ay, &anoy);
     std::vector<RfxbWork> a1, a2;
     balance_segments(aplain, 4 * sm_count(), 3.0, a1);
     balance_segments(acpml, 3 * sm_count(), 3.0, a2);
@@ -859,6 +898,27 @@ int build_group(RfxbBatch* g) {
         RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
       }
       g->adj_split = true;
+      std::vector<RfxbWork> a2y, a4;
+      balance_segments(ay, 3 * sm_count(), 3.0, a2y);
+      int zp = 4;
+      for (auto* p : g->plans) zp = std::max(zp, p->inst.ncp4);
+      // resident CTAs of variant 4: four per SM when its shared memory (plus
+      // the 1 KB the runtime reserves per CTA) fits four times
+      const int per_sm = (int)(4 * (adj_step_smem_bytes(4, zp) + 1024) <= (size_t)smem_per_sm() ? 4 : 3);
+      balance_segments(anoy, per_sm * sm_count(), 3.0, a4);
+      if (adj_lite_enabled() && !a4.empty()) {
+        if (!a2y.empty()) {
+          if (int rc = galloc((void**)&g->d_wa2y, sizeof(RfxbWork) * a2y.size())) return rc;
+          RFXB_CUDA(cudaMemcpy(g->d_wa2y, a2y.data(), sizeof(RfxbWork) * a2y.size(), cudaMemcpyHostToDevice));
+        }
+        if (int rc = galloc((void**)&g->d_wa4, sizeof(RfxbWork) * a4.size())) return rc;
+        RFXB_CUDA(cudaMemcpy(g->d_wa4, a4.data(), sizeof(RfxbWork) * a4.size(), cudaMemcpyHostToDevice));
+        g->n_wa2y = (int)a2y.size();
+        g->n_wa4 = (int)a4.size();
+        RFXB_CUDA(cudaStreamCreateWithFlags(&g->side2, cudaStreamNonBlocking));
+        RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join2, cudaEventDisableTiming));
+        g->adj_lite = true;
+      }
     }
   }
   if (int rc = galloc((void**)&g->d_inst, sizeof(RfxbInst) * g->plans.size())) return rc;
@@ -1230,13 +1290,29 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
         adj_pass_b<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
       } else {
         if (g->adj_split && amode != 0) {
+          // CPML tiles on the caller's stream, plain tiles beside them, and
+          // (variant 2 groups) the CPML work without a y slab on variant 4
+          const bool lite = g->adj_lite && amode == 2;
           RFXB_CUDA(cudaEventRecord(g->ev_fork, cs));
           RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
-          akern<<<g->n_wa2, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2, g->d_maps, s, par, fpar, zp);
+          if (lite) {
+            RFXB_CUDA(cudaStreamWaitEvent(g->side2, g->ev_fork, 0));
+            if (g->n_wa2y > 0)
+              akern<<<g->n_wa2y, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2y, g->d_maps, s, par, fpar,
+                                                             zp);
+            adj_kernel(4)<<<g->n_wa4, dim3(32, kTY), adj_step_smem_bytes(4, zp), g->side2>>>(
+                g->d_inst, g->d_adj, g->d_wa4, g->d_maps, s, par, fpar, zp);
+          } else {
+            akern<<<g->n_wa2, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2, g->d_maps, s, par, fpar, zp);
+          }
           adj_kernel(3)<<<g->n_wa1, dim3(32, kTY), adj_step_smem_bytes(3, zp), g->side_stream>>>(
               g->d_inst, g->d_adj, g->d_wa1, g->d_maps, s, par, fpar, zp);
           RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
           RFXB_CUDA(cudaStreamWaitEvent(cs, g->ev_join, 0));
+          if (lite) {
+            RFXB_CUDA(cudaEventRecord(g->ev_join2, g->side2));
+            RFXB_CUDA(cudaStreamWaitEvent(cs, g->ev_join2, 0));
+          }
         } else {
           akern<<<g->n_work, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_work, g->d_maps, s, par, fpar,
                                                          zp);
