@@ -314,8 +314,11 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_port(args, n_workers=1, n_time=args.cpu_time_steps)
 
-    # our kernels per bench step: N forward steps, one adjoint init, N fused reverse steps
-    launches = args.steps * (2 * N + 1)
+    # our kernels per bench step: N forward steps, one adjoint init per
+    # simulation launch group, N reverse steps, each step as many step-kernel
+    # launches as the library reports (CPML / plain split, variant 4)
+    fl, rl = sw.step_launches()
+    launches = args.steps * (N * (fl + rl) + (1 if sw.batch is not None else len(sw.plans)))
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 2), "higher_is_better": True,

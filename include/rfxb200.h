@@ -301,6 +301,14 @@ int rfxb_batch_forward_variant(const RfxbBatch* batch);
 int rfxb_plan_adjoint_variant(const RfxbPlan* plan);
 int rfxb_batch_adjoint_variant(const RfxbBatch* batch);
 
+/* Step-kernel launches per forward time step (*fwd: 1, or 2 with the split
+ * into CPML and plain tiles) and per reverse time step (*rev: 1, 2 with the
+ * split, 3 when variant 4 takes the CPML work without a y slab; -1 before
+ * the first adjoint advance), not counting DFT / flux / NTFF epilogue
+ * kernels.  A diagnostic of this implementation. */
+int rfxb_plan_step_launches(const RfxbPlan* plan, int* fwd, int* rev);
+int rfxb_batch_step_launches(const RfxbBatch* batch, int* fwd, int* rev);
+
 #ifdef __cplusplus
 }
 #endif

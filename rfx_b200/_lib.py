@@ -112,6 +112,8 @@ SIGNATURES = {
     "rfxb_batch_forward_variant": (C.c_int, [C.c_void_p]),
     "rfxb_plan_adjoint_variant": (C.c_int, [C.c_void_p]),
     "rfxb_batch_adjoint_variant": (C.c_int, [C.c_void_p]),
+    "rfxb_plan_step_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "rfxb_batch_step_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rfxb_forward_noalloc": (C.c_int, [C.POINTER(RfxbDesc), C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
                                        C.POINTER(RfxbStepIO), C.c_int, C.c_int, C.c_void_p]),
 }

@@ -130,6 +130,17 @@ class Sweep:
         Js, gs = self.objectives()
         return Js, self.backward(gs)
 
+    def step_launches(self):
+        """Step-kernel launches of one forward time step and one reverse
+        time step of the whole sweep (every instance included)."""
+        if self.batch is not None:
+            return self.batch.step_launches()
+        f = r = 0
+        for p in self.plans:
+            a, b = p.step_launches()
+            f, r = f + a, r + b
+        return f, r
+
     def check_device(self):
         """Synchronise and raise if a bounded wait inside a kernel ran out."""
         if self.batch is not None:

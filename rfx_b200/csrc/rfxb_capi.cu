@@ -1880,6 +1880,31 @@ int rfxb_batch_forward_variant(const RfxbBatch* g) {
   return g->fwd_mode;
 }
 
+namespace {
+void step_launches(const RfxbBatch* g, int* fwd, int* rev) {
+  if (fwd) *fwd = g->fwd_split ? 2 : 1;
+  if (rev) {
+    if (g->adj_mode < 0) *rev = -1;
+    else if (use_twopass()) *rev = 2;
+    else if (g->adj_split && g->adj_mode != 0)
+      *rev = (g->adj_lite && g->adj_mode == 2) ? (g->n_wa2y > 0 ? 3 : 2) : 2;
+    else *rev = 1;
+  }
+}
+}  // namespace
+
+int rfxb_plan_step_launches(const RfxbPlan* p, int* fwd, int* rev) {
+  if (!p || !p->self_group) return fail(RFXB_E_INVALID, "null plan");
+  step_launches(p->self_group, fwd, rev);
+  return 0;
+}
+
+int rfxb_batch_step_launches(const RfxbBatch* g, int* fwd, int* rev) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  step_launches(g, fwd, rev);
+  return 0;
+}
+
 int rfxb_plan_adjoint_variant(const RfxbPlan* p) {
   if (!p || !p->self_group) return -1;
   return p->self_group->adj_mode;

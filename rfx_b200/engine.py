@@ -224,6 +224,13 @@ class Plan:
         adjoint psi; -1 before the first adjoint advance."""
         return int(self._lib.rfxb_plan_adjoint_variant(self._h))
 
+    def step_launches(self):
+        """(step-kernel launches per forward step, per reverse step; -1
+        before the first adjoint advance)."""
+        f, r = C.c_int(), C.c_int()
+        check(self._lib.rfxb_plan_step_launches(self._h, C.byref(f), C.byref(r)), "rfxb_plan_step_launches")
+        return f.value, r.value
+
     # -- state ---------------------------------------------------------------
     def _dev(self, a, dtype=torch.float32):
         t = torch.as_tensor(np.asarray(a) if not isinstance(a, torch.Tensor) else a)
@@ -386,6 +393,12 @@ class Batch:
 
     def check_device(self):
         check(self._lib.rfxb_batch_device_status(self._h, _stream()), "rfxb_batch_device_status")
+
+    def step_launches(self):
+        """(step-kernel launches per forward step, per reverse step)."""
+        f, r = C.c_int(), C.c_int()
+        check(self._lib.rfxb_batch_step_launches(self._h, C.byref(f), C.byref(r)), "rfxb_batch_step_launches")
+        return f.value, r.value
 
     def adjoint_begin(self, n_total, aios):
         arr = (RfxbAdjointIO * len(self.plans))(*[Plan.adjoint_io(**kw) for kw in aios])
