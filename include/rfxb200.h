@@ -295,8 +295,10 @@ int rfxb_batch_forward_variant(const RfxbBatch* batch);
  * 0 cp.async staging, 1 TMA staging with CPML psi read from global memory,
  * 2 TMA staging with the adjoint psi and ce staged by TMA one plane ahead,
  * 3 TMA staging without any CPML (groups without CPML); with 1 or 2, tiles
- * whose reverse step touches no slab run on 3 beside it.  -1 before the
- * first adjoint advance or for a null handle.  A diagnostic of this
+ * whose reverse step touches no slab run on 3 beside it, and with 2 the
+ * CPML work of tiles that reach no y slab runs on variant 4 (variant 2
+ * without the y-slab terms, four CTAs per SM) on a third stream.  -1 before
+ * the first adjoint advance or for a null handle.  A diagnostic of this
  * implementation, no counterpart in the reference. */
 int rfxb_plan_adjoint_variant(const RfxbPlan* plan);
 int rfxb_batch_adjoint_variant(const RfxbBatch* batch);
