@@ -164,6 +164,13 @@ typedef struct {
   const float* dca_dev;        /* d ca / d eps_r over grad_box */
   const float* dcb_dev;        /* d cb / d eps_r over grad_box */
   float* src_adj_dev;          /* dJ/d(source table) [n_total_steps][n_src], may be NULL */
+  /* DFT-plane objectives (the transpose of the running DFT,
+   * rfx/simulation.py:1574-1588): per DFT plane of the plan a complex64
+   * cotangent (n_freqs, n1, n2) = dJ/dRe(acc) + i dJ/dIm(acc), or NULL, and
+   * the phase table the forward accumulated with ([n_total_steps][n_freqs]
+   * (cos, sin) * dt).  Both arrays NULL: no DFT-plane cotangents. */
+  const void* const* dft_cot_dev;
+  const void* const* dft_phase_dev;
 } RfxbAdjointIO;
 
 int rfxb_version(void);

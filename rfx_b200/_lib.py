@@ -73,6 +73,8 @@ class RfxbAdjointIO(C.Structure):
         ("dca_dev", C.c_void_p),
         ("dcb_dev", C.c_void_p),
         ("src_adj_dev", C.c_void_p),
+        ("dft_cot_dev", C.POINTER(C.c_void_p)),
+        ("dft_phase_dev", C.POINTER(C.c_void_p)),
     ]
 
 

@@ -1,8 +1,9 @@
 """Hand-written reverse-time adjoint: forward with history, then the
 transposed step backwards in time.  Replaces ``jax.grad`` through the scan
 (rfx/simulation.py:1972-2058 with ``checkpoint_segments``; rfx/nonuniform.py:
-1755-1796 with ``checkpoint_every``) for gradients of probe-trace
-objectives with respect to eps_r over a region of cells.
+1755-1796 with ``checkpoint_every``) for gradients of objectives of the probe
+traces and of running-DFT plane accumulators with respect to eps_r over a
+region of cells and to the source table.
 
 Field history.  The gradient needs, at every step n and every cell of the
 region, E^n and curl H^{n+1/2} (the two factors of d E^{n+1} / d eps_r).
@@ -23,7 +24,7 @@ import torch
 from .cpml import build_cpml
 from .engine import Plan, PlanSpec, require_cuda
 from .grid import EPS_0, spacing_tables
-from .simulation import tangential_edge_masks
+from .simulation import dft_phase_table, tangential_edge_masks
 
 
 def coefficient_derivatives(eps_r, sigma, dt):
@@ -55,7 +56,10 @@ class AdjointRunner:
 
     def __init__(self, grid, materials, n_steps, *, sources, probes, box, boundary="cpml", cpml_axes="xyz",
                  pec_axes="", pec_mask=None, checkpoint_every=None, mode="auto",
-                 history_budget_bytes=8 << 30, device=None, _plan=None):
+                 history_budget_bytes=8 << 30, dft_planes=None, dft_time_offset=1, device=None, _plan=None):
+        """``dft_planes``: ``DFTPlaneProbe`` values accumulated by the forward
+        pass (sample time (n + dft_time_offset) dt: 1 on the uniform lane, 0 on
+        the graded one); their accumulators can carry cotangents."""
         self.device = require_cuda(device)
         self.grid = grid
         self.n_steps = int(n_steps)
@@ -72,11 +76,13 @@ class AdjointRunner:
         self.sources = [tuple(s[:4]) for s in sources]
         self.src_waves = [np.asarray(s[4], np.float32) for s in sources]
         self.probes = [tuple(p[:4]) for p in probes]
+        self.dft_planes = list(dft_planes or [])
         spec = PlanSpec(shape=shape, dt=float(grid.dt), tables=spacing_tables(grid),
                         cpml=build_cpml(grid, cpml_axes if use_cpml else "",
                                         noop_faces=set(getattr(grid, "pec_faces", None) or ())) if use_cpml else None,
                         pec_axes=pec_axes, sources=self.sources,
-                        probes=[(i, j, k, c, False) for (i, j, k, c) in self.probes], grad_box=self.box)
+                        probes=[(i, j, k, c, False) for (i, j, k, c) in self.probes], grad_box=self.box,
+                        dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in self.dft_planes])
         self.plan = _plan or Plan(spec, self.device)
         self.eps = torch.as_tensor(np.asarray(materials.eps_r, np.float32)).to(self.device).contiguous()
         self.sigma = torch.as_tensor(np.asarray(materials.sigma, np.float32)).to(self.device).contiguous()
@@ -93,6 +99,9 @@ class AdjointRunner:
             self.plan.checkpoint_reserve((self.n_steps + self.K - 1) // self.K)
         tab = np.stack(self.src_waves, axis=-1)[: self.n_steps] if self.src_waves else np.zeros((self.n_steps, 0))
         self.src_table = torch.from_numpy(np.ascontiguousarray(tab, np.float32)).to(self.device)
+        self.dft_phases = [torch.from_numpy(dft_phase_table(d.freqs, self.n_steps, grid.dt, dft_time_offset))
+                           .to(self.device) for d in self.dft_planes]
+        self.dft_accs = []
         self._dirty = True
 
     # materials ------------------------------------------------------------
@@ -108,7 +117,8 @@ class AdjointRunner:
 
     # passes ---------------------------------------------------------------
     def forward(self, src_table=None):
-        """Run the forward pass; returns the probe traces (n_steps, n_probes)."""
+        """Run the forward pass; returns the probe traces (n_steps, n_probes)
+        (the DFT-plane accumulators are left in ``dft_accs``)."""
         self._sync_materials()
         if src_table is not None:
             self.src_table = src_table.detach().to(self.device, torch.float32).contiguous()
@@ -116,19 +126,24 @@ class AdjointRunner:
         p.reset()
         ts = torch.zeros((N, len(self.probes)), device=self.device, dtype=torch.float32)
         st = self.src_table if self.sources else None
+        accs = [torch.zeros(d.accumulator.shape, device=self.device, dtype=torch.complex64) for d in self.dft_planes]
+        dk = dict(dft_accs=accs, dft_phases=self.dft_phases) if accs else {}
         if self.mode == "history":
             p.record_history(0, N)
-            p.advance(0, N, st, ts)
+            p.advance(0, N, st, ts, **dk)
         else:
             for q, s0 in enumerate(range(0, N, self.K)):
                 p.checkpoint_save(q)
-                p.advance(s0, min(self.K, N - s0), st, ts)
+                p.advance(s0, min(self.K, N - s0), st, ts, **dk)
+        self.dft_accs = accs
         p.check_device()
         self.ts = ts
         return ts
 
-    def backward(self, g_ts, want_source_grad=True):
-        """Adjoint sweep for probe cotangents ``g_ts`` (n_steps, n_probes).
+    def backward(self, g_ts, want_source_grad=True, g_dft=None):
+        """Adjoint sweep for probe cotangents ``g_ts`` (n_steps, n_probes; may
+        be None) and DFT-plane cotangents ``g_dft`` (per plane a complex
+        (n_freqs, n1, n2) array dJ/dRe + i dJ/dIm, or None).
 
         Returns (dJ/d eps_r over the box as float64, dJ/d source table)."""
         p, N = self.plan, self.n_steps
@@ -138,10 +153,22 @@ class AdjointRunner:
         dca = torch.from_numpy(dca.astype(np.float32).ravel()).to(self.device)
         dcb = torch.from_numpy(dcb.astype(np.float32).ravel()).to(self.device)
         grad = torch.zeros(int(np.prod(self.box_shape)), device=self.device, dtype=torch.float64)
+        if g_ts is None:
+            g_ts = torch.zeros((N, len(self.probes)), device=self.device, dtype=torch.float32)
         g = g_ts.detach().to(self.device, torch.float32).contiguous()
         src_adj = (torch.zeros((N, len(self.sources)), device=self.device, dtype=torch.float32)
                    if (want_source_grad and self.sources) else None)
         kw = dict(g=g, grad=grad, dca=dca, dcb=dcb, src_adj=src_adj)
+        if g_dft is not None and any(c is not None for c in g_dft):
+            if len(g_dft) != len(self.dft_planes):
+                raise ValueError("one DFT-plane cotangent (or None) per DFT plane")
+            cots = [None if c is None else torch.as_tensor(c).to(self.device, torch.complex64).contiguous()
+                    for c in g_dft]
+            for c, d in zip(cots, self.dft_planes):
+                if c is not None and tuple(c.shape) != tuple(d.accumulator.shape):
+                    raise ValueError(f"DFT-plane cotangent of shape {tuple(c.shape)}, accumulator "
+                                     f"{tuple(d.accumulator.shape)}")
+            kw.update(dft_cots=cots, dft_phases=self.dft_phases)
         p.adjoint_begin(N, **kw)
         st = self.src_table if self.sources else None
         if self.mode == "history":
@@ -163,9 +190,10 @@ class AdjointRunner:
 
 
 class FDTDFunction(torch.autograd.Function):
-    """Probe traces as a differentiable function of eps_r over the runner's
-    box and of the source table: the ``torch.autograd.Function`` face of the
-    hand-written adjoint."""
+    """Probe traces (and, when the runner has DFT planes, their complex64
+    accumulators as further outputs) as a differentiable function of eps_r
+    over the runner's box and of the source table: the
+    ``torch.autograd.Function`` face of the hand-written adjoint."""
 
     @staticmethod
     def forward(ctx, eps_box, src_table, runner):
@@ -173,11 +201,13 @@ class FDTDFunction(torch.autograd.Function):
         ts = runner.forward(src_table.detach() if src_table is not None else None)
         ctx.runner = runner
         ctx.has_src = src_table is not None
+        if runner.dft_planes:
+            return (ts.clone(), *[a.clone() for a in runner.dft_accs])
         return ts.clone()
 
     @staticmethod
-    def backward(ctx, g_ts):
-        grad, src_adj = ctx.runner.backward(g_ts, want_source_grad=ctx.has_src)
+    def backward(ctx, g_ts, *g_dft):
+        grad, src_adj = ctx.runner.backward(g_ts, want_source_grad=ctx.has_src, g_dft=list(g_dft) or None)
         return grad.to(torch.float32), (src_adj if ctx.has_src else None), None
 
 

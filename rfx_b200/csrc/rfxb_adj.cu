@@ -257,4 +257,54 @@ __global__ void adj_init_kernel(const RfxbInst* __restrict__ insts, const AdjIns
   }
 }
 
+// Transpose of the running-DFT planes for sample s (the fields after step s:
+// E^{s+1} after the sources, H^{s+1/2}): each plane cell receives
+// sum_f Re(G_f) cos_f(s) dt + Im(G_f) sin_f(s) dt, added to the adjoint field
+// of the current parity.  It lands where an E / H probe cotangent of sample s
+// lands: an E component also feeds the source adjoint of a source on that
+// cell, and is dropped where the PEC faces or the edge mask zero the
+// component (the transposes of those zeroings, which the forward applies
+// before the sources).  Planes may share cells, so the adds are atomic.
+__global__ void dft_adj_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
+                               const RfxbDftPlane* __restrict__ planes, int nplanes, int s, int apar) {
+  int q = 0;
+  while (q + 1 < nplanes && planes[q + 1].block0 <= (int)blockIdx.x) ++q;
+  const RfxbDftPlane& D = planes[q];
+  if (D.acc == nullptr) return;
+  const int c = (blockIdx.x - D.block0) * blockDim.x + threadIdx.x;
+  const int cells = D.n1 * D.n2;
+  if (c >= cells) return;
+  const float2* ph = D.phase + (long long)s * D.nf;
+  float g = 0.f;
+  for (int f = 0; f < D.nf; ++f) {
+    const float2 G = D.acc[(long long)f * cells + c], w = __ldg(ph + f);
+    g = fmaf(G.x, w.x, g);
+    g = fmaf(G.y, w.y, g);
+  }
+  if (g == 0.f) return;
+  const RfxbInst& P = insts[D.inst];
+  const AdjInst& A = adjs[D.inst];
+  const int a = c / D.n2, b = c - a * D.n2;
+  int i, j, k;
+  if (D.axis == 0) { i = D.index; j = a; k = b; }
+  else if (D.axis == 1) { i = a; j = D.index; k = b; }
+  else { i = a; j = b; k = D.index; }
+  const int comp = D.comp;
+  const long long e = P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
+  bool zero = false;
+  if (comp < 3) {
+    if (P.src_adj)
+      for (int t = 0; t < P.nsrc; ++t) {
+        const int4 sc = P.src[t];
+        if (sc.x == i && sc.y == j && sc.z == k && sc.w == comp) atomicAdd(P.src_adj + (long long)s * P.src_ld + t, g);
+      }
+    if ((P.pec_axes & 1u) && (i == 0 || i == P.nx - 1) && comp != 0) zero = true;
+    if ((P.pec_axes & 2u) && (j == 0 || j == P.ny - 1) && comp != 1) zero = true;
+    if ((P.pec_axes & 4u) && (k == 0 || k == P.nz - 1) && comp != 2) zero = true;
+    if ((P.pec_axes & 4u) && k == P.nz - 1 && comp == 2) zero = true;
+    if (P.emask && (P.emask[e] >> comp) & 1u) zero = true;
+  }
+  if (!zero) atomicAdd(A.aF[apar][comp] + e, g);
+}
+
 }  // namespace rfxb

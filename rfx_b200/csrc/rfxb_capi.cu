@@ -32,6 +32,7 @@ __global__ void coef_kernel(RfxbInst, float*, float*, float*, float*, const floa
 __global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
+__global__ void dft_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbDftPlane*, int, int, int);
 __global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
 __global__ void flux_kernel(const RfxbInst*, const RfxbFluxPlane*, int, int, int);
 __global__ void ntff_kernel(const RfxbInst*, const RfxbNtffFace*, int, int, int);
@@ -186,6 +187,9 @@ struct RfxbBatch {
   cudaStream_t side2 = nullptr;
   cudaEvent_t ev_join2 = nullptr;
   RfxbDftPlane* d_dft = nullptr;
+  RfxbDftPlane* d_dfta = nullptr;   // the same planes with the adjoint call's cotangents
+  std::vector<RfxbDftPlane> dfta;
+  bool has_dft_cot = false;
   RfxbFluxPlane* d_flux = nullptr;
   std::vector<RfxbFluxPlane> flux;
   int flux_blocks = 0;
@@ -1015,6 +1019,7 @@ int build_group(RfxbBatch* g) {
   }
   if (!g->dft.empty()) {
     if (int rc = galloc((void**)&g->d_dft, sizeof(RfxbDftPlane) * g->dft.size())) return rc;
+    if (int rc = galloc((void**)&g->d_dfta, sizeof(RfxbDftPlane) * g->dft.size())) return rc;
   }
   if (int rc = galloc((void**)&g->d_maps, sizeof(CUtensorMap) * RFXB_NMAPS * g->plans.size())) return rc;
   if (int rc = galloc((void**)&g->d_status, sizeof(int))) return rc;
@@ -1248,6 +1253,23 @@ int upload_adjoint(RfxbBatch* g, const RfxbAdjointIO* aios, cudaStream_t st) {
       return fail(RFXB_E_STATE, "gradient requested without a gradient region or coefficient derivatives");
     adjs[q] = p->adj;
   }
+  // DFT-plane cotangents (planes of the group in plan order, as in build_group)
+  g->dfta = g->dft;
+  g->has_dft_cot = false;
+  size_t di = 0;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    const RfxbAdjointIO& a = aios[q];
+    for (size_t d = 0; d < g->plans[q]->dft.size(); ++d, ++di) {
+      const bool on = a.dft_cot_dev && a.dft_phase_dev && a.dft_cot_dev[d] && a.dft_phase_dev[d];
+      g->dfta[di].acc = on ? const_cast<float2*>(static_cast<const float2*>(a.dft_cot_dev[d])) : nullptr;
+      g->dfta[di].cmp = nullptr;
+      g->dfta[di].phase = on ? static_cast<const float2*>(a.dft_phase_dev[d]) : nullptr;
+      if (on) g->has_dft_cot = true;
+    }
+  }
+  if (!g->dfta.empty())
+    RFXB_CUDA(cudaMemcpyAsync(g->d_dfta, g->dfta.data(), sizeof(RfxbDftPlane) * g->dfta.size(),
+                              cudaMemcpyHostToDevice, st));
   for (auto& I : insts) I.status = g->d_status;
   RFXB_CUDA(cudaMemcpyAsync(g->d_inst, insts.data(), sizeof(RfxbInst) * insts.size(), cudaMemcpyHostToDevice, st));
   RFXB_CUDA(cudaMemcpyAsync(g->d_adj, adjs.data(), sizeof(AdjInst) * adjs.size(), cudaMemcpyHostToDevice, st));
@@ -1262,6 +1284,9 @@ int group_adjoint_begin(RfxbBatch* g, const RfxbAdjointIO* aios, int n_total, cu
   if (int rc = upload_adjoint(g, aios, st)) return rc;
   adj_init_kernel<<<(unsigned)g->plans.size(), 32, 0, st>>>(g->d_inst, g->d_adj, (int)g->plans.size(), n_total - 1,
                                                              g->plans[0]->adj_fpar);
+  if (g->has_dft_cot)   // DFT-plane cotangent of the last sample
+    dft_adj_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_adj, g->d_dfta, (int)g->dfta.size(), n_total - 1,
+                                                  g->plans[0]->adj_fpar);
   RFXB_CUDA(cudaGetLastError());
   return 0;
 }
@@ -1319,13 +1344,18 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
         }
         fpar ^= 1;
       }
+      // DFT-plane cotangent of sample s-1 into the state the next reverse
+      // step reads (the point where an E / H probe cotangent of s-1 lands)
+      if (g->has_dft_cot && s >= 1)
+        dft_adj_kernel<<<g->dft_blocks, 256, 0, cs>>>(g->d_inst, g->d_adj, g->d_dfta, (int)g->dfta.size(), s - 1,
+                                                      fpar);
       par ^= 1;
     }
     RFXB_CUDA(cudaGetLastError());
     return 0;
   };
   if (graphs_enabled() && n_steps >= 4) {
-    const GraphKey key{1 + (two ? 1 : 0), step_hi, n_steps, par0, fpar0, 0};
+    const GraphKey key{1 + (two ? 1 : 0), step_hi, n_steps, par0, fpar0, g->has_dft_cot ? 1 : 0};
     if (int rc = run_graph(g, key, st, launch)) return rc;
   } else {
     if (int rc = launch(st)) return rc;

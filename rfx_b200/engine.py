@@ -335,13 +335,21 @@ class Plan:
 
     # -- adjoint -------------------------------------------------------------
     @staticmethod
-    def adjoint_io(g=None, grad=None, dca=None, dcb=None, src_adj=None):
+    def adjoint_io(g=None, grad=None, dca=None, dcb=None, src_adj=None, dft_cots=None, dft_phases=None):
+        """``dft_cots``: per DFT plane a complex64 cotangent (n_freqs, n1, n2)
+        or None; ``dft_phases``: the phase tables the forward used."""
         a = RfxbAdjointIO()
         a.g_dev = g.data_ptr() if g is not None else None
         a.grad_dev = grad.data_ptr() if grad is not None else None
         a.dca_dev = dca.data_ptr() if dca is not None else None
         a.dcb_dev = dcb.data_ptr() if dcb is not None else None
         a.src_adj_dev = src_adj.data_ptr() if src_adj is not None else None
+        if dft_cots is not None and any(c is not None for c in dft_cots):
+            cot = (C.c_void_p * len(dft_cots))(*[c.data_ptr() if c is not None else None for c in dft_cots])
+            ph = (C.c_void_p * len(dft_phases))(*[t.data_ptr() for t in dft_phases])
+            a.dft_cot_dev = C.cast(cot, C.POINTER(C.c_void_p))
+            a.dft_phase_dev = C.cast(ph, C.POINTER(C.c_void_p))
+            a._keep = (cot, ph)   # the pointer arrays live as long as the struct
         return a
 
     def adjoint_begin(self, n_total, **kw):
@@ -401,10 +409,14 @@ class Batch:
         return f.value, r.value
 
     def adjoint_begin(self, n_total, aios):
-        arr = (RfxbAdjointIO * len(self.plans))(*[Plan.adjoint_io(**kw) for kw in aios])
+        ios = [Plan.adjoint_io(**kw) for kw in aios]   # keeps the pointer arrays alive for the call
+        arr = (RfxbAdjointIO * len(self.plans))(*ios)
         check(self._lib.rfxb_batch_adjoint_begin(self._h, arr, int(n_total), _stream()), "rfxb_batch_adjoint_begin")
+        del ios
 
     def adjoint_advance(self, step_hi, n_steps, aios):
-        arr = (RfxbAdjointIO * len(self.plans))(*[Plan.adjoint_io(**kw) for kw in aios])
+        ios = [Plan.adjoint_io(**kw) for kw in aios]
+        arr = (RfxbAdjointIO * len(self.plans))(*ios)
         check(self._lib.rfxb_batch_adjoint_advance(self._h, arr, int(step_hi), int(n_steps), _stream()),
               "rfxb_batch_adjoint_advance")
+        del ios

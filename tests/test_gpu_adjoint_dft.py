@@ -1,0 +1,125 @@
+"""GPU tests of the adjoint with DFT-plane objectives (the transpose of the
+running DFT, rfx/simulation.py:1574-1588 and rfx/nonuniform.py:1458-1472,
+which the reference differentiates with jax.grad through the scan).
+
+1. Exact transpose: a DFT accumulator is linear in the source table, so for
+   J = sum Re(conj(G) acc) (plus <g, ts> of the probes) the source adjoint
+   must reproduce J.  The planes of the uniform scene cross a source cell
+   (the cotangent feeds the source adjoint there) and a PEC sheet whose edge
+   mask zeroes the sampled component (the cotangent is dropped there).
+2. dJ/d eps_r of J = sum |acc|^2 against central finite differences of the
+   float64 oracle along three seeded directions (tolerance 1e-3 relative).
+3. The torch.autograd face returns the accumulators as outputs and accepts
+   their gradients.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle  # noqa: F401
+from tests.scenarios import small_nonuniform, small_uniform
+
+pytestmark = pytest.mark.gpu
+
+
+def _planes(sc):
+    extra = [(2, 15, "ex", sc.dft[0][3])] if sc.lane == "uniform" else []   # crosses the PEC sheet
+    return list(sc.dft) + extra
+
+
+def _runner(sc, box, planes, mode="history", K=None):
+    import rfx_b200
+    from rfx_b200.adjoint import AdjointRunner
+    g = sc.product_grid()
+    mats = rfx_b200.MaterialArrays(*sc.materials)
+    if sc.lane == "nonuniform":
+        pads = (g.pad_x_lo + g.pad_x_hi, g.pad_y_lo + g.pad_y_hi, g.pad_z_lo + g.pad_z_hi)
+        axes, pec_axes = "".join(a for a, p in zip("xyz", pads) if p > 0), "xyz"
+    else:
+        axes, pec_axes = "xyz", (sc.pec_axes if sc.pec_axes is not None else "xyz")
+    dfts = [rfx_b200.init_dft_plane_probe(a, ix, c, f, g.shape) for (a, ix, c, f) in planes]
+    return AdjointRunner(g, mats, sc.n_steps, sources=sc.sources, probes=sc.probes, box=box, boundary=sc.boundary,
+                         cpml_axes=axes, pec_axes=pec_axes, pec_mask=sc.pec_mask, mode=mode, checkpoint_every=K,
+                         dft_planes=dfts, dft_time_offset=1 if sc.lane == "uniform" else 0)
+
+
+@pytest.mark.parametrize("build,box", [(small_uniform, (14, 18, 14, 18, 12, 14)),
+                                       (small_nonuniform, (12, 16, 12, 16, 11, 13))])
+@pytest.mark.parametrize("mode", ["history", "segments"])
+def test_dft_adjoint_is_exact_transpose(cuda, build, box, mode):
+    sc = build(n_steps=150)
+    planes = _planes(sc)
+    r = _runner(sc, box, planes, mode=mode, K=64)
+    ts = r.forward()
+    rng = np.random.default_rng(9)
+    G = [torch.from_numpy((rng.standard_normal(a.shape) + 1j * rng.standard_normal(a.shape)).astype(np.complex64))
+         .cuda() for a in r.dft_accs]
+    g = torch.from_numpy(rng.standard_normal(ts.shape).astype(np.float32)).cuda()
+    J_dft = sum(float((Gq.real.double() * a.real.double() + Gq.imag.double() * a.imag.double()).sum())
+                for Gq, a in zip(G, r.dft_accs))
+    J_prb = float((g.double() * ts.double()).sum())
+    _, s1 = r.backward(None, g_dft=G)
+    _, s2 = r.backward(g, g_dft=G)
+    J1 = float((s1.double() * r.src_table.double()).sum())
+    J2 = float((s2.double() * r.src_table.double()).sum())
+    print(sc.name, mode, "J_dft", J_dft, "via adjoint", J1, "| J_dft + J_probe", J_dft + J_prb, "via adjoint", J2)
+    assert abs(J1 - J_dft) <= 2e-5 * abs(J_dft)
+    assert abs(J2 - (J_dft + J_prb)) <= 2e-5 * abs(J_dft + J_prb)
+    r.close()
+
+
+def _oracle_dft_J(sc, eps_full, planes):
+    mats = (eps_full, sc.materials[1], sc.materials[2])
+    kw = dict(sources=sc.sources, probes=sc.probes, dft_planes=planes, pec_mask=sc.pec_mask, dtype=np.float64,
+              exact_materials=True)
+    if sc.lane == "uniform":
+        r = oracle.run_uniform(sc.ogrid, mats, sc.n_steps, boundary=sc.boundary, pec_axes=sc.pec_axes, **kw)
+    else:
+        r = oracle.run_nonuniform(sc.ogrid, mats, sc.n_steps, **kw)
+    return float(sum(np.sum(np.abs(a) ** 2) for a in r.dft_planes))
+
+
+@pytest.mark.parametrize("build,box", [(small_uniform, (14, 20, 14, 20, 12, 14)),
+                                       (small_nonuniform, (12, 18, 12, 18, 11, 13))])
+def test_dft_gradient_matches_fp64_finite_differences(cuda, build, box):
+    sc = build(n_steps=160)
+    planes = _planes(sc)
+    r = _runner(sc, box, planes)
+    r.forward()
+    grad, _ = r.backward(None, g_dft=[2 * a for a in r.dft_accs])   # d|a|^2 = 2 Re(conj(a) da)
+    grad = grad.cpu().numpy()
+    i0, i1, j0, j1, k0, k1 = box
+    rng = np.random.default_rng(13)
+    for _ in range(3):
+        d = rng.standard_normal((i1 - i0, j1 - j0, k1 - k0))
+        h = 1e-3
+        ep = sc.materials[0].astype(np.float64).copy()
+        em = ep.copy()
+        ep[i0:i1, j0:j1, k0:k1] += h * d
+        em[i0:i1, j0:j1, k0:k1] -= h * d
+        fd = (_oracle_dft_J(sc, ep, planes) - _oracle_dft_J(sc, em, planes)) / (2 * h)
+        ad = float(np.sum(grad * d))
+        print(sc.name, "directional AD", ad, "FD64", fd, "rel", abs(ad - fd) / abs(fd))
+        assert abs(ad - fd) <= 1e-3 * abs(fd)
+    r.close()
+
+
+def test_autograd_function_with_dft_outputs(cuda):
+    from rfx_b200.adjoint import FDTDFunction
+    sc = small_uniform(n_steps=120)
+    box = (14, 18, 14, 18, 12, 14)
+    r = _runner(sc, box, _planes(sc))
+    eps_box = torch.tensor(sc.materials[0][14:18, 14:18, 12:14], device="cuda", requires_grad=True)
+    src = r.src_table.clone().requires_grad_(True)
+    ts, *accs = FDTDFunction.apply(eps_box, src, r)
+    assert len(accs) == 3 and all(a.dtype == torch.complex64 for a in accs)
+    J = sum((a.abs() ** 2).sum() for a in accs) + ts.square().sum()
+    J.backward()
+    ge, gs = eps_box.grad, src.grad
+    assert torch.isfinite(ge).all() and float(ge.abs().sum()) > 0
+    # the same gradients from the runner directly
+    g2, s2 = r.backward(2 * ts.detach(), g_dft=[2 * a.detach() for a in accs])
+    assert torch.allclose(ge.double(), g2, rtol=1e-6, atol=0)
+    assert torch.allclose(gs, s2, rtol=1e-6, atol=0)
+    r.close()
