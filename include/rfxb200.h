@@ -171,6 +171,12 @@ typedef struct {
    * (cos, sin) * dt).  Both arrays NULL: no DFT-plane cotangents. */
   const void* const* dft_cot_dev;
   const void* const* dft_phase_dev;
+  /* NTFF-box objectives (the transpose of rfx/farfield.py:208-313): a
+   * complex64 cotangent laid out like the running sums of RfxbStepIO
+   * (faces x_lo .. z_hi, each (n_freqs, n1, n2, 4)) and the phase table the
+   * forward used ([n_total_steps][2][n_freqs]).  NULL: none. */
+  const void* ntff_cot_dev;
+  const void* ntff_phase_dev;
 } RfxbAdjointIO;
 
 int rfxb_version(void);

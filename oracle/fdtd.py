@@ -562,43 +562,50 @@ NTFF_FACES = ("x_lo", "x_hi", "y_lo", "y_hi", "z_lo", "z_hi")
 _NTFF_COMPONENTS = {0: ("ey", "ez", "hy", "hz"), 1: ("ex", "ez", "hx", "hz"), 2: ("ex", "ey", "hx", "hy")}
 
 
-def ntff_init(box):
+def ntff_init(box, dtype=np.float32):
     """Zeroed NTFF running sums and Kahan residuals (rfx/farfield.py:164-205):
     ``box`` = (i_lo, i_hi, j_lo, j_hi, k_lo, k_hi, freqs); x faces are
-    (n_f, nj, nk, 4), y faces (n_f, ni, nk, 4), z faces (n_f, ni, nj, 4)."""
+    (n_f, nj, nk, 4), y faces (n_f, ni, nk, 4), z faces (n_f, ni, nj, 4);
+    complex64 for float32 fields, complex128 for float64 ones
+    (rfx/farfield.py:144-161 ntff_accum_dtype)."""
     i0, i1, j0, j1, k0, k1, freqs = box
     nf = len(freqs)
+    cdt = np.complex64 if np.dtype(dtype) == np.float32 else np.complex128
     dims = {0: (j1 - j0, k1 - k0), 1: (i1 - i0, k1 - k0), 2: (i1 - i0, j1 - j0)}
     out = {}
     for q, name in enumerate(NTFF_FACES):
-        out[name] = np.zeros((nf,) + dims[q // 2] + (4,), np.complex64)
+        out[name] = np.zeros((nf,) + dims[q // 2] + (4,), cdt)
         out["c_" + name] = np.zeros_like(out[name])
     return out
 
 
-def ntff_phases(freqs, step, dt):
-    """E and H step factors of rfx/farfield.py:230-244 in float32 / complex64:
-    t = f32(step) * f32(dt), omega = f32(2 pi) * f32(f), E factor
-    exp(-1j omega t) dt, H factor exp(-1j omega (t + dt/2)) dt."""
-    d = np.float32(dt)
-    t = np.float32(step) * d
-    om = np.float32(2 * np.pi) * np.asarray(freqs, np.float32)
-    th = np.float32(t + d * np.float32(0.5))
+def ntff_phases(freqs, step, dt, dtype=np.float32):
+    """E and H step factors of rfx/farfield.py:230-244: t = step dt,
+    omega = 2 pi f, E factor exp(-1j omega t) dt, H factor
+    exp(-1j omega (t + dt/2)) dt, in float32 arithmetic (or float64 for a
+    float64 run)."""
+    f = np.dtype(dtype).type
+    d = f(dt)
+    t = f(step) * d
+    om = f(2 * np.pi) * np.asarray(freqs, dtype)
+    th = f(t + d * f(0.5))
     out = []
     for tt in (t, th):
-        a = (om * tt).astype(np.float32).astype(np.float64)
-        c = np.cos(a).astype(np.float32) * d
-        sn = -np.sin(a).astype(np.float32) * d
-        out.append((c.astype(np.float32), sn.astype(np.float32)))
+        a = (om * tt).astype(dtype).astype(np.float64)
+        c = np.cos(a).astype(dtype) * d
+        sn = -np.sin(a).astype(dtype) * d
+        out.append((c.astype(dtype), sn.astype(dtype)))
     return out
 
 
 def ntff_step(F, box, acc, step, dt):
     """One step of rfx/farfield.py:208-313: on each face the four tangential
     components times the step's factor (E factor for the E pair, H factor for
-    the H pair), Kahan-added per real and imaginary part in float32."""
+    the H pair), Kahan-added per real and imaginary part in the accumulators'
+    real type (float32 for complex64 sums)."""
     i0, i1, j0, j1, k0, k1, freqs = box
-    (ce, se), (chh, sh) = ntff_phases(freqs, step, dt)
+    rt = np.float32 if acc["x_lo"].dtype == np.complex64 else np.float64
+    (ce, se), (chh, sh) = ntff_phases(freqs, step, dt, rt)
     lo = (i0, j0, k0)
     hi = (i1, j1, k1)
     for q, name in enumerate(NTFF_FACES):
@@ -606,17 +613,17 @@ def ntff_step(F, box, acc, step, dt):
         idx = hi[ax] if q & 1 else lo[ax]
         sl = [slice(i0, i1), slice(j0, j1), slice(k0, k1)]
         sl[ax] = idx
-        vals = np.stack([np.asarray(F[c][tuple(sl)], np.float32) for c in _NTFF_COMPONENTS[ax]], axis=-1)
+        vals = np.stack([np.asarray(F[c][tuple(sl)], rt) for c in _NTFF_COMPONENTS[ax]], axis=-1)
         wr = np.stack([ce, ce, chh, chh], axis=-1)[:, None, None, :]
         wi = np.stack([se, se, sh, sh], axis=-1)[:, None, None, :]
         s, c = acc[name], acc["c_" + name]
         for part, w in (("real", wr), ("imag", wi)):
-            sv = getattr(s, part).astype(np.float32)
-            cv = getattr(c, part).astype(np.float32)
-            val = (vals[None] * w).astype(np.float32)
-            y = (val - cv).astype(np.float32)
-            t = (sv + y).astype(np.float32)
-            cv = ((t - sv).astype(np.float32) - y).astype(np.float32)
+            sv = getattr(s, part).astype(rt)
+            cv = getattr(c, part).astype(rt)
+            val = (vals[None] * w).astype(rt)
+            y = (val - cv).astype(rt)
+            t = (sv + y).astype(rt)
+            cv = ((t - sv).astype(rt) - y).astype(rt)
             if part == "real":
                 s.real, c.real = t, cv
             else:
@@ -636,7 +643,7 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
     vi = np.zeros((n_steps, len(vi_ports), 2), f) if vi_ports else None
     dt = st.g.dt
     flux_accs = [np.zeros((4, len(m[6]), m[3] - m[2], m[5] - m[4]), np.complex128) for m in flux_monitors]
-    ntff_acc = ntff_init(ntff) if ntff is not None else None
+    ntff_acc = ntff_init(ntff, f) if ntff is not None else None
     for n in range(n_steps):
         st.update_h()
         st.cpml_h()

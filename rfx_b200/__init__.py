@@ -23,8 +23,8 @@ from .checkpoint import (  # noqa: F401
     load_plan_state, load_snapshots, load_state, save_plan_state, save_snapshots, save_state,
 )
 from .farfield import (  # noqa: F401
-    FarFieldResult, NTFFBox, NTFFData, compute_far_field, directivity, init_ntff_data, make_ntff_box,
-    radiation_pattern,
+    FarFieldResult, NTFFBox, NTFFData, compute_far_field, directivity, directivity_torch, far_field,
+    init_ntff_data, make_ntff_box, radiation_pattern,
 )
 
 __version__ = "0.1.0"

@@ -75,6 +75,8 @@ class RfxbAdjointIO(C.Structure):
         ("src_adj_dev", C.c_void_p),
         ("dft_cot_dev", C.POINTER(C.c_void_p)),
         ("dft_phase_dev", C.POINTER(C.c_void_p)),
+        ("ntff_cot_dev", C.c_void_p),
+        ("ntff_phase_dev", C.c_void_p),
     ]
 
 

@@ -2,8 +2,9 @@
 transposed step backwards in time.  Replaces ``jax.grad`` through the scan
 (rfx/simulation.py:1972-2058 with ``checkpoint_segments``; rfx/nonuniform.py:
 1755-1796 with ``checkpoint_every``) for gradients of objectives of the probe
-traces and of running-DFT plane accumulators with respect to eps_r over a
-region of cells and to the source table.
+traces, of running-DFT plane accumulators and of the NTFF box (far-field
+objectives) with respect to eps_r over a region of cells and to the source
+table.
 
 Field history.  The gradient needs, at every step n and every cell of the
 region, E^n and curl H^{n+1/2} (the two factors of d E^{n+1} / d eps_r).
@@ -23,6 +24,7 @@ import torch
 
 from .cpml import build_cpml
 from .engine import Plan, PlanSpec, require_cuda
+from .farfield import face_views, init_ntff_data, ntff_descriptor, ntff_phase_table, pack_ntff
 from .grid import EPS_0, spacing_tables
 from .simulation import dft_phase_table, tangential_edge_masks
 
@@ -56,10 +58,12 @@ class AdjointRunner:
 
     def __init__(self, grid, materials, n_steps, *, sources, probes, box, boundary="cpml", cpml_axes="xyz",
                  pec_axes="", pec_mask=None, checkpoint_every=None, mode="auto",
-                 history_budget_bytes=8 << 30, dft_planes=None, dft_time_offset=1, device=None, _plan=None):
+                 history_budget_bytes=8 << 30, dft_planes=None, dft_time_offset=1, ntff=None, device=None,
+                 _plan=None):
         """``dft_planes``: ``DFTPlaneProbe`` values accumulated by the forward
         pass (sample time (n + dft_time_offset) dt: 1 on the uniform lane, 0 on
-        the graded one); their accumulators can carry cotangents."""
+        the graded one); ``ntff``: an ``NTFFBox`` accumulated by the forward
+        pass.  Their accumulators can carry cotangents."""
         self.device = require_cuda(device)
         self.grid = grid
         self.n_steps = int(n_steps)
@@ -77,12 +81,14 @@ class AdjointRunner:
         self.src_waves = [np.asarray(s[4], np.float32) for s in sources]
         self.probes = [tuple(p[:4]) for p in probes]
         self.dft_planes = list(dft_planes or [])
+        self.ntff = ntff
         spec = PlanSpec(shape=shape, dt=float(grid.dt), tables=spacing_tables(grid),
                         cpml=build_cpml(grid, cpml_axes if use_cpml else "",
                                         noop_faces=set(getattr(grid, "pec_faces", None) or ())) if use_cpml else None,
                         pec_axes=pec_axes, sources=self.sources,
                         probes=[(i, j, k, c, False) for (i, j, k, c) in self.probes], grad_box=self.box,
-                        dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in self.dft_planes])
+                        dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in self.dft_planes],
+                        ntff=ntff_descriptor(ntff) if ntff is not None else None)
         self.plan = _plan or Plan(spec, self.device)
         self.eps = torch.as_tensor(np.asarray(materials.eps_r, np.float32)).to(self.device).contiguous()
         self.sigma = torch.as_tensor(np.asarray(materials.sigma, np.float32)).to(self.device).contiguous()
@@ -102,6 +108,9 @@ class AdjointRunner:
         self.dft_phases = [torch.from_numpy(dft_phase_table(d.freqs, self.n_steps, grid.dt, dft_time_offset))
                            .to(self.device) for d in self.dft_planes]
         self.dft_accs = []
+        self.ntff_phase = (torch.from_numpy(ntff_phase_table(ntff.freqs, self.n_steps, grid.dt)).to(self.device)
+                           if ntff is not None else None)
+        self.ntff_faces = []
         self._dirty = True
 
     # materials ------------------------------------------------------------
@@ -128,6 +137,9 @@ class AdjointRunner:
         st = self.src_table if self.sources else None
         accs = [torch.zeros(d.accumulator.shape, device=self.device, dtype=torch.complex64) for d in self.dft_planes]
         dk = dict(dft_accs=accs, dft_phases=self.dft_phases) if accs else {}
+        if self.ntff is not None:
+            nacc, ncmp = pack_ntff(init_ntff_data(self.ntff), self.device)
+            dk["ntff"] = (nacc, ncmp, self.ntff_phase)
         if self.mode == "history":
             p.record_history(0, N)
             p.advance(0, N, st, ts, **dk)
@@ -136,14 +148,17 @@ class AdjointRunner:
                 p.checkpoint_save(q)
                 p.advance(s0, min(self.K, N - s0), st, ts, **dk)
         self.dft_accs = accs
+        self.ntff_faces = face_views(dk["ntff"][0], self.ntff) if self.ntff is not None else []
         p.check_device()
         self.ts = ts
         return ts
 
-    def backward(self, g_ts, want_source_grad=True, g_dft=None):
+    def backward(self, g_ts, want_source_grad=True, g_dft=None, g_ntff=None):
         """Adjoint sweep for probe cotangents ``g_ts`` (n_steps, n_probes; may
-        be None) and DFT-plane cotangents ``g_dft`` (per plane a complex
-        (n_freqs, n1, n2) array dJ/dRe + i dJ/dIm, or None).
+        be None), DFT-plane cotangents ``g_dft`` (per plane a complex
+        (n_freqs, n1, n2) array dJ/dRe + i dJ/dIm, or None) and NTFF
+        cotangents ``g_ntff`` (the six faces x_lo .. z_hi, each like its
+        accumulator, or None).
 
         Returns (dJ/d eps_r over the box as float64, dJ/d source table)."""
         p, N = self.plan, self.n_steps
@@ -169,6 +184,16 @@ class AdjointRunner:
                     raise ValueError(f"DFT-plane cotangent of shape {tuple(c.shape)}, accumulator "
                                      f"{tuple(d.accumulator.shape)}")
             kw.update(dft_cots=cots, dft_phases=self.dft_phases)
+        if g_ntff is not None and any(c is not None for c in g_ntff):
+            if self.ntff is None or len(g_ntff) != 6:
+                raise ValueError("NTFF cotangents need the runner's NTFF box and one entry per face")
+            parts = []
+            for c, f in zip(g_ntff, self.ntff_faces):
+                c = torch.zeros_like(f) if c is None else torch.as_tensor(c).to(self.device, torch.complex64)
+                if tuple(c.shape) != tuple(f.shape):
+                    raise ValueError(f"NTFF face cotangent of shape {tuple(c.shape)}, face {tuple(f.shape)}")
+                parts.append(c.reshape(-1))
+            kw.update(ntff=(torch.cat(parts).contiguous(), self.ntff_phase))
         p.adjoint_begin(N, **kw)
         st = self.src_table if self.sources else None
         if self.mode == "history":
@@ -190,8 +215,9 @@ class AdjointRunner:
 
 
 class FDTDFunction(torch.autograd.Function):
-    """Probe traces (and, when the runner has DFT planes, their complex64
-    accumulators as further outputs) as a differentiable function of eps_r
+    """Probe traces (and, when the runner has them, the complex64 DFT-plane
+    accumulators and the six NTFF face accumulators x_lo .. z_hi as further
+    outputs) as a differentiable function of eps_r
     over the runner's box and of the source table: the
     ``torch.autograd.Function`` face of the hand-written adjoint."""
 
@@ -201,13 +227,16 @@ class FDTDFunction(torch.autograd.Function):
         ts = runner.forward(src_table.detach() if src_table is not None else None)
         ctx.runner = runner
         ctx.has_src = src_table is not None
-        if runner.dft_planes:
-            return (ts.clone(), *[a.clone() for a in runner.dft_accs])
+        if runner.dft_planes or runner.ntff is not None:
+            return (ts.clone(), *[a.clone() for a in runner.dft_accs], *[f.clone() for f in runner.ntff_faces])
         return ts.clone()
 
     @staticmethod
-    def backward(ctx, g_ts, *g_dft):
-        grad, src_adj = ctx.runner.backward(g_ts, want_source_grad=ctx.has_src, g_dft=list(g_dft) or None)
+    def backward(ctx, g_ts, *g_rest):
+        nd = len(ctx.runner.dft_planes)
+        g_dft, g_ntff = list(g_rest[:nd]), list(g_rest[nd:])
+        grad, src_adj = ctx.runner.backward(g_ts, want_source_grad=ctx.has_src, g_dft=g_dft or None,
+                                            g_ntff=g_ntff or None)
         return grad.to(torch.float32), (src_adj if ctx.has_src else None), None
 
 

@@ -307,4 +307,59 @@ __global__ void dft_adj_kernel(const RfxbInst* __restrict__ insts, const AdjInst
   if (!zero) atomicAdd(A.aF[apar][comp] + e, g);
 }
 
+// Transpose of the NTFF box for sample s: on every face cell each of the four
+// tangential components receives sum_f Re(G) Re(w) + Im(G) Im(w) with w the E
+// factor (E components) or the H factor (H components) of step s, injected as
+// a DFT-plane cotangent is (E components: source adjoint, PEC / edge-mask
+// drop).  Faces share their edge cells, so the adds are atomic.
+__global__ void ntff_adj_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
+                                const RfxbNtffFace* __restrict__ faces, int nfaces, int s, int apar) {
+  int q = 0;
+  while (q + 1 < nfaces && faces[q + 1].block0 <= (int)blockIdx.x) ++q;
+  const RfxbNtffFace& F = faces[q];
+  if (F.acc == nullptr) return;
+  const int c = (blockIdx.x - F.block0) * blockDim.x + threadIdx.x;
+  const int cells = F.n1 * F.n2;
+  if (c >= cells) return;
+  const int a = F.lo1 + c / F.n2, b = F.lo2 + c % F.n2;
+  int i, j, k;
+  if (F.axis == 0) { i = F.index; j = a; k = b; }
+  else if (F.axis == 1) { i = a; j = F.index; k = b; }
+  else { i = a; j = b; k = F.index; }
+  const RfxbInst& P = insts[F.inst];
+  const AdjInst& A = adjs[F.inst];
+  const long long e = P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
+  const float2* ph = F.phase + (long long)s * 2 * F.nf;
+  float g[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int f = 0; f < F.nf; ++f) {
+    const float2 we = __ldg(ph + f), wh = __ldg(ph + F.nf + f);
+    const float4* gp = reinterpret_cast<const float4*>(F.acc + ((long long)f * cells + c) * 4);
+    const float4 g01 = gp[0], g23 = gp[1];
+    g[0] = fmaf(g01.x, we.x, fmaf(g01.y, we.y, g[0]));
+    g[1] = fmaf(g01.z, we.x, fmaf(g01.w, we.y, g[1]));
+    g[2] = fmaf(g23.x, wh.x, fmaf(g23.y, wh.y, g[2]));
+    g[3] = fmaf(g23.z, wh.x, fmaf(g23.w, wh.y, g[3]));
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    if (g[t] == 0.f) continue;
+    const int comp = F.comp[t];
+    bool zero = false;
+    if (comp < 3) {
+      if (P.src_adj)
+        for (int u = 0; u < P.nsrc; ++u) {
+          const int4 sc = P.src[u];
+          if (sc.x == i && sc.y == j && sc.z == k && sc.w == comp)
+            atomicAdd(P.src_adj + (long long)s * P.src_ld + u, g[t]);
+        }
+      if ((P.pec_axes & 1u) && (i == 0 || i == P.nx - 1) && comp != 0) zero = true;
+      if ((P.pec_axes & 2u) && (j == 0 || j == P.ny - 1) && comp != 1) zero = true;
+      if ((P.pec_axes & 4u) && (k == 0 || k == P.nz - 1) && comp != 2) zero = true;
+      if ((P.pec_axes & 4u) && k == P.nz - 1 && comp == 2) zero = true;
+      if (P.emask && (P.emask[e] >> comp) & 1u) zero = true;
+    }
+    if (!zero) atomicAdd(A.aF[apar][comp] + e, g[t]);
+  }
+}
+
 }  // namespace rfxb

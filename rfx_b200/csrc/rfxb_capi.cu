@@ -33,6 +33,7 @@ __global__ void adj_pass_a(const RfxbInst*, const AdjInst*, const RfxbWork*, int
 __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int, int, int);
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
 __global__ void dft_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbDftPlane*, int, int, int);
+__global__ void ntff_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbNtffFace*, int, int, int);
 __global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
 __global__ void flux_kernel(const RfxbInst*, const RfxbFluxPlane*, int, int, int);
 __global__ void ntff_kernel(const RfxbInst*, const RfxbNtffFace*, int, int, int);
@@ -194,6 +195,9 @@ struct RfxbBatch {
   std::vector<RfxbFluxPlane> flux;
   int flux_blocks = 0;
   RfxbNtffFace* d_ntff = nullptr;
+  RfxbNtffFace* d_ntffa = nullptr;   // the same faces with the adjoint call's cotangents
+  std::vector<RfxbNtffFace> ntffa;
+  bool has_ntff_cot = false;
   std::vector<RfxbNtffFace> ntff;   // six faces per plan with a box
   std::vector<long long> ntff_off;  // float2 offset of each face in its plan's buffers
   int ntff_blocks = 0;
@@ -1016,6 +1020,7 @@ int build_group(RfxbBatch* g) {
   g->ntff_blocks = nblocks;
   if (!g->ntff.empty()) {
     if (int rc = galloc((void**)&g->d_ntff, sizeof(RfxbNtffFace) * g->ntff.size())) return rc;
+    if (int rc = galloc((void**)&g->d_ntffa, sizeof(RfxbNtffFace) * g->ntff.size())) return rc;
   }
   if (!g->dft.empty()) {
     if (int rc = galloc((void**)&g->d_dft, sizeof(RfxbDftPlane) * g->dft.size())) return rc;
@@ -1270,6 +1275,21 @@ int upload_adjoint(RfxbBatch* g, const RfxbAdjointIO* aios, cudaStream_t st) {
   if (!g->dfta.empty())
     RFXB_CUDA(cudaMemcpyAsync(g->d_dfta, g->dfta.data(), sizeof(RfxbDftPlane) * g->dfta.size(),
                               cudaMemcpyHostToDevice, st));
+  // NTFF cotangents (faces of each plan's box at the offsets of the forward)
+  g->ntffa = g->ntff;
+  g->has_ntff_cot = false;
+  for (size_t f = 0; f < g->ntffa.size(); ++f) {
+    RfxbNtffFace& F = g->ntffa[f];
+    const RfxbAdjointIO& a = aios[F.inst];
+    const bool on = a.ntff_cot_dev && a.ntff_phase_dev;
+    F.acc = on ? const_cast<float2*>(static_cast<const float2*>(a.ntff_cot_dev)) + g->ntff_off[f] : nullptr;
+    F.cmp = nullptr;
+    F.phase = on ? static_cast<const float2*>(a.ntff_phase_dev) : nullptr;
+    if (on) g->has_ntff_cot = true;
+  }
+  if (!g->ntffa.empty())
+    RFXB_CUDA(cudaMemcpyAsync(g->d_ntffa, g->ntffa.data(), sizeof(RfxbNtffFace) * g->ntffa.size(),
+                              cudaMemcpyHostToDevice, st));
   for (auto& I : insts) I.status = g->d_status;
   RFXB_CUDA(cudaMemcpyAsync(g->d_inst, insts.data(), sizeof(RfxbInst) * insts.size(), cudaMemcpyHostToDevice, st));
   RFXB_CUDA(cudaMemcpyAsync(g->d_adj, adjs.data(), sizeof(AdjInst) * adjs.size(), cudaMemcpyHostToDevice, st));
@@ -1287,6 +1307,9 @@ int group_adjoint_begin(RfxbBatch* g, const RfxbAdjointIO* aios, int n_total, cu
   if (g->has_dft_cot)   // DFT-plane cotangent of the last sample
     dft_adj_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_adj, g->d_dfta, (int)g->dfta.size(), n_total - 1,
                                                   g->plans[0]->adj_fpar);
+  if (g->has_ntff_cot)  // NTFF cotangent of the last sample
+    ntff_adj_kernel<<<g->ntff_blocks, 256, 0, st>>>(g->d_inst, g->d_adj, g->d_ntffa, (int)g->ntffa.size(),
+                                                    n_total - 1, g->plans[0]->adj_fpar);
   RFXB_CUDA(cudaGetLastError());
   return 0;
 }
@@ -1349,13 +1372,17 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
       if (g->has_dft_cot && s >= 1)
         dft_adj_kernel<<<g->dft_blocks, 256, 0, cs>>>(g->d_inst, g->d_adj, g->d_dfta, (int)g->dfta.size(), s - 1,
                                                       fpar);
+      if (g->has_ntff_cot && s >= 1)
+        ntff_adj_kernel<<<g->ntff_blocks, 256, 0, cs>>>(g->d_inst, g->d_adj, g->d_ntffa, (int)g->ntffa.size(), s - 1,
+                                                        fpar);
       par ^= 1;
     }
     RFXB_CUDA(cudaGetLastError());
     return 0;
   };
   if (graphs_enabled() && n_steps >= 4) {
-    const GraphKey key{1 + (two ? 1 : 0), step_hi, n_steps, par0, fpar0, g->has_dft_cot ? 1 : 0};
+    const GraphKey key{1 + (two ? 1 : 0), step_hi, n_steps, par0, fpar0,
+                       (g->has_dft_cot ? 1 : 0) | (g->has_ntff_cot ? 2 : 0)};
     if (int rc = run_graph(g, key, st, launch)) return rc;
   } else {
     if (int rc = launch(st)) return rc;

@@ -335,9 +335,12 @@ class Plan:
 
     # -- adjoint -------------------------------------------------------------
     @staticmethod
-    def adjoint_io(g=None, grad=None, dca=None, dcb=None, src_adj=None, dft_cots=None, dft_phases=None):
+    def adjoint_io(g=None, grad=None, dca=None, dcb=None, src_adj=None, dft_cots=None, dft_phases=None,
+                   ntff=None):
         """``dft_cots``: per DFT plane a complex64 cotangent (n_freqs, n1, n2)
-        or None; ``dft_phases``: the phase tables the forward used."""
+        or None; ``dft_phases``: the phase tables the forward used; ``ntff``:
+        (flat complex64 cotangent of the NTFF faces, the forward's NTFF phase
+        table) or None."""
         a = RfxbAdjointIO()
         a.g_dev = g.data_ptr() if g is not None else None
         a.grad_dev = grad.data_ptr() if grad is not None else None
@@ -350,6 +353,8 @@ class Plan:
             a.dft_cot_dev = C.cast(cot, C.POINTER(C.c_void_p))
             a.dft_phase_dev = C.cast(ph, C.POINTER(C.c_void_p))
             a._keep = (cot, ph)   # the pointer arrays live as long as the struct
+        if ntff is not None:
+            a.ntff_cot_dev, a.ntff_phase_dev = ntff[0].data_ptr(), ntff[1].data_ptr()
         return a
 
     def adjoint_begin(self, n_total, **kw):

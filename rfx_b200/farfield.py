@@ -8,10 +8,13 @@ rfx/farfield.py:208-313 does.  The accumulators live in one flat device
 buffer per run (faces x_lo, x_hi, y_lo, y_hi, z_lo, z_hi back to back, each
 (n_freqs, n1, n2, 4)); ``NTFFData`` returns them in the reference's layout.
 
-``compute_far_field`` is the post-run transform of rfx/farfield.py:393-556
-(surface currents J = n x H, M = -n x E, radiation vectors N and L, far-field
-E_theta / E_phi), evaluated on the device in float64 / complex128 with one
-complex matrix product per face and frequency.
+``far_field`` is the post-run transform of rfx/farfield.py:393-556 (surface
+currents J = n x H, M = -n x E, radiation vectors N and L, far-field E_theta /
+E_phi) on torch tensors in complex128, one complex matrix product per face
+and frequency, differentiable with respect to the face accumulators (with
+``directivity_torch`` and the NTFF outputs of ``rfx_b200.adjoint.FDTDFunction``
+it gives far-field objectives a gradient through the hand-written adjoint);
+``compute_far_field`` wraps it with the reference's NumPy interface.
 """
 
 from __future__ import annotations
@@ -127,6 +130,17 @@ def ntff_phase_table(freqs, n_steps, dt, step0=0):
     return out
 
 
+def face_views(flat, box: NTFFBox):
+    """The six (n_freqs, n1, n2, 4) face views of a flat NTFF buffer."""
+    nf = len(box.freqs)
+    out, o = [], 0
+    for (n1, n2) in face_shapes(box):
+        m = nf * n1 * n2 * 4
+        out.append(flat[o:o + m].view(nf, n1, n2, 4))
+        o += m
+    return out
+
+
 def pack_ntff(data: NTFFData, device):
     """Flat device buffers (sums, residuals) of an ``NTFFData``."""
     def flat(arrs):
@@ -195,16 +209,17 @@ def _face_positions(grid, box, axis, idx, r1, r2, z_edges, lo):
     return np.stack([X, Y, Z], -1)
 
 
-def compute_far_field(ntff_data: NTFFData, box: NTFFBox, grid, theta, phi, device=None,
-                      chunk_cells: int = 1 << 14) -> FarFieldResult:
-    """rfx/farfield.py:393-556 on the device: for every face, frequency and
+def far_field(faces, box: NTFFBox, grid, theta, phi, chunk_cells: int = 1 << 14):
+    """rfx/farfield.py:393-556 on torch tensors: ``faces`` = the six NTFF face
+    tensors (x_lo .. z_hi, complex, (n_freqs, n1, n2, 4), all on one CUDA
+    device).  Returns (E_theta, E_phi), complex128 (n_freqs, n_theta, n_phi),
+    differentiable with respect to the faces: for every face, frequency and
     observation direction the radiation vectors N = sum J exp(jk r.r') dS and
     L = sum M exp(jk r.r') dS (a complex matrix product over face cells,
-    ``chunk_cells`` cells at a time), projected onto theta/phi unit vectors.
-    Graded grids (a ``dz`` table) use the z edge positions and per-cell dS of
-    the reference."""
-    from .engine import require_cuda
-    dev = require_cuda(device)
+    ``chunk_cells`` cells at a time), projected onto theta / phi.  Graded
+    grids (a ``dz`` table) use the z edge positions and per-cell dS of the
+    reference."""
+    dev = faces[0].device
     theta = np.asarray(theta, np.float64)
     phi = np.asarray(phi, np.float64)
     freqs = np.asarray(box.freqs, np.float64)
@@ -232,8 +247,8 @@ def compute_far_field(ntff_data: NTFFData, box: NTFFBox, grid, theta, phi, devic
     specs = [(0, -1, i0, (j0, j1), (k0, k1)), (0, 1, i1, (j0, j1), (k0, k1)),
              (1, -1, j0, (i0, i1), (k0, k1)), (1, 1, j1, (i0, i1), (k0, k1)),
              (2, -1, k0, (i0, i1), (j0, j1)), (2, 1, k1, (i0, i1), (j0, j1))]
-    for name, (axis, sign, idx, r1, r2) in zip(FACES, specs):
-        fd = torch.as_tensor(np.asarray(getattr(ntff_data, name)), device=dev).to(torch.complex128)
+    for fd, (axis, sign, idx, r1, r2) in zip(faces, specs):
+        fd = fd.to(torch.complex128)
         n1, n2 = fd.shape[1], fd.shape[2]
         if n1 == 0 or n2 == 0:
             continue
@@ -250,10 +265,13 @@ def compute_far_field(ntff_data: NTFFData, box: NTFFBox, grid, theta, phi, devic
         for c0 in range(0, nc, chunk_cells):
             c1 = min(nc, c0 + chunk_cells)
             dot = r_d @ pos[c0:c1].T                               # (n_dir, cells)
+            Nc, Lc = [], []
             for fi in range(nf):
                 ph = torch.polar(torch.ones_like(dot), float(k_arr[fi]) * dot)
-                N[fi] += ph @ J[fi, c0:c1]
-                L[fi] += ph @ M[fi, c0:c1]
+                Nc.append(ph @ J[fi, c0:c1])
+                Lc.append(ph @ M[fi, c0:c1])
+            N = N + torch.stack(Nc)
+            L = L + torch.stack(Lc)
     th_d = torch.from_numpy(th_hat).to(dev).to(torch.complex128)
     ph_d = torch.from_numpy(ph_hat).to(dev).to(torch.complex128)
     N_th, N_ph = (N * th_d).sum(-1), (N * ph_d).sum(-1)
@@ -261,9 +279,35 @@ def compute_far_field(ntff_data: NTFFData, box: NTFFBox, grid, theta, phi, devic
     jk = torch.from_numpy(1j * k_arr).to(dev)[:, None]
     E_th = -jk / (4 * np.pi) * (L_ph + ETA_0 * N_th)
     E_ph = jk / (4 * np.pi) * (L_th - ETA_0 * N_ph)
-    n_th, n_ph = len(theta), len(phi)
-    return FarFieldResult(E_th.reshape(nf, n_th, n_ph).cpu().numpy(), E_ph.reshape(nf, n_th, n_ph).cpu().numpy(),
-                          theta, phi, freqs)
+    return E_th.reshape(nf, len(theta), len(phi)), E_ph.reshape(nf, len(theta), len(phi))
+
+
+def compute_far_field(ntff_data: NTFFData, box: NTFFBox, grid, theta, phi, device=None,
+                      chunk_cells: int = 1 << 14) -> FarFieldResult:
+    """rfx/farfield.py:393-556 on the device (``far_field`` on the faces of
+    an ``NTFFData``), returned as NumPy arrays like the reference's."""
+    from .engine import require_cuda
+    dev = require_cuda(device)
+    faces = [torch.as_tensor(np.asarray(getattr(ntff_data, name)), device=dev) for name in FACES]
+    E_th, E_ph = far_field(faces, box, grid, theta, phi, chunk_cells)
+    return FarFieldResult(E_th.cpu().numpy(), E_ph.cpu().numpy(), np.asarray(theta, np.float64),
+                          np.asarray(phi, np.float64), np.asarray(box.freqs, np.float64))
+
+
+def directivity_torch(E_theta, E_phi, theta, phi):
+    """``directivity`` (rfx/farfield.py:780-802) as a linear ratio
+    4 pi U / P_rad on torch tensors, per frequency and direction
+    (n_freqs, n_theta, n_phi), differentiable: the objective of far-field
+    inverse design (rfx/optimize_objectives.py maximize_directivity takes its
+    logarithm at a target direction)."""
+    p = E_theta.real ** 2 + E_theta.imag ** 2 + E_phi.real ** 2 + E_phi.imag ** 2
+    th = np.asarray(theta, np.float64)
+    ph = np.asarray(phi, np.float64)
+    dth = np.gradient(th) if len(th) > 1 else np.array([np.pi])
+    dph = np.gradient(ph) if len(ph) > 1 else np.array([2 * np.pi])
+    w = torch.from_numpy(np.sin(th)[:, None] * dth[:, None] * dph[None, :]).to(p.device)
+    prad = (p * w[None]).sum(dim=(1, 2))
+    return 4 * np.pi * p / prad[:, None, None]
 
 
 def radiation_pattern(ff: FarFieldResult) -> np.ndarray:

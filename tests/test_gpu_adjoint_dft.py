@@ -1,6 +1,7 @@
-"""GPU tests of the adjoint with DFT-plane objectives (the transpose of the
-running DFT, rfx/simulation.py:1574-1588 and rfx/nonuniform.py:1458-1472,
-which the reference differentiates with jax.grad through the scan).
+"""GPU tests of the adjoint with DFT-plane and NTFF objectives (the transposes
+of the running DFT, rfx/simulation.py:1574-1588 and rfx/nonuniform.py:
+1458-1472, and of the NTFF box, rfx/farfield.py:208-313, which the reference
+differentiates with jax.grad through the scan).
 
 1. Exact transpose: a DFT accumulator is linear in the source table, so for
    J = sum Re(conj(G) acc) (plus <g, ts> of the probes) the source adjoint
@@ -11,6 +12,9 @@ which the reference differentiates with jax.grad through the scan).
    float64 oracle along three seeded directions (tolerance 1e-3 relative).
 3. The torch.autograd face returns the accumulators as outputs and accepts
    their gradients.
+4. NTFF: the exact transpose for a face objective, and the directivity at
+   one direction (through the differentiable device far-field transform)
+   against float64 finite differences of the oracle.
 """
 
 import numpy as np
@@ -122,4 +126,96 @@ def test_autograd_function_with_dft_outputs(cuda):
     g2, s2 = r.backward(2 * ts.detach(), g_dft=[2 * a.detach() for a in accs])
     assert torch.allclose(ge.double(), g2, rtol=1e-6, atol=0)
     assert torch.allclose(gs, s2, rtol=1e-6, atol=0)
+    r.close()
+
+
+# ---------------------------------------------------------------- NTFF box
+# The box of the uniform scene: its x_lo face passes through the ez source
+# (12, 13, 13) and its z_hi face lies on the PEC sheet (k = 15), whose edge
+# mask zeroes ex / ey there.
+_NTFF_BOX = (12, 30, 9, 26, 10, 15)
+_NTFF_FREQS = np.array([12e9, 15e9], np.float32)
+
+
+def _ntff_runner(sc, box, mode="history", K=None):
+    import rfx_b200
+    from rfx_b200.adjoint import AdjointRunner
+    g = sc.product_grid()
+    nb = rfx_b200.NTFFBox(*_NTFF_BOX, _NTFF_FREQS, *(sc.ogrid.cpml_layers,) * 6)
+    return AdjointRunner(g, rfx_b200.MaterialArrays(*sc.materials), sc.n_steps, sources=sc.sources,
+                         probes=sc.probes, box=box, boundary=sc.boundary, cpml_axes="xyz",
+                         pec_axes=sc.pec_axes if sc.pec_axes is not None else "xyz", pec_mask=sc.pec_mask,
+                         mode=mode, checkpoint_every=K, ntff=nb), nb
+
+
+@pytest.mark.parametrize("mode", ["history", "segments"])
+def test_ntff_adjoint_is_exact_transpose(cuda, mode):
+    sc = small_uniform(n_steps=150)
+    r, _ = _ntff_runner(sc, (14, 18, 14, 18, 12, 14), mode=mode, K=64)
+    r.forward()
+    rng = np.random.default_rng(21)
+    G = [torch.from_numpy((rng.standard_normal(f.shape) + 1j * rng.standard_normal(f.shape)).astype(np.complex64))
+         .cuda() for f in r.ntff_faces]
+    J = sum(float((Gq.real.double() * f.real.double() + Gq.imag.double() * f.imag.double()).sum())
+            for Gq, f in zip(G, r.ntff_faces))
+    _, s1 = r.backward(None, g_ntff=G)
+    J1 = float((s1.double() * r.src_table.double()).sum())
+    print(mode, "J_ntff", J, "via adjoint", J1)
+    assert abs(J1 - J) <= 2e-5 * abs(J)
+    r.close()
+
+
+def _oracle_directivity(sc, eps_full, theta, phi, it, ip):
+    from oracle import farfield as off
+    mats = (eps_full, sc.materials[1], sc.materials[2])
+    r = oracle.run_uniform(sc.ogrid, mats, sc.n_steps, boundary=sc.boundary, pec_axes=sc.pec_axes,
+                           sources=sc.sources, probes=sc.probes, pec_mask=sc.pec_mask, dtype=np.float64,
+                           exact_materials=True, ntff=(*_NTFF_BOX, _NTFF_FREQS))
+    n = sc.ogrid.cpml_layers
+    Et, Ep = off.compute_far_field(r.ntff, (*_NTFF_BOX, _NTFF_FREQS), sc.ogrid.dx, (n, n, n), theta, phi)
+    p = np.abs(Et) ** 2 + np.abs(Ep) ** 2
+    dth, dph = np.gradient(theta), np.gradient(phi)
+    prad = np.sum(p * np.sin(theta)[None, :, None] * dth[None, :, None] * dph[None, None, :], axis=(1, 2))
+    return float(np.sum(4 * np.pi * p[:, it, ip] / prad))
+
+
+def test_directivity_gradient_matches_fp64_finite_differences(cuda):
+    """The far-field objective of rfx's directivity optimisation, restated:
+    J = sum over the NTFF frequencies of the directivity (4 pi U / P_rad) at
+    one direction, through the device far-field transform and the NTFF
+    outputs of FDTDFunction (rfx tests/test_directivity_gradient.py checks
+    the same path through jax.grad for a nonzero, finite value)."""
+    import rfx_b200
+    from rfx_b200.adjoint import FDTDFunction
+    sc = small_uniform(n_steps=160)
+    box = (14, 20, 14, 20, 12, 14)
+    r, nb = _ntff_runner(sc, box)
+    theta = np.linspace(0.05, np.pi - 0.05, 19)
+    phi = np.linspace(0.0, 2 * np.pi, 12, endpoint=False)
+    it, ip = 9, 0
+    g = sc.product_grid()
+    eps_box = torch.tensor(sc.materials[0][box[0]:box[1], box[2]:box[3], box[4]:box[5]], device="cuda",
+                           requires_grad=True)
+    ts, *faces = FDTDFunction.apply(eps_box, None, r)
+    Et, Ep = rfx_b200.far_field(faces, nb, g, theta, phi)
+    J = rfx_b200.directivity_torch(Et, Ep, theta, phi)[:, it, ip].sum()
+    J.backward()
+    grad = eps_box.grad.double().cpu().numpy()
+    J0 = _oracle_directivity(sc, sc.materials[0].astype(np.float64), theta, phi, it, ip)
+    Jv = float(J.detach())
+    print("directivity objective CUDA", Jv, "oracle f64", J0)
+    assert abs(Jv - J0) <= 1e-4 * abs(J0)
+    i0, i1, j0, j1, k0, k1 = box
+    rng = np.random.default_rng(17)
+    for _ in range(3):
+        d = rng.standard_normal((i1 - i0, j1 - j0, k1 - k0))
+        h = 1e-3
+        ep = sc.materials[0].astype(np.float64).copy()
+        em = ep.copy()
+        ep[i0:i1, j0:j1, k0:k1] += h * d
+        em[i0:i1, j0:j1, k0:k1] -= h * d
+        fd = (_oracle_directivity(sc, ep, theta, phi, it, ip) - _oracle_directivity(sc, em, theta, phi, it, ip)) / (2 * h)
+        ad = float(np.sum(grad * d))
+        print("directivity directional AD", ad, "FD64", fd, "rel", abs(ad - fd) / abs(fd))
+        assert abs(ad - fd) <= 1e-3 * abs(fd)
     r.close()
