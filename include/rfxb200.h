@@ -177,6 +177,12 @@ typedef struct {
    * forward used ([n_total_steps][2][n_freqs]).  NULL: none. */
   const void* ntff_cot_dev;
   const void* ntff_phase_dev;
+  /* Flux-monitor objectives (the transpose of rfx/simulation.py:1590-1642):
+   * per monitor a complex128 cotangent laid out like its accumulator
+   * ([4][n_freqs][n1][n2]) or NULL, and the kernel table the forward used.
+   * Both arrays NULL: none. */
+  const void* const* flux_cot_dev;
+  const void* const* flux_kernel_dev;
 } RfxbAdjointIO;
 
 int rfxb_version(void);

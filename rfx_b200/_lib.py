@@ -77,6 +77,8 @@ class RfxbAdjointIO(C.Structure):
         ("dft_phase_dev", C.POINTER(C.c_void_p)),
         ("ntff_cot_dev", C.c_void_p),
         ("ntff_phase_dev", C.c_void_p),
+        ("flux_cot_dev", C.POINTER(C.c_void_p)),
+        ("flux_kernel_dev", C.POINTER(C.c_void_p)),
     ]
 
 

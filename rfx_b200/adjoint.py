@@ -2,9 +2,9 @@
 transposed step backwards in time.  Replaces ``jax.grad`` through the scan
 (rfx/simulation.py:1972-2058 with ``checkpoint_segments``; rfx/nonuniform.py:
 1755-1796 with ``checkpoint_every``) for gradients of objectives of the probe
-traces, of running-DFT plane accumulators and of the NTFF box (far-field
-objectives) with respect to eps_r over a region of cells and to the source
-table.
+traces, of running-DFT plane accumulators, of Poynting-flux monitors and of
+the NTFF box (far-field objectives) with respect to eps_r over a region of
+cells and to the source table.
 
 Field history.  The gradient needs, at every step n and every cell of the
 region, E^n and curl H^{n+1/2} (the two factors of d E^{n+1} / d eps_r).
@@ -26,7 +26,7 @@ from .cpml import build_cpml
 from .engine import Plan, PlanSpec, require_cuda
 from .farfield import face_views, init_ntff_data, ntff_descriptor, ntff_phase_table, pack_ntff
 from .grid import EPS_0, spacing_tables
-from .simulation import dft_phase_table, tangential_edge_masks
+from .simulation import dft_phase_table, flux_kernel_table, tangential_edge_masks
 
 
 def coefficient_derivatives(eps_r, sigma, dt):
@@ -58,12 +58,13 @@ class AdjointRunner:
 
     def __init__(self, grid, materials, n_steps, *, sources, probes, box, boundary="cpml", cpml_axes="xyz",
                  pec_axes="", pec_mask=None, checkpoint_every=None, mode="auto",
-                 history_budget_bytes=8 << 30, dft_planes=None, dft_time_offset=1, ntff=None, device=None,
-                 _plan=None):
+                 history_budget_bytes=8 << 30, dft_planes=None, dft_time_offset=1, ntff=None, flux_monitors=None,
+                 device=None, _plan=None):
         """``dft_planes``: ``DFTPlaneProbe`` values accumulated by the forward
         pass (sample time (n + dft_time_offset) dt: 1 on the uniform lane, 0 on
-        the graded one); ``ntff``: an ``NTFFBox`` accumulated by the forward
-        pass.  Their accumulators can carry cotangents."""
+        the graded one); ``ntff``: an ``NTFFBox`` and ``flux_monitors``:
+        ``FluxMonitor`` values accumulated by the forward pass (uniform lane).
+        Their accumulators can carry cotangents."""
         self.device = require_cuda(device)
         self.grid = grid
         self.n_steps = int(n_steps)
@@ -82,13 +83,15 @@ class AdjointRunner:
         self.probes = [tuple(p[:4]) for p in probes]
         self.dft_planes = list(dft_planes or [])
         self.ntff = ntff
+        self.flux_monitors = list(flux_monitors or [])
         spec = PlanSpec(shape=shape, dt=float(grid.dt), tables=spacing_tables(grid),
                         cpml=build_cpml(grid, cpml_axes if use_cpml else "",
                                         noop_faces=set(getattr(grid, "pec_faces", None) or ())) if use_cpml else None,
                         pec_axes=pec_axes, sources=self.sources,
                         probes=[(i, j, k, c, False) for (i, j, k, c) in self.probes], grad_box=self.box,
                         dft=[(d.axis, d.index, d.component, len(d.freqs)) for d in self.dft_planes],
-                        ntff=ntff_descriptor(ntff) if ntff is not None else None)
+                        ntff=ntff_descriptor(ntff) if ntff is not None else None,
+                        flux=[(m.axis, m.index, m.lo1, m.hi1, m.lo2, m.hi2, len(m.freqs)) for m in self.flux_monitors])
         self.plan = _plan or Plan(spec, self.device)
         self.eps = torch.as_tensor(np.asarray(materials.eps_r, np.float32)).to(self.device).contiguous()
         self.sigma = torch.as_tensor(np.asarray(materials.sigma, np.float32)).to(self.device).contiguous()
@@ -111,6 +114,9 @@ class AdjointRunner:
         self.ntff_phase = (torch.from_numpy(ntff_phase_table(ntff.freqs, self.n_steps, grid.dt)).to(self.device)
                            if ntff is not None else None)
         self.ntff_faces = []
+        self.flux_kernels = [torch.from_numpy(flux_kernel_table(m, self.n_steps, grid.dt)).to(self.device)
+                             for m in self.flux_monitors]
+        self.flux_accs = []
         self._dirty = True
 
     # materials ------------------------------------------------------------
@@ -140,6 +146,10 @@ class AdjointRunner:
         if self.ntff is not None:
             nacc, ncmp = pack_ntff(init_ntff_data(self.ntff), self.device)
             dk["ntff"] = (nacc, ncmp, self.ntff_phase)
+        faccs = [torch.zeros((4,) + tuple(np.shape(m.e1_dft)), device=self.device, dtype=torch.complex128)
+                 for m in self.flux_monitors]
+        if faccs:
+            dk.update(flux_accs=faccs, flux_kernels=self.flux_kernels)
         if self.mode == "history":
             p.record_history(0, N)
             p.advance(0, N, st, ts, **dk)
@@ -149,16 +159,18 @@ class AdjointRunner:
                 p.advance(s0, min(self.K, N - s0), st, ts, **dk)
         self.dft_accs = accs
         self.ntff_faces = face_views(dk["ntff"][0], self.ntff) if self.ntff is not None else []
+        self.flux_accs = faccs
         p.check_device()
         self.ts = ts
         return ts
 
-    def backward(self, g_ts, want_source_grad=True, g_dft=None, g_ntff=None):
+    def backward(self, g_ts, want_source_grad=True, g_dft=None, g_ntff=None, g_flux=None):
         """Adjoint sweep for probe cotangents ``g_ts`` (n_steps, n_probes; may
         be None), DFT-plane cotangents ``g_dft`` (per plane a complex
         (n_freqs, n1, n2) array dJ/dRe + i dJ/dIm, or None) and NTFF
         cotangents ``g_ntff`` (the six faces x_lo .. z_hi, each like its
-        accumulator, or None).
+        accumulator, or None), flux cotangents ``g_flux`` (per monitor a
+        complex (4, n_freqs, n1, n2) array for E1 E2 H1 H2, or None).
 
         Returns (dJ/d eps_r over the box as float64, dJ/d source table)."""
         p, N = self.plan, self.n_steps
@@ -194,6 +206,12 @@ class AdjointRunner:
                     raise ValueError(f"NTFF face cotangent of shape {tuple(c.shape)}, face {tuple(f.shape)}")
                 parts.append(c.reshape(-1))
             kw.update(ntff=(torch.cat(parts).contiguous(), self.ntff_phase))
+        if g_flux is not None and any(c is not None for c in g_flux):
+            if len(g_flux) != len(self.flux_monitors):
+                raise ValueError("one flux cotangent (or None) per flux monitor")
+            fc = [None if c is None else torch.as_tensor(c).to(self.device, torch.complex128).contiguous()
+                  for c in g_flux]
+            kw.update(flux_cots=fc, flux_kernels=self.flux_kernels)
         p.adjoint_begin(N, **kw)
         st = self.src_table if self.sources else None
         if self.mode == "history":
@@ -216,7 +234,8 @@ class AdjointRunner:
 
 class FDTDFunction(torch.autograd.Function):
     """Probe traces (and, when the runner has them, the complex64 DFT-plane
-    accumulators and the six NTFF face accumulators x_lo .. z_hi as further
+    accumulators, the six NTFF face accumulators x_lo .. z_hi and the
+    complex128 flux-monitor accumulators (4, n_freqs, n1, n2) as further
     outputs) as a differentiable function of eps_r
     over the runner's box and of the source table: the
     ``torch.autograd.Function`` face of the hand-written adjoint."""
@@ -227,16 +246,18 @@ class FDTDFunction(torch.autograd.Function):
         ts = runner.forward(src_table.detach() if src_table is not None else None)
         ctx.runner = runner
         ctx.has_src = src_table is not None
-        if runner.dft_planes or runner.ntff is not None:
-            return (ts.clone(), *[a.clone() for a in runner.dft_accs], *[f.clone() for f in runner.ntff_faces])
+        if runner.dft_planes or runner.ntff is not None or runner.flux_monitors:
+            return (ts.clone(), *[a.clone() for a in runner.dft_accs], *[f.clone() for f in runner.ntff_faces],
+                    *[a.clone() for a in runner.flux_accs])
         return ts.clone()
 
     @staticmethod
     def backward(ctx, g_ts, *g_rest):
-        nd = len(ctx.runner.dft_planes)
-        g_dft, g_ntff = list(g_rest[:nd]), list(g_rest[nd:])
-        grad, src_adj = ctx.runner.backward(g_ts, want_source_grad=ctx.has_src, g_dft=g_dft or None,
-                                            g_ntff=g_ntff or None)
+        r = ctx.runner
+        nd, nn = len(r.dft_planes), len(r.ntff_faces)
+        g_dft, g_ntff, g_flux = list(g_rest[:nd]), list(g_rest[nd:nd + nn]), list(g_rest[nd + nn:])
+        grad, src_adj = r.backward(g_ts, want_source_grad=ctx.has_src, g_dft=g_dft or None, g_ntff=g_ntff or None,
+                                   g_flux=g_flux or None)
         return grad.to(torch.float32), (src_adj if ctx.has_src else None), None
 
 

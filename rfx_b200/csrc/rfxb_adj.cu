@@ -362,4 +362,68 @@ __global__ void ntff_adj_kernel(const RfxbInst* __restrict__ insts, const AdjIns
   }
 }
 
+// Transpose of the flux monitors for sample s: per region cell the E pair
+// receives sum_f Re(G) Re(k_E) + Im(G) Im(k_E) on the monitor plane (source
+// adjoint and PEC / edge-mask drop as for a DFT plane), the H pair the same
+// with the H factor, split in halves over the two planes the forward
+// averaged (both halves on plane 0 when the monitor is on plane 0).
+__global__ void flux_adj_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
+                                const RfxbFluxPlane* __restrict__ planes, int nplanes, int s, int apar) {
+  int q = 0;
+  while (q + 1 < nplanes && planes[q + 1].block0 <= (int)blockIdx.x) ++q;
+  const RfxbFluxPlane& M = planes[q];
+  if (M.acc == nullptr) return;
+  const int c = (blockIdx.x - M.block0) * blockDim.x + threadIdx.x;
+  const int cells = M.n1 * M.n2;
+  if (c >= cells) return;
+  const int a = M.lo1 + c / M.n2, b = M.lo2 + c % M.n2;
+  auto at = [&](int plane, int& i, int& j, int& k) {
+    if (M.axis == 0) { i = plane; j = a; k = b; }
+    else if (M.axis == 1) { i = a; j = plane; k = b; }
+    else { i = a; j = b; k = plane; }
+  };
+  const double2* kn = M.kern + (long long)s * 2 * M.nf;
+  double g[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int f = 0; f < M.nf; ++f) {
+    const double2 ke = kn[f], kh = kn[M.nf + f];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const double2 G = M.acc[((long long)t * M.nf + f) * cells + c];
+      const double2 w = t < 2 ? ke : kh;
+      g[t] += G.x * w.x + G.y * w.y;
+    }
+  }
+  const RfxbInst& P = insts[M.inst];
+  const AdjInst& A = adjs[M.inst];
+  int i, j, k;
+  at(M.index, i, j, k);
+  const long long e = P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
+  for (int t = 0; t < 2; ++t) {   // E pair on the monitor plane
+    const float v = (float)g[t];
+    if (v == 0.f) continue;
+    const int comp = M.comp[t];
+    if (P.src_adj)
+      for (int u = 0; u < P.nsrc; ++u) {
+        const int4 sc = P.src[u];
+        if (sc.x == i && sc.y == j && sc.z == k && sc.w == comp) atomicAdd(P.src_adj + (long long)s * P.src_ld + u, v);
+      }
+    bool zero = false;
+    if ((P.pec_axes & 1u) && (i == 0 || i == P.nx - 1) && comp != 0) zero = true;
+    if ((P.pec_axes & 2u) && (j == 0 || j == P.ny - 1) && comp != 1) zero = true;
+    if ((P.pec_axes & 4u) && (k == 0 || k == P.nz - 1) && comp != 2) zero = true;
+    if ((P.pec_axes & 4u) && k == P.nz - 1 && comp == 2) zero = true;
+    if (P.emask && (P.emask[e] >> comp) & 1u) zero = true;
+    if (!zero) atomicAdd(A.aF[apar][comp] + e, v);
+  }
+  int i1, j1, k1;
+  at(M.im1, i1, j1, k1);
+  const long long e1 = P.off0 + (long long)i1 * P.ps + (long long)j1 * P.zs + k1;
+  for (int t = 2; t < 4; ++t) {   // H pair: (H(im1) + H(index)) / 2
+    const float v = (float)(0.5 * g[t]);
+    if (v == 0.f) continue;
+    atomicAdd(A.aF[apar][M.comp[t]] + e1, v);
+    atomicAdd(A.aF[apar][M.comp[t]] + e, v);
+  }
+}
+
 }  // namespace rfxb

@@ -34,6 +34,7 @@ __global__ void adj_pass_b(const RfxbInst*, const AdjInst*, const RfxbWork*, int
 __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
 __global__ void dft_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbDftPlane*, int, int, int);
 __global__ void ntff_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbNtffFace*, int, int, int);
+__global__ void flux_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbFluxPlane*, int, int, int);
 __global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
 __global__ void flux_kernel(const RfxbInst*, const RfxbFluxPlane*, int, int, int);
 __global__ void ntff_kernel(const RfxbInst*, const RfxbNtffFace*, int, int, int);
@@ -192,6 +193,9 @@ struct RfxbBatch {
   std::vector<RfxbDftPlane> dfta;
   bool has_dft_cot = false;
   RfxbFluxPlane* d_flux = nullptr;
+  RfxbFluxPlane* d_fluxa = nullptr;   // the same monitors with the adjoint call's cotangents
+  std::vector<RfxbFluxPlane> fluxa;
+  bool has_flux_cot = false;
   std::vector<RfxbFluxPlane> flux;
   int flux_blocks = 0;
   RfxbNtffFace* d_ntff = nullptr;
@@ -983,6 +987,7 @@ int build_group(RfxbBatch* g) {
   g->flux_blocks = fblocks;
   if (!g->flux.empty()) {
     if (int rc = galloc((void**)&g->d_flux, sizeof(RfxbFluxPlane) * g->flux.size())) return rc;
+    if (int rc = galloc((void**)&g->d_fluxa, sizeof(RfxbFluxPlane) * g->flux.size())) return rc;
   }
   // NTFF boxes: faces x_lo, x_hi, y_lo, y_hi, z_lo, z_hi with the tangential
   // components of rfx/farfield.py:247-269
@@ -1275,6 +1280,22 @@ int upload_adjoint(RfxbBatch* g, const RfxbAdjointIO* aios, cudaStream_t st) {
   if (!g->dfta.empty())
     RFXB_CUDA(cudaMemcpyAsync(g->d_dfta, g->dfta.data(), sizeof(RfxbDftPlane) * g->dfta.size(),
                               cudaMemcpyHostToDevice, st));
+  // flux-monitor cotangents (monitors of the group in plan order)
+  g->fluxa = g->flux;
+  g->has_flux_cot = false;
+  size_t fi = 0;
+  for (size_t q = 0; q < g->plans.size(); ++q) {
+    const RfxbAdjointIO& a = aios[q];
+    for (size_t d = 0; d < g->plans[q]->flux.size(); ++d, ++fi) {
+      const bool on = a.flux_cot_dev && a.flux_kernel_dev && a.flux_cot_dev[d] && a.flux_kernel_dev[d];
+      g->fluxa[fi].acc = on ? const_cast<double2*>(static_cast<const double2*>(a.flux_cot_dev[d])) : nullptr;
+      g->fluxa[fi].kern = on ? static_cast<const double2*>(a.flux_kernel_dev[d]) : nullptr;
+      if (on) g->has_flux_cot = true;
+    }
+  }
+  if (!g->fluxa.empty())
+    RFXB_CUDA(cudaMemcpyAsync(g->d_fluxa, g->fluxa.data(), sizeof(RfxbFluxPlane) * g->fluxa.size(),
+                              cudaMemcpyHostToDevice, st));
   // NTFF cotangents (faces of each plan's box at the offsets of the forward)
   g->ntffa = g->ntff;
   g->has_ntff_cot = false;
@@ -1309,6 +1330,9 @@ int group_adjoint_begin(RfxbBatch* g, const RfxbAdjointIO* aios, int n_total, cu
                                                   g->plans[0]->adj_fpar);
   if (g->has_ntff_cot)  // NTFF cotangent of the last sample
     ntff_adj_kernel<<<g->ntff_blocks, 256, 0, st>>>(g->d_inst, g->d_adj, g->d_ntffa, (int)g->ntffa.size(),
+                                                    n_total - 1, g->plans[0]->adj_fpar);
+  if (g->has_flux_cot)  // flux-monitor cotangent of the last sample
+    flux_adj_kernel<<<g->flux_blocks, 256, 0, st>>>(g->d_inst, g->d_adj, g->d_fluxa, (int)g->fluxa.size(),
                                                     n_total - 1, g->plans[0]->adj_fpar);
   RFXB_CUDA(cudaGetLastError());
   return 0;
@@ -1375,6 +1399,9 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
       if (g->has_ntff_cot && s >= 1)
         ntff_adj_kernel<<<g->ntff_blocks, 256, 0, cs>>>(g->d_inst, g->d_adj, g->d_ntffa, (int)g->ntffa.size(), s - 1,
                                                         fpar);
+      if (g->has_flux_cot && s >= 1)
+        flux_adj_kernel<<<g->flux_blocks, 256, 0, cs>>>(g->d_inst, g->d_adj, g->d_fluxa, (int)g->fluxa.size(), s - 1,
+                                                        fpar);
       par ^= 1;
     }
     RFXB_CUDA(cudaGetLastError());
@@ -1382,7 +1409,7 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
   };
   if (graphs_enabled() && n_steps >= 4) {
     const GraphKey key{1 + (two ? 1 : 0), step_hi, n_steps, par0, fpar0,
-                       (g->has_dft_cot ? 1 : 0) | (g->has_ntff_cot ? 2 : 0)};
+                       (g->has_dft_cot ? 1 : 0) | (g->has_ntff_cot ? 2 : 0) | (g->has_flux_cot ? 4 : 0)};
     if (int rc = run_graph(g, key, st, launch)) return rc;
   } else {
     if (int rc = launch(st)) return rc;

@@ -336,11 +336,12 @@ class Plan:
     # -- adjoint -------------------------------------------------------------
     @staticmethod
     def adjoint_io(g=None, grad=None, dca=None, dcb=None, src_adj=None, dft_cots=None, dft_phases=None,
-                   ntff=None):
+                   ntff=None, flux_cots=None, flux_kernels=None):
         """``dft_cots``: per DFT plane a complex64 cotangent (n_freqs, n1, n2)
         or None; ``dft_phases``: the phase tables the forward used; ``ntff``:
         (flat complex64 cotangent of the NTFF faces, the forward's NTFF phase
-        table) or None."""
+        table) or None; ``flux_cots``: per flux monitor a complex128 cotangent
+        (4, n_freqs, n1, n2) or None, with the forward's ``flux_kernels``."""
         a = RfxbAdjointIO()
         a.g_dev = g.data_ptr() if g is not None else None
         a.grad_dev = grad.data_ptr() if grad is not None else None
@@ -355,6 +356,12 @@ class Plan:
             a._keep = (cot, ph)   # the pointer arrays live as long as the struct
         if ntff is not None:
             a.ntff_cot_dev, a.ntff_phase_dev = ntff[0].data_ptr(), ntff[1].data_ptr()
+        if flux_cots is not None and any(c is not None for c in flux_cots):
+            fc = (C.c_void_p * len(flux_cots))(*[c.data_ptr() if c is not None else None for c in flux_cots])
+            fk = (C.c_void_p * len(flux_kernels))(*[t.data_ptr() for t in flux_kernels])
+            a.flux_cot_dev = C.cast(fc, C.POINTER(C.c_void_p))
+            a.flux_kernel_dev = C.cast(fk, C.POINTER(C.c_void_p))
+            a._keep_flux = (fc, fk)
         return a
 
     def adjoint_begin(self, n_total, **kw):

@@ -1,5 +1,5 @@
-"""GPU tests of the adjoint with DFT-plane and NTFF objectives (the transposes
-of the running DFT, rfx/simulation.py:1574-1588 and rfx/nonuniform.py:
+"""GPU tests of the adjoint with DFT-plane, NTFF and flux objectives (the
+transposes of the running DFT, rfx/simulation.py:1574-1588 and rfx/nonuniform.py:
 1458-1472, and of the NTFF box, rfx/farfield.py:208-313, which the reference
 differentiates with jax.grad through the scan).
 
@@ -15,6 +15,9 @@ differentiates with jax.grad through the scan).
 4. NTFF: the exact transpose for a face objective, and the directivity at
    one direction (through the differentiable device far-field transform)
    against float64 finite differences of the oracle.
+5. Flux monitors (rfx/simulation.py:1590-1642): the exact transpose, and the
+   power through two planes (one windowed) against float64 finite
+   differences.
 """
 
 import numpy as np
@@ -217,5 +220,92 @@ def test_directivity_gradient_matches_fp64_finite_differences(cuda):
         fd = (_oracle_directivity(sc, ep, theta, phi, it, ip) - _oracle_directivity(sc, em, theta, phi, it, ip)) / (2 * h)
         ad = float(np.sum(grad * d))
         print("directivity directional AD", ad, "FD64", fd, "rel", abs(ad - fd) / abs(fd))
+        assert abs(ad - fd) <= 1e-3 * abs(fd)
+    r.close()
+
+
+# ---------------------------------------------------------- flux monitors
+def _flux_mons(sc):
+    f = np.array([10e9, 14e9, 18e9])
+    nx, ny, nz = sc.ogrid.shape
+    # an x plane through the ez source (12, 13, 13), a windowed z plane on the PEC sheet (k = 15)
+    return [(0, 12, 6, ny - 6, 6, nz - 6, f, 0, "rect", 0.25),
+            (2, 15, 6, nx - 6, 6, ny - 6, f[:2], sc.n_steps, "hann", 0.25)]
+
+
+def _flux_runner(sc, box, mode="history", K=None):
+    import rfx_b200
+    from rfx_b200.adjoint import AdjointRunner
+    g = sc.product_grid()
+    fms = [rfx_b200.init_flux_monitor(m[0], m[1], m[6], g.shape, g.dx, g.dx, dft_total_steps=m[7], dft_window=m[8],
+                                      dft_window_alpha=m[9], lo1=m[2], hi1=m[3], lo2=m[4], hi2=m[5])
+           for m in _flux_mons(sc)]
+    return AdjointRunner(g, rfx_b200.MaterialArrays(*sc.materials), sc.n_steps, sources=sc.sources,
+                         probes=sc.probes, box=box, boundary=sc.boundary, cpml_axes="xyz",
+                         pec_axes=sc.pec_axes if sc.pec_axes is not None else "xyz", pec_mask=sc.pec_mask,
+                         mode=mode, checkpoint_every=K, flux_monitors=fms), fms
+
+
+@pytest.mark.parametrize("mode", ["history", "segments"])
+def test_flux_adjoint_is_exact_transpose(cuda, mode):
+    sc = small_uniform(n_steps=150)
+    r, _ = _flux_runner(sc, (14, 18, 14, 18, 12, 14), mode=mode, K=64)
+    r.forward()
+    rng = np.random.default_rng(23)
+    G = [torch.from_numpy(rng.standard_normal(a.shape) + 1j * rng.standard_normal(a.shape)).cuda()
+         for a in r.flux_accs]
+    J = sum(float((Gq.real * a.real + Gq.imag * a.imag).sum()) for Gq, a in zip(G, r.flux_accs))
+    _, s1 = r.backward(None, g_flux=G)
+    J1 = float((s1.double() * r.src_table.double()).sum())
+    print(mode, "J_flux", J, "via adjoint", J1)
+    assert abs(J1 - J) <= 2e-5 * abs(J)
+    r.close()
+
+
+def _power(acc, dA):
+    """flux_spectrum of a (4, n_f, n1, n2) accumulator, summed over frequency."""
+    e1, e2, h1, h2 = acc[0], acc[1], acc[2], acc[3]
+    return ((e1 * h2.conj() - e2 * h1.conj()).real * dA).sum()
+
+
+def test_flux_gradient_matches_fp64_finite_differences(cuda):
+    from rfx_b200.adjoint import FDTDFunction
+    sc = small_uniform(n_steps=160)
+    box = (14, 20, 14, 20, 12, 14)
+    r, fms = _flux_runner(sc, box)
+    mons = _flux_mons(sc)
+    eps_box = torch.tensor(sc.materials[0][box[0]:box[1], box[2]:box[3], box[4]:box[5]], device="cuda",
+                           requires_grad=True)
+    ts, *accs = FDTDFunction.apply(eps_box, None, r)
+    assert len(accs) == 2 and accs[0].dtype == torch.complex128
+    dA = [torch.as_tensor(np.asarray(m.dA, np.float64), device="cuda") for m in fms]
+    J = sum(_power(a, d) for a, d in zip(accs, dA))
+    J.backward()
+    grad = eps_box.grad.double().cpu().numpy()
+
+    def oracle_J(eps_full):
+        mats = (eps_full, sc.materials[1], sc.materials[2])
+        o = oracle.run_uniform(sc.ogrid, mats, sc.n_steps, boundary=sc.boundary, pec_axes=sc.pec_axes,
+                               sources=sc.sources, probes=sc.probes, pec_mask=sc.pec_mask, dtype=np.float64,
+                               exact_materials=True, flux_monitors=mons)
+        return float(sum(_power(torch.from_numpy(a), torch.from_numpy(np.asarray(m.dA, np.float64)))
+                         for a, m in zip(o.flux, fms)))
+
+    J0 = oracle_J(sc.materials[0].astype(np.float64))
+    Jv = float(J.detach())
+    print("flux objective CUDA", Jv, "oracle f64", J0)
+    assert abs(Jv - J0) <= 1e-4 * abs(J0)
+    i0, i1, j0, j1, k0, k1 = box
+    rng = np.random.default_rng(19)
+    for _ in range(3):
+        d = rng.standard_normal((i1 - i0, j1 - j0, k1 - k0))
+        h = 1e-3
+        ep = sc.materials[0].astype(np.float64).copy()
+        em = ep.copy()
+        ep[i0:i1, j0:j1, k0:k1] += h * d
+        em[i0:i1, j0:j1, k0:k1] -= h * d
+        fd = (oracle_J(ep) - oracle_J(em)) / (2 * h)
+        ad = float(np.sum(grad * d))
+        print("flux directional AD", ad, "FD64", fd, "rel", abs(ad - fd) / abs(fd))
         assert abs(ad - fd) <= 1e-3 * abs(fd)
     r.close()
