@@ -532,10 +532,12 @@ def flux_window_weight(step, total_steps, window, alpha):
         np.float32(2.0) * x / np.float32(a) - np.float32(2.0 / a) + np.float32(1.0))))
 
 
-def _flux_step(F, mon, acc, step, dt):
+def _flux_step(F, mon, acc, step, dt, graded=False):
     """rfx/simulation.py:1590-1642: E at plane index, H averaged over index-1
     and index (float32), times exp(-j 2 pi f t) dt w (E, t = step dt) and
-    exp(-j 2 pi f (t - dt/2)) dt w (H), accumulated in complex128."""
+    exp(-j 2 pi f (t - dt/2)) dt w (H), accumulated in complex128.  On the
+    graded lane (rfx/nonuniform.py:1483-1520) t = f32(step) * dt is rounded to
+    float32."""
     axis, index, lo1, hi1, lo2, hi2, freqs, total, window, alpha = mon
     c = _FLUX_COMPONENTS[axis]
     im1 = max(index - 1, 0)
@@ -550,7 +552,7 @@ def _flux_step(F, mon, acc, step, dt):
     h1 = (cut(F[c[2]], im1) + cut(F[c[2]], index)) * np.float32(0.5)
     h2 = (cut(F[c[3]], im1) + cut(F[c[3]], index)) * np.float32(0.5)
     f = np.asarray(freqs, np.float64)
-    t = float(step) * dt
+    t = float(np.float32(step) * np.float32(dt)) if graded else float(step) * dt
     w = float(flux_window_weight(step, total, window, alpha))
     ke = np.exp(-1j * 2.0 * np.pi * f * t) * dt * w
     kh = np.exp(-1j * 2.0 * np.pi * f * (t - dt * 0.5)) * dt * w
@@ -688,7 +690,7 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
             _dft()
             _probes()
         for m, acc in zip(flux_monitors, flux_accs):
-            _flux_step(F, m, acc, n + 1, dt)
+            _flux_step(F, m, acc, n + dft_time_offset, dt, graded=dft_time_offset == 0)
         if ntff is not None:
             ntff_step(F, ntff, ntff_acc, n, dt)
         if stop is not None and stop(n, F):
@@ -721,7 +723,8 @@ def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
 
 
 def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_planes=(),
-                   pec_mask=None, kappa_max=1.0, dtype=np.float32, exact_materials=False, ntff=None):
+                   pec_mask=None, kappa_max=1.0, dtype=np.float32, exact_materials=False, ntff=None,
+                   flux_monitors=()):
     """``rfx.nonuniform.run_nonuniform`` (rfx/nonuniform.py:1589-1804), scan body
     of rfx/nonuniform.py:1256-1568: PEC on every axis, DFT time stamp ``n dt``
     (rfx/nonuniform.py:1461), DFT before probes."""
@@ -733,7 +736,7 @@ def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_plane
                   pec_axes="xyz", pec_mask=pec_mask, kappa_max=kappa_max,
                   exact_materials=exact_materials)
     return _run(st, n_steps, sources, probes, dft_planes, (), 0,
-                probes_before_dft=False, dx_vi=grid.dx, ntff=ntff)
+                probes_before_dft=False, dx_vi=grid.dx, ntff=ntff, flux_monitors=flux_monitors)
 
 
 def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100,

@@ -62,8 +62,9 @@ class AdjointRunner:
                  device=None, _plan=None):
         """``dft_planes``: ``DFTPlaneProbe`` values accumulated by the forward
         pass (sample time (n + dft_time_offset) dt: 1 on the uniform lane, 0 on
-        the graded one); ``ntff``: an ``NTFFBox`` and ``flux_monitors``:
-        ``FluxMonitor`` values accumulated by the forward pass (uniform lane).
+        the graded one; it also selects the flux monitors' sample times);
+        ``ntff``: an ``NTFFBox`` and ``flux_monitors``: ``FluxMonitor`` values
+        accumulated by the forward pass.
         Their accumulators can carry cotangents."""
         self.device = require_cuda(device)
         self.grid = grid
@@ -114,8 +115,8 @@ class AdjointRunner:
         self.ntff_phase = (torch.from_numpy(ntff_phase_table(ntff.freqs, self.n_steps, grid.dt)).to(self.device)
                            if ntff is not None else None)
         self.ntff_faces = []
-        self.flux_kernels = [torch.from_numpy(flux_kernel_table(m, self.n_steps, grid.dt)).to(self.device)
-                             for m in self.flux_monitors]
+        self.flux_kernels = [torch.from_numpy(flux_kernel_table(m, self.n_steps, grid.dt, dft_time_offset))
+                             .to(self.device) for m in self.flux_monitors]
         self.flux_accs = []
         self._dirty = True
 

@@ -5,7 +5,8 @@ the features on this path: the same source tuples ``(i, j, k, comp, wave)``,
 probe tuples ``(i, j, k, comp)``, DFT planes and PEC mask, and the same
 result dict keys.  Step order per rfx/nonuniform.py:1256-1568: H, CPML-H,
 E, CPML-E, PEC on every axis, PEC mask, sources, DFT planes at ``t = n dt``,
-NTFF box (``ntff_box`` with its initial ``ntff_data``), probes.  ``checkpoint_every`` and ``n_warmup`` only shape the reference's
+NTFF box (``ntff_box`` with its initial ``ntff_data``), flux monitors
+(E at t = n dt rounded to float32, H half a step earlier), probes.  ``checkpoint_every`` and ``n_warmup`` only shape the reference's
 AD tape and do not change forward values; they are validated and accepted.
 """
 
@@ -22,7 +23,7 @@ def run_nonuniform(grid, materials, n_steps, *, pec_mask=None, pec_occupancy=Non
                    checkpoint_every=None, n_warmup=0, aniso_eps=None, sheet_impedance=None, device=None) -> dict:
     _unsupported(pec_occupancy=pec_occupancy, wire_ports=wire_ports, debye=debye, lorentz=lorentz,
                  pmc_faces=pmc_faces, rlc_metas=rlc_metas, waveguide_ports=waveguide_ports,
-                 tfsf=tfsf, flux_monitors=flux_monitors, aniso_eps=aniso_eps, sheet_impedance=sheet_impedance)
+                 tfsf=tfsf, aniso_eps=aniso_eps, sheet_impedance=sheet_impedance)
     if n_warmup and n_warmup >= n_steps:
         raise ValueError(f"n_warmup ({n_warmup}) must be < n_steps ({n_steps})")
     pads = face_pads(grid)
@@ -32,13 +33,16 @@ def run_nonuniform(grid, materials, n_steps, *, pec_mask=None, pec_occupancy=Non
     prbs = [tuple(p) for p in (probes or [])]
     if ntff_box is None or ntff_data is None:   # both or neither (rfx/nonuniform.py:1046)
         ntff_box = ntff_data = None
-    ts, planes, _, state, _, ntff_out = run_device(
+    ts, planes, _, state, flux, ntff_out = run_device(
         grid, materials, n_steps, cpml_axes=axes if use_cpml else "", pec_axes="xyz", sources=srcs,
         probes=prbs, dft_planes=list(dft_planes or []), pec_mask=pec_mask, dft_time_offset=0,
-        return_state=True, noop_faces=set(pec_faces or ()), ntff_box=ntff_box, ntff_data=ntff_data, device=device)
+        return_state=True, noop_faces=set(pec_faces or ()), flux_monitors=list(flux_monitors or []),
+        ntff_box=ntff_box, ntff_data=ntff_data, device=device)
     out = {"state": state, "time_series": ts if emit_time_series else None, "dt": grid.dt}
     if dft_planes:
         out["dft_planes"] = planes
+    if flux_monitors:
+        out["flux_monitors"] = flux
     if ntff_box is not None:
         out["ntff_data"] = ntff_out
     return out

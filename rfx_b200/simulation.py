@@ -144,14 +144,19 @@ def dft_window_weight(step, total_steps, window, alpha):
     raise ValueError(f"unknown DFT window {window!r}")
 
 
-def flux_kernel_table(mon: FluxMonitor, n_steps, dt):
-    """(n_steps, 2, n_freqs) complex128 step factors of a flux monitor
-    (rfx/simulation.py:1590-1642): E sampled at t = (n+1) dt, H at t - dt/2,
-    times dt and the window weight of step n+1."""
+def flux_kernel_table(mon: FluxMonitor, n_steps, dt, time_offset=1):
+    """(n_steps, 2, n_freqs) complex128 step factors of a flux monitor: E
+    sampled at t, H at t - dt/2, times dt and the window weight.  Uniform lane
+    (time_offset 1, rfx/simulation.py:1590-1642): t = (n+1) dt in float64 and
+    the weight of step n+1.  Graded lane (time_offset 0, rfx/nonuniform.py:
+    1483-1520): t = f32(n) * dt rounded to float32, the weight of step n."""
     f = np.asarray(mon.freqs, np.float64)
-    t = np.arange(1, n_steps + 1, dtype=np.float64) * float(dt)
-    w = np.array([dft_window_weight(n, mon.total_steps, mon.window, mon.window_alpha)
-                  for n in range(1, n_steps + 1)], np.float64)
+    steps = np.arange(time_offset, time_offset + n_steps)
+    if time_offset == 1:
+        t = steps.astype(np.float64) * float(dt)
+    else:
+        t = (steps.astype(np.float32) * np.float32(dt)).astype(np.float64)
+    w = np.array([dft_window_weight(n, mon.total_steps, mon.window, mon.window_alpha) for n in steps], np.float64)
     out = np.empty((n_steps, 2, len(f)), np.complex128)
     out[:, 0, :] = np.exp(-1j * 2.0 * np.pi * f[None, :] * t[:, None]) * float(dt) * w[:, None]
     out[:, 1, :] = np.exp(-1j * 2.0 * np.pi * f[None, :] * (t[:, None] - float(dt) * 0.5)) * float(dt) * w[:, None]
@@ -268,6 +273,8 @@ class DeviceRun(NamedTuple):
 def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources, probes, dft_planes, pec_mask,
                        dft_time_offset, lumped_specs=(), kappa_max=None, noop_faces=(), flux_monitors=(),
                        ntff_box=None, ntff_data=None, device=None) -> DeviceRun:
+    """``dft_time_offset`` (1 uniform lane, 0 graded lane) also selects the
+    flux monitors' sample times."""
     """Build the plan of one simulation and upload its inputs (the set-up half
     of ``run_device``); the caller owns the plan and closes it."""
     dev = require_cuda(device)
@@ -310,7 +317,7 @@ def prepare_device_run(grid, materials, n_steps, *, cpml_axes, pec_axes, sources
         for m in flux_monitors:
             faccs.append(torch.from_numpy(np.stack([np.asarray(a, np.complex128) for a in
                                                     (m.e1_dft, m.e2_dft, m.h1_dft, m.h2_dft)])).to(dev).contiguous())
-            fkerns.append(torch.from_numpy(flux_kernel_table(m, n_steps, grid.dt)).to(dev))
+            fkerns.append(torch.from_numpy(flux_kernel_table(m, n_steps, grid.dt, dft_time_offset)).to(dev))
         ntff = None
         if ntff_box is not None:
             acc, cmp = pack_ntff(ntff_data if ntff_data is not None else init_ntff_data(ntff_box), dev)

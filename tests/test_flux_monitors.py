@@ -87,3 +87,65 @@ def test_flux_monitors_match_oracle(cuda):
         print("monitor", q, "flux", sp, "oracle", sp_ref)
         errs.append(rel_l2(sp, sp_ref) / 10)
     assert max(errs) < TOL
+
+
+def _graded_scene(n_steps=220):
+    dz = np.concatenate([np.full(6, 1e-3), np.linspace(1e-3, 0.5e-3, 6), np.full(8, 0.5e-3)])
+    g = oracle.make_nonuniform_grid((0.014, 0.012), dz, 1e-3, cpml_layers=4)
+    eps = np.ones(g.shape, np.float32)
+    eps[:, :, 10:14] = 2.5
+    mats = (eps, np.zeros(g.shape, np.float32), np.ones(g.shape, np.float32))
+    src = (g.nx // 2, g.ny // 2, 8)
+    w = oracle.current_source_waveform(g, src, "ez", mats, n_steps, f0=40e9, bandwidth=0.8)
+    f = np.array([30e9, 45e9])
+    mons = [(2, 14, 4, g.nx - 4, 4, g.ny - 4, f, 0, "rect", 0.25),
+            (0, g.nx // 2 + 3, 3, g.ny - 3, 3, g.nz - 3, f[:1], n_steps, "tukey", 0.25)]
+    return g, mats, [(*src, "ez", w)], mons, dz
+
+
+def test_oracle_graded_flux_matches_post_hoc_dft():
+    """The graded lane samples at t = f32(n) * dt rounded to float32 (E) and
+    half a step earlier (H), with the window weight of step n
+    (rfx/nonuniform.py:1483-1520)."""
+    g, mats, srcs, mons, _ = _graded_scene()
+    m = mons[0]
+    axis, index, lo1, lo2, freqs = m[0], m[1], m[2], m[4], m[6]
+    a, b = lo1 + 4, lo2 + 3
+    probes = [(a, b, index, "ex"), (a, b, index, "ey"), (a, b, index - 1, "hx"), (a, b, index, "hx"),
+              (a, b, index - 1, "hy"), (a, b, index, "hy")]
+    n = 200
+    r = oracle.run_nonuniform(g, mats, n, sources=srcs, probes=probes, flux_monitors=[m])
+    ts = r.time_series
+    t = (np.arange(n, dtype=np.float32) * np.float32(g.dt)).astype(np.float64)
+    ke = np.exp(-1j * 2 * np.pi * freqs[:, None] * t[None, :]) * g.dt
+    kh = np.exp(-1j * 2 * np.pi * freqs[:, None] * (t[None, :] - g.dt / 2)) * g.dt
+    h1 = ((ts[:, 2] + ts[:, 3]) * np.float32(0.5)).astype(np.float64)
+    h2 = ((ts[:, 4] + ts[:, 5]) * np.float32(0.5)).astype(np.float64)
+    for slot, series, k in ((0, ts[:, 0].astype(np.float64), ke), (1, ts[:, 1].astype(np.float64), ke),
+                            (2, h1, kh), (3, h2, kh)):
+        post = k @ series
+        got = r.flux[0][slot][:, a - lo1, b - lo2]
+        assert np.allclose(got, post, rtol=1e-10, atol=1e-12 * np.abs(post).max()), slot
+
+
+@pytest.mark.gpu
+def test_graded_flux_monitors_match_oracle(cuda):
+    import rfx_b200
+    g, mats, srcs, mons, dz = _graded_scene()
+    n = 220
+    ref = oracle.run_nonuniform(g, mats, n, sources=srcs, flux_monitors=mons)
+    pg = rfx_b200.make_nonuniform_grid((0.014, 0.012), dz, 1e-3, cpml_layers=4)
+    assert tuple(pg.shape) == tuple(g.shape)
+    fms = [rfx_b200.init_flux_monitor(m[0], m[1], m[6], pg.shape, pg.dx, pg.dx, dft_total_steps=m[7],
+                                      dft_window=m[8], dft_window_alpha=m[9], lo1=m[2], hi1=m[3], lo2=m[4], hi2=m[5])
+           for m in mons]
+    out = rfx_b200.run_nonuniform(pg, rfx_b200.MaterialArrays(*mats), n, sources=srcs, flux_monitors=fms)
+    assert len(out["flux_monitors"]) == len(mons)
+    for q, (fm, acc) in enumerate(zip(out["flux_monitors"], ref.flux)):
+        got = np.stack([fm.e1_dft, fm.e2_dft, fm.h1_dft, fm.h2_dft])
+        e = np.linalg.norm(got - acc) / np.linalg.norm(acc)
+        sp = rfx_b200.flux_spectrum(fm)
+        sp_ref = rfx_b200.flux_spectrum(fm._replace(e1_dft=acc[0], e2_dft=acc[1], h1_dft=acc[2], h2_dft=acc[3]))
+        print("graded monitor", q, "relL2", e, "flux", sp, "oracle", sp_ref)
+        assert e < 1e-4
+        assert np.allclose(sp, sp_ref, rtol=1e-3, atol=1e-3 * np.abs(sp_ref).max())
