@@ -454,7 +454,7 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
     ``monitor_position`` (default: the domain centre) keeps a running peak
     over every step, and a check step with value^2 < decay_by * peak stops.
     The steps run between checks are replayed as one captured chunk."""
-    _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf, flux_monitors=flux_monitors,
+    _unsupported(debye=debye, lorentz=lorentz, tfsf=tfsf,
                  waveguide_ports=waveguide_ports, aniso_eps=aniso_eps, aniso_inv_eps=aniso_inv_eps,
                  pec_occupancy=pec_occupancy, conformal_weights=conformal_weights,
                  wire_port_sparams=wire_port_sparams, lumped_port_sparams=lumped_port_sparams,
@@ -490,7 +490,8 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
     planes = list(dft_planes or [])
     r = prepare_device_run(grid, materials, max_steps, cpml_axes=cpml_axes if use_cpml else "", pec_axes=pec_axes,
                            sources=srcs, probes=prbs, dft_planes=planes, pec_mask=pec_mask, dft_time_offset=1,
-                           noop_faces=set(getattr(grid, "pec_faces", None) or ()), ntff_box=ntff, device=device)
+                           noop_faces=set(getattr(grid, "pec_faces", None) or ()), ntff_box=ntff,
+                           flux_monitors=list(flux_monitors or []), device=device)
     plan = r.plan
     try:
         box = (grid.pad_x_lo, grid.nx - grid.pad_x_hi, grid.pad_y_lo, grid.ny - grid.pad_y_hi,
@@ -506,7 +507,8 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
             plan.advance(0, target - done,
                          r.src_table[done:] if r.src_table is not None else None,
                          r.probe_out[done:] if r.probe_out is not None else None,
-                         r.dft_accs, [ph[done:] for ph in r.dft_phases],
+                         r.dft_accs, [ph[done:] for ph in r.dft_phases], r.flux_accs,
+                         [k[done:] for k in r.flux_kernels],
                          ntff=(r.ntff[0], r.ntff[1], r.ntff[2][done:]) if r.ntff is not None else None)
             first, done = done, target
             if done - 1 != n_check:
@@ -534,8 +536,15 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
         if return_state:
             state = FDTDState(*[t.cpu().numpy() for t in plan.store_fields()], step=done)
         ntff_data = unpack_ntff(ntff, r.ntff[0], r.ntff[1]) if ntff is not None else None
+        flux = None
+        if flux_monitors:
+            flux = []
+            for m, a in zip(flux_monitors, r.flux_accs):
+                a = a.cpu().numpy()
+                flux.append(m._replace(e1_dft=a[0], e2_dft=a[1], h1_dft=a[2], h2_dft=a[3]))
+            flux = tuple(flux)
         return SimResult(state=state, time_series=ts, ntff_data=ntff_data,
-                         dft_planes=out_planes if planes else None, ntff_box=ntff, grid=grid)
+                         dft_planes=out_planes if planes else None, flux_monitors=flux, ntff_box=ntff, grid=grid)
     finally:
         plan.close()
 

@@ -149,3 +149,27 @@ def test_graded_flux_monitors_match_oracle(cuda):
         print("graded monitor", q, "relL2", e, "flux", sp, "oracle", sp_ref)
         assert e < 1e-4
         assert np.allclose(sp, sp_ref, rtol=1e-3, atol=1e-3 * np.abs(sp_ref).max())
+
+
+@pytest.mark.gpu
+def test_run_until_decay_flux_matches_a_plain_run(cuda):
+    """run_until_decay replays check intervals from the flux kernel tables at
+    their step offset: the monitors equal those of a plain run of the same
+    length."""
+    import rfx_b200
+    g, mats, srcs, mons = _scene()
+    long = 900
+    pg = rfx_b200.Grid(freq_max=10e9, domain=(0.030, 0.022, 0.020), dx=1e-3, cpml_layers=6)
+    sl = [rfx_b200.SourceSpec(*s[:4], np.concatenate([s[4], np.zeros(long - len(s[4]), np.float32)])) for s in srcs]
+    fms = [rfx_b200.init_flux_monitor(m[0], m[1], m[6], pg.shape, pg.dx, pg.dx, lo1=m[2], hi1=m[3], lo2=m[4],
+                                      hi2=m[5]) for m in mons[:2]]
+    m = rfx_b200.MaterialArrays(*mats)
+    r1 = rfx_b200.run_until_decay(pg, m, decay_by=1e-2, check_interval=40, min_steps=80, max_steps=long,
+                                  boundary="cpml", pec_axes="", sources=sl, flux_monitors=fms)
+    steps = int(r1.state.step)
+    assert steps < long
+    r2 = rfx_b200.run(pg, m, steps, boundary="cpml", pec_axes="", sources=sl, flux_monitors=fms)
+    for a, b in zip(r1.flux_monitors, r2.flux_monitors):
+        for name in ("e1_dft", "e2_dft", "h1_dft", "h2_dft"):
+            x, y = getattr(a, name), getattr(b, name)
+            assert np.linalg.norm(x - y) <= 1e-6 * np.linalg.norm(y), name
