@@ -1125,10 +1125,12 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, b
       // staged-psi tiles on the caller's stream, CPML-free tiles beside them
       RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
       RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
-      fwd_kernel(2, em)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps, n,
-                                                                              par);
+      // capture order: the plain tiles first (measured 2 % faster on the
+      // sweep's forward phase than the CPML tiles first, equal on one grid)
       fwd_kernel(1, em)<<<g->n_wf1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(g->d_inst, g->d_wf1,
                                                                                           g->d_maps, n, par);
+      fwd_kernel(2, em)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps, n,
+                                                                              par);
       RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
       RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0));
     } else {
@@ -1367,18 +1369,33 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
           const bool lite = g->adj_lite && amode == 2;
           RFXB_CUDA(cudaEventRecord(g->ev_fork, cs));
           RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
-          if (lite) {
-            RFXB_CUDA(cudaStreamWaitEvent(g->side2, g->ev_fork, 0));
-            if (g->n_wa2y > 0)
-              akern<<<g->n_wa2y, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2y, g->d_maps, s, par, fpar,
-                                                             zp);
-            adj_kernel(4)<<<g->n_wa4, dim3(32, kTY), adj_step_smem_bytes(4, zp), g->side2>>>(
-                g->d_inst, g->d_adj, g->d_wa4, g->d_maps, s, par, fpar, zp);
-          } else {
-            akern<<<g->n_wa2, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2, g->d_maps, s, par, fpar, zp);
-          }
-          adj_kernel(3)<<<g->n_wa1, dim3(32, kTY), adj_step_smem_bytes(3, zp), g->side_stream>>>(
-              g->d_inst, g->d_adj, g->d_wa1, g->d_maps, s, par, fpar, zp);
+          auto v2 = [&]() {
+            if (lite) {
+              if (g->n_wa2y > 0)
+                akern<<<g->n_wa2y, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2y, g->d_maps, s, par,
+                                                               fpar, zp);
+            } else {
+              akern<<<g->n_wa2, dim3(32, kTY), asmem, cs>>>(g->d_inst, g->d_adj, g->d_wa2, g->d_maps, s, par, fpar,
+                                                            zp);
+            }
+          };
+          auto v4 = [&]() {
+            if (lite)
+              adj_kernel(4)<<<g->n_wa4, dim3(32, kTY), adj_step_smem_bytes(4, zp), g->side2>>>(
+                  g->d_inst, g->d_adj, g->d_wa4, g->d_maps, s, par, fpar, zp);
+          };
+          auto v3 = [&]() {
+            adj_kernel(3)<<<g->n_wa1, dim3(32, kTY), adj_step_smem_bytes(3, zp), g->side_stream>>>(
+                g->d_inst, g->d_adj, g->d_wa1, g->d_maps, s, par, fpar, zp);
+          };
+          // capture order = the order the graph hands the branches' CTAs to
+          // the SMs: the largest, four-per-SM variant 4 first, then the y-slab
+          // variant 2, the plain variant 3 last (measured best of the six
+          // orders, 3 % on the sweep's reverse phase)
+          if (lite) RFXB_CUDA(cudaStreamWaitEvent(g->side2, g->ev_fork, 0));
+          v4();
+          v2();
+          v3();
           RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
           RFXB_CUDA(cudaStreamWaitEvent(cs, g->ev_join, 0));
           if (lite) {
