@@ -298,6 +298,15 @@ int rfxb_forward_noalloc(const RfxbDesc* desc, const float* eps_r_dev, const flo
  * run_until_decay (rfx/simulation.py:2493-2505). */
 int rfxb_plan_box_energy(RfxbPlan* plan, const int* box, double* energy_dev, void* stream);
 
+/* Net outgoing co-located Poynting flux through the faces of the box
+ * (faces at i = box[0] and i = box[1], j = box[2] and box[3], k = box[4] and
+ * box[5], each over the half-open ranges of its tangential axes): on an x
+ * face Ey Hz - Ez Hy, on a y face Ez Hx - Ex Hz, on a z face Ex Hy - Ey Hx,
+ * with sign + on the high face and - on the low one, summed in float64 and
+ * written (overwritten) to *flux_dev in stream order: the radiated-flux stop
+ * of run_until_decay (rfx/simulation.py:2513-2540). */
+int rfxb_plan_box_flux(RfxbPlan* plan, const int* box, double* flux_dev, void* stream);
+
 /* Bytes of device memory a plan holds (state, coefficients, psi, history,
  * checkpoints). */
 int64_t rfxb_plan_device_bytes(const RfxbPlan* plan);

@@ -742,7 +742,7 @@ def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_plane
 def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100,
                             max_steps=50_000, decay_energy_consecutive=2, monitor=None, boundary="pec",
                             cpml_axes="xyz", pec_axes=None, sources=(), probes=(), pec_mask=None,
-                            dtype=np.float32):
+                            dtype=np.float32, flux_box=None, flux_env_checks=4):
     """``rfx.simulation.run_until_decay`` (rfx/simulation.py:2198-2700), energy
     and point-field stops only.  Absorbing boundary: at step n with n+1 >=
     min_steps and n % check_interval == 0 the interior energy
@@ -752,6 +752,12 @@ def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50
     Closed boundary: the squared field at ``monitor`` = (i, j, k, comp)
     (after the step's source injection) keeps a running peak every step, and a
     check step with value^2 < decay_by * peak stops (:2623-2633).
+    ``flux_box`` = (i0, i1, j0, j1, k0, k1) selects the radiated-flux stop on
+    an absorbing boundary (:2513-2540, 2580-2600): at every check step from
+    the first, |net outgoing co-located Poynting flux| through the box faces
+    (float32 products, float64 sum), enveloped by the maximum over the last
+    ``flux_env_checks`` checks, against decay_by times its running peak,
+    once n+1 >= min_steps.
     Returns (OracleResult, steps run)."""
     if pec_axes is None:
         pec_axes = "xyz"
@@ -761,10 +767,37 @@ def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50
                   pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=1.0)
     p = grid.pads
     sl = (slice(p[0], grid.nx - p[1]), slice(p[2], grid.ny - p[3]), slice(p[4], grid.nz - p[5]))
-    state = {"peak_U": 0.0, "below": 0, "peak_sq": 0.0, "steps": 0}
+    state = {"peak_U": 0.0, "below": 0, "peak_sq": 0.0, "steps": 0, "peak_flux": 0.0, "hist": []}
+
+    def radiated_power(F):
+        i0, i1, j0, j1, k0, k1 = flux_box
+        f32 = np.float32
+        g = {c: F[c] for c in COMPONENTS}
+        jj, kk, ii = slice(j0, j1), slice(k0, k1), slice(i0, i1)
+
+        def term(a, b, c, d, sel):
+            return np.sum(((g[a][sel] * g[b][sel]).astype(f32) - (g[c][sel] * g[d][sel]).astype(f32))
+                          .astype(np.float64))
+
+        p = term("ey", "hz", "ez", "hy", (i1, jj, kk)) - term("ey", "hz", "ez", "hy", (i0, jj, kk))
+        p += term("ez", "hx", "ex", "hz", (ii, j1, kk)) - term("ez", "hx", "ex", "hz", (ii, j0, kk))
+        p += term("ex", "hy", "ey", "hx", (ii, jj, k1)) - term("ex", "hy", "ey", "hx", (ii, jj, k0))
+        return float(p)
 
     def stop(n, F):
         state["steps"] = n + 1
+        if absorbing and flux_box is not None:
+            if n % check_interval == 0:
+                state["hist"].append(abs(radiated_power(F)))
+                env = max(state["hist"][-flux_env_checks:])
+                state["peak_flux"] = max(state["peak_flux"], env)
+                if n + 1 >= min_steps and state["peak_flux"] > 0.0 and env < decay_by * state["peak_flux"]:
+                    state["below"] += 1
+                    if state["below"] >= decay_energy_consecutive:
+                        return True
+                else:
+                    state["below"] = 0
+            return False
         if absorbing:
             if n + 1 >= min_steps and n % check_interval == 0:
                 U = float(sum(np.sum(np.asarray(F[c][sl], np.float64) ** 2) for c in COMPONENTS))

@@ -36,6 +36,7 @@ __global__ void dft_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbDftPla
 __global__ void ntff_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbNtffFace*, int, int, int);
 __global__ void flux_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbFluxPlane*, int, int, int);
 __global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
+__global__ void box_flux_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
 __global__ void flux_kernel(const RfxbInst*, const RfxbFluxPlane*, int, int, int);
 __global__ void ntff_kernel(const RfxbInst*, const RfxbNtffFace*, int, int, int);
 template <int TY, int MODE>
@@ -1967,6 +1968,21 @@ int rfxb_plan_box_energy(RfxbPlan* p, const int* b, double* out, void* stream) {
   const long long cells = (long long)(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]);
   const int blocks = (int)std::max<long long>(1, std::min<long long>((cells + 255) / 256, 8LL * sm_count()));
   box_energy_kernel<<<blocks, 256, 0, st>>>(p->inst, p->par, b[0], b[1], b[2], b[3], b[4], b[5], out);
+  RFXB_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int rfxb_plan_box_flux(RfxbPlan* p, const int* b, double* out, void* stream) {
+  if (!p || !b || !out) return fail(RFXB_E_INVALID, "plan, box and output are required");
+  if (b[0] < 0 || b[1] >= p->nx || b[2] < 0 || b[3] >= p->ny || b[4] < 0 || b[5] >= p->nz || b[0] >= b[1] ||
+      b[2] >= b[3] || b[4] >= b[5])
+    return fail(RFXB_E_INVALID, "flux box out of range or empty");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  RFXB_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+  const long long cells = 2LL * ((long long)(b[3] - b[2]) * (b[5] - b[4]) + (long long)(b[1] - b[0]) * (b[5] - b[4]) +
+                                 (long long)(b[1] - b[0]) * (b[3] - b[2]));
+  const int blocks = (int)std::max<long long>(1, std::min<long long>((cells + 255) / 256, 8LL * sm_count()));
+  box_flux_kernel<<<blocks, 256, 0, st>>>(p->inst, p->par, b[0], b[1], b[2], b[3], b[4], b[5], out);
   RFXB_CUDA(cudaGetLastError());
   return 0;
 }

@@ -41,6 +41,48 @@ __global__ void __launch_bounds__(256) box_energy_kernel(RfxbInst P, int par, in
   }
 }
 
+// Net outgoing co-located Poynting flux through the six faces of a box
+// (rfx/simulation.py:2521-2540 _radiated_power): grid-stride over the face
+// cells of faces x_lo, x_hi, y_lo, y_hi, z_lo, z_hi (tangential ranges
+// half-open), float32 products as in the reference, float64 accumulation,
+// one atomic add per block.
+__global__ void __launch_bounds__(256) box_flux_kernel(RfxbInst P, int par, int i0, int i1, int j0, int j1, int k0,
+                                                       int k1, double* __restrict__ out) {
+  const int ni = i1 - i0, nj = j1 - j0, nk = k1 - k0;
+  const long long fx = (long long)nj * nk, fy = (long long)ni * nk, fz = (long long)ni * nj;
+  const long long total = 2 * (fx + fy + fz);
+  const float* const* F = P.F[par];
+  double acc = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long u = t;
+    int axis, hi;
+    if (u < 2 * fx) { axis = 0; hi = u >= fx; u -= hi ? fx : 0; }
+    else if ((u -= 2 * fx) < 2 * fy) { axis = 1; hi = u >= fy; u -= hi ? fy : 0; }
+    else { u -= 2 * fy; axis = 2; hi = u >= fz; u -= hi ? fz : 0; }
+    int i, j, k;
+    if (axis == 0) { i = hi ? i1 : i0; j = j0 + (int)(u / nk); k = k0 + (int)(u % nk); }
+    else if (axis == 1) { i = i0 + (int)(u / nk); j = hi ? j1 : j0; k = k0 + (int)(u % nk); }
+    else { i = i0 + (int)(u / nj); j = j0 + (int)(u % nj); k = hi ? k1 : k0; }
+    const long long e = P.off0 + (long long)i * P.ps + (long long)j * P.zs + k;
+    float s;
+    if (axis == 0) s = __fmul_rn(F[1][e], F[5][e]) - __fmul_rn(F[2][e], F[4][e]);        // Ey Hz - Ez Hy
+    else if (axis == 1) s = __fmul_rn(F[2][e], F[3][e]) - __fmul_rn(F[0][e], F[5][e]);   // Ez Hx - Ex Hz
+    else s = __fmul_rn(F[0][e], F[4][e]) - __fmul_rn(F[1][e], F[3][e]);                 // Ex Hy - Ey Hx
+    acc += hi ? (double)s : -(double)s;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  __shared__ double part[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) part[warp] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    acc = lane < (int)(blockDim.x >> 5) ? part[lane] : 0.0;
+    for (int o = 4; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) atomicAdd(out, acc);
+  }
+}
+
 // Poynting-flux monitor accumulation for one step (rfx/simulation.py:1590-
 // 1642): E1, E2 at the plane, H1, H2 averaged over the plane and the one
 // before it in float32, each multiplied by its complex128 step factor and

@@ -214,6 +214,16 @@ class Plan:
               "rfxb_plan_box_energy")
         return out
 
+    def box_flux(self, box, out=None):
+        """Device scalar (float64 tensor) of the net outgoing co-located
+        Poynting flux through the faces of ``box`` = (i0, i1, j0, j1, k0, k1)
+        (face planes i0, i1, ...; tangential ranges half-open)."""
+        if out is None:
+            out = torch.empty((), device=self.device, dtype=torch.float64)
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        check(self._lib.rfxb_plan_box_flux(self._h, b, C.c_void_p(out.data_ptr()), _stream()), "rfxb_plan_box_flux")
+        return out
+
     def forward_variant(self) -> int:
         """0 generic step kernel, 1 TMA staging without CPML, 2 TMA staging
         with TMA-staged CPML psi."""

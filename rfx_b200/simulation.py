@@ -450,6 +450,13 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
     done) the interior energy U = sum(E^2 + H^2) over the non-CPML slice is
     reduced on the device (float64 accumulation); the run stops after
     ``decay_energy_consecutive`` consecutive checks with U < decay_by * peak U.
+    With ``radiated_flux_box`` = ((x0, y0, z0), (x1, y1, z1)) on an absorbing
+    boundary the stop uses the net outgoing Poynting flux through that box
+    instead (rfx/simulation.py:2513-2540, 2580-2600): computed on the device
+    at every check step from the first, its |value| enveloped by the maximum
+    over the last ``flux_env_checks`` checks, and ``decay_energy_consecutive``
+    checks (once ``min_steps`` are done) with the envelope below decay_by
+    times its running peak stop the run.
     Closed boundary: the squared field ``monitor_component`` at
     ``monitor_position`` (default: the domain centre) keeps a running peak
     over every step, and a check step with value^2 < decay_by * peak stops.
@@ -459,7 +466,7 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
                  pec_occupancy=pec_occupancy, conformal_weights=conformal_weights,
                  wire_port_sparams=wire_port_sparams, lumped_port_sparams=lumped_port_sparams,
                  lumped_rlc=lumped_rlc, kerr_chi3=kerr_chi3, mag_sources=mag_sources,
-                 sheet_impedance=sheet_impedance, radiated_flux_box=radiated_flux_box)
+                 sheet_impedance=sheet_impedance)
     if checkpoint_segments is not None:
         raise NotImplementedError("checkpoint_segments is not supported by run_until_decay "
                                   "(rfx/simulation.py:2289-2294)")
@@ -498,7 +505,16 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
                grid.pad_z_lo, grid.nz - grid.pad_z_hi)
         energy = torch.empty((), device=plan.device, dtype=torch.float64)
         peak_u, below, peak_sq = 0.0, 0, 0.0
-        n_check = -(-(max(min_steps, 1) - 1) // check_interval) * check_interval   # first eligible check step
+        flux_stop = radiated_flux_box is not None and absorbing
+        if flux_stop:
+            lo = grid.position_to_index(radiated_flux_box[0])
+            hi = grid.position_to_index(radiated_flux_box[1])
+            fbox = (min(lo[0], hi[0]), max(lo[0], hi[0]), min(lo[1], hi[1]), max(lo[1], hi[1]),
+                    min(lo[2], hi[2]), max(lo[2], hi[2]))
+            peak_flux, flux_hist = 0.0, []
+        # first check step: the flux stop tracks its peak from step 0, the
+        # other stops only check once min_steps are done
+        n_check = 0 if flux_stop else -(-(max(min_steps, 1) - 1) // check_interval) * check_interval
         done = 0
         while done < max_steps:
             target = min(n_check + 1, max_steps)
@@ -513,7 +529,17 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
             first, done = done, target
             if done - 1 != n_check:
                 break
-            if absorbing:
+            if flux_stop:
+                flux_hist.append(abs(float(plan.box_flux(fbox, energy).item())))
+                env = max(flux_hist[-flux_env_checks:])
+                peak_flux = max(peak_flux, env)
+                if done >= min_steps and peak_flux > 0.0 and env < decay_by * peak_flux:
+                    below += 1
+                    if below >= decay_energy_consecutive:
+                        break
+                else:
+                    below = 0
+            elif absorbing:
                 u = float(plan.box_energy(box, energy).item())
                 peak_u = max(peak_u, u)
                 if u < decay_by * peak_u:

@@ -68,3 +68,41 @@ def test_run_until_decay_matches_oracle(cuda, boundary):
         e = rel_l2(out.time_series[:, p], res.time_series[:, p])
         print(boundary, "probe", p, "relL2", e)
         assert e < TOL
+
+
+FLUX_BOX = ((0.004, 0.004, 0.004), (0.020, 0.016, 0.014))
+
+
+def _oracle_flux():
+    g, mats, srcs, probes = _scene("cpml")
+    idx = [tuple(int(round(c / 1e-3)) + 6 for c in corner) for corner in FLUX_BOX]
+    box = (idx[0][0], idx[1][0], idx[0][1], idx[1][1], idx[0][2], idx[1][2])
+    return oracle.run_until_decay_uniform(g, mats, boundary="cpml", sources=srcs, probes=probes, flux_box=box,
+                                          flux_env_checks=4, **KW)
+
+
+@pytest.mark.slow
+def test_oracle_radiated_flux_stop():
+    """The radiated-flux stop (rfx/simulation.py:2513-2540, 2580-2600) fires
+    on a check step after min_steps."""
+    res, steps = _oracle_flux()
+    print("oracle radiated-flux stop after", steps, "steps")
+    assert KW["min_steps"] <= steps < KW["max_steps"]
+    assert (steps - 1) % KW["check_interval"] == 0
+
+
+@pytest.mark.gpu
+def test_radiated_flux_stop_matches_oracle(cuda):
+    import rfx_b200
+    g, mats, srcs, probes = _scene("cpml")
+    res, steps = _oracle_flux()
+    pg = rfx_b200.Grid(freq_max=10e9, domain=(0.024, 0.020, 0.018), dx=1e-3, cpml_layers=6)
+    out = rfx_b200.run_until_decay(pg, rfx_b200.MaterialArrays(*mats), boundary="cpml",
+                                   sources=[rfx_b200.SourceSpec(*s) for s in srcs],
+                                   probes=[rfx_b200.ProbeSpec(*p) for p in probes], radiated_flux_box=FLUX_BOX,
+                                   flux_env_checks=4, **KW)
+    n = out.time_series.shape[0]
+    print("radiated-flux stop: CUDA after", n, "steps; oracle", steps)
+    assert n == steps
+    for p in range(len(probes)):
+        assert rel_l2(out.time_series[:, p], res.time_series[:, p]) < TOL
