@@ -306,7 +306,7 @@ __device__ __forceinline__ void adj_tma_stage(AdjSmem<TY, EMS>& S, const CUtenso
   tma_load_4d(smem_u32(&S.st[s].ca[0][0]), tm + 10, z0, y0 + 1, ip + 1, 0, mb);
 }
 
-// r_E / r_H of one relation from a given old psi (mode 2: staged); the new
+// r_E / r_H of one relation from a given old psi (modes 2, 4: staged); the new
 // psi goes to the other parity at index qi.
 __device__ __forceinline__ float re_core(const AdjInst& A, const AdjCtx& C, int axis, const float4& cf, long long qi,
                                          float psi, float sgn, float ce, float at, bool write) {
@@ -322,7 +322,7 @@ __device__ __forceinline__ float rh_core(const AdjInst& A, const AdjCtx& C, int 
 }
 
 // Which CPML slab of an axis the cells lo..hi of a CTA reach: side or -1
-// (mode 2 guarantees at most one side per axis).
+// (modes 2 and 4 guarantee at most one side per axis).
 __device__ __forceinline__ int atile_side(int lo, int hi, int n, int ncp) {
   if (lo < ncp) return 0;
   if (hi >= n - ncp) return 1;
