@@ -2,6 +2,8 @@
 // objects, device allocation, descriptor upload, launch sequencing and the
 // CUDA-graph replay of step chunks.
 #include <cuda.h>
+#include <mutex>
+#include <set>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
@@ -536,18 +538,26 @@ void make_stream_work(const std::vector<RfxbPlan*>& plans, int planes, std::vect
     }
 }
 
+// Raise a kernel's dynamic shared memory limit once per device (the
+// attribute belongs to the kernel in each device's context).
+void allow_smem(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.insert({dev, kernel}).second)
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // Forward step kernel of a mode with its dynamic shared memory enabled.
 using FwdKernel = void (*)(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
 FwdKernel fwd_kernel(int mode, bool em = false) {
-  static bool init[3][2] = {{false, false}, {false, false}, {false, false}};
   em = em && mode != 0;
   FwdKernel k = mode == 2 ? (em ? fwd_step_kernel<kTY, 2, true> : fwd_step_kernel<kTY, 2, false>)
                 : mode == 1 ? (em ? fwd_step_kernel<kTY, 1, true> : fwd_step_kernel<kTY, 1, false>)
                             : fwd_step_kernel<kTY, 0, false>;
-  if (!init[mode][em]) {
-    init[mode][em] = true;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_step_smem_bytes(mode));
-  }
+  allow_smem(reinterpret_cast<const void*>(k), fwd_step_smem_bytes(mode));
   return k;
 }
 
@@ -821,16 +831,12 @@ void group_adj_mode(RfxbBatch* g) {
 
 using AdjKernel = void (*)(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int, int);
 AdjKernel adj_kernel(int mode) {
-  static bool init[5] = {false, false, false, false, false};
   AdjKernel k = mode == 4   ? adj_step_kernel<kTY, 4>
                 : mode == 3 ? adj_step_kernel<kTY, 3>
                 : mode == 2 ? adj_step_kernel<kTY, 2>
                 : mode == 1 ? adj_step_kernel<kTY, 1>
                             : adj_step_kernel<kTY, 0>;
-  if (!init[mode]) {
-    init[mode] = true;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_step_smem_bytes(mode, 16));
-  }
+  allow_smem(reinterpret_cast<const void*>(k), adj_step_smem_bytes(mode, 16));
   return k;
 }
 
