@@ -50,7 +50,9 @@ def _workload_config(args, cells, world):
                         f"dJ/d eps_r over 16x16x2 regions",
             "instances_per_gpu": args.instances, "time_steps": args.time_steps,
             "cells_per_gpu": int(cells), "adjoint_mode": "history (design-region E^n and curl H recorded in HBM)",
-            "l2": "inputs larger than L2 (state of 161 M cells)", "parallelism": f"independent instances x {world} GPU"}
+            "l2": f"inputs larger than L2 (a step reads the fields and coefficients of {cells / 1e6:.1f} M cells, "
+                  f"{cells * 32 / 1e9:.2f} GB)",
+            "parallelism": f"independent instances x {world} GPU"}
 
 
 # ---------------------------------------------------------------------------
@@ -251,8 +253,9 @@ def run_ours(args, rank, world, local_rank):
                 "share_of_step": round(ms / total_ms, 3), "what": what}
 
     roof_adj = roof("adj_step_kernel", sum(p.adjoint_algorithmic_bytes_per_step() for p in sw.plans), adj_ms,
-                    "fused reverse step, batched over all instances: variant 2 on the CPML tiles and variant 3 "
-                    "on the plain tiles, two streams; one step = both launches")
+                    "fused reverse step, batched over all instances: variant 2 on the tiles that reach a y slab, "
+                    "variant 4 on the other CPML work, variant 3 on the plain tiles, three streams; one step = "
+                    "the three launches")
     roof_fwd = roof("fwd_step_kernel", sum(p.algorithmic_bytes_per_step() for p in sw.plans), fwd_ms,
                     "fused forward step, batched over all instances: variant 2 on the CPML tiles and variant 1 "
                     "on the plain tiles, two streams; one step = both launches")

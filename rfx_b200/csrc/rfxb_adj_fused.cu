@@ -489,18 +489,18 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   };
   if (TMA) {
     if (tid == 0)
-      for (int p = xa - 1; p <= min(xa + NST - 2, C.nx); ++p) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, p);
+      for (int p = xa - 1; p <= min(xa + NST - 2, xb); ++p) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, p);
     psi_fill(xa);
     const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa - 1)]), astage_parity<NST>(xa - 1, xa)) &&
                     mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa)]), astage_parity<NST>(xa, xa));
-    if (__syncthreads_or(!ok)) { bail(min(xa + NST - 2, C.nx), xa - 1); return; }
+    if (__syncthreads_or(!ok)) { bail(min(xa + NST - 2, xb), xa - 1); return; }
   } else {
     adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa - 1, tid);
     adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa, tid);
     cp_async_commit();
     adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 1, tid);
     cp_async_commit();
-    if (xa + 2 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 2, tid);
+    if (xa + 2 <= xb) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa + 2, tid);
     cp_async_commit();
     cp_async_wait<2>();
     __syncthreads();
@@ -565,13 +565,13 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
       // i-1's stage takes plane i+NST-1 and its psi slot plane i+1
       const bool ok =
           mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(i + 1)]), astage_parity<NST>(i + 1, xa)) && psi_wait(i);
-      if (__syncthreads_or(!ok)) { bail(min(i + NST - 2, C.nx), i + 1); return; }
-      if (tid == 0 && i + NST - 1 <= C.nx) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, i + NST - 1);
+      if (__syncthreads_or(!ok)) { bail(min(i + NST - 2, xb), i + 1); return; }
+      if (tid == 0 && i + NST - 1 <= xb) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, i + NST - 1);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();
       __syncthreads();
-      if (i + 3 <= C.nx) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, i + 3, tid);
+      if (i + 3 <= xb) adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, i + 3, tid);
       cp_async_commit();
     }
     const int b0 = astage_of<NST>(i), b1 = astage_of<NST>(i + 1);

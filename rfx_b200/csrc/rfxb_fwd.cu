@@ -506,13 +506,13 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   };
   if (TMA) {
     if (tid == 0) {
-      for (int p = xa - 1; p <= min(xa + 2, C.nx); ++p) tma_stage<TY, EM>(S, tm, par, y0, z0, p);
+      for (int p = xa - 1; p <= min(xa + 2, xb); ++p) tma_stage<TY, EM>(S, tm, par, y0, z0, p);
     }
     psi_fill(xa - 1);
     psi_fill(xa);
     const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa - 1)]), stage_parity(xa - 1, xa)) &&
                     mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa)]), stage_parity(xa, xa)) && psi_wait(xa - 1);
-    if (__syncthreads_or(!ok)) { bail(min(xa + 2, C.nx), xa - 1); return; }
+    if (__syncthreads_or(!ok)) { bail(min(xa + 2, xb), xa - 1); return; }
   } else {
     // pipeline: planes xa-1 and xa (group 0), xa+1 (group 1), xa+2 (group 2)
     load_stage<TY>(S, C, ca, cb, y0, z0, xa - 1, tid);
@@ -520,7 +520,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     cp_async_commit();
     load_stage<TY>(S, C, ca, cb, y0, z0, xa + 1, tid);
     cp_async_commit();
-    if (xa + 2 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, xa + 2, tid);
+    if (xa + 2 <= xb) load_stage<TY>(S, C, ca, cb, y0, z0, xa + 2, tid);
     cp_async_commit();
     cp_async_wait<2>();
     __syncthreads();
@@ -566,13 +566,13 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
       // thread is done with plane i-1, whose stage takes plane i+3 and whose
       // psi slot takes plane i+1
       const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), stage_parity(i + 1, xa)) && psi_wait(i);
-      if (__syncthreads_or(!ok)) { bail(min(i + 2, C.nx), i + 1); return; }
-      if (tid == 0 && i + 3 <= C.nx) tma_stage<TY, EM>(S, tm, par, y0, z0, i + 3);
+      if (__syncthreads_or(!ok)) { bail(min(i + 2, xb), i + 1); return; }
+      if (tid == 0 && i + 3 <= xb) tma_stage<TY, EM>(S, tm, par, y0, z0, i + 3);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
       __syncthreads();      // ... for every thread; plane i-1's stage is free
-      if (i + 3 <= C.nx) load_stage<TY>(S, C, ca, cb, y0, z0, i + 3, tid);
+      if (i + 3 <= xb) load_stage<TY>(S, C, ca, cb, y0, z0, i + 3, tid);
       cp_async_commit();
     }
     const int b0 = stage_of(i), b1 = stage_of(i + 1);
