@@ -199,6 +199,14 @@ def run_ours(args, rank, world, local_rank):
     cells = sw.cells()
     N = args.time_steps
     stream = torch.cuda.current_stream()
+    # launch configuration chosen by the autotuner (trial steps of this
+    # workload, before the warm-up; the first forward resets the state)
+    launch = None
+    if not args.no_autotune:
+        tune = sw.autotune(trial_steps=min(32, N), repeats=2)
+        launch = {"chosen_by": "rfx_b200.autotune (32 trial steps per candidate)", **tune.as_json()}
+    else:
+        launch = {"chosen_by": "defaults", "config": sw.batch.launch_config()[0]}
 
     def one_step():
         e0 = torch.cuda.Event(enable_timing=True)
@@ -328,7 +336,7 @@ def run_ours(args, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                 "config": _workload_config(args, cells, world), "roofline": roofline,
                 "roofline_other_kernel": roofline_other, "cpu_baseline": cpu,
-                "e2e": e2e, "single": single, "gpu_launches": launches,
+                "e2e": e2e, "single": single, "gpu_launches": launches, "launch": launch,
                 "clocks": clk.summary(), "host_wall_s_timed": round(t_host, 3)}
         print(json.dumps(line), flush=True)
     sw.close()
@@ -470,6 +478,7 @@ def main():
     ap.add_argument("--no-single", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch configuration")
     ap.add_argument("--workload", default="batched_sweep",
                     choices=["batched_sweep", "large_uniform", "graded", "adjoint_region"],
                     help="batched_sweep is the headline line; the others print a secondary forward (or "

@@ -339,6 +339,39 @@ int rfxb_batch_adjoint_variant(const RfxbBatch* batch);
 int rfxb_plan_step_launches(const RfxbPlan* plan, int* fwd, int* rev);
 int rfxb_batch_step_launches(const RfxbBatch* batch, int* fwd, int* rev);
 
+/* Launch configuration of a plan's (or batch's) step launches: the choices
+ * the autotuner (rfx_b200/autotune.py) searches.  Every setting computes the
+ * same steps; they differ in how the tiles are split among kernel variants
+ * and streams and in which launch a captured graph hands to the SMs first.
+ *   fwd_split  1: forward tiles split, the CPML-free variant 1 beside the
+ *                 staged-psi variant 2 on two streams; 0: one launch
+ *   fwd_order  with the split, 0: plain-tile launch first, 1: CPML-tile
+ *                 launch first
+ *   adj_lite   1: reverse CPML work of tiles that reach no y slab on
+ *                 variant 4 (third stream); 0: on variant 2
+ *   adj_order  order of the reverse launches, a permutation of (variant 4,
+ *                 variant 2, variant 3) by index: 0 (4,2,3), 1 (4,3,2),
+ *                 2 (2,4,3), 3 (2,3,4), 4 (3,4,2), 5 (3,2,4); without
+ *                 variant 4 only the relative order of 2 and 3 counts
+ * rfxb_*_launch_config writes the current setting to *current and the
+ * largest value each field accepts on this plan/batch to *limits (0 where a
+ * choice does not exist, e.g. fwd_split on a group without staged-psi CPML).
+ * rfxb_*_set_launch_config checks each field against those limits
+ * (RFXB_E_INVALID otherwise), synchronises the device and drops the cached
+ * step graphs.  A tuning interface of this implementation; the reference
+ * has no counterpart (XLA schedules its scan body itself). */
+typedef struct RfxbLaunchConfig {
+  int32_t fwd_split;
+  int32_t fwd_order;
+  int32_t adj_lite;
+  int32_t adj_order;
+} RfxbLaunchConfig;
+
+int rfxb_plan_launch_config(const RfxbPlan* plan, RfxbLaunchConfig* current, RfxbLaunchConfig* limits);
+int rfxb_plan_set_launch_config(RfxbPlan* plan, const RfxbLaunchConfig* config);
+int rfxb_batch_launch_config(const RfxbBatch* batch, RfxbLaunchConfig* current, RfxbLaunchConfig* limits);
+int rfxb_batch_set_launch_config(RfxbBatch* batch, const RfxbLaunchConfig* config);
+
 #ifdef __cplusplus
 }
 #endif

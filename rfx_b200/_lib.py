@@ -52,6 +52,11 @@ class RfxbDesc(C.Structure):
     ]
 
 
+class RfxbLaunchConfig(C.Structure):
+    _fields_ = [("fwd_split", C.c_int32), ("fwd_order", C.c_int32), ("adj_lite", C.c_int32),
+                ("adj_order", C.c_int32)]
+
+
 class RfxbStepIO(C.Structure):
     _fields_ = [
         ("src_wave_dev", C.c_void_p),
@@ -121,6 +126,10 @@ SIGNATURES = {
     "rfxb_batch_adjoint_variant": (C.c_int, [C.c_void_p]),
     "rfxb_plan_step_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "rfxb_batch_step_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "rfxb_plan_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig), C.POINTER(RfxbLaunchConfig)]),
+    "rfxb_plan_set_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig)]),
+    "rfxb_batch_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig), C.POINTER(RfxbLaunchConfig)]),
+    "rfxb_batch_set_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig)]),
     "rfxb_forward_noalloc": (C.c_int, [C.POINTER(RfxbDesc), C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
                                        C.POINTER(RfxbStepIO), C.c_int, C.c_int, C.c_void_p]),
 }

@@ -1,0 +1,171 @@
+"""Launch-configuration autotuner for plans and batched sweeps.
+
+A plan or batch can launch its step kernels in several equivalent ways (the
+``RfxbLaunchConfig`` fields of ``rfxb200.h``): the forward tiles split
+between the CPML-free kernel and the staged-psi kernel on two streams or run
+as one launch, which of the concurrent launches the captured graph hands to
+the SMs first, and whether the reverse step's CPML work without a y slab runs
+on variant 4 or on variant 2.  Every setting computes the same steps; which
+one is fastest depends on the workload (grid sizes, CPML share, number of
+instances).  The autotuner times a few steps of each candidate with CUDA
+events on the real workload, keeps the fastest, and caches the choice by a
+workload signature (in memory, and in a JSON file when a path is given).
+
+The reference has no counterpart: XLA schedules its scan body itself.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+from dataclasses import dataclass, field
+
+# Reverse launch orders (rfxb200.h): permutations of (variant 4, variant 2,
+# variant 3) by index.  Without variant 4 only the relative order of 2 and 3
+# counts, so orders 0 (2 before 3) and 1 (3 before 2) represent all six.
+REVERSE_ORDERS = ((4, 2, 3), (4, 3, 2), (2, 4, 3), (2, 3, 4), (3, 4, 2), (3, 2, 4))
+
+_memory_cache: dict = {}
+
+
+@dataclass
+class TuneResult:
+    """The chosen launch configuration and the measured milliseconds of
+    every candidate (keyed by the candidate's fields as a tuple)."""
+    config: dict
+    forward_ms: dict = field(default_factory=dict)
+    reverse_ms: dict = field(default_factory=dict)
+    cached: bool = False
+
+    def as_json(self) -> dict:
+        return {"config": self.config, "cached": self.cached,
+                "forward_ms": {_key_str(k): v for k, v in self.forward_ms.items()},
+                "reverse_ms": {_key_str(k): v for k, v in self.reverse_ms.items()}}
+
+
+def _key_str(k) -> str:
+    return ",".join(f"{a}={b}" for a, b in k)
+
+
+def forward_candidates(limits: dict, current: dict) -> list:
+    """Forward settings to time: split with either launch order, and the
+    single launch, as far as the limits allow (the current setting first)."""
+    c = []
+    if limits["fwd_split"]:
+        c += [{"fwd_split": 1, "fwd_order": 0}, {"fwd_split": 1, "fwd_order": 1}, {"fwd_split": 0, "fwd_order": 0}]
+    else:
+        c.append({"fwd_split": 0, "fwd_order": 0})
+    cur = {"fwd_split": current["fwd_split"], "fwd_order": current["fwd_order"] if current["fwd_split"] else 0}
+    return [cur] + [x for x in c if x != cur]
+
+
+def reverse_candidates(limits: dict, current: dict) -> list:
+    """Reverse settings to time: every order with variant 4, and the two
+    distinct orders without it, as far as the limits allow (the current
+    setting first)."""
+    c = []
+    if limits["adj_order"] > 0:
+        if limits["adj_lite"]:
+            c += [{"adj_lite": 1, "adj_order": o} for o in range(len(REVERSE_ORDERS))]
+        c += [{"adj_lite": 0, "adj_order": 0}, {"adj_lite": 0, "adj_order": 1}]
+    else:
+        c.append({"adj_lite": 0, "adj_order": 0})
+    cur = {"adj_lite": current["adj_lite"], "adj_order": current["adj_order"]}
+    if not cur["adj_lite"]:   # the representative of the current relative order of 2 and 3
+        o = REVERSE_ORDERS[cur["adj_order"]]
+        cur["adj_order"] = 0 if o.index(2) < o.index(3) else 1
+    if cur in c:
+        c.remove(cur)
+    elif limits["adj_order"] == 0:
+        return c
+    return [cur] + c
+
+
+def pick(timings: dict, rel_margin: float = 0.01):
+    """The fastest candidate, keeping the first (current) one unless another
+    is faster by more than ``rel_margin`` (timing noise is not a reason to
+    change)."""
+    items = list(timings.items())
+    first_k, first_t = items[0]
+    best_k, best_t = min(items, key=lambda kv: kv[1])
+    return best_k if best_t < first_t * (1.0 - rel_margin) else first_k
+
+
+def cuda_timer(fn) -> float:
+    """Milliseconds of ``fn()`` on the current stream, measured with CUDA events."""
+    import torch
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    fn()
+    b.record()
+    torch.cuda.synchronize()
+    return float(a.elapsed_time(b))
+
+
+def _time(fn, repeats, timer):
+    fn()   # first call captures the step graphs of the new configuration
+    return min(timer(fn) for _ in range(max(1, repeats)))
+
+
+def _load_cache(path):
+    if path and os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def autotune(target, run_forward, run_reverse=None, *, signature=None, cache_path=None, repeats=2,
+             timer=None, rel_margin=0.01) -> TuneResult:
+    """Choose the launch configuration of ``target`` (a ``Plan`` or ``Batch``:
+    anything with ``launch_config()`` and ``set_launch_config(**fields)``).
+
+    ``run_forward()`` runs a few forward steps of the real workload and
+    ``run_reverse()`` (optional) a few reverse steps; each is run once per
+    candidate untimed (graph capture) and then ``repeats`` times timed, the
+    minimum counting.  The forward fields are chosen first, then the reverse
+    fields with the forward choice in place.  With a ``signature`` the choice
+    is cached (and with ``cache_path`` stored as JSON) and reused without
+    timing.  The target is left on the chosen configuration; its state after
+    the trial steps is arbitrary, so the caller resets it before a real run.
+    """
+    timer = timer or cuda_timer
+    key = None
+    if signature is not None:
+        key = hashlib.sha1(json.dumps(signature, sort_keys=True, default=str).encode()).hexdigest()
+        hit = _memory_cache.get(key) or _load_cache(cache_path).get(key)
+        if hit is not None:
+            target.set_launch_config(**hit)
+            _memory_cache[key] = dict(hit)
+            return TuneResult(config=dict(hit), cached=True)
+    current, limits = target.launch_config()
+    res = TuneResult(config=dict(current))
+    fc = forward_candidates(limits, current)
+    if len(fc) > 1:
+        for c in fc:
+            target.set_launch_config(**c)
+            res.forward_ms[tuple(sorted(c.items()))] = _time(run_forward, repeats, timer)
+        best = dict(pick(res.forward_ms, rel_margin))
+        target.set_launch_config(**best)
+        res.config.update(best)
+    rc = reverse_candidates(limits, current) if run_reverse is not None else []
+    if len(rc) > 1:
+        for c in rc:
+            target.set_launch_config(**c)
+            res.reverse_ms[tuple(sorted(c.items()))] = _time(run_reverse, repeats, timer)
+        best = dict(pick(res.reverse_ms, rel_margin))
+        target.set_launch_config(**best)
+        res.config.update(best)
+    res.config = target.launch_config()[0]
+    if key is not None:
+        _memory_cache[key] = dict(res.config)
+        if cache_path:
+            data = _load_cache(cache_path)
+            data[key] = dict(res.config)
+            tmp = cache_path + ".tmp"
+            with open(tmp, "w") as f:
+                json.dump(data, f, indent=1, sort_keys=True)
+            os.replace(tmp, cache_path)
+    return res

@@ -130,6 +130,42 @@ class Sweep:
         Js, gs = self.objectives()
         return Js, self.backward(gs)
 
+    def signature(self):
+        """What the fastest launch configuration depends on: the instances'
+        grid shapes and CPML / PEC axes, batching, and the device."""
+        dev = torch.cuda.get_device_name(self.device) if torch.cuda.is_available() else "cpu"
+        return {"device": dev, "batched": self.batched,
+                "instances": [(tuple(int(n) for n in s.grid.shape), s.cpml_axes, s.pec_axes) for s in self.inst]}
+
+    def autotune(self, trial_steps=32, repeats=2, cache_path=None):
+        """Pick the batch's launch configuration (``rfx_b200.autotune``) by
+        timing ``trial_steps`` forward and reverse steps of this sweep per
+        candidate.  The next ``forward`` resets the state the trials leave.
+        Returns the ``TuneResult``; None for an unbatched sweep (each
+        simulation keeps the default of its plan)."""
+        from .autotune import autotune
+        if not self.batched:
+            return None
+        T = max(1, min(int(trial_steps), self.n_steps))
+        ios = [dict(src_table=io["src"], probe_out=io["ts"]) for io in self.io]
+        zero_g = [torch.zeros_like(io["ts"]) for io in self.io]
+        for p in self.plans:
+            p.reset()
+            p.record_history(0, T)
+
+        def run_forward():
+            self.batch.advance(0, T, ios)
+
+        def run_reverse():
+            aios = [dict(g=g, grad=io["grad"], dca=io["dca"], dcb=io["dcb"], src_adj=None)
+                    for io, g in zip(self.io, zero_g)]
+            self.batch.adjoint_begin(T, aios)
+            self.batch.adjoint_advance(T, T, aios)
+
+        run_forward()   # history of the trial steps for the reverse trials
+        return autotune(self.batch, run_forward, run_reverse, signature=self.signature(), cache_path=cache_path,
+                        repeats=repeats)
+
     def step_launches(self):
         """Step-kernel launches of one forward time step and one reverse
         time step of the whole sweep (every instance included)."""

@@ -171,6 +171,8 @@ struct RfxbBatch {
   // forward steps split between the CPML-free kernel (list 1) and the
   // staged-psi kernel (list 2), launched side by side on two streams
   bool fwd_split = false;
+  bool fwd_split_avail = false;   // both forward lists exist (fwd_split may be chosen)
+  int fwd_order = 0;              // split forward: 0 plain-tile launch first, 1 CPML-tile launch first
   RfxbWork* d_wf1 = nullptr;
   int n_wf1 = 0;
   RfxbWork* d_wf2 = nullptr;
@@ -185,6 +187,8 @@ struct RfxbBatch {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // reverse variant 4 (CPML work that reaches no y slab) on a third stream
   bool adj_lite = false;
+  bool adj_lite_avail = false;    // the variant-4 lists exist (adj_lite may be chosen)
+  int adj_order = 0;              // permutation index of the reverse launches (rfxb200.h)
   RfxbWork* d_wa2y = nullptr;   // variant 2 list when variant 4 takes the rest
   int n_wa2y = 0;
   RfxbWork* d_wa4 = nullptr;
@@ -875,9 +879,10 @@ int build_group(RfxbBatch* g) {
     g->allocs.push_back(*ptr);
     return 0;
   };
-  // forward split (variant 2 groups, balanced lists; RFXB_FWD_SPLIT=0 keeps one list)
+  // forward split (variant 2 groups, balanced lists; RFXB_FWD_SPLIT=0 starts
+  // with the single list, which stays available as a launch configuration)
   g->fwd_split = false;
-  if (g->fwd_mode == 2 && work_mode() == 1 && fwd_split_enabled()) {
+  if (g->fwd_mode == 2 && work_mode() == 1) {
     std::vector<WorkSeg> plain, cpml;
     split_segments(g->plans, slab_weight(), plain, cpml);
     std::vector<RfxbWork> w1, w2;
@@ -893,7 +898,8 @@ int build_group(RfxbBatch* g) {
       RFXB_CUDA(cudaStreamCreateWithFlags(&g->side_stream, cudaStreamNonBlocking));
       RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
       RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
-      g->fwd_split = true;
+      g->fwd_split_avail = true;
+      g->fwd_split = fwd_split_enabled();
     }
     // reverse split (used when the reverse kernel is variant 1 or 2); with
     // variant 2, the CPML work of tiles that reach no y slab can go to
@@ -925,7 +931,7 @@ int build_group(RfxbBatch* g) {
       // the 1 KB the runtime reserves per CTA) fits four times
       const int per_sm = (int)(4 * (adj_step_smem_bytes(4, zp) + 1024) <= (size_t)smem_per_sm() ? 4 : 3);
       balance_segments(anoy, per_sm * sm_count(), 3.0, a4);
-      if (adj_lite_enabled() && !a4.empty()) {
+      if (!a4.empty()) {
         if (!a2y.empty()) {
           if (int rc = galloc((void**)&g->d_wa2y, sizeof(RfxbWork) * a2y.size())) return rc;
           RFXB_CUDA(cudaMemcpy(g->d_wa2y, a2y.data(), sizeof(RfxbWork) * a2y.size(), cudaMemcpyHostToDevice));
@@ -936,7 +942,8 @@ int build_group(RfxbBatch* g) {
         g->n_wa4 = (int)a4.size();
         RFXB_CUDA(cudaStreamCreateWithFlags(&g->side2, cudaStreamNonBlocking));
         RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join2, cudaEventDisableTiming));
-        g->adj_lite = true;
+        g->adj_lite_avail = true;
+        g->adj_lite = adj_lite_enabled();
       }
     }
   }
@@ -1132,12 +1139,19 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, b
       // staged-psi tiles on the caller's stream, CPML-free tiles beside them
       RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
       RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
-      // capture order: the plain tiles first (measured 2 % faster on the
-      // sweep's forward phase than the CPML tiles first, equal on one grid)
-      fwd_kernel(1, em)<<<g->n_wf1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(g->d_inst, g->d_wf1,
-                                                                                          g->d_maps, n, par);
-      fwd_kernel(2, em)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps, n,
-                                                                              par);
+      // capture order (fwd_order): by default the plain tiles first
+      // (measured 2 % faster on the sweep's forward phase than the CPML tiles
+      // first, equal on one grid)
+      auto plain = [&]() {
+        fwd_kernel(1, em)<<<g->n_wf1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(g->d_inst, g->d_wf1,
+                                                                                            g->d_maps, n, par);
+      };
+      auto staged = [&]() {
+        fwd_kernel(2, em)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps,
+                                                                                n, par);
+      };
+      if (g->fwd_order == 0) { plain(); staged(); }
+      else { staged(); plain(); }
       RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
       RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0));
     } else {
@@ -1396,13 +1410,18 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
                 g->d_inst, g->d_adj, g->d_wa1, g->d_maps, s, par, fpar, zp);
           };
           // capture order = the order the graph hands the branches' CTAs to
-          // the SMs: the largest, four-per-SM variant 4 first, then the y-slab
-          // variant 2, the plain variant 3 last (measured best of the six
-          // orders, 3 % on the sweep's reverse phase)
+          // the SMs (adj_order); the default 0 puts the largest, four-per-SM
+          // variant 4 first, then the y-slab variant 2, the plain variant 3
+          // last (measured best of the six orders, 3 % on the sweep's
+          // reverse phase)
           if (lite) RFXB_CUDA(cudaStreamWaitEvent(g->side2, g->ev_fork, 0));
-          v4();
-          v2();
-          v3();
+          static const char kOrder[6][3] = {{4, 2, 3}, {4, 3, 2}, {2, 4, 3}, {2, 3, 4}, {3, 4, 2}, {3, 2, 4}};
+          for (int t = 0; t < 3; ++t) {
+            const int v = kOrder[g->adj_order][t];
+            if (v == 4) v4();
+            else if (v == 2) v2();
+            else v3();
+          }
           RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
           RFXB_CUDA(cudaStreamWaitEvent(cs, g->ev_join, 0));
           if (lite) {
@@ -2026,6 +2045,55 @@ int rfxb_batch_step_launches(const RfxbBatch* g, int* fwd, int* rev) {
   if (!g) return fail(RFXB_E_INVALID, "null batch");
   step_launches(g, fwd, rev);
   return 0;
+}
+
+namespace {
+void launch_config(const RfxbBatch* g, RfxbLaunchConfig* cur, RfxbLaunchConfig* lim) {
+  if (cur) *cur = RfxbLaunchConfig{g->fwd_split ? 1 : 0, g->fwd_order, g->adj_lite ? 1 : 0, g->adj_order};
+  if (lim) *lim = RfxbLaunchConfig{g->fwd_split_avail ? 1 : 0, g->fwd_split_avail ? 1 : 0, g->adj_lite_avail ? 1 : 0,
+                                   g->adj_split ? 5 : 0};
+}
+
+int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
+  if (!c) return fail(RFXB_E_INVALID, "null launch configuration");
+  RfxbLaunchConfig lim;
+  launch_config(g, nullptr, &lim);
+  auto in = [](int v, int hi) { return v >= 0 && v <= hi; };
+  if (!in(c->fwd_split, lim.fwd_split) || !in(c->fwd_order, lim.fwd_order) || !in(c->adj_lite, lim.adj_lite) ||
+      !in(c->adj_order, lim.adj_order))
+    return fail(RFXB_E_INVALID, "launch configuration outside the limits of this plan/batch");
+  // cached graphs hold the old launch sequence: drop them once nothing runs
+  RFXB_CUDA(cudaDeviceSynchronize());
+  for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  g->graphs.clear();
+  g->fwd_split = c->fwd_split != 0;
+  g->fwd_order = c->fwd_order;
+  g->adj_lite = c->adj_lite != 0;
+  g->adj_order = c->adj_order;
+  return 0;
+}
+}  // namespace
+
+int rfxb_plan_launch_config(const RfxbPlan* p, RfxbLaunchConfig* current, RfxbLaunchConfig* limits) {
+  if (!p || !p->self_group) return fail(RFXB_E_INVALID, "null plan");
+  launch_config(p->self_group, current, limits);
+  return 0;
+}
+
+int rfxb_plan_set_launch_config(RfxbPlan* p, const RfxbLaunchConfig* config) {
+  if (!p || !p->self_group) return fail(RFXB_E_INVALID, "null plan");
+  return set_launch_config(p->self_group, config);
+}
+
+int rfxb_batch_launch_config(const RfxbBatch* g, RfxbLaunchConfig* current, RfxbLaunchConfig* limits) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  launch_config(g, current, limits);
+  return 0;
+}
+
+int rfxb_batch_set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* config) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  return set_launch_config(g, config);
 }
 
 int rfxb_plan_adjoint_variant(const RfxbPlan* p) {

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import RfxbAdjointIO, RfxbDesc, RfxbDftDesc, RfxbStepIO, check
+from ._lib import RfxbAdjointIO, RfxbDesc, RfxbDftDesc, RfxbLaunchConfig, RfxbStepIO, check
 
 COMP = {"ex": 0, "ey": 1, "ez": 2, "hx": 3, "hy": 4, "hz": 5}
 PROBE_PRESOURCE = 16
@@ -41,6 +41,24 @@ def require_cuda(device=None) -> torch.device:
 
 def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+_LAUNCH_FIELDS = ("fwd_split", "fwd_order", "adj_lite", "adj_order")
+
+
+def _get_launch(getter, h):
+    cur, lim = RfxbLaunchConfig(), RfxbLaunchConfig()
+    check(getter(h, C.byref(cur), C.byref(lim)), getter.__name__)
+    return ({f: int(getattr(cur, f)) for f in _LAUNCH_FIELDS}, {f: int(getattr(lim, f)) for f in _LAUNCH_FIELDS})
+
+
+def _set_launch(getter, setter, h, fields):
+    unknown = set(fields) - set(_LAUNCH_FIELDS)
+    if unknown:
+        raise ValueError(f"unknown launch configuration fields {sorted(unknown)}")
+    cur, _ = _get_launch(getter, h)
+    cur.update({k: int(v) for k, v in fields.items()})
+    check(setter(h, C.byref(RfxbLaunchConfig(**cur))), setter.__name__)
 
 
 def _fptr(a: np.ndarray):
@@ -241,6 +259,16 @@ class Plan:
         check(self._lib.rfxb_plan_step_launches(self._h, C.byref(f), C.byref(r)), "rfxb_plan_step_launches")
         return f.value, r.value
 
+    def launch_config(self):
+        """(current, limits) launch configuration dicts (``rfxb200.h``
+        ``RfxbLaunchConfig``: fwd_split, fwd_order, adj_lite, adj_order)."""
+        return _get_launch(self._lib.rfxb_plan_launch_config, self._h)
+
+    def set_launch_config(self, **fields):
+        """Change some launch-configuration fields (the rest keep their
+        value); synchronises the device and drops the cached step graphs."""
+        _set_launch(self._lib.rfxb_plan_launch_config, self._lib.rfxb_plan_set_launch_config, self._h, fields)
+
     # -- state ---------------------------------------------------------------
     def _dev(self, a, dtype=torch.float32):
         t = torch.as_tensor(np.asarray(a) if not isinstance(a, torch.Tensor) else a)
@@ -429,6 +457,14 @@ class Batch:
         f, r = C.c_int(), C.c_int()
         check(self._lib.rfxb_batch_step_launches(self._h, C.byref(f), C.byref(r)), "rfxb_batch_step_launches")
         return f.value, r.value
+
+    def launch_config(self):
+        """(current, limits) launch configuration dicts, as ``Plan.launch_config``."""
+        return _get_launch(self._lib.rfxb_batch_launch_config, self._h)
+
+    def set_launch_config(self, **fields):
+        """As ``Plan.set_launch_config``, for the whole batch."""
+        _set_launch(self._lib.rfxb_batch_launch_config, self._lib.rfxb_batch_set_launch_config, self._h, fields)
 
     def adjoint_begin(self, n_total, aios):
         ios = [Plan.adjoint_io(**kw) for kw in aios]   # keeps the pointer arrays alive for the call

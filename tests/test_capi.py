@@ -43,6 +43,7 @@ def test_struct_layout_matches_header(tmp_path):
         "RfxbDftDesc": _lib.RfxbDftDesc, "RfxbFluxDesc": _lib.RfxbFluxDesc, "RfxbNtffDesc": _lib.RfxbNtffDesc,
         "RfxbDesc": _lib.RfxbDesc,
         "RfxbStepIO": _lib.RfxbStepIO, "RfxbAdjointIO": _lib.RfxbAdjointIO,
+        "RfxbLaunchConfig": _lib.RfxbLaunchConfig,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():
