@@ -701,10 +701,17 @@ def _run(st, n_steps, sources, probes, dft_planes, vi_ports, dft_time_offset,
                         flux_accs if flux_monitors else None, ntff_acc)
 
 
+def _set_fields(st, init_fields):
+    """Start from given fields (a dict of the six components) instead of zero:
+    a test device, not part of the reference's run."""
+    for c, v in (init_fields or {}).items():
+        st.F[c][...] = np.asarray(v, st.f)
+
+
 def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
                 pec_axes=None, sources=(), probes=(), dft_planes=(), pec_mask=None,
                 vi_ports=(), kappa_max=1.0, dtype=np.float32, exact_materials=False, flux_monitors=(),
-                ntff=None):
+                ntff=None, init_fields=None):
     """``rfx.simulation.run`` (rfx/simulation.py:1686-2138), scan body order of
     rfx/simulation.py:1255-1685.  ``pec_axes=None`` means all axes
     (rfx/simulation.py:684-691).  ``sources`` are ``(i, j, k, comp, waveform)``,
@@ -718,13 +725,14 @@ def run_uniform(grid, materials, n_steps, *, boundary="cpml", cpml_axes="xyz",
                   cpml_axes=cpml_axes if boundary == "cpml" else "",
                   pec_axes=pec_axes, pec_mask=pec_mask, kappa_max=kappa_max,
                   exact_materials=exact_materials)
+    _set_fields(st, init_fields)
     return _run(st, n_steps, sources, probes, dft_planes, vi_ports, 1,
                 probes_before_dft=True, dx_vi=grid.dx, flux_monitors=flux_monitors, ntff=ntff)
 
 
 def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_planes=(),
                    pec_mask=None, kappa_max=1.0, dtype=np.float32, exact_materials=False, ntff=None,
-                   flux_monitors=()):
+                   flux_monitors=(), init_fields=None):
     """``rfx.nonuniform.run_nonuniform`` (rfx/nonuniform.py:1589-1804), scan body
     of rfx/nonuniform.py:1256-1568: PEC on every axis, DFT time stamp ``n dt``
     (rfx/nonuniform.py:1461), DFT before probes."""
@@ -735,6 +743,7 @@ def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_plane
                   cpml_axes=axes if grid.cpml_layers > 0 else "",
                   pec_axes="xyz", pec_mask=pec_mask, kappa_max=kappa_max,
                   exact_materials=exact_materials)
+    _set_fields(st, init_fields)
     return _run(st, n_steps, sources, probes, dft_planes, (), 0,
                 probes_before_dft=False, dx_vi=grid.dx, ntff=ntff, flux_monitors=flux_monitors)
 

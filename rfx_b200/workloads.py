@@ -65,13 +65,23 @@ def large_uniform(seed=0, n_steps=4000, n_interior=256):
     return g, eps, sig, src, probes, dft
 
 
-def graded(seed=0, n_steps=6000):
-    rng = np.random.default_rng(seed)
-    dx = 0.5e-3
+def _graded_dz(rng):
     dz = [float(rng.uniform(1e-4, 5e-4))]
     for _ in range(95):
         dz.append(min(5e-4, max(1e-4, dz[-1] * float(rng.uniform(1 / 1.2, 1.2)))))
-    g = make_nonuniform_grid((192 * dx, 192 * dx), np.asarray(dz), dx, cpml_layers=12)
+    return np.asarray(dz)
+
+
+def graded_dz(seed=0):
+    """The 96-cell z profile of ``graded(seed)`` (its first draws)."""
+    return _graded_dz(np.random.default_rng(seed))
+
+
+def graded(seed=0, n_steps=6000):
+    rng = np.random.default_rng(seed)
+    dx = 0.5e-3
+    dz = _graded_dz(rng)
+    g = make_nonuniform_grid((192 * dx, 192 * dx), dz, dx, cpml_layers=12)
     shape = g.shape
     eps = np.ones(shape, np.float32)
     sig = np.zeros(shape, np.float32)
