@@ -372,6 +372,18 @@ int rfxb_plan_set_launch_config(RfxbPlan* plan, const RfxbLaunchConfig* config);
 int rfxb_batch_launch_config(const RfxbBatch* batch, RfxbLaunchConfig* current, RfxbLaunchConfig* limits);
 int rfxb_batch_set_launch_config(RfxbBatch* batch, const RfxbLaunchConfig* config);
 
+/* Host only, no device needed: the work list (x ranges of (TY x 32) tiles)
+ * that a batch of plans with these shapes launches for one step, for tests
+ * of the tiling.  dims: 5 ints per plan (nx, ny, nz, CPML layers, CPML axes
+ * bits x=1 y=2 z=4); resident: the CTA capacity the lists are balanced for.
+ * which: 0 every tile on one kernel; 1 / 2 forward CPML-free / staged-psi
+ * tiles; 3 / 4 reverse CPML-free / CPML tiles; 5 / 6 the reverse CPML tiles
+ * split into those that reach a y slab (variant 2) and the rest (variant 4).
+ * out: 5 ints per item (plan, y0, z0, xa, xb), *n_out the item count (with
+ * out == NULL only the count).  A diagnostic of this implementation. */
+int rfxb_debug_work_lists(int n_plans, const int32_t* dims, int32_t resident, int32_t which, int32_t* out,
+                          int32_t cap, int32_t* n_out);
+
 #ifdef __cplusplus
 }
 #endif

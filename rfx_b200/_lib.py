@@ -130,6 +130,8 @@ SIGNATURES = {
     "rfxb_plan_set_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig)]),
     "rfxb_batch_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig), C.POINTER(RfxbLaunchConfig)]),
     "rfxb_batch_set_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig)]),
+    "rfxb_debug_work_lists": (C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                        C.c_int32, C.POINTER(C.c_int32)]),
     "rfxb_forward_noalloc": (C.c_int, [C.POINTER(RfxbDesc), C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
                                        C.POINTER(RfxbStepIO), C.c_int, C.c_int, C.c_void_p]),
 }

@@ -2,6 +2,7 @@
 // objects, device allocation, descriptor upload, launch sequencing and the
 // CUDA-graph replay of step chunks.
 #include <cuda.h>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <cudaTypedefs.h>
@@ -2094,6 +2095,56 @@ int rfxb_batch_launch_config(const RfxbBatch* g, RfxbLaunchConfig* current, Rfxb
 int rfxb_batch_set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* config) {
   if (!g) return fail(RFXB_E_INVALID, "null batch");
   return set_launch_config(g, config);
+}
+
+int rfxb_debug_work_lists(int n_plans, const int32_t* dims, int32_t resident, int32_t which, int32_t* out,
+                          int32_t cap, int32_t* n_out) {
+  if (n_plans <= 0 || !dims || resident <= 0 || which < 0 || which > 6 || !n_out)
+    return fail(RFXB_E_INVALID, "rfxb_debug_work_lists: bad arguments");
+  std::vector<std::unique_ptr<RfxbPlan>> own;
+  std::vector<RfxbPlan*> plans;
+  for (int q = 0; q < n_plans; ++q) {
+    const int32_t* d = dims + 5 * q;
+    if (d[0] < 2 || d[1] < 2 || d[2] < 2 || d[3] < 0 || d[4] < 0 || d[4] > 7)
+      return fail(RFXB_E_INVALID, "rfxb_debug_work_lists: bad plan dims");
+    auto p = std::make_unique<RfxbPlan>();
+    p->nx = d[0];
+    p->ny = d[1];
+    p->nz = d[2];
+    p->inst.ncp = d[3];
+    p->inst.cpml_axes = (unsigned)d[4];
+    plans.push_back(p.get());
+    own.push_back(std::move(p));
+  }
+  const double slab = slab_weight();
+  std::vector<RfxbWork> w;
+  if (which == 0) {
+    make_balanced_work(plans, resident, slab, 3.0, w);
+  } else if (which <= 2) {
+    std::vector<WorkSeg> plain, cpml;
+    split_segments(plans, slab, plain, cpml);
+    balance_segments(which == 1 ? plain : cpml, resident, 3.0, w);
+  } else if (which <= 4) {
+    std::vector<WorkSeg> plain, cpml;
+    split_adj_segments(plans, slab, plain, cpml);
+    balance_segments(which == 3 ? plain : cpml, resident, 3.0, w);
+  } else {
+    std::vector<WorkSeg> plain, ys, noy;
+    split_adj_segments(plans, slab, plain, ys, &noy);
+    balance_segments(which == 5 ? ys : noy, resident, 3.0, w);
+  }
+  *n_out = (int32_t)w.size();
+  if (!out) return 0;
+  if (cap < (int32_t)w.size()) return fail(RFXB_E_INVALID, "rfxb_debug_work_lists: output capacity too small");
+  for (size_t t = 0; t < w.size(); ++t) {
+    int32_t* o = out + 5 * t;
+    o[0] = w[t].inst;
+    o[1] = w[t].y0;
+    o[2] = w[t].z0;
+    o[3] = w[t].xa;
+    o[4] = w[t].xb;
+  }
+  return 0;
 }
 
 int rfxb_plan_adjoint_variant(const RfxbPlan* p) {

@@ -1,0 +1,118 @@
+"""The step kernels' work lists, on CPU (no device: ``rfxb_debug_work_lists``
+runs the host-side split and balancing of ``rfxb_capi.cu``).
+
+Every list a batch launches for one step must update each (tile, x plane)
+of every plan exactly once -- a missed plane leaves stale fields, a doubled
+one races with itself -- and the CPML-free kernels may only be given tiles
+and planes whose update needs no CPML term:
+
+* forward: all tiles on one kernel (0), or CPML-free (1) + staged-psi (2);
+  a CPML-free forward item's cells (rows y0-1 .. y0+7, columns z0-1 ..
+  z0+31) reach no y / z slab and its planes lie in ncp+1 .. nx-ncp-1;
+* reverse: CPML-free (3) + CPML (4), or CPML-free (3) + y-slab (5) + the
+  rest (6); a reverse CPML-free item's rows y0-1 .. y0+8 and columns z0-1 ..
+  z0+32 reach no slab and its planes lie in ncp+1 .. nx-ncp-2; a variant-4
+  item (6) reaches no y slab.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from rfx_b200 import _lib
+
+TY, TZ = 8, 32
+
+
+def _lists(plans, which, resident=444):
+    lib = _lib.load()
+    dims = (C.c_int32 * (5 * len(plans)))(*[int(v) for p in plans for v in p])
+    n = C.c_int32()
+    rc = lib.rfxb_debug_work_lists(len(plans), dims, resident, which, None, 0, C.byref(n))
+    assert rc == 0, _lib.load().rfxb_last_error()
+    out = (C.c_int32 * max(1, 5 * n.value))()
+    assert lib.rfxb_debug_work_lists(len(plans), dims, resident, which, out, n.value, C.byref(n)) == 0
+    return np.frombuffer(out, np.int32)[: 5 * n.value].reshape(-1, 5).copy()
+
+
+def _coverage(plans, items):
+    """Count of updates per (plan, y tile, z tile, x plane)."""
+    cov = [np.zeros(((p[1] + TY - 1) // TY, (p[2] + TZ - 1) // TZ, p[0]), np.int32) for p in plans]
+    for q, y0, z0, xa, xb in items:
+        assert y0 % TY == 0 and z0 % TZ == 0
+        assert 0 <= xa < xb <= plans[q][0]
+        cov[q][y0 // TY, z0 // TZ, xa:xb] += 1
+    return cov
+
+
+def _reaches(lo, hi, n, ncp):
+    """Rows (or columns) lo .. hi include a cell of a CPML slab of width ncp."""
+    return lo < ncp or hi >= n - ncp
+
+
+def _random_plans(rng, k):
+    plans = []
+    for _ in range(k):
+        ncp = int(rng.choice([0, 4, 8, 10, 12]))
+        axes = int(rng.integers(0, 8)) if ncp else 0
+        lo = 2 * ncp + 6
+        plans.append((int(rng.integers(lo, lo + 90)), int(rng.integers(lo, lo + 90)), int(rng.integers(lo, lo + 90)),
+                      ncp, axes))
+    return plans
+
+
+CASES = [
+    [(87, 47, 42, 8, 7)],                   # README quick start grid
+    [(81, 81, 81, 8, 7), (177, 177, 177, 8, 7), (100, 37, 140, 8, 3)],
+    [(221, 141, 69, 10, 7)],                # adjoint configuration
+    [(40, 40, 40, 0, 0), (30, 31, 33, 12, 6)],
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES) + 6))
+@pytest.mark.parametrize("resident", [148, 592])
+def test_work_lists_cover_each_plane_once(case, resident):
+    plans = CASES[case] if case < len(CASES) else _random_plans(np.random.default_rng(case), 4)
+    groups = {"all": [0], "fwd split": [1, 2], "rev split": [3, 4], "rev lite": [3, 5, 6]}
+    for name, ids in groups.items():
+        items = np.concatenate([_lists(plans, w, resident) for w in ids])
+        for q, c in enumerate(_coverage(plans, items)):
+            assert c.min() == 1 and c.max() == 1, (name, plans[q])
+
+
+@pytest.mark.parametrize("case", range(len(CASES) + 6))
+def test_cpml_free_lists_touch_no_slab(case):
+    plans = CASES[case] if case < len(CASES) else _random_plans(np.random.default_rng(100 + case), 4)
+    for q, y0, z0, xa, xb in _lists(plans, 1):
+        nx, ny, nz, ncp, ax = plans[q]
+        if not ncp or not ax:
+            continue
+        assert not ((ax & 2) and _reaches(y0 - 1, y0 + TY - 1, ny, ncp))
+        assert not ((ax & 4) and _reaches(z0 - 1, z0 + TZ - 1, nz, ncp))
+        if ax & 1:
+            assert xa >= ncp + 1 and xb <= nx - ncp
+    for q, y0, z0, xa, xb in _lists(plans, 3):
+        nx, ny, nz, ncp, ax = plans[q]
+        if not ncp or not ax:
+            continue
+        assert not ((ax & 2) and _reaches(y0 - 1, y0 + TY, ny, ncp))
+        assert not ((ax & 4) and _reaches(z0 - 1, z0 + TZ, nz, ncp))
+        if ax & 1:
+            assert xa >= ncp + 1 and xb <= nx - ncp - 1
+    for q, y0, z0, xa, xb in _lists(plans, 6):
+        nx, ny, nz, ncp, ax = plans[q]
+        assert not ((ax & 2) and _reaches(y0 - 1, y0 + TY, ny, ncp))
+
+
+def test_bad_arguments_are_rejected():
+    lib = _lib.load()
+    n = C.c_int32()
+    dims = (C.c_int32 * 5)(1, 10, 10, 0, 0)
+    invalid = -1   # RFXB_E_INVALID
+    assert lib.rfxb_debug_work_lists(1, dims, 100, 0, None, 0, C.byref(n)) == invalid
+    dims = (C.c_int32 * 5)(20, 20, 20, 4, 7)
+    assert lib.rfxb_debug_work_lists(1, dims, 100, 7, None, 0, C.byref(n)) == invalid
+    assert lib.rfxb_debug_work_lists(1, dims, 100, 0, None, 0, C.byref(n)) == 0 and n.value > 0
+    small = (C.c_int32 * 5)()
+    assert lib.rfxb_debug_work_lists(1, dims, 100, 0, small, 1, C.byref(n)) == invalid
