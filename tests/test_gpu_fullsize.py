@@ -67,7 +67,8 @@ def _advance(r, n, table=None, init=None, chunks=1):
         p.advance(int(a), int(b - a), r.src_table, r.probe_out, r.dft_accs, r.dft_phases)
     torch.cuda.synchronize()
     p.check_device()
-    return r.probe_out.cpu().numpy().copy(), [a.cpu().numpy().copy() for a in r.dft_accs]
+    ts = r.probe_out.cpu().numpy().copy() if r.probe_out is not None else np.zeros((n, 0), np.float32)
+    return ts, [a.cpu().numpy().copy() for a in r.dft_accs]
 
 
 def _compare_with_oracle(label, r, ref, n, init):
