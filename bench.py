@@ -438,6 +438,20 @@ def run_secondary(args, which):
         alg = 3 * plan.algorithmic_bytes_per_step()
         metric = "Mcell-steps/s fwd+adjoint grad (checkpoint every 64), 1 B200"
         kernel = "fwd_step_kernel x2 + adj_step_kernel (whole step)"
+    # launch configuration of this plan chosen by the autotuner (trial runs
+    # before the warm-up; every timed run starts from a reset state)
+    launch = {"chosen_by": "defaults", "config": plan.launch_config()[0]}
+    if not args.no_autotune:
+        from rfx_b200.autotune import autotune
+        if which == "adjoint_region":
+            res = autotune(plan, lambda: runner.forward(), one, repeats=1)
+            launch = {"chosen_by": "rfx_b200.autotune (whole forward / forward + adjoint runs per candidate)",
+                      **res.as_json()}
+        else:
+            T = min(64, N)
+            res = autotune(plan, lambda: plan.advance(0, T, r.src_table, r.probe_out, r.dft_accs, r.dft_phases),
+                           None, repeats=2)
+            launch = {"chosen_by": f"rfx_b200.autotune ({T} trial steps per candidate)", **res.as_json()}
     for _ in range(args.warmup):
         one()
     torch.cuda.synchronize()
@@ -460,7 +474,7 @@ def run_secondary(args, which):
             "roofline": {"kernel": kernel, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                          "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "peak_source": peak_src,
                          "traffic": None, "algorithmic_bytes_per_step": int(alg)},
-            "clocks": clk.summary()}
+            "launch": launch, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     plan.close()
 
