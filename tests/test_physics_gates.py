@@ -151,3 +151,63 @@ def test_cuda_cavity_resonance_follows_yee_dispersion(cuda):
     f = _peak_frequency(np.asarray(r.time_series)[:, 0], g.dt, f_yee)
     _dispersion_gate(f, g.dt, "CUDA")
     assert abs(f - f_yee) / f_yee < 1e-6
+
+
+def _cuda_reflection_db(n_layers, n_steps=160):
+    """The CPML reflection measurement of the oracle gate
+    (tests/test_cpml.py:43-110 as restated in tests/test_oracle.py) through
+    ``rfx_b200.run``: peak deviation of an n-layer CPML run from a free-space
+    run whose PEC walls are too far to echo within the window."""
+    import rfx_b200
+    f0, freq_max = 2e9, 5e9
+    dx = oracle.C0 / freq_max / 20.0
+    dt = dx / (oracle.C0 * np.sqrt(3.0)) * 0.99
+    ref_extent = 1.15 * n_steps * dt * oracle.C0
+    out = []
+    for extent, layers, bnd in ((ref_extent, 0, "pec"), (0.06, n_layers, "cpml")):
+        og = oracle.make_uniform_grid((extent,) * 3, dx, cpml_layers=layers)
+        g = rfx_b200.Grid(freq_max=freq_max, domain=(extent,) * 3, dx=dx, cpml_layers=layers)
+        assert tuple(g.shape) == tuple(og.shape)
+        c = (g.nx // 2, g.ny // 2, g.nz // 2)
+        w = oracle.gaussian_pulse(np.arange(n_steps, dtype=np.float32) * np.float32(og.dt), f0, 0.5)
+        mats = rfx_b200.MaterialArrays(*(np.full(g.shape, v, np.float32) for v in (1.0, 0.0, 1.0)))
+        r = rfx_b200.run(g, mats, n_steps, boundary=bnd, pec_axes="xyz" if bnd == "pec" else "",
+                         sources=[rfx_b200.SourceSpec(*c, "ez", w.astype(np.float32))],
+                         probes=[rfx_b200.ProbeSpec(c[0] + 3, c[1], c[2], "ez")])
+        out.append(np.asarray(r.time_series)[:, 0].astype(np.float64))
+    ref, cp = out
+    return 20 * np.log10(np.max(np.abs(cp - ref)) / np.max(np.abs(ref)))
+
+
+@pytest.mark.gpu
+def test_cuda_cpml_reflection_gate(cuda):
+    """tests/test_cpml.py:130-184 on the CUDA path: an 8-layer CPML stays
+    below -55 dB and a 2-layer one reflects more."""
+    db8, db2 = _cuda_reflection_db(8), _cuda_reflection_db(2)
+    print(f"CUDA CPML reflection: 8 layers {db8:.1f} dB, 2 layers {db2:.1f} dB")
+    assert db8 < -55
+    assert db2 > db8
+
+
+@pytest.mark.gpu
+def test_cuda_nonuniform_reduces_to_uniform(cuda):
+    """tests/test_nonuniform_uniform_end_to_end_reduction.py on the CUDA path:
+    a graded grid with a constant profile reproduces the uniform lane (PEC
+    faces, same dt, sources and probes) until the graded lane's extra
+    bounding cell can influence the probes."""
+    import rfx_b200
+    dx, n, steps = 1e-3, 14, 80
+    gnu = rfx_b200.make_nonuniform_grid((n * dx, n * dx), np.full(n, dx), dx, cpml_layers=0)
+    nx, ny, nz = (int(v) for v in gnu.shape)
+    gu = rfx_b200.Grid(freq_max=10e9, domain=((nx - 1) * dx, (ny - 1) * dx, (nz - 1) * dx), dx=dx, cpml_layers=0)
+    assert tuple(gu.shape) == (nx, ny, nz) and abs(gu.dt - gnu.dt) <= 1e-9 * gnu.dt
+    mats = rfx_b200.MaterialArrays(*(np.full((nx, ny, nz), v, np.float32) for v in (1.0, 0.0, 1.0)))
+    w = oracle.gaussian_pulse(np.arange(steps, dtype=np.float32) * np.float32(gnu.dt), 60e9, 0.8).astype(np.float32)
+    prb = [(9, 7, 7, "ez"), (7, 9, 8, "ex")]
+    a = rfx_b200.run_nonuniform(gnu, mats, steps, sources=[(7, 7, 7, "ez", w)], probes=prb)["time_series"]
+    b = rfx_b200.run(gu, mats, steps, boundary="pec", pec_axes="xyz", sources=[rfx_b200.SourceSpec(7, 7, 7, "ez", w)],
+                     probes=[rfx_b200.ProbeSpec(*p) for p in prb]).time_series
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    e = float(np.linalg.norm(a[:20] - b[:20]) / np.linalg.norm(b[:20]))
+    print(f"CUDA graded-to-uniform reduction, first 20 steps: relL2 {e:.2e}")
+    assert e < 1e-5 and np.abs(b[:20]).max() > 0
