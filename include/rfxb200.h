@@ -297,6 +297,12 @@ int rfxb_forward_noalloc(const RfxbDesc* desc, const float* eps_r_dev, const flo
  * overwritten) to *energy_dev in stream order: the interior-energy check of
  * run_until_decay (rfx/simulation.py:2493-2505). */
 int rfxb_plan_box_energy(RfxbPlan* plan, const int* box, double* energy_dev, void* stream);
+/* The same sum with every cell weighted by wx[i] * wy[j] * wz[k] (device
+ * float64 tables of length nx, ny, nz): the graded lane's interior-energy
+ * check, weighted by the primal cell volume dx[i] dy[j] dz[k]
+ * (rfx/nonuniform.py:2143-2156). */
+int rfxb_plan_box_energy_weighted(RfxbPlan* plan, const int* box, const double* wx_dev, const double* wy_dev,
+                                  const double* wz_dev, double* energy_dev, void* stream);
 
 /* Net outgoing co-located Poynting flux through the faces of the box
  * (faces at i = box[0] and i = box[1], j = box[2] and box[3], k = box[4] and

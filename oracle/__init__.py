@@ -23,7 +23,8 @@ from .fdtd import (  # noqa: F401
     profile_to_inv_arrays, cpml_profile, build_cpml,
     gaussian_pulse, j_source_waveform, current_source_waveform,
     port_source_waveform, port_sigma,
-    tangential_edge_masks, run_uniform, run_nonuniform, run_until_decay_uniform, OracleResult,
+    tangential_edge_masks, run_uniform, run_nonuniform, run_until_decay_uniform, run_until_decay_nonuniform,
+    OracleResult,
     NTFF_FACES, ntff_init, ntff_phases, ntff_step,
 )
 from . import farfield  # noqa: F401

@@ -748,6 +748,25 @@ def run_nonuniform(grid, materials, n_steps, *, sources=(), probes=(), dft_plane
                 probes_before_dft=False, dx_vi=grid.dx, ntff=ntff, flux_monitors=flux_monitors)
 
 
+def _box_flux(F, flux_box):
+    """Net outgoing co-located Poynting flux through the faces of the index
+    box (i0, i1, j0, j1, k0, k1): float32 products, float64 sum
+    (rfx/simulation.py:2513-2540, rfx/nonuniform.py:2171-2184)."""
+    i0, i1, j0, j1, k0, k1 = flux_box
+    f32 = np.float32
+    g = {c: F[c] for c in COMPONENTS}
+    jj, kk, ii = slice(j0, j1), slice(k0, k1), slice(i0, i1)
+
+    def term(a, b, c, d, sel):
+        return np.sum(((g[a][sel] * g[b][sel]).astype(f32) - (g[c][sel] * g[d][sel]).astype(f32))
+                      .astype(np.float64))
+
+    p = term("ey", "hz", "ez", "hy", (i1, jj, kk)) - term("ey", "hz", "ez", "hy", (i0, jj, kk))
+    p += term("ez", "hx", "ex", "hz", (ii, j1, kk)) - term("ez", "hx", "ex", "hz", (ii, j0, kk))
+    p += term("ex", "hy", "ey", "hx", (ii, jj, k1)) - term("ex", "hy", "ey", "hx", (ii, jj, k0))
+    return float(p)
+
+
 def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100,
                             max_steps=50_000, decay_energy_consecutive=2, monitor=None, boundary="pec",
                             cpml_axes="xyz", pec_axes=None, sources=(), probes=(), pec_mask=None,
@@ -779,19 +798,7 @@ def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50
     state = {"peak_U": 0.0, "below": 0, "peak_sq": 0.0, "steps": 0, "peak_flux": 0.0, "hist": []}
 
     def radiated_power(F):
-        i0, i1, j0, j1, k0, k1 = flux_box
-        f32 = np.float32
-        g = {c: F[c] for c in COMPONENTS}
-        jj, kk, ii = slice(j0, j1), slice(k0, k1), slice(i0, i1)
-
-        def term(a, b, c, d, sel):
-            return np.sum(((g[a][sel] * g[b][sel]).astype(f32) - (g[c][sel] * g[d][sel]).astype(f32))
-                          .astype(np.float64))
-
-        p = term("ey", "hz", "ez", "hy", (i1, jj, kk)) - term("ey", "hz", "ez", "hy", (i0, jj, kk))
-        p += term("ez", "hx", "ex", "hz", (ii, j1, kk)) - term("ez", "hx", "ex", "hz", (ii, j0, kk))
-        p += term("ex", "hy", "ey", "hx", (ii, jj, k1)) - term("ex", "hy", "ey", "hx", (ii, jj, k0))
-        return float(p)
+        return _box_flux(F, flux_box)
 
     def stop(n, F):
         state["steps"] = n + 1
@@ -826,3 +833,64 @@ def run_until_decay_uniform(grid, materials, *, decay_by=1e-3, check_interval=50
 
     res = _run(st, max_steps, sources, probes, (), (), 1, probes_before_dft=True, dx_vi=grid.dx, stop=stop)
     return res, state["steps"]
+
+
+def run_until_decay_nonuniform(grid, materials, *, decay_by=1e-3, check_interval=50, min_steps=100,
+                               max_steps=50_000, decay_energy_consecutive=2, sources=(), probes=(),
+                               pec_mask=None, dtype=np.float32, flux_box=None, flux_env_checks=4,
+                               dx_arr=None, dy_arr=None):
+    """``rfx.nonuniform.run_nonuniform_until_decay`` (rfx/nonuniform.py:1988-2260),
+    energy and radiated-flux stops.  Checks fall after every ``check_interval``
+    steps (and after the last, shorter chunk): the energy U = sum((E^2 + H^2)
+    dV) over the non-CPML cells, dV = dx[i] dy[j] dz[k] from the padded
+    per-axis cell sizes (``dx_arr``, ``dy_arr``: the x and y profiles of the
+    grid, ``grid.dz`` for z), once ``min_steps`` are done, peak updated before
+    the compare, ``decay_energy_consecutive`` consecutive checks below
+    decay_by * peak stop; with ``flux_box`` (index box) the |net flux| is
+    tracked from the first check, enveloped over the last ``flux_env_checks``
+    checks, and gated on ``min_steps``.  Returns (OracleResult, steps run,
+    [(steps, U, peak U), ...])."""
+    axes = "".join(a for a, p in zip("xyz", (grid.pads[0] + grid.pads[1], grid.pads[2] + grid.pads[3],
+                                             grid.pads[4] + grid.pads[5])) if p > 0)
+    st = _Stepper(grid, materials, dtype=dtype, nonuniform=True,
+                  cpml_axes=axes if grid.cpml_layers > 0 else "",
+                  pec_axes="xyz", pec_mask=pec_mask, kappa_max=1.0)
+    p = grid.pads
+    sl = (slice(p[0], grid.nx - p[1]), slice(p[2], grid.ny - p[3]), slice(p[4], grid.nz - p[5]))
+    dx_arr = np.full(grid.nx, grid.dx) if dx_arr is None else np.asarray(dx_arr, np.float64)
+    dy_arr = np.full(grid.ny, grid.dx) if dy_arr is None else np.asarray(dy_arr, np.float64)
+    dV = (dx_arr[sl[0], None, None] * dy_arr[None, sl[1], None] *
+          np.asarray(grid.dz, np.float64)[None, None, sl[2]])
+    state = {"peak_U": 0.0, "below": 0, "steps": 0, "peak_flux": 0.0, "hist": [], "checks": []}
+
+    def stop(n, F):
+        done = n + 1
+        state["steps"] = done
+        if done % check_interval != 0 and done != max_steps:
+            return False
+        if flux_box is not None:
+            state["hist"].append(abs(_box_flux(F, flux_box)))
+            env = max(state["hist"][-flux_env_checks:])
+            state["peak_flux"] = max(state["peak_flux"], env)
+            if done >= min_steps and state["peak_flux"] > 0.0 and env < decay_by * state["peak_flux"]:
+                state["below"] += 1
+                return state["below"] >= decay_energy_consecutive
+            state["below"] = 0
+            return False
+        if done < min_steps:
+            return False
+        U = float(sum(np.sum(np.asarray(F[c][sl], np.float64) ** 2 * dV) for c in COMPONENTS))
+        state["peak_U"] = max(state["peak_U"], U)
+        state["checks"].append((done, U, state["peak_U"]))
+        if U < decay_by * state["peak_U"]:
+            state["below"] += 1
+            return state["below"] >= decay_energy_consecutive
+        state["below"] = 0
+        return False
+
+    src = []
+    for (i, j, k, comp, w) in sources:
+        w = np.asarray(w, np.float32)[:max_steps]
+        src.append((i, j, k, comp, np.concatenate([w, np.zeros(max_steps - len(w), np.float32)])))
+    res = _run(st, max_steps, src, probes, (), (), 0, probes_before_dft=False, dx_vi=grid.dx, stop=stop)
+    return res, state["steps"], state["checks"]

@@ -18,7 +18,7 @@ from .sources import (  # noqa: F401
     GaussianPulse, LumpedPort, SourceSpec, make_current_source, make_j_source, make_port_source,
     make_source, setup_lumped_port,
 )
-from .nonuniform import run_nonuniform  # noqa: F401
+from .nonuniform import run_nonuniform, run_nonuniform_until_decay  # noqa: F401
 from .checkpoint import (  # noqa: F401
     load_plan_state, load_snapshots, load_state, save_plan_state, save_snapshots, save_state,
 )

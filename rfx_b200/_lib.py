@@ -116,6 +116,8 @@ SIGNATURES = {
     "rfxb_plan_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rfxb_batch_device_status": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rfxb_plan_box_energy": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),
+    "rfxb_plan_box_energy_weighted": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_void_p]),
     "rfxb_plan_box_flux": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p]),
     "rfxb_plan_state_bytes": (C.c_longlong, [C.c_void_p]),
     "rfxb_plan_save_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -38,7 +38,8 @@ __global__ void adj_init_kernel(const RfxbInst*, const AdjInst*, int, int, int);
 __global__ void dft_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbDftPlane*, int, int, int);
 __global__ void ntff_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbNtffFace*, int, int, int);
 __global__ void flux_adj_kernel(const RfxbInst*, const AdjInst*, const RfxbFluxPlane*, int, int, int);
-__global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
+__global__ void box_energy_kernel(RfxbInst, int, int, int, int, int, int, int, const double*, const double*,
+                                  const double*, double*);
 __global__ void box_flux_kernel(RfxbInst, int, int, int, int, int, int, int, double*);
 __global__ void flux_kernel(const RfxbInst*, const RfxbFluxPlane*, int, int, int);
 __global__ void ntff_kernel(const RfxbInst*, const RfxbNtffFace*, int, int, int);
@@ -1984,7 +1985,9 @@ int rfxb_batch_device_status(RfxbBatch* g, void* stream) {
   return 0;
 }
 
-int rfxb_plan_box_energy(RfxbPlan* p, const int* b, double* out, void* stream) {
+namespace {
+int box_energy(RfxbPlan* p, const int* b, const double* wx, const double* wy, const double* wz, double* out,
+               void* stream) {
   if (!p || !b || !out) return fail(RFXB_E_INVALID, "plan, box and output are required");
   if (b[0] < 0 || b[1] > p->nx || b[2] < 0 || b[3] > p->ny || b[4] < 0 || b[5] > p->nz || b[0] >= b[1] ||
       b[2] >= b[3] || b[4] >= b[5])
@@ -1993,9 +1996,20 @@ int rfxb_plan_box_energy(RfxbPlan* p, const int* b, double* out, void* stream) {
   RFXB_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
   const long long cells = (long long)(b[1] - b[0]) * (b[3] - b[2]) * (b[5] - b[4]);
   const int blocks = (int)std::max<long long>(1, std::min<long long>((cells + 255) / 256, 8LL * sm_count()));
-  box_energy_kernel<<<blocks, 256, 0, st>>>(p->inst, p->par, b[0], b[1], b[2], b[3], b[4], b[5], out);
+  box_energy_kernel<<<blocks, 256, 0, st>>>(p->inst, p->par, b[0], b[1], b[2], b[3], b[4], b[5], wx, wy, wz, out);
   RFXB_CUDA(cudaGetLastError());
   return 0;
+}
+}  // namespace
+
+int rfxb_plan_box_energy(RfxbPlan* p, const int* b, double* out, void* stream) {
+  return box_energy(p, b, nullptr, nullptr, nullptr, out, stream);
+}
+
+int rfxb_plan_box_energy_weighted(RfxbPlan* p, const int* b, const double* wx_dev, const double* wy_dev,
+                                  const double* wz_dev, double* out, void* stream) {
+  if (!wx_dev || !wy_dev || !wz_dev) return fail(RFXB_E_INVALID, "the three weight tables are required");
+  return box_energy(p, b, wx_dev, wy_dev, wz_dev, out, stream);
 }
 
 int rfxb_plan_box_flux(RfxbPlan* p, const int* b, double* out, void* stream) {

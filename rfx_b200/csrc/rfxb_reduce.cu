@@ -10,7 +10,9 @@
 namespace rfxb {
 
 __global__ void __launch_bounds__(256) box_energy_kernel(RfxbInst P, int par, int i0, int i1, int j0, int j1, int k0,
-                                                         int k1, double* __restrict__ out) {
+                                                         int k1, const double* __restrict__ wx,
+                                                         const double* __restrict__ wy,
+                                                         const double* __restrict__ wz, double* __restrict__ out) {
   const int nk = k1 - k0, nj = j1 - j0;
   const long long total = (long long)(i1 - i0) * nj * nk;
   double acc = 0.0;
@@ -27,7 +29,8 @@ __global__ void __launch_bounds__(256) box_energy_kernel(RfxbInst P, int par, in
       const float v = P.F[par][c][e];
       s = fmaf(v, v, s);
     }
-    acc += (double)s;
+    // graded lane: weighted by the cell volume dx[i] dy[j] dz[k]
+    acc += wx ? (double)s * (wx[i] * wy[j] * wz[k]) : (double)s;
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   __shared__ double part[8];

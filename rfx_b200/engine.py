@@ -232,6 +232,21 @@ class Plan:
               "rfxb_plan_box_energy")
         return out
 
+    def box_energy_weighted(self, box, wx, wy, wz, out=None):
+        """As ``box_energy`` with cell (i, j, k) weighted by wx[i] wy[j] wz[k]
+        (float64 device tensors of length nx, ny, nz)."""
+        if out is None:
+            out = torch.empty((), device=self.device, dtype=torch.float64)
+        ws = [w.to(device=self.device, dtype=torch.float64).contiguous() for w in (wx, wy, wz)]
+        for w, n in zip(ws, self.shape):
+            if w.numel() != n:
+                raise ValueError("weight tables must have lengths nx, ny, nz")
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        check(self._lib.rfxb_plan_box_energy_weighted(self._h, b, *[C.c_void_p(w.data_ptr()) for w in ws],
+                                                      C.c_void_p(out.data_ptr()), _stream()),
+              "rfxb_plan_box_energy_weighted")
+        return out
+
     def box_flux(self, box, out=None):
         """Device scalar (float64 tensor) of the net outgoing co-located
         Poynting flux through the faces of ``box`` = (i0, i1, j0, j1, k0, k1)

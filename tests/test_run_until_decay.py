@@ -106,3 +106,87 @@ def test_radiated_flux_stop_matches_oracle(cuda):
     assert n == steps
     for p in range(len(probes)):
         assert rel_l2(out.time_series[:, p], res.time_series[:, p]) < TOL
+
+
+# ---------------------------------------------------------------------------
+# graded lane: rfx.nonuniform.run_nonuniform_until_decay (rfx/nonuniform.py:1988-2260)
+
+GDZ = 1e-3 * np.array([1.0, 0.9, 0.75, 0.6, 0.5, 0.5, 0.6, 0.75, 0.9, 1.0, 1.0, 1.0, 0.8, 0.7, 0.8, 1.0])
+GKW = dict(decay_by=1e-3, check_interval=50, min_steps=100, max_steps=3000, decay_energy_consecutive=2)
+GFLUX_BOX = ((0.004, 0.004, 0.003), (0.018, 0.016, 0.010))
+
+
+def _graded_scene():
+    dx = 1e-3
+    g = oracle.make_nonuniform_grid((0.022, 0.020), GDZ, dx, cpml_layers=6)
+    eps = np.ones(g.shape, np.float32)
+    eps[10:18, 9:15, 8:13] = np.float32(2.5)
+    mats = (eps, np.zeros(g.shape, np.float32), np.ones(g.shape, np.float32))
+    t = np.arange(GKW["max_steps"], dtype=np.float32) * np.float32(g.dt)
+    w = (oracle.gaussian_pulse(t, 20e9, 0.8) * 50.0).astype(np.float32)
+    src = [(g.nx // 2 - 2, g.ny // 2, g.nz // 2, "ez", w)]
+    probes = [(g.nx // 2 + 3, g.ny // 2, g.nz // 2, "ez"), (g.nx // 2, g.ny // 2 + 2, g.nz // 2 - 1, "hx")]
+    return g, mats, src, probes
+
+
+def _product_graded_grid():
+    import rfx_b200
+    return rfx_b200.make_nonuniform_grid((0.022, 0.020), GDZ, 1e-3, cpml_layers=6)
+
+
+def test_graded_position_to_index():
+    """Nearest interior cell edge per axis plus the low pad
+    (rfx/nonuniform.py:477-524); with uniform x/y cells it reduces to
+    round(pos / dx) + pad, and on z it follows the graded edges."""
+    from rfx_b200.nonuniform import position_to_index
+    g = _product_graded_grid()
+    assert position_to_index(g, (0.0, 0.0, 0.0)) == (6, 6, 6)
+    assert position_to_index(g, (0.0104, 0.0196, 0.0)) == (6 + 10, 6 + 20, 6)
+    edges = np.insert(np.cumsum(GDZ), 0, 0.0)
+    for q in (3, 7, 12):
+        assert position_to_index(g, (0.0, 0.0, edges[q] + 1e-6))[2] == 6 + q
+
+
+def _oracle_graded(flux):
+    g, mats, srcs, probes = _graded_scene()
+    box = None
+    if flux:
+        from rfx_b200.nonuniform import position_to_index
+        pg = _product_graded_grid()
+        lo, hi = (position_to_index(pg, c) for c in GFLUX_BOX)
+        box = (lo[0], hi[0], lo[1], hi[1], lo[2], hi[2])
+    return oracle.run_until_decay_nonuniform(g, mats, sources=srcs, probes=probes, flux_box=box, **GKW)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("flux", [False, True])
+def test_oracle_graded_run_until_decay_stops(flux):
+    res, steps, checks = _oracle_graded(flux)
+    print("graded", "flux" if flux else "energy", "stop: oracle after", steps, "steps")
+    assert GKW["min_steps"] <= steps < GKW["max_steps"]
+    assert steps % GKW["check_interval"] == 0          # checks after k * interval steps
+    assert res.time_series.shape[0] == steps
+    if not flux:
+        assert checks[-1][0] == steps and all(u >= 0 for _, u, _ in checks)
+        assert all(u < GKW["decay_by"] * p for _, u, p in checks[-2:])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flux", [False, True])
+def test_graded_run_until_decay_matches_oracle(cuda, flux):
+    import rfx_b200
+    g, mats, srcs, probes = _graded_scene()
+    res, steps, checks = _oracle_graded(flux)
+    pg = _product_graded_grid()
+    assert tuple(pg.shape) == tuple(g.shape)
+    out = rfx_b200.run_nonuniform_until_decay(pg, rfx_b200.MaterialArrays(*mats), sources=srcs, probes=probes,
+                                              radiated_flux_box=GFLUX_BOX if flux else None, **GKW)
+    n = out["time_series"].shape[0]
+    print("graded", "flux" if flux else "energy", "stop: CUDA after", n, "steps; oracle", steps)
+    assert n == steps and out["state"].step == steps
+    for p in range(len(probes)):
+        assert rel_l2(out["time_series"][:, p], res.time_series[:, p]) < TOL
+    if not flux:
+        assert len(out["decay_checks"]) == len(checks)
+        for (s1, u1, p1), (s2, u2, p2) in zip(out["decay_checks"], checks):
+            assert s1 == s2 and abs(u1 - u2) <= 1e-3 * p2
