@@ -190,3 +190,18 @@ def test_graded_run_until_decay_matches_oracle(cuda, flux):
         assert len(out["decay_checks"]) == len(checks)
         for (s1, u1, p1), (s2, u2, p2) in zip(out["decay_checks"], checks):
             assert s1 == s2 and abs(u1 - u2) <= 1e-3 * p2
+
+
+def test_graded_run_until_decay_rejects_bad_arguments():
+    """The reference's argument checks (rfx/nonuniform.py:2096-2100) and the
+    features outside this path, raised before any device work."""
+    import rfx_b200
+    g, mats, srcs, probes = _graded_scene()
+    pg = _product_graded_grid()
+    m = rfx_b200.MaterialArrays(*mats)
+    with pytest.raises(ValueError, match="check_interval"):
+        rfx_b200.run_nonuniform_until_decay(pg, m, check_interval=0, sources=srcs)
+    with pytest.raises(ValueError, match="max_steps"):
+        rfx_b200.run_nonuniform_until_decay(pg, m, max_steps=0, sources=srcs)
+    with pytest.raises(NotImplementedError):
+        rfx_b200.run_nonuniform_until_decay(pg, m, debye=((1.0,), (1e-9,)), sources=srcs)
