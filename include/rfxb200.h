@@ -286,9 +286,14 @@ int rfxb_batch_device_status(RfxbBatch* batch, void* stream);
  * internal state lives in one fixed 64 MiB device array inside the library:
  * grids whose state does not fit (about 0.8 M cells) get RFXB_E_NOMEM, and DFT
  * planes or gradient regions get RFXB_E_INVALID (use a plan for those).  The
- * first call on a device looks up the array's address (make it before any
- * stream capture).  Calls share the array: each clears what must start at
- * zero, and two calls whose GPU work overlaps race on it. */
+ * first call on a device sets it up (the array's address, the kernel's
+ * shared-memory limit); make that first call before any stream capture.  Each
+ * call uploads small host tables from memory that lives only during the call,
+ * so a call on a capturing stream is refused with RFXB_E_INVALID; no call may
+ * follow a cudaDeviceReset of the device.  Calls share the array: each clears
+ * what must start at zero, and two calls whose GPU work overlaps race on it.
+ * Negative counts and null source / probe tables with a positive count are
+ * refused with RFXB_E_INVALID. */
 int rfxb_forward_noalloc(const RfxbDesc* desc, const float* eps_r_dev, const float* sigma_dev,
                          float* const* fields_dev, const RfxbStepIO* io, int step0, int n_steps, void* stream);
 

@@ -1495,6 +1495,11 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
       if ((d->cpml_axes >> a) & 1u)
         if (dims[a] < 2 * ncp) return fail(RFXB_E_SHAPE, "CPML slabs of one axis overlap (axis shorter than 2*cpml_layers)");
   }
+  if (d->n_src < 0 || d->n_probe < 0 || d->n_dft < 0 || d->n_flux < 0)
+    return fail(RFXB_E_INVALID, "negative source, probe, DFT-plane or flux-monitor count");
+  if ((d->n_src > 0 && !d->src_cells_host) || (d->n_probe > 0 && !d->probe_cells_host) ||
+      (d->n_dft > 0 && !d->dft_host) || (d->n_flux > 0 && !d->flux_host))
+    return fail(RFXB_E_INVALID, "null source, probe, DFT-plane or flux-monitor table with a positive count");
   for (int s = 0; s < d->n_src; ++s) {
     const int32_t* c = d->src_cells_host + 4 * s;
     if (c[0] < 0 || c[0] >= d->nx || c[1] < 0 || c[1] >= d->ny || c[2] < 0 || c[2] >= d->nz || c[3] < 0 || c[3] > 2)

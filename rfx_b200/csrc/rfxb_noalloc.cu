@@ -14,9 +14,14 @@
 //
 // Properties a caller must know:
 //  * every GPU that loads the library holds the array until the process exits;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture;
+//  * the first call on a device sets that device up with it current: it looks
+//    up the array's device address (cudaGetSymbolAddress) and raises the step
+//    kernel's dynamic shared-memory limit; make that first call before any
+//    stream capture.  The address is kept for the life of the process, so a
+//    cudaDeviceReset of that device leaves it stale: no call may follow one;
+//  * every call uploads small host tables (descriptor, work list, CPML
+//    profile, sources, probes) from memory that only lives during the call,
+//    so a call on a stream that is capturing is refused with RFXB_E_INVALID;
 //  * all calls share the array and it keeps the last call's contents: each
 //    call clears what must start at zero (fields' guards, the second field
 //    buffer, psi), so calls are independent, but two calls whose work
@@ -28,7 +33,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/rfxb200.h"
 #include "rfxb_common.cuh"
@@ -59,25 +66,44 @@ int noalloc_fail(int code, const char* msg) {
   return code;
 }
 
-// Device address of the scratch array, looked up once per device.
+// Per-device set-up, done once with that device current: the device address
+// of the scratch array, and the step kernel's dynamic shared-memory opt-in
+// (its stages take close to the 48 KB default).  Host threads may race to the
+// first call: the lock makes one of them do the set-up, the atomic publishes
+// the address to the others.
 unsigned char* scratch_address(int* rc) {
-  static unsigned char* addr[64] = {nullptr};
+  constexpr int kMaxDev = 64;
+  static std::atomic<unsigned char*> addr[kMaxDev];
+  static std::mutex mu;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) {
     *rc = noalloc_fail(RFXB_E_LAUNCH, "rfxb_forward_noalloc: no current CUDA device");
     return nullptr;
   }
-  if (!addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_rfxb_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      *rc = noalloc_fail(RFXB_E_LAUNCH, "rfxb_forward_noalloc: cudaGetSymbolAddress of the scratch array failed");
-      return nullptr;
+  unsigned char* a = addr[dev].load(std::memory_order_acquire);
+  if (!a) {
+    std::lock_guard<std::mutex> lock(mu);
+    a = addr[dev].load(std::memory_order_relaxed);
+    if (!a) {
+      const cudaError_t ea = cudaFuncSetAttribute(reinterpret_cast<const void*>(fwd_step_kernel<8, 0, false>),
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)fwd_step_smem_bytes(0));
+      if (ea != cudaSuccess) {
+        *rc = noalloc_fail(RFXB_E_LAUNCH, "rfxb_forward_noalloc: raising the step kernel's shared-memory limit failed");
+        return nullptr;
+      }
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_rfxb_noalloc_scratch);
+      if (e != cudaSuccess || p == nullptr) {
+        *rc = noalloc_fail(RFXB_E_LAUNCH, "rfxb_forward_noalloc: cudaGetSymbolAddress of the scratch array failed");
+        return nullptr;
+      }
+      a = static_cast<unsigned char*>(p);
+      addr[dev].store(a, std::memory_order_release);
     }
-    addr[dev] = static_cast<unsigned char*>(p);
   }
   *rc = 0;
-  return addr[dev];
+  return a;
 }
 
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
@@ -112,6 +138,12 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   for (int a = 0; a < 3; ++a)
     if (ncp > 0 && ((d->cpml_axes >> a) & 1u) && dims[a] < 2 * ncp)
       return noalloc_fail(RFXB_E_SHAPE, "rfxb_forward_noalloc: CPML slabs of one axis overlap");
+  if (d->n_src < 0 || d->n_probe < 0)
+    return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: negative source or probe count");
+  if (d->n_src > 0 && !d->src_cells_host)
+    return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: null source cell table");
+  if (d->n_probe > 0 && !d->probe_cells_host)
+    return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: null probe cell table");
   for (int s = 0; s < d->n_src; ++s) {
     const int32_t* c = d->src_cells_host + 4 * s;
     if (c[0] < 0 || c[0] >= d->nx || c[1] < 0 || c[1] >= d->ny || c[2] < 0 || c[2] >= d->nz || c[3] < 0 || c[3] > 2)
@@ -178,6 +210,11 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   unsigned char* base = scratch_address(&rc);
   if (!base) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+    return noalloc_fail(RFXB_E_INVALID, "rfxb_forward_noalloc: the stream is capturing (or its capture state is "
+                                        "unknown); this entry point uploads host tables that live only during "
+                                        "the call");
 
   // --- descriptor pointers into the scratch ---
   float* coef = reinterpret_cast<float*>(base + o_coef);

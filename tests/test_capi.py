@@ -179,3 +179,32 @@ def test_unsupported_features_raise():
         rfx_b200.run(g, mats, 10, periodic=(True, False, False))
     with pytest.raises(ValueError):
         rfx_b200.run(g, mats, 10, checkpoint_segments=3)
+
+
+@pytest.mark.parametrize("n_src,n_probe,null_src,null_prb", [
+    (-1, 0, False, False), (0, -2, False, False), (1, 0, True, False), (0, 1, False, True),
+])
+def test_negative_counts_and_null_tables_rejected(n_src, n_probe, null_src, null_prb):
+    """Negative source / probe counts, and a null cell table with a positive
+    count, are refused with RFXB_E_INVALID by plan creation and by the no-alloc
+    forward entry point, before any CUDA call (so on a host without a GPU)."""
+    lib = _lib.load()
+    src = np.array([[1, 1, 1, 2]], np.int32)
+    prb = np.array([[2, 2, 2, 2]], np.int32)
+    over = dict(n_src=n_src, n_probe=n_probe)
+    if not null_src:
+        over["src_cells_host"] = src.ctypes.data_as(_lib.c_int32_p)
+    if not null_prb:
+        over["probe_cells_host"] = prb.ctypes.data_as(_lib.c_int32_p)
+    d, keep = _desc(**over)
+    h = C.c_void_p()
+    assert lib.rfxb_plan_create(C.byref(d), C.byref(h)) == -1
+    assert h.value is None
+    assert "count" in lib.rfxb_last_error().decode()
+    # placeholder device addresses: the arguments are refused before any use
+    fake = C.c_void_p(0x1000)
+    fields = (C.c_void_p * 6)(*([0x1000] * 6))
+    rc = lib.rfxb_forward_noalloc(C.byref(d), fake, fake, fields, None, 0, 1, None)
+    assert rc == -1
+    msg = lib.rfxb_last_error().decode()
+    assert "count" in msg or "table" in msg, msg

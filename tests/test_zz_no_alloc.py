@@ -1,11 +1,15 @@
 """``rfxb_forward_noalloc`` (forward steps in the library's fixed device
 array, no allocation) against ``rfxb_forward`` on a freshly reset plan, both
 through the C ABI.  Collected last so that it also runs after every other GPU
-test in the same process."""
+test in the same process; one test also runs it in a fresh process whose first
+library call is this entry point (no plan created before it)."""
 
 from __future__ import annotations
 
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -105,3 +109,76 @@ def test_noalloc_rejects_oversized_grid(cuda):
     fields = [torch.zeros((n, n, n), device="cuda") for _ in range(6)]
     with pytest.raises(RuntimeError, match=r"code -\d+\).*64 MiB"):
         forward_noalloc(spec, eps, sig, fields, None, None, 0, 4)
+
+
+def _compare(seed, step0, n, scale, noalloc_first):
+    """One scene through both paths; returns the worst relative L2 over the
+    fields and the probe series."""
+    n_total = step0 + n
+    sc, spec, src, f0 = _case(seed, n_total, scale)
+    if noalloc_first:
+        got_f, got_p = _via_noalloc(spec, sc, src, f0, step0, n, n_total)
+        ref_f, ref_p = _via_plan(spec, sc, src, f0, step0, n, n_total)
+    else:
+        ref_f, ref_p = _via_plan(spec, sc, src, f0, step0, n, n_total)
+        got_f, got_p = _via_noalloc(spec, sc, src, f0, step0, n, n_total)
+    assert all(np.isfinite(a).all() for a in got_f)
+    assert float(np.abs(ref_p[step0:]).max()) > 0.0
+    errs = [rel_l2(a, b) for a, b in zip(got_f, ref_f)] + [rel_l2(got_p[step0:], ref_p[step0:])]
+    return max(errs)
+
+
+def fresh_process_main():
+    """Entry of the fresh-process test: the no-alloc call is the first thing
+    the library does on the device (it does its own per-device set-up, the
+    kernel's shared-memory opt-in included), then the plan path, twice."""
+    import torch
+    torch.cuda.set_device(0)
+    worst = max(_compare(3, 0, 60, 0.0, True), _compare(4, 10, 50, 1e-3, True))
+    print(f"fresh-process worst relL2 {worst:.3e}")
+    if not worst < TOL:
+        raise SystemExit(f"no-alloc path disagrees with the plan path: {worst:.3e}")
+
+
+@pytest.mark.gpu
+def test_noalloc_first_call_in_a_fresh_process(cuda):
+    """In a new process, with no plan created first, the no-alloc entry point
+    agrees with the plan path within 1e-4 relative L2 on two calls in a row."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", "from tests.test_zz_no_alloc import fresh_process_main; "
+                        "fresh_process_main()"], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "fresh-process worst relL2" in r.stdout
+
+
+@pytest.mark.gpu
+def test_noalloc_refused_on_a_capturing_stream(cuda):
+    """A call made while its stream is capturing a CUDA graph is refused with
+    RFXB_E_INVALID (each call uploads host tables that live only during the
+    call), and the capture itself stays usable."""
+    import torch
+    sc, spec, src, f0 = _case(2, 20, 0.0)
+    eps = torch.from_numpy(sc.materials[0]).cuda()
+    sig = torch.from_numpy(sc.materials[1]).cuda()
+    fields = [torch.from_numpy(f).cuda() for f in f0]
+    probe = torch.zeros((20, len(spec.probes)), device="cuda", dtype=torch.float32)
+    from rfx_b200.noalloc import forward_noalloc
+    forward_noalloc(spec, eps, sig, fields, src, probe, 0, 2)   # set-up outside any capture
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    err = None
+    with torch.cuda.stream(side):
+        g.capture_begin()
+        try:
+            forward_noalloc(spec, eps, sig, fields, src, probe, 0, 2)
+        except RuntimeError as e:
+            err = str(e)
+        finally:
+            g.capture_end()
+    torch.cuda.synchronize()
+    assert err is not None and "capturing" in err, err
+    # the device is still usable afterwards
+    forward_noalloc(spec, eps, sig, fields, src, probe, 0, 2)
+    torch.cuda.synchronize()
+    assert all(torch.isfinite(f).all().item() for f in fields)
