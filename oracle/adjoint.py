@@ -11,8 +11,11 @@ rfx/boundaries/cpml.py:522-1065, rfx/boundaries/pec.py:13-47, 179-208):
 
 with the eps_r derivative taken where the reference's autodiff takes it:
 ca and cb of rfx/core/yee.py:387-393 (d ca/d eps_r, d cb/d eps_r) times the
-recorded E^n and curl H^{n+1/2}.  It is used to check the CUDA adjoint and
-as the CPU baseline of the forward+adjoint workload.
+recorded E^n and curl H^{n+1/2}, and, in CPML slab cells, the E-side
+coefficient ce = dt/(eps_r eps0) of rfx/boundaries/cpml.py:536-546
+(d ce/d eps_r = -ce/eps_r) times the recorded correction
+sign * (psi + (1/kappa - 1) curl) of each axis.  It is used to check the
+CUDA adjoint and as the CPU baseline of the forward+adjoint workload.
 """
 
 from __future__ import annotations
@@ -27,6 +30,12 @@ def _coef_derivs(eps_r, sigma, dt):
     s = np.asarray(sigma, np.float64)
     L = s * dt / (2.0 * EPS_0 * e)
     return 2.0 * L / (e * (1.0 + L) ** 2), -dt * EPS_0 / (EPS_0 * e + s * dt / 2.0) ** 2
+
+
+def _ce_deriv(eps_r, dt):
+    """d ce / d eps_r of ce = dt / (eps_r eps0) (rfx/boundaries/cpml.py:536)."""
+    e = np.asarray(eps_r, np.float64)
+    return -dt / (EPS_0 * e * e)
 
 
 class _RecStepper(_Stepper):
@@ -61,6 +70,16 @@ class _RecStepper(_Stepper):
         F["ey"] = ca * F["ey"] + cb * cy
         F["ez"] = ca * F["ez"] + cb * cz
         self.step_count += 1
+
+    def cpml_e(self):
+        """CPML-E pass that also records, over the box, the correction of
+        each E component before its ce scaling (zero off the slabs)."""
+        corr = {c: np.zeros(self.g.shape, np.float64) for c in ("ex", "ey", "ez")}
+        if self.psi:
+            ce = self.g.dt / (self.eps_r * EPS_0)
+            self._apply_cpml(_CPML_E, ce, fwd=False, corr=corr)
+        b = self.box
+        self.hist[-1] = np.concatenate([self.hist[-1], np.stack([corr[c][b] for c in ("ex", "ey", "ez")])])
 
 
 def _mask_e(st, aF):
@@ -154,6 +173,7 @@ def forward_adjoint(grid, materials, n_steps, *, nonuniform=False, boundary="cpm
     ch = dt / (st.mu_r * MU_0)
     bx = st.box
     dca, dcb = _coef_derivs(st.eps_r[bx], st.sigma[bx], dt)
+    dce = _ce_deriv(st.eps_r[bx], dt)
     aF = {c: np.zeros(grid.shape, f) for c in COMPONENTS}
     apsi = {k: np.zeros_like(v) for k, v in st.psi.items()}
     grad = np.zeros(dca.shape, np.float64)
@@ -182,7 +202,7 @@ def forward_adjoint(grid, materials, n_steps, *, nonuniform=False, boundary="cpm
         _cpml_transpose(st, aF, apsi, _CPML_E, ce, fwd=False)   # CE^T
         # UE^T and the eps_r gradient
         h = st.hist[n]
-        grad += sum(aF[c][bx] * (dca * h[q] + dcb * h[3 + q]) for q, c in enumerate(("ex", "ey", "ez")))
+        grad += sum(aF[c][bx] * (dca * h[q] + dcb * h[3 + q] + dce * h[6 + q]) for q, c in enumerate(("ex", "ey", "ez")))
         qx, qy, qz = cb * aF["ex"], cb * aF["ey"], cb * aF["ez"]
         # curl_x = dHz/dy - dHy/dz, curl_y = dHx/dz - dHz/dx, curl_z = dHy/dx - dHx/dy (backward diffs)
         vyx, vzx = iy * qx, iz * qx

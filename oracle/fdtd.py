@@ -420,9 +420,13 @@ class _Stepper:
         F["ez"] = ca * F["ez"] + cb * cz
         self.step_count += 1
 
-    def _apply_cpml(self, table, coef_full, fwd):
+    def _apply_cpml(self, table, coef_full, fwd, corr=None):
         """rfx/boundaries/cpml.py:522-801 (E) and :804-1065 (H).  The curl
-        slices read the field values from before this correction pass."""
+        slices read the field values from before this correction pass.
+        ``corr`` (optional, per component float64 arrays of the grid shape)
+        accumulates each correction before its coefficient scaling,
+        sign * (psi + (1/kappa - 1) curl): the factor that d coef / d eps_r
+        multiplies in the reference's autodiff of the same two adds."""
         F, n = self.F, self.n
         src = {c: F[c] for c in COMPONENTS}
         work = {c: F[c].copy() for c in COMPONENTS}
@@ -455,6 +459,9 @@ class _Stepper:
                     else:
                         work[fc][sl] = work[fc][sl] + cf * psi
                         work[fc][sl] = work[fc][sl] + cf * (km * curl)
+                    if corr is not None:
+                        corr[fc][sl] = corr[fc][sl] + sgn * (np.asarray(psi, np.float64)
+                                                             + np.asarray(km * curl, np.float64))
         for c in COMPONENTS:
             F[c] = work[c]
 

@@ -7,7 +7,12 @@ the NTFF box (far-field objectives) with respect to eps_r over a region of
 cells and to the source table.
 
 Field history.  The gradient needs, at every step n and every cell of the
-region, E^n and curl H^{n+1/2} (the two factors of d E^{n+1} / d eps_r).
+region, E^n and curl H^{n+1/2} (the factors of d E^{n+1} / d eps_r through
+ca and cb).  In CPML slab cells the E-side correction ce (psi + (1/kappa-1)
+curl) of rfx/boundaries/cpml.py:536-546 also depends on eps_r through
+ce = dt / (eps_r eps0); since d ce / d eps_r = (ce / cb)^2 d cb / d eps_r,
+the forward kernel records curl + (ce / cb)^2 corr in the curl slot, so the
+region may reach into the absorber like the reference's.
 When that history for all steps fits the HBM budget it is recorded during
 the single forward pass and the adjoint runs straight through ("history"
 mode: forward + adjoint, no recomputation).  Otherwise the forward pass
@@ -75,10 +80,6 @@ class AdjointRunner:
         n = int(grid.cpml_layers)
         use_cpml = boundary == "cpml" and n > 0 and bool(cpml_axes)
         shape = tuple(int(v) for v in grid.shape)
-        if use_cpml:
-            for ax, (lo, hi) in enumerate(((i0, i1), (j0, j1), (k0, k1))):
-                if "xyz"[ax] in cpml_axes and (lo < n or hi > shape[ax] - n):
-                    raise ValueError("the gradient region must lie outside the CPML slabs")
         self.sources = [tuple(s[:4]) for s in sources]
         self.src_waves = [np.asarray(s[4], np.float32) for s in sources]
         self.probes = [tuple(p[:4]) for p in probes]

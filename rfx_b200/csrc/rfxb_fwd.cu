@@ -663,9 +663,13 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
       float ey = cav * Ey + cbv * cy_;
       float ez = cav * Ez + cbv * cz_;
       const int ncp = C.ncp;
+      // CPML-E correction of each component before its ce scaling (the
+      // factor d ce / d eps_r multiplies in the gradient) and this cell's ce
+      float kx = 0.f, ky = 0.f, kz = 0.f, ceh = 0.f;
       if (MODE == 2) {
         if (cx.on || cy.on || cz.on) {
           const float ce = PS[L::CE + ty * RFXB_TZ + lane];
+          ceh = ce;
           constexpr int RE = TY * RFXB_TZ;   // q stride of an E box
           const int o = ty * RFXB_TZ + lane;
           if (cx.on) {   // Ey -= ce psi(dHz/dx) [q0], Ez += ce psi(dHy/dx) [q1]
@@ -678,6 +682,8 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
             ey = ey - ce * (cx.c.z * dHz_x);
             ez = ez + ce * p1;
             ez = ez + ce * (cx.c.z * dHy_x);
+            ky -= p0 + cx.c.z * dHz_x;
+            kz += p1 + cx.c.z * dHy_x;
           }
           if (cy.on) {   // Ex += ce psi(dHz/dy) [q0], Ez -= ce psi(dHx/dy) [q1]
             const int qs = C.nx * ncp * C.zs;
@@ -689,6 +695,8 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
             ex = ex + ce * (cy.c.z * dHz_y);
             ez = ez - ce * p1;
             ez = ez - ce * (cy.c.z * dHx_y);
+            kx += p0 + cy.c.z * dHz_y;
+            kz -= p1 + cy.c.z * dHx_y;
           }
           if (cz.on) {   // Ex -= ce psi(dHy/dz) [q0], Ey += ce psi(dHx/dz) [q1]
             const int n4 = P.ncp4;
@@ -702,6 +710,8 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
             ex = ex - ce * (cz.c.z * dHy_z);
             ey = ey + ce * p1;
             ey = ey + ce * (cz.c.z * dHx_z);
+            kx -= p0 + cz.c.z * dHy_z;
+            ky += p1 + cz.c.z * dHx_z;
           }
         }
       } else if (C.cpx || C.cpy || C.cpz) {
@@ -723,6 +733,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
               P.psE[par ^ 1][0][q] = p;
               ey = ey - ce * p;
               ey = ey - ce * km * g;
+              ky -= p + km * g;
             }
             {  // Ez += ce psi(dHy/dx)
               const long long q = psi_index_x(P, sd, 1, s, j, k);
@@ -731,6 +742,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
               P.psE[par ^ 1][0][q] = p;
               ez = ez + ce * p;
               ez = ez + ce * km * g;
+              kz += p + km * g;
             }
           }
         }
@@ -748,6 +760,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
               P.psE[par ^ 1][1][q] = p;
               ex = ex + ce * p;
               ex = ex + ce * (km * g);
+              kx += p + km * g;
             }
             {  // Ez -= ce psi(dHx/dy)
               const long long q = psi_index_y(P, sd, 1, s, i, k);
@@ -756,6 +769,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
               P.psE[par ^ 1][1][q] = p;
               ez = ez - ce * p;
               ez = ez - ce * (km * g);
+              kz -= p + km * g;
             }
           }
         }
@@ -773,6 +787,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
               P.psE[par ^ 1][2][q] = p;
               ex = ex - ce * p;
               ex = ex - ce * (km * g);
+              kx -= p + km * g;
             }
             {  // Ey += ce psi(dHx/dz)
               const long long q = psi_index_z(P, sd, 1, s, i, j);
@@ -781,9 +796,11 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
               P.psE[par ^ 1][2][q] = p;
               ey = ey + ce * p;
               ey = ey + ce * (km * g);
+              ky += p + km * g;
             }
           }
         }
+        ceh = ce;
       }
       // PEC faces
       if ((pec & 1u) && (i == 0 || i == C.nx - 1)) { ey = 0.f; ez = 0.f; }
@@ -805,7 +822,12 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
           const int ci = ((i - P.hb[0]) * sy + (j - P.hb[2])) * sz + (k - P.hb[4]);
           float* hp = P.hist + (long long)(n - P.hist_step0) * P.hist_ld + ci;
           hp[0] = Ex; hp[hc] = Ey; hp[2 * hc] = Ez;
-          hp[3 * hc] = cx_; hp[4 * hc] = cy_; hp[5 * hc] = cz_;
+          // d E^{n+1} / d eps_r = dca E^n + dcb curl + dce corr, and
+          // dce / dcb = (1 + sigma dt / (2 eps))^2 = (ce / cb)^2: the
+          // recorded curl carries the CPML term so that the reverse step's
+          // dca E + dcb curl is the whole derivative (ceh = 0 off the slabs)
+          const float rr = ceh != 0.f ? (ceh / cbv) * (ceh / cbv) : 0.f;
+          hp[3 * hc] = cx_ + rr * kx; hp[4 * hc] = cy_ + rr * ky; hp[5 * hc] = cz_ + rr * kz;
         }
       }
       if (pmask | smask | (unsigned)src_tail | (unsigned)prb_tail) {

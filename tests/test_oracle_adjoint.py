@@ -49,3 +49,33 @@ def test_oracle_gradient_matches_finite_differences(build, box):
     fd = (J_of(ep) - J_of(em)) / (2 * h)
     ad = float((grad * d).sum())
     assert abs(ad - fd) <= 1e-5 * abs(fd)
+
+
+@pytest.mark.parametrize("build", [small_uniform, small_nonuniform])
+def test_oracle_gradient_inside_cpml_matches_finite_differences(build):
+    """A region that reaches into the absorber (the x lo slab, both y slabs
+    across the full transverse extent, the z hi slab and their corners): the
+    CPML-E coefficient ce = dt/(eps_r eps0) of rfx/boundaries/cpml.py:536-546
+    depends on eps_r there, and the gradient includes that term."""
+    sc = build(n_steps=100)
+    nx, ny, nz = sc.ogrid.shape
+    n = sc.ogrid.cpml_layers
+    box = (n - 4, n + 3, 0, ny, nz - n - 2, nz)
+    rng = np.random.default_rng(2)
+    G = rng.standard_normal((sc.n_steps, len(sc.probes)))
+    _, grad, _ = _fa(sc, box, G)
+    i0, i1, j0, j1, k0, k1 = box
+    d = rng.standard_normal(grad.shape)
+    h = 1e-4
+
+    def J_of(eps):
+        s2 = sc.__class__(**{**sc.__dict__, "materials": (eps, sc.materials[1], sc.materials[2])})
+        return float((G * s2.run_oracle(np.float64, exact_materials=True).time_series).sum())
+
+    ep = sc.materials[0].astype(np.float64).copy()
+    em = ep.copy()
+    ep[i0:i1, j0:j1, k0:k1] += h * d
+    em[i0:i1, j0:j1, k0:k1] -= h * d
+    fd = (J_of(ep) - J_of(em)) / (2 * h)
+    ad = float((grad * d).sum())
+    assert abs(ad - fd) <= 1e-5 * abs(fd), (ad, fd)

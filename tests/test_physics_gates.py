@@ -211,3 +211,72 @@ def test_cuda_nonuniform_reduces_to_uniform(cuda):
     e = float(np.linalg.norm(a[:20] - b[:20]) / np.linalg.norm(b[:20]))
     print(f"CUDA graded-to-uniform reduction, first 20 steps: relL2 {e:.2e}")
     assert e < 1e-5 and np.abs(b[:20]).max() > 0
+
+
+# Graded lane: the same x-uniform Ex cavity mode with a graded z spacing.  Its
+# discrete frequency follows from the eigenvalues of the graded second
+# difference the lane applies: with the H metric ih[k] = 1/d[k] and the E
+# metric ie[k] = 2/(d[k-1] + d[k]) of rfx/nonuniform.py:187-224,
+#   (A_z e)[k] = -ie[k] (ih[k] (e[k+1] - e[k]) - ih[k-1] (e[k] - e[k-1])),
+# e = 0 on the PEC faces, and the leapfrog gives
+#   sin^2(w dt / 2) = dt^2 / (eps0 mu0) (lambda_y + lambda_z) / 4,
+# lambda_y = (2 / dy)^2 sin^2(pi / (2 (ny - 1))), lambda_z the lowest
+# eigenvalue of A_z.  Nothing here comes from the time stepping itself, so a
+# grading error in either lane moves the measured resonance off it.
+GCAV_NYI = 8
+GCAV_DZ = 0.4e-3 * 1.15 ** np.arange(9)     # 0.40 .. 1.22 mm, adjacent ratio 1.15
+
+
+def _graded_cavity_inputs():
+    g = oracle.make_nonuniform_grid((CAV_DX, GCAV_NYI * CAV_DX), GCAV_DZ, CAV_DX, cpml_layers=0)
+    n = np.arange(CAV_STEPS)
+    w = np.exp(-((n - 30) / 6.0) ** 2).astype(np.float32)
+    mats = (np.ones(g.shape, np.float32), np.zeros(g.shape, np.float32), np.ones(g.shape, np.float32))
+    return g, w, mats
+
+
+def _graded_cavity_frequency(g):
+    from oracle.fdtd import EPS_0 as E0, MU_0 as M0
+    ie = np.asarray(g.inv_dz, np.float64)
+    ih = np.asarray(g.inv_dz_h, np.float64)
+    nz = g.nz
+    m = nz - 2                                   # interior E nodes k = 1 .. nz-2
+    A = np.zeros((m, m))
+    for r, k in enumerate(range(1, nz - 1)):
+        A[r, r] = ie[k] * (ih[k] + ih[k - 1])
+        if k + 1 <= nz - 2:
+            A[r, r + 1] = -ie[k] * ih[k]
+        if k - 1 >= 1:
+            A[r, r - 1] = -ie[k] * ih[k - 1]
+    lam_z = float(np.min(np.real(np.linalg.eigvals(A))))
+    ny = g.ny
+    lam_y = (2.0 / float(g.dy) * np.sin(np.pi / (2 * (ny - 1)))) ** 2
+    s = g.dt * np.sqrt((lam_y + lam_z) / (E0 * M0)) / 2.0
+    return np.arcsin(s) / (np.pi * g.dt)
+
+
+def test_oracle_graded_cavity_resonance_matches_graded_operator():
+    g, w, mats = _graded_cavity_inputs()
+    assert g.shape == (2, GCAV_NYI + 1, len(GCAV_DZ) + 1)
+    f_pred = _graded_cavity_frequency(g)
+    r = oracle.run_nonuniform(g, mats, CAV_STEPS, sources=[(0, 3, 2, "ex", w)], probes=[(0, 5, 4, "ex")],
+                              dtype=np.float32)
+    f = _peak_frequency(r.time_series[:, 0], g.dt, f_pred)
+    print(f"oracle graded cavity: {f / 1e9:.7f} GHz, graded operator {f_pred / 1e9:.7f}, "
+          f"rel {(f - f_pred) / f_pred:.2e}")
+    assert abs(f - f_pred) / f_pred < 1e-6
+
+
+@pytest.mark.gpu
+def test_cuda_graded_cavity_resonance_matches_graded_operator(cuda):
+    import rfx_b200
+    g, w, mats = _graded_cavity_inputs()
+    pg = rfx_b200.make_nonuniform_grid((CAV_DX, GCAV_NYI * CAV_DX), GCAV_DZ, CAV_DX, cpml_layers=0)
+    assert tuple(pg.shape) == tuple(g.shape) and pg.dt == g.dt
+    f_pred = _graded_cavity_frequency(g)
+    r = rfx_b200.run_nonuniform(pg, rfx_b200.MaterialArrays(*mats), CAV_STEPS, sources=[(0, 3, 2, "ex", w)],
+                                probes=[(0, 5, 4, "ex")])
+    f = _peak_frequency(np.asarray(r["time_series"])[:, 0], g.dt, f_pred)
+    print(f"CUDA graded cavity: {f / 1e9:.7f} GHz, graded operator {f_pred / 1e9:.7f}, "
+          f"rel {(f - f_pred) / f_pred:.2e}")
+    assert abs(f - f_pred) / f_pred < 1e-6
