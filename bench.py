@@ -13,8 +13,11 @@ configuration's shapes (the reference publishes no dataset).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank runs its own seeded sweep (independent instances, no
-data-path collective: weak scaling); the time is the max over ranks.
+With N GPUs (``--gpus N``; launched under torchrun, or re-launched under it
+by this script) the sweep has 64 x N instances drawn from seed 0 and each rank
+takes a cell-balanced share (``rfx_b200.distributed.shard_instances``) of them:
+independent instances, no data-path collective, weak scaling.  The time is
+the max over ranks and ``value`` counts the cells of every rank's share.
 """
 
 from __future__ import annotations
@@ -38,21 +41,25 @@ METRIC = "Mcell-steps/s fwd+adjoint grad, batched vs single, 1 B200; % HBM roofl
 UNIT = "Mcell-steps/s"
 
 
-def _sweep_cells(args):
-    """Cells of rank 0's sweep (the reference arm runs on rank 0 alone)."""
+def _sweep_cells(args, world=1):
+    """Cells of the whole sweep at ``world`` GPUs."""
     from rfx_b200.workloads import batched_sweep_cells
-    return batched_sweep_cells(seed=0, n_inst=args.instances)
+    return batched_sweep_cells(seed=0, n_inst=args.instances * world)
 
 
 def _workload_config(args, cells, world):
-    return {"workload": f"batched_sweep: {args.instances} instances (n+17)^3, n~U{{64..160}} seed {{rank}}, "
+    """``cells``: all ranks' cells together."""
+    n_all = args.instances * world
+    return {"workload": f"batched_sweep: {n_all} instances (n+17)^3, n~U{{64..160}} seed 0, "
                         f"CPML 8, {args.time_steps} time steps, forward + probe-DFT objective + adjoint "
                         f"dJ/d eps_r over 16x16x2 regions",
             "instances_per_gpu": args.instances, "time_steps": args.time_steps,
-            "cells_per_gpu": int(cells), "adjoint_mode": "history (design-region E^n and curl H recorded in HBM)",
-            "l2": f"inputs larger than L2 (a step reads the fields and coefficients of {cells / 1e6:.1f} M cells, "
-                  f"{cells * 32 / 1e9:.2f} GB)",
-            "parallelism": f"independent instances x {world} GPU"}
+            "cells_total": int(cells), "adjoint_mode": "history (design-region E^n and curl H recorded in HBM)",
+            "l2": f"inputs larger than L2 (a step reads the fields and coefficients of {cells / world / 1e6:.1f} M "
+                  f"cells per GPU, {cells / world * 32 / 1e9:.2f} GB)",
+            "parallelism": (f"{n_all} independent instances sharded over {world} GPUs by cells "
+                            f"(rfx_b200.distributed.shard_instances), no data-path collective"
+                            if world > 1 else "independent instances x 1 GPU")}
 
 
 # ---------------------------------------------------------------------------
@@ -165,12 +172,13 @@ def cpu_baseline_port(args, n_workers=1, n_time=60):
 
 def _traffic_per_cell(kernel):
     """DRAM bytes per cell and time step of a step kernel (all its launches
-    of one step) from its committed ncu summary (profiles/<kernel>.md), or
-    None."""
+    of one step), measured by ncu on the 4-instance case of the same sweep
+    (committed in profiles/<kernel>.md) and scaled by cells to the workload;
+    None if the summary has no such line."""
     path = os.path.join(ROOT, "profiles", f"{kernel}.md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"dram_bytes_per_cell_per_step:\s*([0-9.eE+-]+)", open(path).read())
+    m = re.search(r"small_case_dram_bytes_per_cell_per_step:\s*([0-9.eE+-]+)", open(path).read())
     return float(m.group(1)) if m else None
 
 
@@ -194,9 +202,21 @@ def run_ours(args, rank, world, local_rank):
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
 
-    insts = batched_sweep(seed=rank, n_inst=args.instances, n_steps=args.time_steps)
+    if world > 1:
+        from rfx_b200.distributed import shard_instances
+        from rfx_b200.workloads import batched_sweep_instance_cells
+        n_all = args.instances * world
+        mine = shard_instances(batched_sweep_instance_cells(seed=0, n_inst=n_all), world)[rank]
+        insts = batched_sweep(seed=0, n_inst=n_all, n_steps=args.time_steps, subset=mine)
+    else:
+        insts = batched_sweep(seed=0, n_inst=args.instances, n_steps=args.time_steps)
     sw = Sweep(insts, args.time_steps, device=dev, batched=True)
     cells = sw.cells()
+    total_cells = cells
+    if world > 1:
+        tc = torch.tensor([float(cells)], device=dev, dtype=torch.float64)
+        dist.all_reduce(tc, op=dist.ReduceOp.SUM)
+        total_cells = int(tc.item())
     N = args.time_steps
     stream = torch.cuda.current_stream()
     # launch configuration chosen by the autotuner (trial steps of this
@@ -245,7 +265,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms, fwd_ms, adj_ms = float(t[0]), float(t[1]), float(t[2])
-    value = cells * N * args.steps * world / (total_ms / 1e3) / 1e6
+    value = total_cells * N * args.steps / (total_ms / 1e3) / 1e6
 
     # rooflines of the two step kernels: algorithmic bytes per launch over the
     # average launch time (one launch per time step in each phase; the
@@ -317,7 +337,7 @@ def run_ours(args, rank, world, local_rank):
         et = torch.tensor([ems], device=dev, dtype=torch.float64)
         if world > 1:
             dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        e2e = {"value": round(cells * N * args.steps * world / (float(et[0]) / 1e3) / 1e6, 1), "unit": UNIT,
+        e2e = {"value": round(total_cells * N * args.steps / (float(et[0]) / 1e3) / 1e6, 1), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "path": "rfx_b200.batch.Sweep.set_materials + run (host pinned eps_r/sigma in, J and dJ/d eps_r out)"}
 
@@ -334,7 +354,7 @@ def run_ours(args, rank, world, local_rank):
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 2), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-                "config": _workload_config(args, cells, world), "roofline": roofline,
+                "config": _workload_config(args, total_cells, world), "roofline": roofline,
                 "roofline_other_kernel": roofline_other, "cpu_baseline": cpu,
                 "e2e": e2e, "single": single, "gpu_launches": launches, "launch": launch,
                 "clocks": clk.summary(), "host_wall_s_timed": round(t_host, 3)}
@@ -359,7 +379,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": _workload_config(args, _sweep_cells(args), world), "cpu_baseline": cb,
+            "config": _workload_config(args, _sweep_cells(args, world), world), "cpu_baseline": cb,
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference = NumPy float32 restatement of rfx's scan body and its transpose (oracle port); "
                     "rfx itself needs JAX, which is not installable offline here"}
@@ -498,9 +518,20 @@ def main():
                     help="batched_sweep is the headline line; the others print a secondary forward (or "
                          "forward+adjoint) line for the other configurations")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: re-launch this command under torchrun
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        os.execv(sys.executable, [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                                  f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+                                  "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]])
     rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
+    world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but {world} ranks were launched")
     if args.workload != "batched_sweep":
         if args.impl == "reference" or world > 1:
             raise SystemExit("secondary workloads run on our arm at one GPU only")

@@ -34,16 +34,22 @@ class _Mats:
         self.eps_r, self.sigma = eps_r, sigma
 
 
-def _boxes(rng, shape, n, eps_lo, eps_hi, sig_hi, margin, size_lo, size_hi):
-    eps = np.ones(shape, np.float32)
-    sig = np.zeros(shape, np.float32)
+def _boxes(rng, shape, n, eps_lo, eps_hi, sig_hi, margin, size_lo, size_hi, build=True):
+    """``n`` seeded boxes; with ``build=False`` only the random draws are made
+    (the stream advances exactly as when building) and (None, None) returned."""
+    eps = np.ones(shape, np.float32) if build else None
+    sig = np.zeros(shape, np.float32) if build else None
     for _ in range(n):
         sz = [int(min(rng.integers(size_lo, size_hi + 1), shape[a] - 2 * margin - 1)) for a in range(3)]
         lo = [int(rng.integers(margin, max(margin + 1, shape[a] - margin - sz[a]))) for a in range(3)]
         sl = tuple(slice(lo[a], lo[a] + sz[a]) for a in range(3))
-        eps[sl] = np.float32(rng.uniform(eps_lo, eps_hi))
+        v = np.float32(rng.uniform(eps_lo, eps_hi))
+        if build:
+            eps[sl] = v
         if sig_hi > 0:
-            sig[sl] = np.float32(rng.uniform(0.0, sig_hi))
+            w = np.float32(rng.uniform(0.0, sig_hi))
+            if build:
+                sig[sl] = w
     return eps, sig
 
 
@@ -117,30 +123,43 @@ def adjoint_region(seed=0, n_steps=3000):
     return g, eps, sig, src, probes, box, freqs
 
 
-def batched_sweep_cells(seed=0, n_inst=64, n_lo=64, n_hi=160):
-    """Total cell count of ``batched_sweep(seed, n_inst, ...)`` without
-    building its material arrays (same size draw, same grids)."""
+def batched_sweep_instance_cells(seed=0, n_inst=64, n_lo=64, n_hi=160):
+    """Per-instance cell counts of ``batched_sweep(seed, n_inst, ...)``
+    without building its material arrays (same size draw, same grids)."""
     sizes = np.random.default_rng(seed).integers(n_lo, n_hi + 1, n_inst)
     dx = 0.5e-3
-    total = 0
+    out = []
     for n in sizes:
         g = Grid(freq_max=20e9, domain=(int(n) * dx,) * 3, dx=dx, cpml_layers=8)
-        total += g.nx * g.ny * g.nz
-    return int(total)
+        out.append(int(g.nx * g.ny * g.nz))
+    return out
 
 
-def batched_sweep(seed=0, n_inst=64, n_steps=2000, n_lo=64, n_hi=160):
+def batched_sweep_cells(seed=0, n_inst=64, n_lo=64, n_hi=160):
+    """Total cell count of ``batched_sweep(seed, n_inst, ...)``."""
+    return int(sum(batched_sweep_instance_cells(seed, n_inst, n_lo, n_hi)))
+
+
+def batched_sweep(seed=0, n_inst=64, n_steps=2000, n_lo=64, n_hi=160, subset=None):
+    """The sweep's instances; with ``subset`` (instance indices) only those
+    are built, from the same random stream (a rank's share of a sweep that is
+    sharded over GPUs)."""
     rng = np.random.default_rng(seed)
     dx = 0.5e-3
     out = []
     sizes = rng.integers(n_lo, n_hi + 1, n_inst)
+    keep = set(range(n_inst)) if subset is None else set(int(q) for q in subset)
     for q in range(n_inst):
         n = int(sizes[q])
         g = Grid(freq_max=20e9, domain=(n * dx,) * 3, dx=dx, cpml_layers=8)
-        eps, sig = _boxes(rng, g.shape, 8, 1.0, 8.0, 0.0, 10, 4, max(5, n // 4))
+        build = q in keep
+        eps, sig = _boxes(rng, g.shape, 8, 1.0, 8.0, 0.0, 10, 4, max(5, n // 4), build=build)
         c = g.nx // 2
         box = (c - 8, c + 8, c - 8, c + 8, c, c + 2)
-        eps[box[0]:box[1], box[2]:box[3], box[4]:box[5]] = 1.0 + 3.4 * rng.uniform(0, 1, (16, 16, 2)).astype(np.float32)
+        rho = rng.uniform(0, 1, (16, 16, 2)).astype(np.float32)
+        if not build:
+            continue
+        eps[box[0]:box[1], box[2]:box[3], box[4]:box[5]] = 1.0 + 3.4 * rho
         s = (10, c, c)
         src = [(*s, "ez", j_wave(g, s, eps, sig, n_steps, 12e9))]
         probes = [(g.nx - 12, c + d, c, "ez") for d in (-6, -2, 2, 6)]

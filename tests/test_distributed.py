@@ -49,3 +49,23 @@ def test_gloo_world_size_2():
     for rank, v, parts in res:
         assert v == 11.0
         assert sorted(parts[0] + parts[1]) == [0, 1, 2, 3, 4]
+
+
+def test_sharded_sweep_reassembles_the_global_sweep():
+    """The bench's multi-GPU workload: each rank builds only its share of one
+    global sweep (same random stream), the shares partition it, and the cells
+    of the shares add up to the whole."""
+    from rfx_b200.workloads import batched_sweep, batched_sweep_instance_cells
+    n_all, world = 6, 2
+    cells = batched_sweep_instance_cells(seed=0, n_inst=n_all, n_lo=8, n_hi=20)
+    parts = shard_instances(cells, world)
+    whole = batched_sweep(seed=0, n_inst=n_all, n_steps=8, n_lo=8, n_hi=20)
+    got = {}
+    for part in parts:
+        for q, inst in zip(part, batched_sweep(seed=0, n_inst=n_all, n_steps=8, n_lo=8, n_hi=20, subset=part)):
+            got[q] = inst
+    assert sorted(got) == list(range(n_all))
+    for q, inst in got.items():
+        assert np.array_equal(inst.eps_r, whole[q].eps_r) and inst.box == whole[q].box
+        assert int(np.prod(inst.grid.shape)) == cells[q]
+    assert sum(cells[q] for p in parts for q in p) == sum(cells)
