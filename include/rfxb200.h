@@ -43,6 +43,7 @@ extern "C" {
 #define RFXB_E_LAUNCH (-4)    /* kernel launch or CUDA runtime failure */
 #define RFXB_E_STATE (-5)     /* call out of order (e.g. adjoint before forward) */
 #define RFXB_E_TIMEOUT (-6)   /* a bounded wait inside a kernel ran out (device status word) */
+#define RFXB_E_WORK (-7)      /* a persistent kernel met an invalid work item (device status word) */
 
 #define RFXB_AXIS_X 1u
 #define RFXB_AXIS_Y 2u
@@ -364,6 +365,13 @@ int rfxb_batch_step_launches(const RfxbBatch* batch, int* fwd, int* rev);
  *                 variant 2, variant 3) by index: 0 (4,2,3), 1 (4,3,2),
  *                 2 (2,4,3), 3 (2,3,4), 4 (3,4,2), 5 (3,2,4); without
  *                 variant 4 only the relative order of 2 and 3 counts
+ *   fwd_persist  0: the launches above; k >= 1: one persistent launch per
+ *                 step over both forward lists (as many CTAs as are resident,
+ *                 each pulling items from device queues), k-1 CTAs per SM
+ *                 taking CPML-free items first, the others CPML items first
+ *   adj_persist  0: the launches above; 1: one persistent launch per reverse
+ *                 step over the three reverse lists, one CTA per SM taking
+ *                 each list first
  * rfxb_*_launch_config writes the current setting to *current and the
  * largest value each field accepts on this plan/batch to *limits (0 where a
  * choice does not exist, e.g. fwd_split on a group without staged-psi CPML).
@@ -376,12 +384,27 @@ typedef struct RfxbLaunchConfig {
   int32_t fwd_order;
   int32_t adj_lite;
   int32_t adj_order;
+  int32_t fwd_persist;
+  int32_t adj_persist;
 } RfxbLaunchConfig;
 
 int rfxb_plan_launch_config(const RfxbPlan* plan, RfxbLaunchConfig* current, RfxbLaunchConfig* limits);
 int rfxb_plan_set_launch_config(RfxbPlan* plan, const RfxbLaunchConfig* config);
 int rfxb_batch_launch_config(const RfxbBatch* batch, RfxbLaunchConfig* current, RfxbLaunchConfig* limits);
 int rfxb_batch_set_launch_config(RfxbBatch* batch, const RfxbLaunchConfig* config);
+
+/* Test hooks of the persistent step kernels (no counterpart in the
+ * reference).  debug_fault: from the next launch on, the CTA with block
+ * index `cta` (-1: none) does not load plane xa of its first work item, and
+ * every pipeline wait gives up after `wait_limit` polls, so that CTA's wait
+ * runs out and rfxb_*_device_status reports RFXB_E_TIMEOUT (no box is left
+ * in flight: the CTA drains the others before leaving).  debug_poison
+ * replaces entry `index` of a work list (0/1 forward CPML/CPML-free, 2/3/4
+ * reverse y-slab/other CPML/CPML-free) with an empty x range, which the
+ * persistent kernels skip and report as RFXB_E_WORK.  Both leave the batch's
+ * state invalid: only the status check is meaningful afterwards. */
+int rfxb_batch_debug_fault(RfxbBatch* batch, int cta, int wait_limit);
+int rfxb_batch_debug_poison(RfxbBatch* batch, int list, int index);
 
 /* Host only, no device needed: the work list (x ranges of (TY x 32) tiles)
  * that a batch of plans with these shapes launches for one step, for tests

@@ -54,7 +54,7 @@ class RfxbDesc(C.Structure):
 
 class RfxbLaunchConfig(C.Structure):
     _fields_ = [("fwd_split", C.c_int32), ("fwd_order", C.c_int32), ("adj_lite", C.c_int32),
-                ("adj_order", C.c_int32)]
+                ("adj_order", C.c_int32), ("fwd_persist", C.c_int32), ("adj_persist", C.c_int32)]
 
 
 class RfxbStepIO(C.Structure):
@@ -134,6 +134,8 @@ SIGNATURES = {
     "rfxb_batch_set_launch_config": (C.c_int, [C.c_void_p, C.POINTER(RfxbLaunchConfig)]),
     "rfxb_debug_work_lists": (C.c_int, [C.c_int, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.POINTER(C.c_int32),
                                         C.c_int32, C.POINTER(C.c_int32)]),
+    "rfxb_batch_debug_fault": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "rfxb_batch_debug_poison": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "rfxb_forward_noalloc": (C.c_int, [C.POINTER(RfxbDesc), C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p),
                                        C.POINTER(RfxbStepIO), C.c_int, C.c_int, C.c_void_p]),
 }

@@ -49,14 +49,22 @@ def _key_str(k) -> str:
 
 
 def forward_candidates(limits: dict, current: dict) -> list:
-    """Forward settings to time: split with either launch order, and the
-    single launch, as far as the limits allow (the current setting first)."""
+    """Forward settings to time: split with either launch order, the single
+    launch, and (where the target offers it) the persistent launch with 0, 1
+    or 2 CPML-free-first CTAs per SM, as far as the limits allow (the current
+    setting first)."""
     c = []
     if limits["fwd_split"]:
         c += [{"fwd_split": 1, "fwd_order": 0}, {"fwd_split": 1, "fwd_order": 1}, {"fwd_split": 0, "fwd_order": 0}]
     else:
         c.append({"fwd_split": 0, "fwd_order": 0})
     cur = {"fwd_split": current["fwd_split"], "fwd_order": current["fwd_order"] if current["fwd_split"] else 0}
+    np_ = limits.get("fwd_persist", 0)
+    if np_:
+        c = [dict(x, fwd_persist=0) for x in c]
+        c += [{"fwd_split": 1, "fwd_order": 0, "fwd_persist": k} for k in range(1, np_ + 1)]
+        k = current.get("fwd_persist", 0)
+        cur = dict(cur, fwd_persist=k) if not k else {"fwd_split": 1, "fwd_order": 0, "fwd_persist": k}
     return [cur] + [x for x in c if x != cur]
 
 
@@ -75,6 +83,11 @@ def reverse_candidates(limits: dict, current: dict) -> list:
     if not cur["adj_lite"]:   # the representative of the current relative order of 2 and 3
         o = REVERSE_ORDERS[cur["adj_order"]]
         cur["adj_order"] = 0 if o.index(2) < o.index(3) else 1
+    if limits.get("adj_persist", 0):
+        # the persistent launch runs variants 2, 4 and 3 over all three lists
+        c = [dict(x, adj_persist=0) for x in c] + [{"adj_lite": 1, "adj_order": 0, "adj_persist": 1}]
+        cur = (dict(cur, adj_persist=0) if not current.get("adj_persist", 0)
+               else {"adj_lite": 1, "adj_order": 0, "adj_persist": 1})
     if cur in c:
         c.remove(cur)
     elif limits["adj_order"] == 0:

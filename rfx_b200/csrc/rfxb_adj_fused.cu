@@ -31,6 +31,8 @@
 //      edge-mask staging compiled out and the ring without its y-slab
 //      arrays, so the shared memory (57 KB) and 64 registers allow four
 //      CTAs per SM instead of three (the host runs it on a third stream).
+#include <algorithm>
+
 #include "rfxb_common.cuh"
 
 namespace rfxb {
@@ -369,24 +371,26 @@ struct AdjBounds<2> { static constexpr int MIN_CTAS = 3; };
 template <>
 struct AdjBounds<4> { static constexpr int MIN_CTAS = 4; };
 
+// One work item of the reverse step (see the forward's fwd_item): returns
+// false when a bounded wait ran out (status set, every issued box waited
+// for); the caller must then leave.  The shared memory at `raw` holds the
+// layout of this mode; the mbarriers sit at the same offsets in every mode.
 template <int TY, int MODE>
-__global__ void __launch_bounds__(32 * TY, AdjBounds<MODE>::MIN_CTAS)
-adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
-                const RfxbWork* __restrict__ work, const CUtensorMap* __restrict__ maps, int n, int par, int apar,
-                int zp) {
+__device__ __forceinline__ bool adj_item(unsigned char* raw, const RfxbInst* __restrict__ insts,
+                                         const AdjInst* __restrict__ adjs, const RfxbWork w,
+                                         const CUtensorMap* __restrict__ maps, int n, int par, int apar, int zp,
+                                         StepPhases& ph, const StepFault& fault, bool first_item) {
   constexpr bool TMA = MODE != 0;
   constexpr bool RING = MODE == 2 || MODE == 4;       // psi ring
   constexpr bool YS = MODE != 4;                      // y-slab relations compiled in
   constexpr int NST = RING ? 3 : RFXB_ANSTAGE;        // plane stages
   using L = APsiSlot<TY, YS>;
   using SM = AdjSmem<TY, MODE != 4>;
-  extern __shared__ __align__(128) unsigned char adj_smem_raw[];
-  SM& S = *reinterpret_cast<SM*>(adj_smem_raw);
+  SM& S = *reinterpret_cast<SM*>(raw);
   float* ring = reinterpret_cast<float*>(&S.st[NST]);   // modes 2, 4: two psi slots after the stages
   auto& rx = *reinterpret_cast<AdjExchange<TY>*>(&S.st[NST]);   // modes 0, 1: the exchange array
   const int lane = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * 32 + lane;
-  const RfxbWork w = work[blockIdx.x];
   load_inst(S.P, insts + w.inst, tid, 32 * TY);
   {
     const int nw = sizeof(AdjInst) / 4;
@@ -394,12 +398,9 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     int* d = reinterpret_cast<int*>(&S.A);
     for (int t = tid; t < nw; t += 32 * TY) d[t] = __ldg(s + t);
   }
-  if (TMA && tid == 0) {
-    for (int q = 0; q < NST; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
-    if (RING) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
-    mbar_fence_init();
-  }
   __syncthreads();
+  const int wlim = fault.wait_limit;
+  const bool skip_first = first_item && (int)blockIdx.x == fault.cta;
   const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const RfxbInst& P = S.P;
   const AdjInst& A = S.A;
@@ -460,7 +461,13 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     if (!RING || p < 0 || p >= C.nx) return false;
     return yz_tile || xslab(p) || xslab(p + 1);
   };
-  unsigned pph = 0u, pout = 0u;
+  unsigned& pph = ph.ring;
+  unsigned pout = 0u;
+  // completion parity of the stage holding plane p (the k-th fill of a stage
+  // in this item is k phases past where the previous items left it)
+  auto sparity = [&](int p) -> uint32_t {
+    return ((ph.stage >> astage_of<NST>(p)) ^ (uint32_t)((p - xa + 1) / NST)) & 1u;
+  };
   auto psi_fill = [&](int p) {
     if (!psi_need(p)) return;
     if (tid == 0)
@@ -471,7 +478,7 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
   auto psi_wait = [&](int p) -> bool {
     if (!psi_need(p)) return true;
     const int sl = p & 1;
-    const bool ok = mbar_wait_bounded(smem_u32(&S.pbar[sl]), (pph >> sl) & 1u);
+    const bool ok = mbar_wait_bounded(smem_u32(&S.pbar[sl]), (pph >> sl) & 1u, wlim);
     if (ok) {
       pph ^= 1u << sl;
       pout &= ~(1u << sl);
@@ -482,18 +489,19 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     if (tid == 0) {
       atomicOr(P.status, 1);
       for (int p = from; p <= last_issued; ++p)
-        mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(p)]), astage_parity<NST>(p, xa));
+        mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(p)]), sparity(p), wlim);
       for (int sl = 0; sl < 2; ++sl)
-        if (pout & (1u << sl)) mbar_wait_bounded(smem_u32(&S.pbar[sl]), (pph >> sl) & 1u);
+        if (pout & (1u << sl)) mbar_wait_bounded(smem_u32(&S.pbar[sl]), (pph >> sl) & 1u, wlim);
     }
   };
   if (TMA) {
     if (tid == 0)
-      for (int p = xa - 1; p <= min(xa + NST - 2, xb); ++p) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, p);
+      for (int p = xa - 1; p <= min(xa + NST - 2, xb); ++p)
+        if (!(skip_first && p == xa)) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, p);
     psi_fill(xa);
-    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa - 1)]), astage_parity<NST>(xa - 1, xa)) &&
-                    mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa)]), astage_parity<NST>(xa, xa));
-    if (__syncthreads_or(!ok)) { bail(min(xa + NST - 2, xb), xa - 1); return; }
+    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa - 1)]), sparity(xa - 1), wlim) &&
+                    mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(xa)]), sparity(xa), wlim);
+    if (__syncthreads_or(!ok)) { bail(min(xa + NST - 2, xb), xa - 1); return false; }
   } else {
     adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa - 1, tid);
     adj_load_stage<TY>(S, C, aF0, ca, cb, y0, z0, xa, tid);
@@ -563,9 +571,8 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     if (TMA) {
       // plane i+1 (and plane i's psi) have landed; after the barrier plane
       // i-1's stage takes plane i+NST-1 and its psi slot plane i+1
-      const bool ok =
-          mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(i + 1)]), astage_parity<NST>(i + 1, xa)) && psi_wait(i);
-      if (__syncthreads_or(!ok)) { bail(min(i + NST - 2, xb), i + 1); return; }
+      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(i + 1)]), sparity(i + 1), wlim) && psi_wait(i);
+      if (__syncthreads_or(!ok)) { bail(min(i + NST - 2, xb), i + 1); return false; }
       if (tid == 0 && i + NST - 1 <= xb) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, i + NST - 1);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
@@ -1003,6 +1010,107 @@ adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ 
     rxh = nxh;
   }
   if (!TMA) cp_async_wait<0>();
+  if (TMA) {   // the phases this item advanced: stage s filled by planes xa-1 .. xb
+    const int T = xb - xa + 2;
+    for (int st = 0; st < NST; ++st) {
+      const int fills = T / NST + ((((st - xa) % NST + NST) % NST) < T % NST ? 1 : 0);
+      ph.stage ^= (uint32_t)(fills & 1) << st;
+    }
+  }
+  __syncthreads();   // every thread is done with the stages, P and A before the next item reuses them
+  return true;
+}
+
+template <int TY>
+__device__ __forceinline__ void adj_init_barriers(unsigned char* raw, int nst, bool ring, int tid) {
+  auto& S = *reinterpret_cast<AdjSmem<TY, true>*>(raw);
+  if (tid == 0) {
+    for (int q = 0; q < nst; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
+    if (ring) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
+    mbar_fence_init();
+  }
+  __syncthreads();
+}
+
+// One launch per reverse step and variant: CTA b runs work item b.
+template <int TY, int MODE>
+__global__ void __launch_bounds__(32 * TY, AdjBounds<MODE>::MIN_CTAS)
+adj_step_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs,
+                const RfxbWork* __restrict__ work, const CUtensorMap* __restrict__ maps, int n, int par, int apar,
+                int zp) {
+  extern __shared__ __align__(128) unsigned char adj_smem_raw[];
+  constexpr bool RING = MODE == 2 || MODE == 4;
+  if (MODE != 0) adj_init_barriers<TY>(adj_smem_raw, RING ? 3 : RFXB_ANSTAGE, RING, threadIdx.y * 32 + threadIdx.x);
+  StepPhases ph;
+  adj_item<TY, MODE>(adj_smem_raw, insts, adjs, work[blockIdx.x], maps, n, par, apar, zp, ph, StepFault{}, true);
+}
+
+__device__ __forceinline__ bool adj_work_valid(const RfxbWork& w, const RfxbInst* insts, int n_inst, int ty) {
+  if (w.inst < 0 || w.inst >= n_inst) return false;
+  const RfxbInst& I = insts[w.inst];
+  return w.y0 >= 0 && w.y0 < I.ny && w.y0 % ty == 0 && w.z0 >= 0 && w.z0 < I.nz && w.z0 % RFXB_TZ == 0 &&
+         w.xa >= 0 && w.xa < w.xb && w.xb <= I.nx;
+}
+
+// Persistent reverse step: one launch per reverse step of as many CTAs as
+// are resident.  Queue 0 holds the tiles that reach a y slab (variant 2),
+// queue 1 the other CPML work (variant 4), queue 2 the CPML-free tiles
+// (variant 3).  CTAs of role 0 (blocks [0, role_ctas), one per SM when the
+// first wave spreads) take CPML-free items first, role 1 variant-4 items,
+// role 2 variant-2 items; an emptied queue sends a CTA to the others, so the
+// latency-bound CPML work and the bandwidth-bound plain work share every SM.
+// Invalid items are skipped and flagged (status bit 2); the last CTA to
+// finish clears the fetch counters for the next launch.
+template <int TY>
+__global__ void __launch_bounds__(32 * TY, 3)
+adj_persist_kernel(const RfxbInst* __restrict__ insts, const AdjInst* __restrict__ adjs, int n_inst,
+                   RfxbAdjQueues Q, const CUtensorMap* __restrict__ maps, int n, int par, int apar) {
+  extern __shared__ __align__(128) unsigned char adj_smem_raw[];
+  __shared__ int pick[2];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  adj_init_barriers<TY>(adj_smem_raw, RFXB_ANSTAGE, true, tid);
+  StepPhases ph;
+  StepFault fault;
+  fault.cta = Q.fault_cta;
+  fault.wait_limit = Q.wait_limit;
+  static constexpr int kOrder[3][3] = {{2, 1, 0}, {1, 0, 2}, {0, 1, 2}};
+  const int role = min(2, (int)blockIdx.x / max(1, Q.role_ctas));
+  bool first_item = true;
+  bool ok = true;
+  while (ok) {
+    if (tid == 0) {
+      pick[0] = -1;
+      for (int t = 0; t < 3; ++t) {
+        const int q = kOrder[role][t];
+        if (*(volatile int*)&Q.ctr[q] >= Q.count[q]) continue;   // drained (counters only grow): no ticket
+        const int k = atomicAdd(&Q.ctr[q], 1);
+        if (k < Q.count[q]) { pick[0] = q; pick[1] = k; break; }
+      }
+    }
+    __syncthreads();
+    const int q = pick[0], k = pick[1];
+    __syncthreads();
+    if (q < 0) break;
+    const RfxbWork w = Q.list[q][k];
+    if (!adj_work_valid(w, insts, n_inst, TY)) {
+      if (tid == 0) atomicOr(Q.status, 2);
+      continue;
+    }
+    if (q == 0) ok = adj_item<TY, 2>(adj_smem_raw, insts, adjs, w, maps, n, par, apar, Q.zp, ph, fault, first_item);
+    else if (q == 1) ok = adj_item<TY, 4>(adj_smem_raw, insts, adjs, w, maps, n, par, apar, Q.zp, ph, fault, first_item);
+    else ok = adj_item<TY, 3>(adj_smem_raw, insts, adjs, w, maps, n, par, apar, Q.zp, ph, fault, first_item);
+    first_item = false;
+  }
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(&Q.ctr[3], 1) == (int)gridDim.x - 1) {
+      Q.ctr[0] = 0;
+      Q.ctr[1] = 0;
+      Q.ctr[2] = 0;
+      Q.ctr[3] = 0;
+      __threadfence();
+    }
+  }
 }
 
 template __global__ void adj_step_kernel<8, 0>(const RfxbInst*, const AdjInst*, const RfxbWork*,
@@ -1015,11 +1123,15 @@ template __global__ void adj_step_kernel<8, 3>(const RfxbInst*, const AdjInst*, 
                                                const CUtensorMap*, int, int, int, int);
 template __global__ void adj_step_kernel<8, 4>(const RfxbInst*, const AdjInst*, const RfxbWork*,
                                                const CUtensorMap*, int, int, int, int);
+template __global__ void adj_persist_kernel<8>(const RfxbInst*, const AdjInst*, int, RfxbAdjQueues,
+                                               const CUtensorMap*, int, int, int);
 
 // Dynamic shared memory of a mode: the fixed part, the plane stages it uses
 // and (modes 2, 4) the two ring slots sized for z-psi rows of zp floats, or
 // (modes 0, 1) the exchange array.
 size_t adj_step_smem_bytes(int mode, int zp) {
+  if (mode == 5)   // the persistent kernel: the largest of variants 2, 3 and 4
+    return std::max(std::max(adj_step_smem_bytes(2, zp), adj_step_smem_bytes(3, zp)), adj_step_smem_bytes(4, zp));
   using Lite = AdjSmem<8, false>;
   using Full = AdjSmem<8, true>;
   if (mode == 4)

@@ -46,6 +46,11 @@ __global__ void ntff_kernel(const RfxbInst*, const RfxbNtffFace*, int, int, int)
 template <int TY, int MODE>
 __global__ void adj_step_kernel(const RfxbInst*, const AdjInst*, const RfxbWork*, const CUtensorMap*, int, int, int,
                                 int);
+template <int TY, bool EM>
+__global__ void fwd_persist_kernel(const RfxbInst*, int, RfxbFwdQueues, const CUtensorMap*, int, int);
+template <int TY>
+__global__ void adj_persist_kernel(const RfxbInst*, const AdjInst*, int, RfxbAdjQueues, const CUtensorMap*, int, int,
+                                   int);
 size_t adj_step_smem_bytes(int mode, int zp);
 }  // namespace rfxb
 
@@ -216,6 +221,13 @@ struct RfxbBatch {
   int ntff_blocks = 0;
   CUtensorMap* d_maps = nullptr;   // RFXB_NMAPS per plan
   int* d_status = nullptr;         // device status word of the group's launches
+  // persistent step launches (one launch per step over the split lists)
+  int* d_qctr = nullptr;           // [8]: fetch counters of the forward (3) and reverse (4) queues
+  int fwd_persist = 0;             // 0: off; k >= 1: on, k-1 CTAs per SM try the CPML-free list first
+  int adj_persist = 0;             // 0: off; 1: on
+  int fault_cta = -1;              // test-only fault injection of the persistent kernels
+  int wait_limit = 1 << 22;
+  int adj_persist_grid = 0;        // CTAs of the persistent reverse launch (resident at once)
   int fwd_mode = 0;                // forward step kernel variant (see rfxb_fwd.cu)
   int adj_mode = -1;               // reverse step kernel variant (see rfxb_adj_fused.cu), -1 not chosen yet
   int adj_zp = 4;                  // z-psi row capacity of the mode-2 reverse ring
@@ -566,6 +578,39 @@ FwdKernel fwd_kernel(int mode, bool em = false) {
   allow_smem(reinterpret_cast<const void*>(k), fwd_step_smem_bytes(mode));
   return k;
 }
+
+using FwdPersistKernel = void (*)(const RfxbInst*, int, RfxbFwdQueues, const CUtensorMap*, int, int);
+FwdPersistKernel fwd_persist_kernel_for(bool em) {
+  FwdPersistKernel k = em ? fwd_persist_kernel<kTY, true> : fwd_persist_kernel<kTY, false>;
+  allow_smem(reinterpret_cast<const void*>(k), fwd_step_smem_bytes(2));
+  return k;
+}
+
+// CTAs of a persistent forward launch: as many as are resident at once.
+int fwd_persist_grid(bool em) {
+  static int r[2] = {-1, -1};
+  if (r[em] < 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fwd_persist_kernel_for(em), 32 * kTY,
+                                                      fwd_step_smem_bytes(2)) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    r[em] = per_sm * sm_count();
+  }
+  return r[em];
+}
+
+// Default of the persistent forward launch (RFXB_PERSIST=0 turns it off,
+// =1 on with one plain-first CTA per SM; without the variable: off).
+int fwd_persist_default() {
+  const char* e = getenv("RFXB_PERSIST");
+  if (!e) return 0;
+  return std::string(e) == "0" ? 0 : 2;
+}
+
+// The persistent reverse launch needs the three reverse lists (variant 2 on
+// y-slab tiles, variant 4 on the other CPML work, variant 3 on plain tiles).
+bool adj_persist_avail(const RfxbBatch* g);
 
 int resident_ctas(int mode) {
   static int r[3] = {-1, -1, -1};
@@ -1050,6 +1095,10 @@ int build_group(RfxbBatch* g) {
   if (int rc = galloc((void**)&g->d_maps, sizeof(CUtensorMap) * RFXB_NMAPS * g->plans.size())) return rc;
   if (int rc = galloc((void**)&g->d_status, sizeof(int))) return rc;
   RFXB_CUDA(cudaMemset(g->d_status, 0, sizeof(int)));
+  if (int rc = galloc((void**)&g->d_qctr, 8 * sizeof(int))) return rc;
+  RFXB_CUDA(cudaMemset(g->d_qctr, 0, 8 * sizeof(int)));
+  g->fwd_persist = g->fwd_split_avail ? fwd_persist_default() : 0;
+  g->adj_persist = (adj_persist_avail(g) && fwd_persist_default() > 0) ? 1 : 0;
   RFXB_CUDA(cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking));
   return 0;
 }
@@ -1135,9 +1184,25 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, b
   int par = par0;
   bool em = false;   // stage the PEC edge masks when a plan of the group has one
   for (auto* p : g->plans) em = em || p->inst.emask != nullptr;
+  // the persistent launches clear their fetch counters when they finish;
+  // clearing them here too keeps a sequence independent of earlier ones
+  if (g->fwd_persist > 0 && g->fwd_split_avail) RFXB_CUDA(cudaMemsetAsync(g->d_qctr, 0, 4 * sizeof(int), st));
   for (int s = 0; s < n_steps; ++s) {
     const int n = step0 + s;
-    if (g->fwd_split) {
+    if (g->fwd_persist > 0 && g->fwd_split_avail) {
+      RfxbFwdQueues Q{};
+      Q.list[0] = g->d_wf2;
+      Q.count[0] = g->n_wf2;
+      Q.list[1] = g->d_wf1;
+      Q.count[1] = g->n_wf1;
+      Q.ctr = g->d_qctr;
+      Q.status = g->d_status;
+      Q.plain_ctas = (g->fwd_persist - 1) * sm_count();
+      Q.fault_cta = g->fault_cta;
+      Q.wait_limit = g->wait_limit;
+      fwd_persist_kernel_for(em)<<<fwd_persist_grid(em), dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(
+          g->d_inst, (int)g->plans.size(), Q, g->d_maps, n, par);
+    } else if (g->fwd_split) {
       // staged-psi tiles on the caller's stream, CPML-free tiles beside them
       RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
       RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
@@ -1230,6 +1295,17 @@ int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, c
   }
   for (auto* p : g->plans) p->par = (par0 + n_steps) & 1;
   return 0;
+}
+
+bool adj_persist_avail(const RfxbBatch* g) { return g->adj_lite_avail && g->n_wa4 > 0 && g->n_wa1 > 0; }
+
+using AdjPersistKernel = void (*)(const RfxbInst*, const AdjInst*, int, RfxbAdjQueues, const CUtensorMap*, int, int,
+                                  int);
+AdjPersistKernel adj_persist_kernel_for(int zp) {
+  AdjPersistKernel k = adj_persist_kernel<kTY>;
+  allow_smem(reinterpret_cast<const void*>(k), adj_step_smem_bytes(5, 16));
+  (void)zp;
+  return k;
 }
 
 int ensure_adjoint(RfxbPlan* p, cudaStream_t st) {
@@ -1381,12 +1457,38 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
   const size_t asmem = adj_step_smem_bytes(amode, zp);
   auto launch = [&](cudaStream_t cs) -> int {
     int par = par0, fpar = fpar0;
+    if (g->adj_persist && amode == 2 && adj_persist_avail(g))
+      RFXB_CUDA(cudaMemsetAsync(g->d_qctr + 4, 0, 4 * sizeof(int), cs));
     for (int s = step_hi - 1; s >= step_hi - n_steps; --s) {
       if (two) {
         adj_pass_a<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
         adj_pass_b<<<g->n_work, dim3(32, kTY), 0, cs>>>(g->d_inst, g->d_adj, g->d_work, s, par, fpar);
       } else {
-        if (g->adj_split && amode != 0) {
+        if (g->adj_persist && amode == 2 && adj_persist_avail(g)) {
+          RfxbAdjQueues Q{};
+          Q.list[0] = g->d_wa2y;
+          Q.count[0] = g->n_wa2y;
+          Q.list[1] = g->d_wa4;
+          Q.count[1] = g->n_wa4;
+          Q.list[2] = g->d_wa1;
+          Q.count[2] = g->n_wa1;
+          Q.ctr = g->d_qctr + 4;
+          Q.status = g->d_status;
+          Q.role_ctas = sm_count();
+          Q.fault_cta = g->fault_cta;
+          Q.wait_limit = g->wait_limit;
+          Q.zp = zp;
+          const size_t psmem = adj_step_smem_bytes(5, zp);
+          AdjPersistKernel pk = adj_persist_kernel_for(zp);
+          if (g->adj_persist_grid <= 0) {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk, 32 * kTY, psmem) != cudaSuccess || per_sm < 1)
+              per_sm = 1;
+            g->adj_persist_grid = per_sm * sm_count();
+          }
+          pk<<<g->adj_persist_grid, dim3(32, kTY), psmem, cs>>>(g->d_inst, g->d_adj, (int)g->plans.size(), Q,
+                                                               g->d_maps, s, par, fpar);
+        } else if (g->adj_split && amode != 0) {
           // CPML tiles on the caller's stream, plain tiles beside them, and
           // (variant 2 groups) the CPML work without a y slab on variant 4
           const bool lite = g->adj_lite && amode == 2;
@@ -1976,7 +2078,8 @@ int rfxb_plan_device_status(RfxbPlan* p, void* stream) {
   RFXB_CUDA(cudaStreamSynchronize(st));
   int v = 0;
   RFXB_CUDA(cudaMemcpy(&v, p->self_group->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-  if (v) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
+  if (v & 1) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
+  if (v & 2) return fail(RFXB_E_WORK, "a persistent step kernel met an invalid work item and skipped it");
   return 0;
 }
 
@@ -1986,7 +2089,8 @@ int rfxb_batch_device_status(RfxbBatch* g, void* stream) {
   RFXB_CUDA(cudaStreamSynchronize(st));
   int v = 0;
   RFXB_CUDA(cudaMemcpy(&v, g->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-  if (v) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
+  if (v & 1) return fail(RFXB_E_TIMEOUT, "a pipeline wait in a step kernel ran out (device status word set)");
+  if (v & 2) return fail(RFXB_E_WORK, "a persistent step kernel met an invalid work item and skipped it");
   return 0;
 }
 
@@ -2044,10 +2148,11 @@ int rfxb_batch_forward_variant(const RfxbBatch* g) {
 
 namespace {
 void step_launches(const RfxbBatch* g, int* fwd, int* rev) {
-  if (fwd) *fwd = g->fwd_split ? 2 : 1;
+  if (fwd) *fwd = (g->fwd_persist > 0 && g->fwd_split_avail) ? 1 : g->fwd_split ? 2 : 1;
   if (rev) {
     if (g->adj_mode < 0) *rev = -1;
     else if (use_twopass()) *rev = 2;
+    else if (g->adj_persist && g->adj_mode == 2 && adj_persist_avail(g)) *rev = 1;
     else if (g->adj_split && g->adj_mode != 0)
       *rev = (g->adj_lite && g->adj_mode == 2) ? (g->n_wa2y > 0 ? 3 : 2) : 2;
     else *rev = 1;
@@ -2069,9 +2174,12 @@ int rfxb_batch_step_launches(const RfxbBatch* g, int* fwd, int* rev) {
 
 namespace {
 void launch_config(const RfxbBatch* g, RfxbLaunchConfig* cur, RfxbLaunchConfig* lim) {
-  if (cur) *cur = RfxbLaunchConfig{g->fwd_split ? 1 : 0, g->fwd_order, g->adj_lite ? 1 : 0, g->adj_order};
-  if (lim) *lim = RfxbLaunchConfig{g->fwd_split_avail ? 1 : 0, g->fwd_split_avail ? 1 : 0, g->adj_lite_avail ? 1 : 0,
-                                   g->adj_split ? 5 : 0};
+  if (cur)
+    *cur = RfxbLaunchConfig{g->fwd_split ? 1 : 0, g->fwd_order, g->adj_lite ? 1 : 0, g->adj_order, g->fwd_persist,
+                            g->adj_persist};
+  if (lim)
+    *lim = RfxbLaunchConfig{g->fwd_split_avail ? 1 : 0, g->fwd_split_avail ? 1 : 0, g->adj_lite_avail ? 1 : 0,
+                            g->adj_split ? 5 : 0, g->fwd_split_avail ? 3 : 0, adj_persist_avail(g) ? 1 : 0};
 }
 
 int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
@@ -2080,7 +2188,8 @@ int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
   launch_config(g, nullptr, &lim);
   auto in = [](int v, int hi) { return v >= 0 && v <= hi; };
   if (!in(c->fwd_split, lim.fwd_split) || !in(c->fwd_order, lim.fwd_order) || !in(c->adj_lite, lim.adj_lite) ||
-      !in(c->adj_order, lim.adj_order))
+      !in(c->adj_order, lim.adj_order) || !in(c->fwd_persist, lim.fwd_persist) ||
+      !in(c->adj_persist, lim.adj_persist))
     return fail(RFXB_E_INVALID, "launch configuration outside the limits of this plan/batch");
   // cached graphs hold the old launch sequence: drop them once nothing runs
   RFXB_CUDA(cudaDeviceSynchronize());
@@ -2090,9 +2199,44 @@ int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
   g->fwd_order = c->fwd_order;
   g->adj_lite = c->adj_lite != 0;
   g->adj_order = c->adj_order;
+  g->fwd_persist = c->fwd_persist;
+  g->adj_persist = c->adj_persist;
+  return 0;
+}
+
+int debug_fault(RfxbBatch* g, int cta, int wait_limit) {
+  if (wait_limit < 1) return fail(RFXB_E_INVALID, "wait_limit must be >= 1");
+  RFXB_CUDA(cudaDeviceSynchronize());
+  for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
+  g->graphs.clear();
+  g->fault_cta = cta;
+  g->wait_limit = wait_limit;
+  return 0;
+}
+
+int debug_poison(RfxbBatch* g, int list, int index) {
+  RfxbWork* lists[5] = {g->d_wf2, g->d_wf1, g->d_wa2y, g->d_wa4, g->d_wa1};
+  const int counts[5] = {g->n_wf2, g->n_wf1, g->n_wa2y, g->n_wa4, g->n_wa1};
+  if (list < 0 || list > 4 || !lists[list] || index < 0 || index >= counts[list])
+    return fail(RFXB_E_INVALID, "no such work list entry");
+  RFXB_CUDA(cudaDeviceSynchronize());
+  RfxbWork w{};
+  RFXB_CUDA(cudaMemcpy(&w, lists[list] + index, sizeof(w), cudaMemcpyDeviceToHost));
+  w.xb = w.xa;   // an empty x range: outside every kernel's contract
+  RFXB_CUDA(cudaMemcpy(lists[list] + index, &w, sizeof(w), cudaMemcpyHostToDevice));
   return 0;
 }
 }  // namespace
+
+int rfxb_batch_debug_fault(RfxbBatch* g, int cta, int wait_limit) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  return debug_fault(g, cta, wait_limit);
+}
+
+int rfxb_batch_debug_poison(RfxbBatch* g, int list, int index) {
+  if (!g) return fail(RFXB_E_INVALID, "null batch");
+  return debug_poison(g, list, index);
+}
 
 int rfxb_plan_launch_config(const RfxbPlan* p, RfxbLaunchConfig* current, RfxbLaunchConfig* limits) {
   if (!p || !p->self_group) return fail(RFXB_E_INVALID, "null plan");

@@ -48,12 +48,31 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: false if the phase did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it)
+// Bounded wait: false if the phase did not complete within `limit` polls
+// (each poll may suspend the thread for a hardware-defined time).
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity, int limit = 1 << 22) {
+  for (int it = 0; it < limit; ++it)
     if (mbar_try_wait(addr, parity)) return true;
   return false;
 }
+// Mbarrier phases carried from one work item to the next by a CTA that
+// processes several (the persistent kernels): bit s of `stage` is the parity
+// of the next completion of plane stage s, bit s of `ring` that of psi ring
+// slot s.  A CTA that runs one item starts from zero.
+struct StepPhases {
+  uint32_t stage = 0u;
+  uint32_t ring = 0u;
+};
+
+// Fault injection of the bounded-wait test (the defaults in every other
+// launch): the CTA whose block index is `cta` does not issue the TMA boxes
+// of plane xa of its first item, so its wait on that plane runs out after
+// `wait_limit` polls and the CTA takes the time-out path.
+struct StepFault {
+  int cta = -1;
+  int wait_limit = 1 << 22;
+};
+
 // 4-D tiled TMA load of one box into shared memory, completing on an mbarrier.
 // The innermost coordinate c0 must be a multiple of 4 (16 bytes of float).
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int c0, int c1, int c2, int c3,

@@ -378,27 +378,23 @@ struct FwdBounds { static constexpr int MIN_CTAS = 4; };
 template <>
 struct FwdBounds<2> { static constexpr int MIN_CTAS = 3; };
 
+// One work item (a (TY x 32) tile over an x range) of the forward step.
+// Returns false when a bounded wait ran out: the status word is then set and
+// every box the CTA issued has been waited for, so the caller must leave.
 // EM: the launch's plans have PEC edge masks, staged by TMA with the planes
 // (TMA modes); without EM the mask (if any) is read from global memory.
 template <int TY, int MODE, bool EM>
-__global__ void __launch_bounds__(32 * TY, FwdBounds<MODE>::MIN_CTAS)
-fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work,
-                const CUtensorMap* __restrict__ maps, int n, int par) {
+__device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const RfxbInst* __restrict__ insts,
+                                         const RfxbWork w, const CUtensorMap* __restrict__ maps, int n, int par,
+                                         StepPhases& ph, const StepFault& fault, bool first_item) {
   constexpr bool TMA = MODE != 0;
   using L = PsiSlot<TY>;
-  extern __shared__ __align__(128) unsigned char fwd_smem_raw[];
-  FwdSmem<TY>& S = *reinterpret_cast<FwdSmem<TY>*>(fwd_smem_raw);
-  float* ring = reinterpret_cast<float*>(fwd_smem_raw + sizeof(FwdSmem<TY>));   // mode 2: 2 slots
   const int lane = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * 32 + lane;
-  const RfxbWork w = work[blockIdx.x];
   load_inst(S.P, insts + w.inst, tid, 32 * TY);
-  if (TMA && tid == 0) {
-    for (int q = 0; q < RFXB_NSTAGE; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
-    if (MODE == 2) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
-    mbar_fence_init();
-  }
   __syncthreads();
+  const int wlim = fault.wait_limit;
+  const bool skip_first = first_item && (int)blockIdx.x == fault.cta;
   const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const RfxbInst& P = S.P;
   FwdCtx C;
@@ -471,13 +467,20 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   const bool pec_kz = ((pec & 4u) != 0) && (k == C.nz - 1);
 
   const int xa = w.xa, xb = w.xb;
+  // completion parity of the stage holding plane p (planes load in order
+  // xa-1, xa, ...: the k-th fill of a stage in this item is k phases past
+  // the phase the previous items left it in)
+  auto sparity = [&](int p) -> uint32_t {
+    return ((ph.stage >> stage_of(p)) ^ (uint32_t)((p - xa + 1) >> 2)) & 1u;
+  };
   // psi ring bookkeeping (mode 2; identical in every thread): which planes
   // need psi, the next phase parity of each slot, and fills in flight
   auto psi_need = [&](int p) {
     if (MODE != 2 || p < 0 || p >= C.nx) return false;
     return psi_tile || (C.cpx && (p < C.ncp || p >= C.nx - C.ncp));
   };
-  unsigned pph = 0u, pout = 0u;
+  unsigned& pph = ph.ring;
+  unsigned pout = 0u;
   auto psi_fill = [&](int p) {
     if (!psi_need(p)) return;
     if (tid == 0)
@@ -487,7 +490,7 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   auto psi_wait = [&](int p) -> bool {
     if (!psi_need(p)) return true;
     const int s = p & 1;
-    const bool ok = mbar_wait_bounded(smem_u32(&S.pbar[s]), (pph >> s) & 1u);
+    const bool ok = mbar_wait_bounded(smem_u32(&S.pbar[s]), (pph >> s) & 1u, wlim);
     if (ok) {
       pph ^= 1u << s;
       pout &= ~(1u << s);
@@ -499,20 +502,21 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
   auto bail = [&](int last_issued, int from) {
     if (tid == 0) {
       atomicOr(P.status, 1);
-      for (int p = from; p <= last_issued; ++p) mbar_wait_bounded(smem_u32(&S.mbar[stage_of(p)]), stage_parity(p, xa));
+      for (int p = from; p <= last_issued; ++p) mbar_wait_bounded(smem_u32(&S.mbar[stage_of(p)]), sparity(p), wlim);
       for (int s = 0; s < 2; ++s)
-        if (pout & (1u << s)) mbar_wait_bounded(smem_u32(&S.pbar[s]), (pph >> s) & 1u);
+        if (pout & (1u << s)) mbar_wait_bounded(smem_u32(&S.pbar[s]), (pph >> s) & 1u, wlim);
     }
   };
   if (TMA) {
     if (tid == 0) {
-      for (int p = xa - 1; p <= min(xa + 2, xb); ++p) tma_stage<TY, EM>(S, tm, par, y0, z0, p);
+      for (int p = xa - 1; p <= min(xa + 2, xb); ++p)
+        if (!(skip_first && p == xa)) tma_stage<TY, EM>(S, tm, par, y0, z0, p);
     }
     psi_fill(xa - 1);
     psi_fill(xa);
-    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa - 1)]), stage_parity(xa - 1, xa)) &&
-                    mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa)]), stage_parity(xa, xa)) && psi_wait(xa - 1);
-    if (__syncthreads_or(!ok)) { bail(min(xa + 2, xb), xa - 1); return; }
+    const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa - 1)]), sparity(xa - 1), wlim) &&
+                    mbar_wait_bounded(smem_u32(&S.mbar[stage_of(xa)]), sparity(xa), wlim) && psi_wait(xa - 1);
+    if (__syncthreads_or(!ok)) { bail(min(xa + 2, xb), xa - 1); return false; }
   } else {
     // pipeline: planes xa-1 and xa (group 0), xa+1 (group 1), xa+2 (group 2)
     load_stage<TY>(S, C, ca, cb, y0, z0, xa - 1, tid);
@@ -565,8 +569,8 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
       // plane i+1 has landed (and plane i's psi); after the barrier every
       // thread is done with plane i-1, whose stage takes plane i+3 and whose
       // psi slot takes plane i+1
-      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), stage_parity(i + 1, xa)) && psi_wait(i);
-      if (__syncthreads_or(!ok)) { bail(min(i + 2, xb), i + 1); return; }
+      const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), sparity(i + 1), wlim) && psi_wait(i);
+      if (__syncthreads_or(!ok)) { bail(min(i + 2, xb), i + 1); return false; }
       if (tid == 0 && i + 3 <= xb) tma_stage<TY, EM>(S, tm, par, y0, z0, i + 3);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
@@ -866,6 +870,109 @@ fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__
     hz_prev = hz;
   }
   if (!TMA) cp_async_wait<0>();
+  if (TMA) {   // the phases this item advanced: stage s filled by planes xa-1 .. xb
+    const int T = xb - xa + 2;
+    for (int st = 0; st < RFXB_NSTAGE; ++st) {
+      const int fills = T / RFXB_NSTAGE + ((((st - xa) % RFXB_NSTAGE + RFXB_NSTAGE) % RFXB_NSTAGE) < T % RFXB_NSTAGE ? 1 : 0);
+      ph.stage ^= (uint32_t)(fills & 1) << st;
+    }
+  }
+  __syncthreads();   // every thread is done with the stages and P before the next item reuses them
+  return true;
+}
+
+template <int TY, int MODE>
+__device__ __forceinline__ void fwd_init_barriers(FwdSmem<TY>& S, int tid) {
+  if (MODE != 0 && tid == 0) {
+    for (int q = 0; q < RFXB_NSTAGE; ++q) mbar_init(smem_u32(&S.mbar[q]), 1);
+    if (MODE == 2) { mbar_init(smem_u32(&S.pbar[0]), 1); mbar_init(smem_u32(&S.pbar[1]), 1); }
+    mbar_fence_init();
+  }
+  __syncthreads();
+}
+
+// One launch per step and variant: CTA b runs work item b.
+template <int TY, int MODE, bool EM>
+__global__ void __launch_bounds__(32 * TY, FwdBounds<MODE>::MIN_CTAS)
+fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work,
+                const CUtensorMap* __restrict__ maps, int n, int par) {
+  extern __shared__ __align__(128) unsigned char fwd_smem_raw[];
+  FwdSmem<TY>& S = *reinterpret_cast<FwdSmem<TY>*>(fwd_smem_raw);
+  float* ring = reinterpret_cast<float*>(fwd_smem_raw + sizeof(FwdSmem<TY>));   // mode 2: 2 slots
+  fwd_init_barriers<TY, MODE>(S, threadIdx.y * 32 + threadIdx.x);
+  StepPhases ph;
+  fwd_item<TY, MODE, EM>(S, ring, insts, work[blockIdx.x], maps, n, par, ph, StepFault{}, true);
+}
+
+// Whether a work item can be run: its instance exists and its tile and x
+// range lie inside that instance's grid on the tiling of the lists.
+template <int TY>
+__device__ __forceinline__ bool work_item_valid(const RfxbWork& w, const RfxbInst* insts, int n_inst) {
+  if (w.inst < 0 || w.inst >= n_inst) return false;
+  const RfxbInst& I = insts[w.inst];
+  return w.y0 >= 0 && w.y0 < I.ny && w.y0 % TY == 0 && w.z0 >= 0 && w.z0 < I.nz && w.z0 % RFXB_TZ == 0 &&
+         w.xa >= 0 && w.xa < w.xb && w.xb <= I.nx;
+}
+
+// Persistent forward step: one launch per step of exactly as many CTAs as
+// fit on the GPU at once.  Each CTA takes items from the two lists of the
+// step -- queue 0 the tiles that reach a CPML slab (the staged-psi path of
+// mode 2), queue 1 the CPML-free tiles (mode 1) -- through fetch counters in
+// device memory until both are empty.  The first `plain_ctas` CTAs (one per
+// SM when the block scheduler spreads the first wave) try queue 1 first,
+// the others queue 0, so latency-bound CPML tiles and bandwidth-bound plain
+// tiles share every SM; a CTA whose queue is empty helps with the other.
+// An item outside its instance's grid is skipped and flagged (status bit 2).
+// The last CTA to finish clears the counters for the next launch.
+template <int TY, bool EM>
+__global__ void __launch_bounds__(32 * TY, 3)
+fwd_persist_kernel(const RfxbInst* __restrict__ insts, int n_inst, RfxbFwdQueues Q,
+                   const CUtensorMap* __restrict__ maps, int n, int par) {
+  extern __shared__ __align__(128) unsigned char fwd_smem_raw[];
+  FwdSmem<TY>& S = *reinterpret_cast<FwdSmem<TY>*>(fwd_smem_raw);
+  float* ring = reinterpret_cast<float*>(fwd_smem_raw + sizeof(FwdSmem<TY>));
+  __shared__ int pick[2];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  fwd_init_barriers<TY, 2>(S, tid);
+  StepPhases ph;
+  StepFault fault;
+  fault.cta = Q.fault_cta;
+  fault.wait_limit = Q.wait_limit;
+  const int first = (int)blockIdx.x < Q.plain_ctas ? 1 : 0;
+  bool first_item = true;
+  bool ok = true;
+  while (ok) {
+    if (tid == 0) {
+      pick[0] = -1;
+      for (int t = 0; t < 2; ++t) {
+        const int q = t == 0 ? first : 1 - first;
+        if (*(volatile int*)&Q.ctr[q] >= Q.count[q]) continue;   // drained (counters only grow): no ticket
+        const int k = atomicAdd(&Q.ctr[q], 1);
+        if (k < Q.count[q]) { pick[0] = q; pick[1] = k; break; }
+      }
+    }
+    __syncthreads();
+    const int q = pick[0], k = pick[1];
+    __syncthreads();
+    if (q < 0) break;
+    const RfxbWork w = Q.list[q][k];
+    if (!work_item_valid<TY>(w, insts, n_inst)) {
+      if (tid == 0) atomicOr(Q.status, 2);
+      continue;
+    }
+    ok = q == 0 ? fwd_item<TY, 2, EM>(S, ring, insts, w, maps, n, par, ph, fault, first_item)
+                : fwd_item<TY, 1, EM>(S, ring, insts, w, maps, n, par, ph, fault, first_item);
+    first_item = false;
+  }
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(&Q.ctr[2], 1) == (int)gridDim.x - 1) {
+      Q.ctr[0] = 0;
+      Q.ctr[1] = 0;
+      Q.ctr[2] = 0;
+      __threadfence();
+    }
+  }
 }
 
 // Running DFT of one plane per launch entry, Kahan-compensated
@@ -963,6 +1070,11 @@ template __global__ void fwd_step_kernel<8, 1, true>(const RfxbInst*, const Rfxb
 template __global__ void fwd_step_kernel<8, 2, false>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int,
                                                       int);
 template __global__ void fwd_step_kernel<8, 2, true>(const RfxbInst*, const RfxbWork*, const CUtensorMap*, int, int);
+
+template __global__ void fwd_persist_kernel<8, false>(const RfxbInst*, int, RfxbFwdQueues, const CUtensorMap*, int,
+                                                       int);
+template __global__ void fwd_persist_kernel<8, true>(const RfxbInst*, int, RfxbFwdQueues, const CUtensorMap*, int,
+                                                      int);
 
 size_t fwd_step_smem_bytes(int mode) { return fwd_smem_bytes<8>(mode); }
 

@@ -108,6 +108,30 @@ struct RfxbWork {          // one CTA: a (y, z) tile over an x range
   int xa, xb;
 };
 
+// Work queues of the persistent forward step (one launch per step).
+struct RfxbFwdQueues {
+  const RfxbWork* list[2];   // 0: tiles that reach a CPML slab (staged psi), 1: CPML-free tiles
+  int count[2];
+  int* ctr;                  // [3]: fetch counters of the two lists, CTAs finished (zero between launches)
+  int* status;               // the group's status word (bit 1: a wait ran out, bit 2: an invalid item)
+  int plain_ctas;            // CTAs from block 0 on that try the CPML-free list first
+  int fault_cta;             // test only: block whose first item does not load its plane xa (-1: none)
+  int wait_limit;            // polls of a bounded mbarrier wait
+};
+
+// Work queues of the persistent reverse step: 0 tiles that reach a y slab
+// (variant 2), 1 the other CPML work (variant 4), 2 CPML-free tiles (variant 3).
+struct RfxbAdjQueues {
+  const RfxbWork* list[3];
+  int count[3];
+  int* ctr;                  // [4]: fetch counters of the three lists, CTAs finished
+  int* status;
+  int role_ctas;             // CTAs per role: blocks [r * role_ctas, (r+1) * role_ctas) have role r
+  int fault_cta;
+  int wait_limit;
+  int zp;                    // largest z-psi row of the group (ring slot size)
+};
+
 struct RfxbNtffFace {      // one face of one instance's NTFF box
   int inst;
   int axis, index;         // normal axis and face plane

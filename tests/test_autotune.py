@@ -62,6 +62,19 @@ def test_candidates_cover_the_limits():
     none = {"fwd_split": 0, "fwd_order": 0, "adj_lite": 0, "adj_order": 0}
     assert at.forward_candidates(none, none) == [{"fwd_split": 0, "fwd_order": 0}]
     assert at.reverse_candidates(none, none) == [{"adj_lite": 0, "adj_order": 0}]
+    # a target with the persistent launches: three more forward candidates
+    # (0, 1, 2 CPML-free-first CTAs per SM) and one more reverse candidate
+    full_p = dict(FULL, fwd_persist=3, adj_persist=1)
+    cur_p = {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": 0, "adj_persist": 0}
+    f = at.forward_candidates(full_p, cur_p)
+    assert f[0] == {"fwd_split": 1, "fwd_order": 0, "fwd_persist": 0} and len(f) == 6
+    assert {d["fwd_persist"] for d in f} == {0, 1, 2, 3}
+    r = at.reverse_candidates(full_p, cur_p)
+    assert r[0] == {"adj_lite": 1, "adj_order": 0, "adj_persist": 0} and len(r) == 9
+    assert r[-1] == {"adj_lite": 1, "adj_order": 0, "adj_persist": 1}
+    cur_p2 = dict(cur_p, fwd_persist=2, adj_persist=1)
+    assert at.forward_candidates(full_p, cur_p2)[0] == {"fwd_split": 1, "fwd_order": 0, "fwd_persist": 2}
+    assert at.reverse_candidates(full_p, cur_p2)[0] == {"adj_lite": 1, "adj_order": 0, "adj_persist": 1}
     # split reverse without variant 4: the two relative orders of 2 and 3
     lim = {"fwd_split": 0, "fwd_order": 0, "adj_lite": 0, "adj_order": 5}
     cur = {"fwd_split": 0, "fwd_order": 0, "adj_lite": 0, "adj_order": 4}   # (3, 4, 2): 3 before 2
@@ -146,7 +159,7 @@ def test_launch_config_bindings_validate_fields():
     lib = Lib()
     lib.get.__func__.__name__ = "rfxb_batch_launch_config"
     cur, lim = engine._get_launch(lib.get, None)
-    assert cur == {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0}
+    assert cur == {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": 0, "adj_persist": 0}
     assert lim["adj_order"] == 5
     engine._set_launch(lib.get, lib.set, None, {"adj_order": 3})
     assert engine._get_launch(lib.get, None)[0]["adj_order"] == 3
@@ -187,12 +200,19 @@ def test_every_launch_configuration_gives_the_same_sweep(cuda):
             configs.append({"fwd_split": 0})
         if lim["adj_lite"]:
             configs.append({"adj_lite": 0, "adj_order": 1})
+        assert lim["fwd_persist"] >= 1 and lim["adj_persist"] == 1
+        # the persistent launches run the same kernel variants on the same
+        # lists: bit-identical to the split launches
+        configs += [{"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": k,
+                     "adj_persist": 1} for k in range(1, lim["fwd_persist"] + 1)]
+        configs.append({"fwd_persist": 0, "adj_persist": 0})
         for c in configs:
             if any(v > lim[k] for k, v in c.items()):
                 continue
             sw.batch.set_launch_config(**c)
             J, g = _run(sw)
-            order_only = set(c) <= {"fwd_order", "adj_order"}
+            order_only = set(c) <= {"fwd_order", "adj_order"} or c.get("fwd_persist", 0) > 0 or (
+                c == {"fwd_persist": 0, "adj_persist": 0})
             for a, b in zip(g, g0):
                 # the launch order cannot change a value; another kernel
                 # variant on the same tiles may round differently
