@@ -350,6 +350,22 @@ def run_ours(args, rank, world, local_rank):
     # launches as the library reports (CPML / plain split, variant 4)
     fl, rl = sw.step_launches()
     launches = args.steps * (N * (fl + rl) + (1 if sw.batch is not None else len(sw.plans)))
+    sw.close()
+
+    # the other configurations, each timed on its own full step count (one
+    # GPU): large uniform, graded, adjoint with checkpoints every 64 steps
+    secondary = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        secondary = {}
+        for name, n_t in (("large_uniform", 4000), ("graded", 6000), ("adjoint_region", 3000)):
+            sargs = argparse.Namespace(**vars(args))
+            sargs.time_steps = n_t
+            sargs.steps = 2
+            sargs.warmup = max(3, min(args.warmup, 3))
+            torch.cuda.empty_cache()
+            sl = run_secondary(sargs, name, emit=False)
+            secondary[name] = {k: sl[k] for k in ("metric", "value", "unit", "steps", "warmup", "ms_per_step",
+                                                  "config", "roofline", "launch", "clocks")}
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 2), "higher_is_better": True,
@@ -357,9 +373,8 @@ def run_ours(args, rank, world, local_rank):
                 "config": _workload_config(args, total_cells, world), "roofline": roofline,
                 "roofline_other_kernel": roofline_other, "cpu_baseline": cpu,
                 "e2e": e2e, "single": single, "gpu_launches": launches, "launch": launch,
-                "clocks": clk.summary(), "host_wall_s_timed": round(t_host, 3)}
+                "clocks": clk.summary(), "host_wall_s_timed": round(t_host, 3), "secondary": secondary}
         print(json.dumps(line), flush=True)
-    sw.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -390,9 +405,10 @@ def run_reference(args, rank, world):
 # secondary workloads (the other configurations, on request)
 # ---------------------------------------------------------------------------
 
-def run_secondary(args, which):
+def run_secondary(args, which, emit=True):
     """One device-timed line for the large uniform, graded or adjoint
-    configuration: each bench step runs the configuration's full step count."""
+    configuration: each bench step runs the configuration's full step count.
+    Prints it (``emit``) or returns it."""
     import torch
 
     from rfx_b200 import workloads
@@ -495,8 +511,10 @@ def run_secondary(args, which):
                          "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "peak_source": peak_src,
                          "traffic": None, "algorithmic_bytes_per_step": int(alg)},
             "launch": launch, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
     plan.close()
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -513,6 +531,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch configuration")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the large-uniform, graded and adjoint configurations in the default line")
     ap.add_argument("--workload", default="batched_sweep",
                     choices=["batched_sweep", "large_uniform", "graded", "adjoint_region"],
                     help="batched_sweep is the headline line; the others print a secondary forward (or "

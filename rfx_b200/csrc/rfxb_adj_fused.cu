@@ -400,6 +400,9 @@ __device__ __forceinline__ bool adj_item(unsigned char* raw, const RfxbInst* __r
   }
   __syncthreads();
   const int wlim = fault.wait_limit;
+  // the thread that issues the TMA boxes: lane 0 of the last warp (warps 0
+  // and 1 compute the halo row and column of phase A)
+  const int producer = 32 * (TY - 1);
   const bool skip_first = first_item && (int)blockIdx.x == fault.cta;
   const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const RfxbInst& P = S.P;
@@ -470,7 +473,7 @@ __device__ __forceinline__ bool adj_item(unsigned char* raw, const RfxbInst* __r
   };
   auto psi_fill = [&](int p) {
     if (!psi_need(p)) return;
-    if (tid == 0)
+    if (tid == producer)
       apsi_issue<TY, YS>(ring + (p & 1) * L::FLOATS(zp), smem_u32(&S.pbar[p & 1]), tm, C, zp, y0, z0, p, yz_tile, ysd,
                      zsd, n4);
     pout |= 1u << (p & 1);
@@ -495,7 +498,7 @@ __device__ __forceinline__ bool adj_item(unsigned char* raw, const RfxbInst* __r
     }
   };
   if (TMA) {
-    if (tid == 0)
+    if (tid == producer)
       for (int p = xa - 1; p <= min(xa + NST - 2, xb); ++p)
         if (!(skip_first && p == xa)) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, p);
     psi_fill(xa);
@@ -567,13 +570,26 @@ __device__ __forceinline__ bool adj_item(unsigned char* raw, const RfxbInst* __r
                     P.ce[cell_index(C, xa, y0 + lane, z0 - 1)], false);
   }
 
+  // x spacing entries of the next plane, loaded one plane ahead
+  const float* xe_tab = P.xe;
+  const float* xh_tab = P.xh;
+  float xe1_n = __ldg(xe_tab + xa + 1), xhm_n = __ldg(xh_tab + xa - 1);
+  float xe0_n = __ldg(xe_tab + xa), xh0_n = __ldg(xh_tab + xa);
+
   for (int i = xa; i < xb; ++i) {
+    const float xe0 = xe0_n, xe1 = xe1_n, xh0 = xh0_n, xhm = xhm_n;
+    if (i + 1 < xb) {
+      xe0_n = xe1;
+      xhm_n = xh0;
+      xe1_n = __ldg(xe_tab + i + 2);
+      xh0_n = __ldg(xh_tab + i + 1);
+    }
     if (TMA) {
       // plane i+1 (and plane i's psi) have landed; after the barrier plane
       // i-1's stage takes plane i+NST-1 and its psi slot plane i+1
       const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[astage_of<NST>(i + 1)]), sparity(i + 1), wlim) && psi_wait(i);
       if (__syncthreads_or(!ok)) { bail(min(i + NST - 2, xb), i + 1); return false; }
-      if (tid == 0 && i + NST - 1 <= xb) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, i + NST - 1);
+      if (tid == producer && i + NST - 1 <= xb) adj_tma_stage<TY, NST>(S, tm, apar, y0, z0, i + NST - 1);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();
@@ -644,8 +660,6 @@ __device__ __forceinline__ bool adj_item(unsigned char* raw, const RfxbInst* __r
       }
       return v;
     };
-    const float xe0 = __ldg(P.xe + i), xe1 = __ldg(P.xe + i + 1);
-    const float xh0 = __ldg(P.xh + i), xhm = __ldg(P.xh + i - 1);
     const long long e = cell_index(C, i, j, k);
 
     // x relations of plane i+1 (written by this CTA when it owns that plane)

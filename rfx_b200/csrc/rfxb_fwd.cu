@@ -62,6 +62,11 @@ template <int TY>
 struct FwdSmem {
   FwdStage<TY> st[RFXB_NSTAGE];      // plane p lives in stage (p + 1) & 3
   float h[3][TY + 1][RFXB_TZ + 1];   // H^{n+1/2} of plane i: [y - y0 + 1][z - z0 + 1]
+  // mode 2: the y / z CPML profiles (b, c/cell, (1/kappa-1)/cell, on) of the
+  // halo cells, fixed along the x march: row y0-1 per lane, column z0-1 per
+  // row (each entry written and read by the same thread)
+  float4 hcp_row[2][RFXB_TZ];
+  float4 hcp_col[2][TY];
   RfxbInst P;
   unsigned long long mbar[RFXB_NSTAGE];
   unsigned long long pbar[2];        // psi ring (mode 2)
@@ -394,6 +399,9 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
   load_inst(S.P, insts + w.inst, tid, 32 * TY);
   __syncthreads();
   const int wlim = fault.wait_limit;
+  // the thread that issues the TMA boxes: lane 0 of the last warp (warps 0
+  // and 1 compute the halo row and column of H)
+  const int producer = 32 * (TY - 1);
   const bool skip_first = first_item && (int)blockIdx.x == fault.cta;
   const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const RfxbInst& P = S.P;
@@ -416,10 +424,17 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
   // spacing table entries of this thread's column and of the halo cells
   const float yh = own ? __ldg(P.yh + j) : 0.f, ye = own ? __ldg(P.ye + j) : 0.f;
   const float zh = own ? __ldg(P.zh + k) : 0.f, ze = own ? __ldg(P.ze + k) : 0.f;
-  const bool row_halo = (ty == 0) && (y0 >= 1) && (k < C.nz);
+  // The halo H is split over four warps so that none carries more than one
+  // extra component: row j = y0-1 hx by warp 0 and hz by warp 2, column
+  // k = z0-1 hx by warp 1 and hy by warp 3 (lanes < TY); the TMA producer is
+  // the last warp.
+  static_assert(TY >= 4, "the halo split needs four warps");
+  const int hcw = 1;                                    // warp writing the column halo profiles
+  const bool row_w = ty == 0 || ty == 2;
+  const bool row_halo = row_w && (y0 >= 1) && (k < C.nz);
   const float yh_row = row_halo ? __ldg(P.yh + y0 - 1) : 0.f;
-  const int hcw = TY > 1 ? 1 : 0;                       // warp computing the z halo column
-  const bool col_halo = (ty == hcw) && (lane < TY) && (z0 >= 1) && (y0 + lane < C.ny);
+  const bool col_w = (ty == 1 || ty == 3) && (lane < TY);
+  const bool col_halo = col_w && (z0 >= 1) && (y0 + lane < C.ny);
   const float yh_col = col_halo ? __ldg(P.yh + y0 + lane) : 0.f;
   const float zh_col = col_halo ? __ldg(P.zh + z0 - 1) : 0.f;
 
@@ -445,6 +460,36 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
     }
   }
   const bool psi_tile = ysd >= 0 || zsd >= 0;   // every plane needs the psi ring
+  // y / z profiles of the halo cells, fixed along the x march, into shared
+  // memory once per item: row y0-1 at this lane's column (warp 0) and column
+  // z0-1 at row y0+lane (warp hcw); .w = 1 where the cell is in the slab
+  if (MODE == 2) {
+    const float4 off = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ty == 0) {
+      float4 a = off, b = off;
+      if ((y0 >= 1) && (k < C.nz)) {
+        const int sy = y0 - 1 - jb;
+        if (ysd >= 0 && sy >= 0 && sy < C.ncp) { a = __ldg(P.cpt + (2 + ysd) * C.ncp + sy); a.w = 1.f; }
+        if (czo.on) { b = czo.c; b.w = 1.f; }
+        else if (zsd >= 0 && k - kb >= 0 && k - kb < C.ncp) {   // own lane past the grid edge only
+          b = __ldg(P.cpt + (4 + zsd) * C.ncp + (k - kb));
+          b.w = 1.f;
+        }
+      }
+      S.hcp_row[0][lane] = a;
+      S.hcp_row[1][lane] = b;
+    }
+    if ((ty == (TY > 1 ? 1 : 0)) && (lane < TY)) {
+      float4 a = off, b = off;
+      if ((z0 >= 1) && (y0 + lane < C.ny)) {
+        const int sy = y0 + lane - jb, sz = z0 - 1 - kb;
+        if (ysd >= 0 && sy >= 0 && sy < C.ncp) { a = __ldg(P.cpt + (2 + ysd) * C.ncp + sy); a.w = 1.f; }
+        if (zsd >= 0 && sz >= 0 && sz < C.ncp) { b = __ldg(P.cpt + (4 + zsd) * C.ncp + sz); b.w = 1.f; }
+      }
+      S.hcp_col[0][lane] = a;
+      S.hcp_col[1][lane] = b;
+    }
+  }
 
   // Sources and probes whose (j, k) is this thread's column.
   unsigned smask = 0u, pmask = 0u;
@@ -483,7 +528,7 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
   unsigned pout = 0u;
   auto psi_fill = [&](int p) {
     if (!psi_need(p)) return;
-    if (tid == 0)
+    if (tid == producer)
       psi_issue<TY>(ring + (p & 1) * L::FLOATS, smem_u32(&S.pbar[p & 1]), tm, P, par, y0, z0, p, C.cpx, ysd, zsd);
     pout |= 1u << (p & 1);
   };
@@ -508,7 +553,7 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
     }
   };
   if (TMA) {
-    if (tid == 0) {
+    if (tid == producer) {
       for (int p = xa - 1; p <= min(xa + 2, xb); ++p)
         if (!(skip_first && p == xa)) tma_stage<TY, EM>(S, tm, par, y0, z0, p);
     }
@@ -564,6 +609,14 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
   const bool has_hist = P.hist != nullptr && (n - P.hist_step0) >= 0 && (n - P.hist_step0) < P.hist_nsteps;
   const bool has_emask = P.emask != nullptr;
 
+  // the x spacing entries and x-slab profile of the next plane are loaded one
+  // plane ahead, so no plane starts by waiting on a global load
+  const float* xh_tab = P.xh;
+  const float* xe_tab = P.xe;
+  float xh_n = __ldg(xh_tab + xa), xe_n = __ldg(xe_tab + xa);
+  CpAx cx_n{false, make_float4(0.f, 0.f, 0.f, 0.f), 0};
+  if (MODE == 2) cx_n = x_ax(xa);
+
   for (int i = xa; i < xb; ++i) {
     if (TMA) {
       // plane i+1 has landed (and plane i's psi); after the barrier every
@@ -571,7 +624,7 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
       // psi slot takes plane i+1
       const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), sparity(i + 1), wlim) && psi_wait(i);
       if (__syncthreads_or(!ok)) { bail(min(i + 2, xb), i + 1); return false; }
-      if (tid == 0 && i + 3 <= xb) tma_stage<TY, EM>(S, tm, par, y0, z0, i + 3);
+      if (tid == producer && i + 3 <= xb) tma_stage<TY, EM>(S, tm, par, y0, z0, i + 3);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
@@ -580,11 +633,13 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
       cp_async_commit();
     }
     const int b0 = stage_of(i), b1 = stage_of(i + 1);
-    const float xh = __ldg(P.xh + i), xe = __ldg(P.xe + i);
+    const float xh = xh_n, xe = xe_n;
+    if (i + 1 < xb) { xh_n = __ldg(xh_tab + i + 1); xe_n = __ldg(xe_tab + i + 1); }
     const float* PS = ring + (i & 1) * L::FLOATS;
     CpAx cx{false, make_float4(0.f, 0.f, 0.f, 0.f), 0}, cy = cyo, cz = czo;
     if (MODE == 2) {
-      cx = x_ax(i);
+      cx = cx_n;
+      if (i + 1 < xb) cx_n = x_ax(i + 1);
       cy.off += i * C.ncp * C.zs;
       cz.off += i * C.ny * P.ncp4;
     }
@@ -606,46 +661,49 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
     S.h[0][ly][lh] = hx;
     S.h[1][ly][lh] = hy;
     S.h[2][ly][lh] = hz;
-    if (ty == 0) {  // halo row j = y0 - 1: hx, hz
+    if (row_w) {  // halo row j = y0 - 1: hx (warp 0), hz (warp 2)
       float a = 0.f, bq = 0.f, cq = 0.f;
       if (row_halo) {
         if (MODE == 2) {
           const int jr = y0 - 1;
           const float chc = C.ch ? C.ch[C.off0 + (long long)i * C.ps + (long long)jr * C.zs + k] : C.ch0;
-          CpAx ry{false, make_float4(0.f, 0.f, 0.f, 0.f), 0};
-          const int sy = jr - jb;
-          if (ysd >= 0 && sy >= 0 && sy < C.ncp) { ry.on = true; ry.c = __ldg(P.cpt + (2 + ysd) * C.ncp + sy); }
-          CpAx rz = czo;
-          if (zsd >= 0 && !rz.on && k - kb >= 0 && k - kb < C.ncp) {   // own lane past the grid edge only
-            rz.on = true;
-            rz.c = __ldg(P.cpt + (4 + zsd) * C.ncp + (k - kb));
-          }
-          h_cell2<TY, 5, false>(P, S, PS, C, b0, b1, 0, lz, 0, k - kb, chc, xh, yh_row, zh, cx, ry, rz, a, bq, cq);
+          const float4 qy = S.hcp_row[0][lane], qz = S.hcp_row[1][lane];
+          const CpAx ry{qy.w != 0.f, qy, 0}, rz{qz.w != 0.f, qz, 0};
+          if (ty == 0)
+            h_cell2<TY, 1, false>(P, S, PS, C, b0, b1, 0, lz, 0, k - kb, chc, xh, yh_row, zh, cx, ry, rz, a, bq, cq);
+          else
+            h_cell2<TY, 4, false>(P, S, PS, C, b0, b1, 0, lz, 0, k - kb, chc, xh, yh_row, zh, cx, ry, rz, a, bq, cq);
         } else {
-          h_cell<TY, 5>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
+          if (ty == 0) h_cell<TY, 1>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
+          else h_cell<TY, 4>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
         }
       }
-      S.h[0][0][lh] = a;
-      S.h[2][0][lh] = cq;
+      if (ty == 0) S.h[0][0][lh] = a;
+      else S.h[2][0][lh] = cq;
     }
-    if (ty == hcw && lane < TY) {  // halo column k = z0 - 1: hx, hy
+    if (col_w) {  // halo column k = z0 - 1: hx (warp 1), hy (warp 3)
       float a = 0.f, bq = 0.f, cq = 0.f;
       if (col_halo) {
         if (MODE == 2) {
           const int jc = y0 + lane, kc = z0 - 1;
           const float chc = C.ch ? C.ch[C.off0 + (long long)i * C.ps + (long long)jc * C.zs + kc] : C.ch0;
-          CpAx ry{false, make_float4(0.f, 0.f, 0.f, 0.f), 0}, rz{false, make_float4(0.f, 0.f, 0.f, 0.f), 0};
-          const int sy = jc - jb, sz = kc - kb;
-          if (ysd >= 0 && sy >= 0 && sy < C.ncp) { ry.on = true; ry.c = __ldg(P.cpt + (2 + ysd) * C.ncp + sy); }
-          if (zsd >= 0 && sz >= 0 && sz < C.ncp) { rz.on = true; rz.c = __ldg(P.cpt + (4 + zsd) * C.ncp + sz); }
-          h_cell2<TY, 3, false>(P, S, PS, C, b0, b1, lane + 1, 3, lane + 1, sz, chc, xh, yh_col, zh_col, cx, ry, rz,
-                                a, bq, cq);
+          const float4 qy = S.hcp_col[0][lane], qz = S.hcp_col[1][lane];
+          const CpAx ry{qy.w != 0.f, qy, 0}, rz{qz.w != 0.f, qz, 0};
+          if (ty == 1)
+            h_cell2<TY, 1, false>(P, S, PS, C, b0, b1, lane + 1, 3, lane + 1, kc - kb, chc, xh, yh_col, zh_col, cx,
+                                  ry, rz, a, bq, cq);
+          else
+            h_cell2<TY, 2, false>(P, S, PS, C, b0, b1, lane + 1, 3, lane + 1, kc - kb, chc, xh, yh_col, zh_col, cx,
+                                  ry, rz, a, bq, cq);
         } else {
-          h_cell<TY, 3>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false, a, bq, cq);
+          if (ty == 1)
+            h_cell<TY, 1>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false, a, bq, cq);
+          else
+            h_cell<TY, 2>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false, a, bq, cq);
         }
       }
-      S.h[0][lane + 1][0] = a;
-      S.h[1][lane + 1][0] = bq;
+      if (ty == 1) S.h[0][lane + 1][0] = a;
+      else S.h[1][lane + 1][0] = bq;
     }
     __syncthreads();
 

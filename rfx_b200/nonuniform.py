@@ -140,6 +140,7 @@ def run_nonuniform_until_decay(grid, materials, *, decay_by=1e-3, check_interval
                     min(lo[2], hi[2]), max(lo[2], hi[2]))
         peak_u, below, peak_flux, flux_hist, checks = 0.0, 0, 0.0, [], []
         done = 0
+        fired = False
         while done < max_steps:
             k = min(int(check_interval), max_steps - done)
             plan.advance(0, k,
@@ -166,12 +167,17 @@ def run_nonuniform_until_decay(grid, materials, *, decay_by=1e-3, check_interval
                 if u < decay_by * peak_u:
                     below += 1
                     if below >= decay_energy_consecutive:
+                        fired = True
                         break
                 else:
                     below = 0
         plan.check_device()
         ts = r.probe_out[:done].cpu().numpy() if r.probe_out is not None else np.zeros((done, 0), np.float32)
-        state = FDTDState(*[t.cpu().numpy() for t in plan.store_fields()], step=done)
+        fields = [t.cpu().numpy() for t in plan.store_fields()]
+        if not flux_stop and not fired:   # rfx/nonuniform.py:2234-2242
+            from .simulation import warn_static_remnant_cap_hit
+            warn_static_remnant_cap_hit(fields, materials, grid)
+        state = FDTDState(*fields, step=done)
         out = {"state": state, "time_series": ts if emit_time_series else None, "dt": grid.dt,
                "decay_checks": checks}
         if planes:

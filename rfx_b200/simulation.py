@@ -19,7 +19,7 @@ import torch
 from .cpml import build_cpml
 from .engine import Plan, PlanSpec, require_cuda
 from .farfield import init_ntff_data, ntff_descriptor, ntff_phase_table, pack_ntff, unpack_ntff
-from .grid import face_pads, spacing_tables
+from .grid import EPS_0, MU_0, face_pads, spacing_tables
 from .sources import SourceSpec  # noqa: F401  (re-export: the reference's spec type)
 
 
@@ -516,6 +516,7 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
         # other stops only check once min_steps are done
         n_check = 0 if flux_stop else -(-(max(min_steps, 1) - 1) // check_interval) * check_interval
         done = 0
+        fired = False
         while done < max_steps:
             target = min(n_check + 1, max_steps)
             # steps done .. target-1, relative to the tables' row `done` (the
@@ -545,6 +546,7 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
                 if u < decay_by * peak_u:
                     below += 1
                     if below >= decay_energy_consecutive:
+                        fired = True
                         break
                 else:
                     below = 0
@@ -559,8 +561,13 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
                                                                                                np.float32)
         out_planes = tuple(d._replace(accumulator=a.cpu().numpy()) for d, a in zip(planes, r.dft_accs))
         state = None
+        fields = None
+        if return_state or (absorbing and not flux_stop and not fired):
+            fields = [t.cpu().numpy() for t in plan.store_fields()]
+        if absorbing and not flux_stop and not fired:
+            warn_static_remnant_cap_hit(fields, materials, grid)
         if return_state:
-            state = FDTDState(*[t.cpu().numpy() for t in plan.store_fields()], step=done)
+            state = FDTDState(*fields, step=done)
         ntff_data = unpack_ntff(ntff, r.ntff[0], r.ntff[1]) if ntff is not None else None
         flux = None
         if flux_monitors:
@@ -573,6 +580,44 @@ def run_until_decay(grid, materials, *, decay_by=1e-3, check_interval=50, min_st
                          dft_planes=out_planes if planes else None, flux_monitors=flux, ntff_box=ntff, grid=grid)
     finally:
         plan.close()
+
+
+def warn_static_remnant_cap_hit(fields, materials, grid) -> bool:
+    """The measured post-run advisory of rfx/simulation.py:2145-2197 (issue
+    #388), used by both lanes' decay loops when max_steps was reached and the
+    interior-energy criterion never fired.
+
+    A soft current source can leave a static charge remnant whose electric
+    self-energy neither radiates nor is absorbed, so the interior energy stays
+    above decay_by * peak.  A radiating field splits its energy roughly evenly
+    between E and H; the remnant is electric only.  When the magnetic share of
+    the final interior energy (0.5 eps |E|^2 vs 0.5 mu |H|^2 over the cells
+    inside the CPML pads) is below 1e-2 this warns (UserWarning) and returns
+    True."""
+    import warnings
+    ex, ey, ez, hx, hy, hz = (np.asarray(f, np.float64) for f in fields)
+    nx, ny, nz = ex.shape
+    sl = (slice(grid.pad_x_lo, nx - grid.pad_x_hi), slice(grid.pad_y_lo, ny - grid.pad_y_hi),
+          slice(grid.pad_z_lo, nz - grid.pad_z_hi))
+    eps = np.asarray(materials.eps_r, np.float64)[sl]
+    mu = getattr(materials, "mu_r", None)
+    mu = np.asarray(mu, np.float64)[sl] if mu is not None and np.ndim(mu) > 0 else 1.0
+    u_e = 0.5 * EPS_0 * float(np.sum(eps * (ex[sl] ** 2 + ey[sl] ** 2 + ez[sl] ** 2)))
+    u_h = 0.5 * MU_0 * float(np.sum(mu * (hx[sl] ** 2 + hy[sl] ** 2 + hz[sl] ** 2)))
+    tot = u_e + u_h
+    if tot <= 0.0:
+        return False
+    h_share = u_h / tot
+    if h_share >= 1e-2:
+        return False
+    warnings.warn(
+        f"run_until_decay reached max_steps without the interior-energy criterion firing, and "
+        f"{100.0 * (1.0 - h_share):.1f}% of the final interior energy is electric (magnetic share "
+        f"{h_share:.1e}): a static charge remnant of the soft source is holding the interior energy "
+        f"above decay_by * peak while the radiating field has settled.  Stop on the radiated flux "
+        f"instead (radiated_flux_box=((x0, y0, z0), (x1, y1, z1)) around the radiator), lower the "
+        f"source's DC content, or run a fixed n_steps.", UserWarning, stacklevel=3)
+    return True
 
 
 def extract_lumped_s11(v_dft, i_dft, z0=50.0):

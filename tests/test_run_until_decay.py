@@ -205,3 +205,30 @@ def test_graded_run_until_decay_rejects_bad_arguments():
         rfx_b200.run_nonuniform_until_decay(pg, m, max_steps=0, sources=srcs)
     with pytest.raises(NotImplementedError):
         rfx_b200.run_nonuniform_until_decay(pg, m, debye=((1.0,), (1e-9,)), sources=srcs)
+
+
+def test_static_remnant_advisory_on_cap_hit():
+    """rfx/simulation.py:2145-2197: after an energy cap-hit, an interior
+    energy that is almost all electric (a static source-charge remnant) draws
+    the advisory warning; an equipartitioned (radiating) field does not."""
+    import warnings
+
+    import rfx_b200
+    from rfx_b200.simulation import warn_static_remnant_cap_hit
+    g = rfx_b200.Grid(freq_max=10e9, domain=(0.01, 0.01, 0.01), dx=1e-3, cpml_layers=4)
+    shape = tuple(g.shape)
+    mats = rfx_b200.MaterialArrays(np.ones(shape, np.float32), np.zeros(shape, np.float32), np.ones(shape, np.float32))
+    rng = np.random.default_rng(0)
+    e = [rng.standard_normal(shape).astype(np.float32) for _ in range(3)]
+    eta = float(np.sqrt(rfx_b200.grid.MU_0 / rfx_b200.grid.EPS_0))
+    static = e + [np.zeros(shape, np.float32)] * 3
+    with pytest.warns(UserWarning, match="static charge remnant"):
+        assert warn_static_remnant_cap_hit(static, mats, g)
+    radiating = e + [(rng.standard_normal(shape) / eta).astype(np.float32) for _ in range(3)]
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        assert not warn_static_remnant_cap_hit(radiating, mats, g)
+    # cells inside the CPML pads do not count
+    pads_only = [np.zeros(shape, np.float32) for _ in range(6)]
+    pads_only[0][0, 0, 0] = 1.0
+    assert not warn_static_remnant_cap_hit(pads_only, mats, g)
