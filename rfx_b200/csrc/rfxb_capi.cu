@@ -974,9 +974,9 @@ int build_group(RfxbBatch* g) {
       balance_segments(ay, 3 * sm_count(), 3.0, a2y);
       int zp = 4;
       for (auto* p : g->plans) zp = std::max(zp, p->inst.ncp4);
-      // resident CTAs of variant 4: four per SM when its shared memory (plus
-      // the 1 KB the runtime reserves per CTA) fits four times
-      const int per_sm = (int)(4 * (adj_step_smem_bytes(4, zp) + 1024) <= (size_t)smem_per_sm() ? 4 : 3);
+      // resident CTAs of variant 4: three per SM (its launch bounds give it
+      // 80 registers)
+      const int per_sm = 3;
       balance_segments(anoy, per_sm * sm_count(), 3.0, a4);
       if (!a4.empty()) {
         if (!a2y.empty()) {

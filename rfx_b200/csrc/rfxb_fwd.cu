@@ -430,10 +430,10 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
   // the last warp.
   static_assert(TY >= 4, "the halo split needs four warps");
   const int hcw = 1;                                    // warp writing the column halo profiles
-  const bool row_w = ty == 0 || ty == 2;
+  const bool row_w = ty == 0;
   const bool row_halo = row_w && (y0 >= 1) && (k < C.nz);
   const float yh_row = row_halo ? __ldg(P.yh + y0 - 1) : 0.f;
-  const bool col_w = (ty == 1 || ty == 3) && (lane < TY);
+  const bool col_w = (ty == 1) && (lane < TY);
   const bool col_halo = col_w && (z0 >= 1) && (y0 + lane < C.ny);
   const float yh_col = col_halo ? __ldg(P.yh + y0 + lane) : 0.f;
   const float zh_col = col_halo ? __ldg(P.zh + z0 - 1) : 0.f;
@@ -661,7 +661,7 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
     S.h[0][ly][lh] = hx;
     S.h[1][ly][lh] = hy;
     S.h[2][ly][lh] = hz;
-    if (row_w) {  // halo row j = y0 - 1: hx (warp 0), hz (warp 2)
+    if (ty == 0) {  // halo row j = y0 - 1: hx, hz
       float a = 0.f, bq = 0.f, cq = 0.f;
       if (row_halo) {
         if (MODE == 2) {
@@ -669,19 +669,15 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
           const float chc = C.ch ? C.ch[C.off0 + (long long)i * C.ps + (long long)jr * C.zs + k] : C.ch0;
           const float4 qy = S.hcp_row[0][lane], qz = S.hcp_row[1][lane];
           const CpAx ry{qy.w != 0.f, qy, 0}, rz{qz.w != 0.f, qz, 0};
-          if (ty == 0)
-            h_cell2<TY, 1, false>(P, S, PS, C, b0, b1, 0, lz, 0, k - kb, chc, xh, yh_row, zh, cx, ry, rz, a, bq, cq);
-          else
-            h_cell2<TY, 4, false>(P, S, PS, C, b0, b1, 0, lz, 0, k - kb, chc, xh, yh_row, zh, cx, ry, rz, a, bq, cq);
+          h_cell2<TY, 5, false>(P, S, PS, C, b0, b1, 0, lz, 0, k - kb, chc, xh, yh_row, zh, cx, ry, rz, a, bq, cq);
         } else {
-          if (ty == 0) h_cell<TY, 1>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
-          else h_cell<TY, 4>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
+          h_cell<TY, 5>(P, S, C, b0, b1, i, y0 - 1, k, 0, lz, xh, yh_row, zh, false, a, bq, cq);
         }
       }
-      if (ty == 0) S.h[0][0][lh] = a;
-      else S.h[2][0][lh] = cq;
+      S.h[0][0][lh] = a;
+      S.h[2][0][lh] = cq;
     }
-    if (col_w) {  // halo column k = z0 - 1: hx (warp 1), hy (warp 3)
+    if (ty == hcw && lane < TY) {  // halo column k = z0 - 1: hx, hy
       float a = 0.f, bq = 0.f, cq = 0.f;
       if (col_halo) {
         if (MODE == 2) {
@@ -689,21 +685,14 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
           const float chc = C.ch ? C.ch[C.off0 + (long long)i * C.ps + (long long)jc * C.zs + kc] : C.ch0;
           const float4 qy = S.hcp_col[0][lane], qz = S.hcp_col[1][lane];
           const CpAx ry{qy.w != 0.f, qy, 0}, rz{qz.w != 0.f, qz, 0};
-          if (ty == 1)
-            h_cell2<TY, 1, false>(P, S, PS, C, b0, b1, lane + 1, 3, lane + 1, kc - kb, chc, xh, yh_col, zh_col, cx,
-                                  ry, rz, a, bq, cq);
-          else
-            h_cell2<TY, 2, false>(P, S, PS, C, b0, b1, lane + 1, 3, lane + 1, kc - kb, chc, xh, yh_col, zh_col, cx,
-                                  ry, rz, a, bq, cq);
+          h_cell2<TY, 3, false>(P, S, PS, C, b0, b1, lane + 1, 3, lane + 1, kc - kb, chc, xh, yh_col, zh_col, cx, ry,
+                                rz, a, bq, cq);
         } else {
-          if (ty == 1)
-            h_cell<TY, 1>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false, a, bq, cq);
-          else
-            h_cell<TY, 2>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false, a, bq, cq);
+          h_cell<TY, 3>(P, S, C, b0, b1, i, y0 + lane, z0 - 1, lane + 1, 3, xh, yh_col, zh_col, false, a, bq, cq);
         }
       }
-      if (ty == 1) S.h[0][lane + 1][0] = a;
-      else S.h[1][lane + 1][0] = bq;
+      S.h[0][lane + 1][0] = a;
+      S.h[1][lane + 1][0] = bq;
     }
     __syncthreads();
 
