@@ -235,7 +235,11 @@ struct RfxbBatch {
   int dft_blocks = 0;
   std::vector<void*> allocs;
   cudaStream_t cap_stream = nullptr;
+  // captured step sequences by key, with the call counter of their last use
+  // (least recently used evicted first)
   std::map<GraphKey, cudaGraphExec_t> graphs;
+  std::map<GraphKey, unsigned long long> graph_use;
+  unsigned long long graph_clock = 0;
   ~RfxbBatch() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -1253,9 +1257,23 @@ template <typename F>
 int run_graph(RfxbBatch* g, const GraphKey& key, cudaStream_t st, F&& launch) {
   auto it = g->graphs.find(key);
   if (it == g->graphs.end()) {
-    if (g->graphs.size() >= 64) {   // bound the cache
-      for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
-      g->graphs.clear();
+    // Bound the cache.  A checkpointed run keeps one forward and one reverse
+    // graph per segment alive (about 100 for 3000 steps at K = 64), so the
+    // bound is well above that and the least recently used graph goes first.
+    constexpr size_t kMaxGraphs = 512;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cap);
+    if (g->graphs.size() >= kMaxGraphs && cap == cudaStreamCaptureStatusNone) {
+      auto victim = g->graphs.begin();
+      unsigned long long oldest = ~0ull;
+      for (auto v = g->graphs.begin(); v != g->graphs.end(); ++v) {
+        const unsigned long long u = g->graph_use[v->first];
+        if (u < oldest) { oldest = u; victim = v; }
+      }
+      RFXB_CUDA(cudaStreamSynchronize(st));   // nothing of the victim may still run
+      cudaGraphExecDestroy(victim->second);
+      g->graph_use.erase(victim->first);
+      g->graphs.erase(victim);
     }
     RFXB_CUDA(cudaStreamBeginCapture(g->cap_stream, cudaStreamCaptureModeThreadLocal));
     const int rc = launch(g->cap_stream);
@@ -1272,6 +1290,7 @@ int run_graph(RfxbBatch* g, const GraphKey& key, cudaStream_t st, F&& launch) {
     if (ei != cudaSuccess) return fail(RFXB_E_LAUNCH, std::string("graph instantiate: ") + cudaGetErrorString(ei));
     it = g->graphs.emplace(key, exec).first;
   }
+  g->graph_use[key] = ++g->graph_clock;
   RFXB_CUDA(cudaGraphLaunch(it->second, st));
   return 0;
 }
@@ -2195,6 +2214,7 @@ int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
   RFXB_CUDA(cudaDeviceSynchronize());
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
   g->graphs.clear();
+  g->graph_use.clear();
   g->fwd_split = c->fwd_split != 0;
   g->fwd_order = c->fwd_order;
   g->adj_lite = c->adj_lite != 0;
@@ -2209,6 +2229,7 @@ int debug_fault(RfxbBatch* g, int cta, int wait_limit) {
   RFXB_CUDA(cudaDeviceSynchronize());
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
   g->graphs.clear();
+  g->graph_use.clear();
   g->fault_cta = cta;
   g->wait_limit = wait_limit;
   return 0;
