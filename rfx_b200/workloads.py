@@ -103,6 +103,23 @@ def graded(seed=0, n_steps=6000):
     return g, eps, sig, pec, src, probes, dft
 
 
+def pec_uniform(n_cells=512, n_steps=1000):
+    """The reference's own GPU throughput benchmark (rfx/gpu.py:58-107, the
+    figure quoted in its README): a PEC-bounded vacuum cube with no CPML,
+    dx = 1 mm, a raw Ez field source GaussianPulse(f0 = 5 GHz) and an Ez probe
+    at the centre, run() for n_steps.  The published grid size is not stated;
+    n_cells = 512 fills a B200 (513^3 cells with the +1 fence)."""
+    from .sources import make_source
+    dx = 1e-3
+    g = Grid(freq_max=10e9, domain=(n_cells * dx,) * 3, dx=dx, cpml_layers=0)
+    eps = np.ones(g.shape, np.float32)
+    sig = np.zeros(g.shape, np.float32)
+    centre = tuple(n_cells * dx / 2 for _ in range(3))
+    src = make_source(g, centre, "ez", GaussianPulse(5e9), n_steps)
+    prb = g.position_to_index(centre)
+    return g, eps, sig, src, prb
+
+
 def adjoint_region(seed=0, n_steps=3000):
     rng = np.random.default_rng(seed)
     dx = 0.5e-3
