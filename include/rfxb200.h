@@ -372,6 +372,9 @@ int rfxb_batch_step_launches(const RfxbBatch* batch, int* fwd, int* rev);
  *   adj_persist  0: the launches above; 1: one persistent launch per reverse
  *                 step over the three reverse lists, one CTA per SM taking
  *                 each list first
+ *   l2_promo   L2 promotion of the plans' TMA boxes: 0 none, 1 64 B,
+ *                 2 128 B, 3 256 B (how much of a partly covered line a halo
+ *                 miss fetches; the plans' maps are re-encoded)
  * rfxb_*_launch_config writes the current setting to *current and the
  * largest value each field accepts on this plan/batch to *limits (0 where a
  * choice does not exist, e.g. fwd_split on a group without staged-psi CPML).
@@ -386,6 +389,7 @@ typedef struct RfxbLaunchConfig {
   int32_t adj_order;
   int32_t fwd_persist;
   int32_t adj_persist;
+  int32_t l2_promo;
 } RfxbLaunchConfig;
 
 int rfxb_plan_launch_config(const RfxbPlan* plan, RfxbLaunchConfig* current, RfxbLaunchConfig* limits);

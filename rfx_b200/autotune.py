@@ -4,8 +4,12 @@ A plan or batch can launch its step kernels in several equivalent ways (the
 ``RfxbLaunchConfig`` fields of ``rfxb200.h``): the forward tiles split
 between the CPML-free kernel and the staged-psi kernel on two streams or run
 as one launch, which of the concurrent launches the captured graph hands to
-the SMs first, and whether the reverse step's CPML work without a y slab runs
-on variant 4 or on variant 2.  Every setting computes the same steps; which
+the SMs first, whether the reverse step's CPML work without a y slab runs
+on variant 4 or on variant 2, whether a persistent launch over device work
+queues replaces the split launches, and the L2 promotion of the TMA boxes
+(how much of a partly covered line a halo miss fetches; 64 B measured 1.6 %
+faster than 128 B on the batched sweep and 2.8 % slower on a 513^3 PEC
+grid).  Every setting computes the same steps; which
 one is fastest depends on the workload (grid sizes, CPML share, number of
 instances).  The autotuner times a few steps of each candidate with CUDA
 events on the real workload, keeps the fastest, and caches the choice by a
@@ -36,12 +40,14 @@ class TuneResult:
     config: dict
     forward_ms: dict = field(default_factory=dict)
     reverse_ms: dict = field(default_factory=dict)
+    promo_ms: dict = field(default_factory=dict)
     cached: bool = False
 
     def as_json(self) -> dict:
         return {"config": self.config, "cached": self.cached,
                 "forward_ms": {_key_str(k): v for k, v in self.forward_ms.items()},
-                "reverse_ms": {_key_str(k): v for k, v in self.reverse_ms.items()}}
+                "reverse_ms": {_key_str(k): v for k, v in self.reverse_ms.items()},
+                "l2_promo_ms": {_key_str(k): v for k, v in self.promo_ms.items()}}
 
 
 def _key_str(k) -> str:
@@ -171,6 +177,21 @@ def autotune(target, run_forward, run_reverse=None, *, signature=None, cache_pat
         best = dict(pick(res.reverse_ms, rel_margin))
         target.set_launch_config(**best)
         res.config.update(best)
+    # the L2 promotion of the TMA boxes, timed on the whole step (forward and
+    # reverse together) with the chosen launches in place
+    if limits.get("l2_promo", 0):
+        cur_p = target.launch_config()[0]["l2_promo"]
+        pc = [cur_p] + [v for v in range(limits["l2_promo"] + 1) if v != cur_p]
+
+        def whole_step():
+            a = run_forward()
+            b = run_reverse() if run_reverse is not None else None
+            return (a or 0.0) + (b or 0.0)   # what a stand-in timer measures; CUDA events ignore it
+        for v in pc:
+            target.set_launch_config(l2_promo=v)
+            res.promo_ms[(("l2_promo", v),)] = _time(whole_step, repeats, timer)
+        best = dict(pick(res.promo_ms, rel_margin))
+        target.set_launch_config(**best)
     res.config = target.launch_config()[0]
     if key is not None:
         _memory_cache[key] = dict(res.config)

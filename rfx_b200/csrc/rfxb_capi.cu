@@ -142,6 +142,7 @@ struct RfxbPlan {
   CUtensorMap tmaps[RFXB_NMAPS];
   bool psi_maps_ok = false;    // the CPML psi maps encoded (staged-psi kernel usable)
   bool adj_psi_maps_ok = false;  // the same for the adjoint psi
+  int l2promo = 2;             // L2 promotion of this plan's TMA maps: 0 none, 1 64 B, 2 128 B, 3 256 B
 
   ~RfxbPlan() {
     for (void* p : allocs) cudaFree(p);
@@ -640,16 +641,22 @@ bool use_tma() {
   return v == 1;
 }
 
-// L2 sector promotion of the TMA boxes (RFXB_L2PROMO = none | 64 | 128 |
-// 256; default 128).  The boxes' halo columns cover only part of a line, so
-// promotion decides how much of the neighbour's line a halo miss drags in.
-CUtensorMapL2promotion l2_promotion() {
+// L2 sector promotion of the TMA boxes.  The boxes' halo columns cover only
+// part of a line, so promotion decides how much of the neighbour's line a
+// halo miss drags in; which setting is fastest depends on the workload (the
+// launch configuration's l2_promo field, chosen by the autotuner).  Default
+// of a new plan: RFXB_L2PROMO = none | 64 | 128 | 256, else 128.
+int l2_promotion_default() {
   static int v = -1;
   if (v < 0) {
     const char* e = getenv("RFXB_L2PROMO");
     const std::string m = e ? e : "128";
     v = m == "none" ? 0 : m == "64" ? 1 : m == "256" ? 3 : 2;
   }
+  return v;
+}
+
+CUtensorMapL2promotion l2_promotion(int v) {
   return v == 0 ? CU_TENSOR_MAP_L2_PROMOTION_NONE
          : v == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
          : v == 3 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B
@@ -685,7 +692,7 @@ int encode_block_map(CUtensorMap* m, const RfxbPlan& p, float* block, int ncomp,
   cuuint32_t box[4] = {bx, by, 1, bc};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, addr, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(p.l2promo),
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return 0;
@@ -703,7 +710,7 @@ int encode_emask_map(RfxbPlan* p) {
   cuuint32_t box[4] = {32, (cuuint32_t)kTY, 1, 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r = fn(&p->tmaps[RFXB_MAP_EMASK], CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, addr, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(p->l2promo),
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled (edge mask) failed (" + std::to_string((int)r) + ")");
   return 0;
@@ -711,7 +718,8 @@ int encode_emask_map(RfxbPlan* p) {
 
 // 4-D map over one CPML psi array: dims (d0, d1, d2, 4 = side*2 + q), rows of
 // d0 floats, box (b0, b1, 1, 2).
-int encode_psi_map(CUtensorMap* m, float* base, long long d0, long long d1, long long d2, unsigned b0, unsigned b1) {
+int encode_psi_map(CUtensorMap* m, float* base, long long d0, long long d1, long long d2, unsigned b0, unsigned b1,
+                   int promo) {
   auto fn = tensor_map_encoder();
   if (!fn) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled is not available from the driver");
   cuuint64_t dims[4] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2, 4};
@@ -719,7 +727,7 @@ int encode_psi_map(CUtensorMap* m, float* base, long long d0, long long d1, long
   cuuint32_t box[4] = {b0, b1, 1, 2};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(promo),
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(RFXB_E_LAUNCH, "cuTensorMapEncodeTiled (psi) failed (" + std::to_string((int)r) + ")");
   return 0;
@@ -752,17 +760,17 @@ int encode_psi_maps(RfxbPlan* p) {
     const long long n = I.ncp, n4 = I.ncp4;
     for (int s = 0; s < 2; ++s) {
       if (I.cpml_axes & 1u) {
-        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + s], I.psH[s][0], I.zs, p->ny, n, 36, ty + 1)) return rc;
-        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + s], I.psE[s][0], I.zs, p->ny, n, 32, ty)) return rc;
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + s], I.psH[s][0], I.zs, p->ny, n, 36, ty + 1, p->l2promo)) return rc;
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + s], I.psE[s][0], I.zs, p->ny, n, 32, ty, p->l2promo)) return rc;
       }
       if (I.cpml_axes & 2u) {
-        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + 2 + s], I.psH[s][1], I.zs, n, p->nx, 36, ty + 1)) return rc;
-        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + 2 + s], I.psE[s][1], I.zs, n, p->nx, 32, ty)) return rc;
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + 2 + s], I.psH[s][1], I.zs, n, p->nx, 36, ty + 1, p->l2promo)) return rc;
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + 2 + s], I.psE[s][1], I.zs, n, p->nx, 32, ty, p->l2promo)) return rc;
       }
       if (I.cpml_axes & 4u) {
-        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + 4 + s], I.psH[s][2], n4, p->ny, p->nx, (unsigned)n4, ty + 1))
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSH + 4 + s], I.psH[s][2], n4, p->ny, p->nx, (unsigned)n4, ty + 1, p->l2promo))
           return rc;
-        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + 4 + s], I.psE[s][2], n4, p->ny, p->nx, (unsigned)n4, ty))
+        if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_PSE + 4 + s], I.psE[s][2], n4, p->ny, p->nx, (unsigned)n4, ty, p->l2promo))
           return rc;
       }
     }
@@ -822,23 +830,23 @@ int encode_adjoint_maps(RfxbPlan* p) {
       const long long n = I.ncp, n4 = I.ncp4;
       for (int s = 0; s < 2; ++s) {
         if (I.cpml_axes & 1u) {
-          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + s], p->adj.aPsiE[s][0], I.zs, p->ny, n, 36, ty + 1))
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + s], p->adj.aPsiE[s][0], I.zs, p->ny, n, 36, ty + 1, p->l2promo))
             return rc;
-          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + s], p->adj.aPsiH[s][0], I.zs, p->ny, n, 32, ty))
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + s], p->adj.aPsiH[s][0], I.zs, p->ny, n, 32, ty, p->l2promo))
             return rc;
         }
         if (I.cpml_axes & 2u) {
-          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + 2 + s], p->adj.aPsiE[s][1], I.zs, n, p->nx, 40, ty + 2))
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + 2 + s], p->adj.aPsiE[s][1], I.zs, n, p->nx, 40, ty + 2, p->l2promo))
             return rc;
-          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + 2 + s], p->adj.aPsiH[s][1], I.zs, n, p->nx, 36, ty + 1))
+          if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + 2 + s], p->adj.aPsiH[s][1], I.zs, n, p->nx, 36, ty + 1, p->l2promo))
             return rc;
         }
         if (I.cpml_axes & 4u) {
           if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APE + 4 + s], p->adj.aPsiE[s][2], n4, p->ny, p->nx,
-                                      (unsigned)n4, ty + 2))
+                                      (unsigned)n4, ty + 2, p->l2promo))
             return rc;
           if (int rc = encode_psi_map(&p->tmaps[RFXB_MAP_APH + 4 + s], p->adj.aPsiH[s][2], n4, p->ny, p->nx,
-                                      (unsigned)n4, ty + 1))
+                                      (unsigned)n4, ty + 1, p->l2promo))
             return rc;
         }
       }
@@ -893,6 +901,17 @@ AdjKernel adj_kernel(int mode) {
                             : adj_step_kernel<kTY, 0>;
   allow_smem(reinterpret_cast<const void*>(k), adj_step_smem_bytes(mode, 16));
   return k;
+}
+
+// Re-encode every TMA map a plan holds with its current L2 promotion (the
+// maps are copied to the device before each launch sequence).
+int reencode_maps(RfxbPlan* p) {
+  if (int rc = encode_forward_maps(p)) return rc;
+  if (p->emask)
+    if (int rc = encode_emask_map(p)) return rc;
+  if (p->adj_alloc)
+    if (int rc = encode_adjoint_maps(p)) return rc;
+  return 0;
 }
 
 int upload_tables(RfxbPlan* p, const float* h, int n, const float** dst) {
@@ -1782,6 +1801,7 @@ int rfxb_plan_create(const RfxbDesc* d, RfxbPlan** out) {
   p->hcells = (long long)(I.hb[1] - I.hb[0]) * (I.hb[3] - I.hb[2]) * (I.hb[5] - I.hb[4]);
   I.hist = nullptr;
   std::memset(p->tmaps, 0, sizeof(p->tmaps));
+  p->l2promo = l2_promotion_default();
   if (int rc = encode_forward_maps(p)) return bail(rc);
   // own single-plan group
   RfxbBatch* g = new RfxbBatch();
@@ -2195,10 +2215,10 @@ namespace {
 void launch_config(const RfxbBatch* g, RfxbLaunchConfig* cur, RfxbLaunchConfig* lim) {
   if (cur)
     *cur = RfxbLaunchConfig{g->fwd_split ? 1 : 0, g->fwd_order, g->adj_lite ? 1 : 0, g->adj_order, g->fwd_persist,
-                            g->adj_persist};
+                            g->adj_persist, g->plans[0]->l2promo};
   if (lim)
     *lim = RfxbLaunchConfig{g->fwd_split_avail ? 1 : 0, g->fwd_split_avail ? 1 : 0, g->adj_lite_avail ? 1 : 0,
-                            g->adj_split ? 5 : 0, g->fwd_split_avail ? 3 : 0, adj_persist_avail(g) ? 1 : 0};
+                            g->adj_split ? 5 : 0, g->fwd_split_avail ? 3 : 0, adj_persist_avail(g) ? 1 : 0, 3};
 }
 
 int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
@@ -2208,7 +2228,7 @@ int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
   auto in = [](int v, int hi) { return v >= 0 && v <= hi; };
   if (!in(c->fwd_split, lim.fwd_split) || !in(c->fwd_order, lim.fwd_order) || !in(c->adj_lite, lim.adj_lite) ||
       !in(c->adj_order, lim.adj_order) || !in(c->fwd_persist, lim.fwd_persist) ||
-      !in(c->adj_persist, lim.adj_persist))
+      !in(c->adj_persist, lim.adj_persist) || !in(c->l2_promo, lim.l2_promo))
     return fail(RFXB_E_INVALID, "launch configuration outside the limits of this plan/batch");
   // cached graphs hold the old launch sequence: drop them once nothing runs
   RFXB_CUDA(cudaDeviceSynchronize());
@@ -2221,6 +2241,11 @@ int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
   g->adj_order = c->adj_order;
   g->fwd_persist = c->fwd_persist;
   g->adj_persist = c->adj_persist;
+  for (auto* p : g->plans)
+    if (p->l2promo != c->l2_promo) {
+      p->l2promo = c->l2_promo;
+      if (int rc = reencode_maps(p)) return rc;
+    }
   return 0;
 }
 

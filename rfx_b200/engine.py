@@ -43,7 +43,7 @@ def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-_LAUNCH_FIELDS = ("fwd_split", "fwd_order", "adj_lite", "adj_order", "fwd_persist", "adj_persist")
+_LAUNCH_FIELDS = ("fwd_split", "fwd_order", "adj_lite", "adj_order", "fwd_persist", "adj_persist", "l2_promo")
 
 
 def _get_launch(getter, h):

@@ -94,6 +94,22 @@ def test_picks_the_fastest_configuration():
     assert len(res.forward_ms) == 3 and len(res.reverse_ms) == 8
 
 
+def test_l2_promotion_stage_times_the_whole_step():
+    """With an l2_promo limit the tuner times every promotion on the forward
+    and reverse runs together, after choosing the launches, current setting
+    first, and keeps the fastest."""
+    lim = dict(FULL, l2_promo=3)
+    cur = {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "l2_promo": 2}
+    t = FakeTarget(lim, cur)
+    fwd = lambda c: 10.0 - (1.0 if c["l2_promo"] == 1 else 0.0)
+    rev = lambda c: 20.0 - (2.0 if c["l2_promo"] == 1 else 0.0)
+    timer, rf, rr, _ = _timer_for(t, fwd, rev)
+    res = at.autotune(t, rf, rr, timer=timer, repeats=1)
+    assert list(res.promo_ms)[0] == (("l2_promo", 2),) and len(res.promo_ms) == 4
+    assert res.promo_ms[(("l2_promo", 1),)] == 27.0 and res.promo_ms[(("l2_promo", 2),)] == 30.0
+    assert res.config["l2_promo"] == 1 and t.cur["l2_promo"] == 1
+
+
 def test_noise_does_not_move_the_current_configuration():
     t = FakeTarget(FULL)
     # the alternatives are faster by 0.5 %, inside the 1 % margin
@@ -159,7 +175,8 @@ def test_launch_config_bindings_validate_fields():
     lib = Lib()
     lib.get.__func__.__name__ = "rfxb_batch_launch_config"
     cur, lim = engine._get_launch(lib.get, None)
-    assert cur == {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": 0, "adj_persist": 0}
+    assert cur == {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": 0, "adj_persist": 0,
+                   "l2_promo": 0}
     assert lim["adj_order"] == 5
     engine._set_launch(lib.get, lib.set, None, {"adj_order": 3})
     assert engine._get_launch(lib.get, None)[0]["adj_order"] == 3
@@ -206,12 +223,15 @@ def test_every_launch_configuration_gives_the_same_sweep(cuda):
         configs += [{"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": k,
                      "adj_persist": 1} for k in range(1, lim["fwd_persist"] + 1)]
         configs.append({"fwd_persist": 0, "adj_persist": 0})
+        # the L2 promotion of the TMA boxes moves no value
+        assert lim["l2_promo"] == 3
+        configs += [{"l2_promo": v} for v in (0, 1, 3, 2)]
         for c in configs:
             if any(v > lim[k] for k, v in c.items()):
                 continue
             sw.batch.set_launch_config(**c)
             J, g = _run(sw)
-            order_only = set(c) <= {"fwd_order", "adj_order"} or c.get("fwd_persist", 0) > 0 or (
+            order_only = set(c) <= {"fwd_order", "adj_order", "l2_promo"} or c.get("fwd_persist", 0) > 0 or (
                 c == {"fwd_persist": 0, "adj_persist": 0})
             for a, b in zip(g, g0):
                 # the launch order cannot change a value; another kernel
