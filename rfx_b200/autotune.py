@@ -186,7 +186,11 @@ def autotune(target, run_forward, run_reverse=None, *, signature=None, cache_pat
         def whole_step():
             a = run_forward()
             b = run_reverse() if run_reverse is not None else None
-            return (a or 0.0) + (b or 0.0)   # what a stand-in timer measures; CUDA events ignore it
+            # runs that report a time (stand-in timers) add up; real runs
+            # return arrays or nothing and are timed with CUDA events
+            if isinstance(a, (int, float)) and isinstance(b, (int, float, type(None))):
+                return float(a) + float(b or 0.0)
+            return None
         for v in pc:
             target.set_launch_config(l2_promo=v)
             res.promo_ms[(("l2_promo", v),)] = _time(whole_step, repeats, timer)

@@ -980,10 +980,13 @@ int build_group(RfxbBatch* g) {
     std::vector<RfxbWork> a1, a2;
     balance_segments(aplain, 4 * sm_count(), 3.0, a1);
     balance_segments(acpml, 3 * sm_count(), 3.0, a2);
-    if (!a1.empty() && !a2.empty()) {
-      if (int rc = galloc((void**)&g->d_wa1, sizeof(RfxbWork) * a1.size())) return rc;
+    // (a grid with no CPML-free tile, e.g. one whose every z tile reaches a z
+    // slab, still splits its CPML work between variants 2 and 4)
+    if (!a2.empty()) {
+      if (int rc = galloc((void**)&g->d_wa1, sizeof(RfxbWork) * std::max<size_t>(a1.size(), 1))) return rc;
       if (int rc = galloc((void**)&g->d_wa2, sizeof(RfxbWork) * a2.size())) return rc;
-      RFXB_CUDA(cudaMemcpy(g->d_wa1, a1.data(), sizeof(RfxbWork) * a1.size(), cudaMemcpyHostToDevice));
+      if (!a1.empty())
+        RFXB_CUDA(cudaMemcpy(g->d_wa1, a1.data(), sizeof(RfxbWork) * a1.size(), cudaMemcpyHostToDevice));
       RFXB_CUDA(cudaMemcpy(g->d_wa2, a2.data(), sizeof(RfxbWork) * a2.size(), cudaMemcpyHostToDevice));
       g->n_wa1 = (int)a1.size();
       g->n_wa2 = (int)a2.size();
@@ -1548,8 +1551,9 @@ int group_adjoint_advance(RfxbBatch* g, const RfxbAdjointIO* aios, int step_hi, 
                   g->d_inst, g->d_adj, g->d_wa4, g->d_maps, s, par, fpar, zp);
           };
           auto v3 = [&]() {
-            adj_kernel(3)<<<g->n_wa1, dim3(32, kTY), adj_step_smem_bytes(3, zp), g->side_stream>>>(
-                g->d_inst, g->d_adj, g->d_wa1, g->d_maps, s, par, fpar, zp);
+            if (g->n_wa1 > 0)
+              adj_kernel(3)<<<g->n_wa1, dim3(32, kTY), adj_step_smem_bytes(3, zp), g->side_stream>>>(
+                  g->d_inst, g->d_adj, g->d_wa1, g->d_maps, s, par, fpar, zp);
           };
           // capture order = the order the graph hands the branches' CTAs to
           // the SMs (adj_order); the default 0 puts the largest, four-per-SM
@@ -2193,7 +2197,7 @@ void step_launches(const RfxbBatch* g, int* fwd, int* rev) {
     else if (use_twopass()) *rev = 2;
     else if (g->adj_persist && g->adj_mode == 2 && adj_persist_avail(g)) *rev = 1;
     else if (g->adj_split && g->adj_mode != 0)
-      *rev = (g->adj_lite && g->adj_mode == 2) ? (g->n_wa2y > 0 ? 3 : 2) : 2;
+      *rev = ((g->adj_lite && g->adj_mode == 2) ? (g->n_wa2y > 0 ? 3 : 2) : 2) - (g->n_wa1 > 0 ? 0 : 1);
     else *rev = 1;
   }
 }

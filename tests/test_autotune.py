@@ -261,3 +261,21 @@ def test_batched_sweep_matches_single_plans(cuda):
     finally:
         a.close()
         b.close()
+
+
+def test_l2_promotion_stage_accepts_runs_that_return_arrays():
+    """The real runs return probe traces (arrays) or nothing; the whole-step
+    closure of the promotion stage must not combine them."""
+    lim = dict(FULL, l2_promo=3)
+    t = FakeTarget(lim, {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "l2_promo": 2})
+    calls = {"n": 0}
+
+    def run_forward():
+        calls["n"] += 1
+        return np.zeros((4, 2))
+
+    def run_reverse():
+        calls["n"] += 1
+
+    res = at.autotune(t, run_forward, run_reverse, timer=lambda fn: (fn(), 1.0)[1], repeats=1)
+    assert len(res.promo_ms) == 4 and res.config["l2_promo"] == 2 and calls["n"] > 0
