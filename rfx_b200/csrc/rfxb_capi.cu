@@ -1292,7 +1292,9 @@ int run_graph(RfxbBatch* g, const GraphKey& key, cudaStream_t st, F&& launch) {
         const unsigned long long u = g->graph_use[v->first];
         if (u < oldest) { oldest = u; victim = v; }
       }
-      RFXB_CUDA(cudaStreamSynchronize(st));   // nothing of the victim may still run
+      // an executable graph destroyed while in flight is not cut short: the
+      // runtime frees it when its launch completes, on whichever stream that
+      // launch went, so no synchronisation is needed here
       cudaGraphExecDestroy(victim->second);
       g->graph_use.erase(victim->first);
       g->graphs.erase(victim);
