@@ -347,9 +347,11 @@ def run_ours(args, rank, world, local_rank):
 
     # our kernels per bench step: N forward steps, one adjoint init per
     # simulation launch group, N reverse steps, each step as many step-kernel
-    # launches as the library reports (CPML / plain split, variant 4)
+    # launches as the library reports (CPML / plain split, variant 4; per
+    # pass of two steps with two-step passes)
     fl, rl = sw.step_launches()
-    launches = args.steps * (N * (fl + rl) + (1 if sw.batch is not None else len(sw.plans)))
+    cfg = (sw.batch or sw.plans[0]).launch_config()[0]
+    launches = args.steps * (forward_launches(fl, cfg, N) + N * rl + (1 if sw.batch is not None else len(sw.plans)))
     sw.close()
 
     # the other configurations, each timed on its own full step count (one
@@ -524,6 +526,16 @@ def run_secondary(args, which, emit=True):
 PUBLISHED_GPU_MCELLS = 7309.0   # README.md:28 of the reference: RTX 4090, rfx.gpu.benchmark (PEC-only run())
 
 
+def forward_launches(per_step, cfg, n):
+    """Forward step-kernel launches of n steps.  ``per_step`` is the
+    library's count (``step_launches()[0]``): launches of one step, or of one
+    pass of two steps when two-step passes run (an odd last step then runs on
+    the one-step launches: both lists, or one)."""
+    if cfg.get("fwd_depth", 1) == 2:
+        return (n // 2) * per_step + (n % 2) * (2 if cfg.get("fwd_split", 0) else 1)
+    return n * per_step
+
+
 def run_pec_uniform(args, emit, hbm_peak, peak_src):
     """The reference's own GPU benchmark on this path: rfx.gpu.benchmark
     (rfx/gpu.py:58-107) times run() on a PEC cube without CPML after a JIT
@@ -562,7 +574,7 @@ def run_pec_uniform(args, emit, hbm_peak, peak_src):
         torch.cuda.synchronize()
     ms = ev[0].elapsed_time(ev[1])
     alg = plan.algorithmic_bytes_per_step()
-    launches = plan.step_launches()[0]
+    launches = forward_launches(plan.step_launches()[0], plan.launch_config()[0], N)
     plan.close()
     torch.cuda.empty_cache()
     # the reference's timing: the public run() call after a warm-up call
@@ -583,7 +595,7 @@ def run_pec_uniform(args, emit, hbm_peak, peak_src):
             "dtype": "f32", "data": "synthetic (vacuum)",
             "config": {"workload": f"pec_uniform: {g.shape[0]}^3 cells (512 mm cube at dx 1 mm + fence), PEC faces, "
                                    f"no CPML, raw Ez field source GaussianPulse(5 GHz) and Ez probe at the centre",
-                       "time_steps": N, "cells": cells, "gpu_launches_per_step": launches,
+                       "time_steps": N, "cells": cells, "gpu_launches_per_run": launches,
                        "l2": "inputs larger than L2"},
             "e2e": {"value": round(e2e, 1), "unit": "Mcells/s", "path": "rfx_b200.run(..., return_state=False), "
                     "host eps_r/sigma in, probe trace out, plan set-up included", "wall_s": round(wall, 3),

@@ -344,7 +344,9 @@ int rfxb_plan_adjoint_variant(const RfxbPlan* plan);
 int rfxb_batch_adjoint_variant(const RfxbBatch* batch);
 
 /* Step-kernel launches per forward time step (*fwd: 1, or 2 with the split
- * into CPML and plain tiles) and per reverse time step (*rev: 1, 2 with the
+ * into CPML and plain tiles; with two-step passes, fwd_depth 2, the launches
+ * of one pass of two steps: the two-step tiles plus two launches of each
+ * one-step list) and per reverse time step (*rev: 1, 2 with the
  * split, 3 when variant 4 takes the CPML work without a y slab; -1 before
  * the first adjoint advance), not counting DFT / flux / NTFF epilogue
  * kernels.  A diagnostic of this implementation. */
@@ -375,6 +377,17 @@ int rfxb_batch_step_launches(const RfxbBatch* batch, int* fwd, int* rev);
  *   l2_promo   L2 promotion of the plans' TMA boxes: 0 none, 1 64 B,
  *                 2 128 B, 3 256 B (how much of a partly covered line a halo
  *                 miss fetches; the plans' maps are re-encoded)
+ *   fwd_depth  time steps per forward pass over HBM: 1 (0 means 1), or 2
+ *                 where the group has tiles for it: temporal blocking, the
+ *                 CPML-free interior tiles away from sources, probes and the
+ *                 gradient region advance two steps per pass on the two-step
+ *                 kernel while the rest runs one launch per step through an
+ *                 intermediate field buffer (allocated on first use, 24 bytes
+ *                 per cell); an odd remaining step runs alone, and every
+ *                 step does while a plan has per-cell mu_r or a PEC edge
+ *                 mask.  Excludes fwd_persist > 0.  Results equal depth 1
+ *                 bit for bit (rfxb_*_step_launches then counts the
+ *                 launches of one pass of two steps).
  * rfxb_*_launch_config writes the current setting to *current and the
  * largest value each field accepts on this plan/batch to *limits (0 where a
  * choice does not exist, e.g. fwd_split on a group without staged-psi CPML).
@@ -390,6 +403,7 @@ typedef struct RfxbLaunchConfig {
   int32_t fwd_persist;
   int32_t adj_persist;
   int32_t l2_promo;
+  int32_t fwd_depth;
 } RfxbLaunchConfig;
 
 int rfxb_plan_launch_config(const RfxbPlan* plan, RfxbLaunchConfig* current, RfxbLaunchConfig* limits);
@@ -416,7 +430,11 @@ int rfxb_batch_debug_poison(RfxbBatch* batch, int list, int index);
  * bits x=1 y=2 z=4); resident: the CTA capacity the lists are balanced for.
  * which: 0 every tile on one kernel; 1 / 2 forward CPML-free / staged-psi
  * tiles; 3 / 4 reverse CPML-free / CPML tiles; 5 / 6 the reverse CPML tiles
- * split into those that reach a y slab (variant 2) and the rest (variant 4).
+ * split into those that reach a y slab (variant 2) and the rest (variant 4);
+ * 7 / 8 / 9 a two-step pass's two-step tiles / one-step CPML-free work /
+ * one-step CPML work (for 7 the plan index carries, from bit 16 on, where the
+ * item also stores its intermediate state: 1 every plane, 2 its first plane,
+ * 4 its last plane).
  * out: 5 ints per item (plan, y0, z0, xa, xb), *n_out the item count (with
  * out == NULL only the count).  A diagnostic of this implementation. */
 int rfxb_debug_work_lists(int n_plans, const int32_t* dims, int32_t resident, int32_t which, int32_t* out,

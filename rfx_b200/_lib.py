@@ -55,7 +55,7 @@ class RfxbDesc(C.Structure):
 class RfxbLaunchConfig(C.Structure):
     _fields_ = [("fwd_split", C.c_int32), ("fwd_order", C.c_int32), ("adj_lite", C.c_int32),
                 ("adj_order", C.c_int32), ("fwd_persist", C.c_int32), ("adj_persist", C.c_int32),
-                ("l2_promo", C.c_int32)]
+                ("l2_promo", C.c_int32), ("fwd_depth", C.c_int32)]
 
 
 class RfxbStepIO(C.Structure):

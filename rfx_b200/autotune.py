@@ -56,9 +56,11 @@ def _key_str(k) -> str:
 
 def forward_candidates(limits: dict, current: dict) -> list:
     """Forward settings to time: split with either launch order, the single
-    launch, and (where the target offers it) the persistent launch with 0, 1
-    or 2 CPML-free-first CTAs per SM, as far as the limits allow (the current
-    setting first)."""
+    launch, (where the target offers it) the persistent launch with 0, 1 or
+    2 CPML-free-first CTAs per SM, and (where the target has two-step tiles)
+    two-step passes, as far as the limits allow (the current setting first).
+    The temporal-block depth is chosen here with the launches: 1 or 2 steps
+    per pass over HBM."""
     c = []
     if limits["fwd_split"]:
         c += [{"fwd_split": 1, "fwd_order": 0}, {"fwd_split": 1, "fwd_order": 1}, {"fwd_split": 0, "fwd_order": 0}]
@@ -71,6 +73,15 @@ def forward_candidates(limits: dict, current: dict) -> list:
         c += [{"fwd_split": 1, "fwd_order": 0, "fwd_persist": k} for k in range(1, np_ + 1)]
         k = current.get("fwd_persist", 0)
         cur = dict(cur, fwd_persist=k) if not k else {"fwd_split": 1, "fwd_order": 0, "fwd_persist": k}
+    if limits.get("fwd_depth", 1) >= 2:
+        # a two-step pass has its own lists; split and order only shape an
+        # odd trailing step
+        two = {"fwd_split": 1 if limits["fwd_split"] else 0, "fwd_order": 0}
+        if np_:
+            two["fwd_persist"] = 0
+        two["fwd_depth"] = 2
+        c = [dict(x, fwd_depth=1) for x in c] + [two]
+        cur = dict(cur, fwd_depth=1) if (current.get("fwd_depth", 1) or 1) == 1 else two
     return [cur] + [x for x in c if x != cur]
 
 

@@ -52,6 +52,9 @@ template <int TY>
 __global__ void adj_persist_kernel(const RfxbInst*, const AdjInst*, int, RfxbAdjQueues, const CUtensorMap*, int, int,
                                    int);
 size_t adj_step_smem_bytes(int mode, int zp);
+template <int TY>
+__global__ void fwd2_step_kernel(const RfxbInst*, const RfxbWork2*, const CUtensorMap*, int, int);
+size_t fwd2_step_smem_bytes();
 }  // namespace rfxb
 
 using namespace rfxb;
@@ -110,7 +113,10 @@ struct RfxbPlan {
   int nx = 0, ny = 0, nz = 0;
   double dt = 0.0;
   long long elems = 0;         // floats per padded per-cell array
-  int par = 0;                 // parity of the buffers holding the current state
+  int par = 0;                 // parity of the field buffers holding the current state
+  int ppar = 0;                // parity of the CPML psi buffers holding the current state (a
+                               // two-step pass flips the fields once and the psi twice)
+  float* mid = nullptr;        // intermediate field state of two-step passes (F[2]), allocated on first use
   std::vector<void*> allocs;
   // per-cell and table arrays
   float* ca = nullptr; float* cb = nullptr; float* ce = nullptr; float* ch = nullptr;
@@ -164,9 +170,10 @@ struct RfxbPlan {
 // A cached CUDA graph of a launch sequence: kind 0 forward steps
 // [step0, step0+k), kind 1 reverse steps [step0-k, step0) of the adjoint.
 struct GraphKey {
-  int kind, step0, k, par0, fpar0, dft;
+  int kind, step0, k, par0, fpar0, dft, ppar0 = 0;
   bool operator<(const GraphKey& o) const {
-    return std::tie(kind, step0, k, par0, fpar0, dft) < std::tie(o.kind, o.step0, o.k, o.par0, o.fpar0, o.dft);
+    return std::tie(kind, step0, k, par0, fpar0, dft, ppar0) <
+           std::tie(o.kind, o.step0, o.k, o.par0, o.fpar0, o.dft, o.ppar0);
   }
 };
 
@@ -203,6 +210,18 @@ struct RfxbBatch {
   int n_wa4 = 0;
   cudaStream_t side2 = nullptr;
   cudaEvent_t ev_join2 = nullptr;
+  // two-step passes (fwd_depth 2): the two-step kernel's tiles, and the
+  // one-step work of a pass -- the other CPML-free tiles (variant 1) and the
+  // CPML tiles (variant 2) -- launched once per step of the pass through the
+  // intermediate buffer F[2]
+  int fwd_depth = 1;
+  bool fwd_depth_avail = false;
+  RfxbWork2* d_wd = nullptr;
+  int n_wd = 0;
+  RfxbWork* d_wd1 = nullptr;
+  int n_wd1 = 0;
+  RfxbWork* d_wd2 = nullptr;
+  int n_wd2 = 0;
   RfxbDftPlane* d_dft = nullptr;
   RfxbDftPlane* d_dfta = nullptr;   // the same planes with the adjoint call's cotangents
   std::vector<RfxbDftPlane> dfta;
@@ -227,7 +246,7 @@ struct RfxbBatch {
   int fwd_persist = 0;             // 0: off; k >= 1: on, k-1 CTAs per SM try the CPML-free list first
   int adj_persist = 0;             // 0: off; 1: on
   int fault_cta = -1;              // test-only fault injection of the persistent kernels
-  int wait_limit = 1 << 22;
+  int wait_limit = rfxb::kWaitLimit;
   int adj_persist_grid = 0;        // CTAs of the persistent reverse launch (resident at once)
   int fwd_mode = 0;                // forward step kernel variant (see rfxb_fwd.cu)
   int adj_mode = -1;               // reverse step kernel variant (see rfxb_adj_fused.cu), -1 not chosen yet
@@ -478,6 +497,120 @@ void split_adj_segments(const std::vector<RfxbPlan*>& plans, double slab, std::v
   }
 }
 
+// Two-step passes.  A tile column (y0, z0) of plan p runs on the two-step
+// kernel when every cell its two steps compute -- rows y0-2 .. y0+TY,
+// columns z0-2 .. z0+32 -- lies inside the grid, off the PEC faces and out of
+// every CPML slab, and no source, probe or gradient-history cell lies within
+// reach (rows y0-2 .. y0+TY+1, columns z0-2 .. z0+33); the plan must have
+// uniform H coefficients and no PEC edge mask.
+bool depth2_plan(const RfxbPlan& p) { return p.inst.emask == nullptr && p.inst.ch == nullptr; }
+
+bool depth2_column(const RfxbPlan& p, int y0, int z0) {
+  const int n = p.inst.ncp;
+  const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
+  const int ylo = std::max(1, (ax & 2u) ? n : 0), zlo = std::max(1, (ax & 4u) ? n : 0);
+  const int yhi = std::min(p.ny - 2, (ax & 2u) ? p.ny - n - 1 : p.ny - 2);
+  const int zhi = std::min(p.nz - 2, (ax & 4u) ? p.nz - n - 1 : p.nz - 2);
+  if (y0 - 2 < ylo || y0 + kTY > yhi || z0 - 2 < zlo || z0 + 32 > zhi) return false;
+  auto near = [&](int j, int k) { return j >= y0 - 2 && j <= y0 + kTY + 1 && k >= z0 - 2 && k <= z0 + 33; };
+  for (const int4& c : p.src)
+    if (near(c.y, c.z)) return false;
+  for (const int4& c : p.prb)
+    if (near(c.y, c.z)) return false;
+  const int* hb = p.inst.hb;
+  if (hb[0] < hb[1] && hb[2] <= y0 + kTY + 1 && hb[3] - 1 >= y0 - 2 && hb[4] <= z0 + 33 && hb[5] - 1 >= z0 - 2)
+    return false;
+  return true;
+}
+
+// The x range of a plan's two-step segments: planes whose x-1 .. x+1
+// neighbours are off the x slabs and the PEC x faces.
+void depth2_xrange(const RfxbPlan& p, int& dlo, int& dhi) {
+  const int n = p.inst.ncp;
+  const int ncpx = (n > 0 && (p.inst.cpml_axes & 1u)) ? n : 0;
+  dlo = std::max(ncpx + 1, 2);
+  dhi = std::min(p.nx - ncpx - 1, p.nx - 2);
+}
+
+// Work of a two-step pass: two-step segments (d2), the other CPML-free work
+// (plain, variant 1) and the CPML work (cpml, variant 2; the same split as
+// split_segments).  Together they cover every cell of every plan once.
+void split_depth2_segments(const std::vector<RfxbPlan*>& plans, double slab, std::vector<WorkSeg>& d2,
+                           std::vector<WorkSeg>& plain, std::vector<WorkSeg>& cpml) {
+  for (size_t q = 0; q < plans.size(); ++q) {
+    const RfxbPlan& p = *plans[q];
+    const int n = p.inst.ncp;
+    const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
+    const int ncpx = (ax & 1u) ? n : 0;
+    const double cx = (ax & 1u) ? slab : 0.0;
+    int dlo, dhi;
+    depth2_xrange(p, dlo, dhi);
+    const bool plan_ok = depth2_plan(p);
+    for (int y0 = 0; y0 < p.ny; y0 += kTY)
+      for (int z0 = 0; z0 < p.nz; z0 += 32) {
+        int lo = 0, hi = p.nx;
+        if (ax != 0u) {
+          if (tile_reaches_yz(p, y0, z0)) {
+            double c = 1.0;
+            if ((ax & 2u) && (y0 - 1 < n || y0 + kTY - 1 >= p.ny - n)) c += slab;
+            if ((ax & 4u) && (z0 - 1 < n || z0 + 31 >= p.nz - n)) c += slab;
+            cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, c, cx});
+            continue;
+          }
+          lo = ncpx > 0 ? ncpx + 1 : 0;
+          hi = ncpx > 0 ? p.nx - ncpx : p.nx;
+          if (hi - lo < 4) {
+            cpml.push_back(WorkSeg{(int)q, y0, z0, 0, p.nx, p.nx, ncpx, 1.0, cx});
+            continue;
+          }
+          if (lo > 0) cpml.push_back(WorkSeg{(int)q, y0, z0, 0, lo, p.nx, ncpx, 1.0, cx});
+          if (hi < p.nx) cpml.push_back(WorkSeg{(int)q, y0, z0, hi, p.nx, p.nx, ncpx, 1.0, cx});
+        }
+        const int a = std::max(lo, dlo), b = std::min(hi, dhi);
+        if (plan_ok && b - a >= 8 && depth2_column(p, y0, z0)) {
+          d2.push_back(WorkSeg{(int)q, y0, z0, a, b, p.nx, 0, 1.0, 0.0});
+          if (a > lo) plain.push_back(WorkSeg{(int)q, y0, z0, lo, a, p.nx, 0, 1.0, 0.0});
+          if (b < hi) plain.push_back(WorkSeg{(int)q, y0, z0, b, hi, p.nx, 0, 1.0, 0.0});
+        } else {
+          plain.push_back(WorkSeg{(int)q, y0, z0, lo, hi, p.nx, 0, 1.0, 0.0});
+        }
+      }
+  }
+}
+
+// Where a two-step item also stores its intermediate state (RfxbWork2::mid):
+// at its first / last plane when that is the end of its column's two-step
+// range (one-step work continues beyond), on every plane when one of the
+// eight neighbouring columns runs one-step work (its halo reads this tile)
+// or when a DFT plane, flux monitor or NTFF face of the plan passes through
+// the item (the observers read every step's state).
+int depth2_mid_flags(const RfxbPlan& p, const RfxbWork& w) {
+  int dlo, dhi;
+  depth2_xrange(p, dlo, dhi);
+  int mid = 0;
+  if (w.xa == dlo) mid |= RFXB_MID_LO;
+  if (w.xb == dhi) mid |= RFXB_MID_HI;
+  for (int dy = -1; dy <= 1; ++dy)
+    for (int dz = -1; dz <= 1; ++dz)
+      if ((dy || dz) && !depth2_column(p, w.y0 + dy * kTY, w.z0 + dz * 32)) mid |= RFXB_MID_ALL;
+  auto through = [&](int axis, int index) {
+    const int lo = axis == 0 ? w.xa : axis == 1 ? w.y0 : w.z0;
+    const int hi = axis == 0 ? w.xb : axis == 1 ? w.y0 + kTY : w.z0 + 32;
+    return index + 1 >= lo && index - 1 < hi;   // the plane or a neighbour plane
+  };
+  for (const RfxbDftDesc& d : p.dft)
+    if (through(d.axis, d.index)) mid |= RFXB_MID_ALL;
+  for (const RfxbFluxDesc& f : p.flux)
+    if (through(f.axis, f.index)) mid |= RFXB_MID_ALL;
+  if (p.has_ntff) {
+    const RfxbNtffDesc& b = p.ntff;
+    if (through(0, b.i_lo) || through(0, b.i_hi) || through(1, b.j_lo) || through(1, b.j_hi) ||
+        through(2, b.k_lo) || through(2, b.k_hi))
+      mid |= RFXB_MID_ALL;
+  }
+  return mid;
+}
+
 void make_balanced_work(const std::vector<RfxbPlan*>& plans, int resident, double slab, double prologue,
                         std::vector<RfxbWork>& out) {
   std::vector<WorkSeg> segs;
@@ -582,6 +715,35 @@ FwdKernel fwd_kernel(int mode, bool em = false) {
                             : fwd_step_kernel<kTY, 0, false>;
   allow_smem(reinterpret_cast<const void*>(k), fwd_step_smem_bytes(mode));
   return k;
+}
+
+// The two-step kernel with its dynamic shared memory enabled.
+using Fwd2Kernel = void (*)(const RfxbInst*, const RfxbWork2*, const CUtensorMap*, int, int);
+Fwd2Kernel fwd2_kernel() {
+  Fwd2Kernel k = fwd2_step_kernel<kTY>;
+  allow_smem(reinterpret_cast<const void*>(k), fwd2_step_smem_bytes());
+  return k;
+}
+
+// CTAs of the two-step kernel resident at once.
+int fwd2_resident() {
+  static int r = -1;
+  if (r < 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fwd2_kernel(), 32 * kTY, fwd2_step_smem_bytes()) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 2;
+    r = per_sm * sm_count();
+  }
+  return r;
+}
+
+// Default depth of the forward passes (RFXB_FWD_DEPTH=2: two steps per pass
+// where the group has two-step tiles; otherwise one).
+int fwd_depth_default() {
+  const char* e = getenv("RFXB_FWD_DEPTH");
+  return (e && std::string(e) == "2") ? 2 : 1;
 }
 
 using FwdPersistKernel = void (*)(const RfxbInst*, int, RfxbFwdQueues, const CUtensorMap*, int, int);
@@ -743,6 +905,16 @@ int encode_forward_maps(RfxbPlan* p) {
   }
   if (int rc = encode_block_map(&p->tmaps[4], *p, p->ca, 3, 32, ty, 2)) return rc;
   if (int rc = encode_block_map(&p->tmaps[10], *p, p->ca, 3, 32, ty, 1)) return rc;
+  // the two-step kernel's boxes (two-cell halo) and the intermediate state
+  for (int s = 0; s < 2; ++s) {
+    if (int rc = encode_block_map(&p->tmaps[RFXB_MAP_E2 + s], *p, p->inst.F[s][0], 6, 40, ty + 4, 3)) return rc;
+    if (int rc = encode_block_map(&p->tmaps[RFXB_MAP_H2 + s], *p, p->inst.F[s][0], 6, 40, ty + 3, 3)) return rc;
+  }
+  if (int rc = encode_block_map(&p->tmaps[RFXB_MAP_C2], *p, p->ca, 3, 40, ty + 2, 2)) return rc;
+  if (p->mid) {
+    if (int rc = encode_block_map(&p->tmaps[RFXB_MAP_MIDE], *p, p->mid, 6, 40, ty + 2, 3)) return rc;
+    if (int rc = encode_block_map(&p->tmaps[RFXB_MAP_MIDH], *p, p->mid, 6, 36, ty + 1, 3)) return rc;
+  }
   const RfxbInst& I = p->inst;
   p->psi_maps_ok = false;
   if (I.ncp > 0) {
@@ -924,6 +1096,18 @@ int upload_tables(RfxbPlan* p, const float* h, int n, const float** dst) {
   return 0;
 }
 
+// The intermediate field buffer of two-step passes, allocated on first use
+// with zero guards (no kernel writes a guard cell), and its tensor maps.
+int ensure_mid(RfxbPlan* p) {
+  if (p->mid) return 0;
+  float* q = nullptr;
+  if (int rc = p->alloc(&q, 6 * p->elems)) return rc;
+  RFXB_CUDA(cudaMemset(q, 0, 6 * p->elems * sizeof(float)));
+  p->mid = q;
+  for (int c = 0; c < 6; ++c) p->inst.F[2][c] = q + c * p->elems;
+  return encode_forward_maps(p);
+}
+
 int build_group(RfxbBatch* g) {
   std::vector<RfxbInst> insts;
   std::vector<RfxbWork> work;
@@ -1017,6 +1201,53 @@ int build_group(RfxbBatch* g) {
         RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join2, cudaEventDisableTiming));
         g->adj_lite_avail = true;
         g->adj_lite = adj_lite_enabled();
+      }
+    }
+  }
+  // two-step pass lists (TMA groups on balanced lists): the two-step tiles
+  // and the one-step work beside them; the pass itself is a launch
+  // configuration (fwd_depth)
+  g->fwd_depth_avail = false;
+  g->fwd_depth = 1;
+  if (g->fwd_mode >= 1 && work_mode() == 1) {
+    std::vector<WorkSeg> d2, plain, cpml;
+    split_depth2_segments(g->plans, slab_weight(), d2, plain, cpml);
+    if (!d2.empty()) {
+      std::vector<RfxbWork> wd, w1, w2;
+      balance_segments(d2, fwd2_resident(), 3.0, wd);
+      balance_segments(plain, resident_ctas(1), 3.0, w1);
+      balance_segments(cpml, resident_ctas(2), 3.0, w2);
+      std::vector<RfxbWork2> wd2;
+      wd2.reserve(wd.size());
+      for (const RfxbWork& w : wd)
+        wd2.push_back(RfxbWork2{w.inst, w.y0, w.z0, w.xa, w.xb, depth2_mid_flags(*g->plans[w.inst], w)});
+      if (int rc = galloc((void**)&g->d_wd, sizeof(RfxbWork2) * wd2.size())) return rc;
+      RFXB_CUDA(cudaMemcpy(g->d_wd, wd2.data(), sizeof(RfxbWork2) * wd2.size(), cudaMemcpyHostToDevice));
+      g->n_wd = (int)wd2.size();
+      if (!w1.empty()) {
+        if (int rc = galloc((void**)&g->d_wd1, sizeof(RfxbWork) * w1.size())) return rc;
+        RFXB_CUDA(cudaMemcpy(g->d_wd1, w1.data(), sizeof(RfxbWork) * w1.size(), cudaMemcpyHostToDevice));
+      }
+      g->n_wd1 = (int)w1.size();
+      if (!w2.empty()) {
+        if (int rc = galloc((void**)&g->d_wd2, sizeof(RfxbWork) * w2.size())) return rc;
+        RFXB_CUDA(cudaMemcpy(g->d_wd2, w2.data(), sizeof(RfxbWork) * w2.size(), cudaMemcpyHostToDevice));
+      }
+      g->n_wd2 = (int)w2.size();
+      if (!g->side_stream) {
+        RFXB_CUDA(cudaStreamCreateWithFlags(&g->side_stream, cudaStreamNonBlocking));
+        RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming));
+        RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming));
+      }
+      if (!g->side2) {
+        RFXB_CUDA(cudaStreamCreateWithFlags(&g->side2, cudaStreamNonBlocking));
+        RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join2, cudaEventDisableTiming));
+      }
+      g->fwd_depth_avail = true;
+      if (fwd_depth_default() == 2) {
+        for (auto* p : g->plans)
+          if (int rc = ensure_mid(p)) return rc;
+        g->fwd_depth = 2;
       }
     }
   }
@@ -1205,16 +1436,86 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
   return 0;
 }
 
-int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, bool has_flux, bool has_ntff,
-                 cudaStream_t st) {
-  int par = par0;
+// Two-step passes run when chosen, when the group has two-step tiles and
+// while every plan still has uniform H coefficients and no PEC edge mask
+// (materials set after the lists were built may add either).
+bool two_step(const RfxbBatch* g) {
+  if (g->fwd_depth != 2 || !g->fwd_depth_avail) return false;
+  for (const RfxbPlan* p : g->plans)
+    if (!depth2_plan(*p)) return false;
+  return true;
+}
+
+// Field and psi parities after n_steps steps from (par, ppar): a one-step
+// launch flips both, a two-step pass flips the fields once and the psi twice.
+void end_parities(const RfxbBatch* g, int n_steps, int& par, int& ppar) {
+  for (int s = 0; s < n_steps;) {
+    if (two_step(g) && s + 2 <= n_steps) { par ^= 1; s += 2; }
+    else { par ^= 1; ppar ^= 1; ++s; }
+  }
+}
+
+// One two-step pass over steps n, n+1 from fields F[par] and psi parity pp:
+// the one-step work of step n (F[par] -> F[2], psi pp -> pp^1) runs beside
+// the two-step tiles (F[par] -> F[par^1], intermediate state to F[2] where
+// one-step work reads it), then the one-step work of step n+1
+// (F[2] -> F[par^1], psi pp^1 -> pp).
+int launch_pass(RfxbBatch* g, int n, int par, int pp, bool em, cudaStream_t st) {
+  RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
+  RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
+  RFXB_CUDA(cudaStreamWaitEvent(g->side2, g->ev_fork, 0));
+  fwd2_kernel()<<<g->n_wd, dim3(32, kTY), fwd2_step_smem_bytes(), g->side2>>>(g->d_inst, g->d_wd, g->d_maps, n, par);
+  if (g->n_wd1 > 0)
+    fwd_kernel(1, em)<<<g->n_wd1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(
+        g->d_inst, g->d_wd1, g->d_maps, n, step_sel(par, 2, pp));
+  if (g->n_wd2 > 0)
+    fwd_kernel(2, em)<<<g->n_wd2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wd2, g->d_maps, n,
+                                                                            step_sel(par, 2, pp));
+  RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
+  RFXB_CUDA(cudaEventRecord(g->ev_join2, g->side2));
+  RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0));
+  RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join2, 0));
+  if (g->n_wd1 > 0) {
+    RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
+    RFXB_CUDA(cudaStreamWaitEvent(g->side_stream, g->ev_fork, 0));
+    fwd_kernel(1, em)<<<g->n_wd1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(
+        g->d_inst, g->d_wd1, g->d_maps, n + 1, step_sel(2, par ^ 1, pp ^ 1));
+  }
+  if (g->n_wd2 > 0)
+    fwd_kernel(2, em)<<<g->n_wd2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wd2, g->d_maps, n + 1,
+                                                                            step_sel(2, par ^ 1, pp ^ 1));
+  if (g->n_wd1 > 0) {
+    RFXB_CUDA(cudaEventRecord(g->ev_join, g->side_stream));
+    RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0));
+  }
+  return 0;
+}
+
+int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, int ppar0, bool has_dft, bool has_flux,
+                 bool has_ntff, cudaStream_t st) {
+  int par = par0, pp = ppar0;
   bool em = false;   // stage the PEC edge masks when a plan of the group has one
   for (auto* p : g->plans) em = em || p->inst.emask != nullptr;
+  // per-step observers of the state after step n, held in buffer b
+  auto observe = [&](int n, int b) {
+    if (has_dft) dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, b);
+    if (has_flux) flux_kernel<<<g->flux_blocks, 256, 0, st>>>(g->d_inst, g->d_flux, (int)g->flux.size(), n, b);
+    if (has_ntff) ntff_kernel<<<g->ntff_blocks, 256, 0, st>>>(g->d_inst, g->d_ntff, (int)g->ntff.size(), n, b);
+  };
   // the persistent launches clear their fetch counters when they finish;
   // clearing them here too keeps a sequence independent of earlier ones
   if (g->fwd_persist > 0 && g->fwd_split_avail) RFXB_CUDA(cudaMemsetAsync(g->d_qctr, 0, 4 * sizeof(int), st));
-  for (int s = 0; s < n_steps; ++s) {
+  for (int s = 0; s < n_steps;) {
     const int n = step0 + s;
+    if (two_step(g) && s + 2 <= n_steps) {
+      if (int rc = launch_pass(g, n, par, pp, em, st)) return rc;
+      observe(n, 2);
+      observe(n + 1, par ^ 1);
+      par ^= 1;
+      s += 2;
+      continue;
+    }
+    const int sel = step_sel(par, par ^ 1, pp);
     if (g->fwd_persist > 0 && g->fwd_split_avail) {
       RfxbFwdQueues Q{};
       Q.list[0] = g->d_wf2;
@@ -1227,7 +1528,7 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, b
       Q.fault_cta = g->fault_cta;
       Q.wait_limit = g->wait_limit;
       fwd_persist_kernel_for(em)<<<fwd_persist_grid(em), dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(
-          g->d_inst, (int)g->plans.size(), Q, g->d_maps, n, par);
+          g->d_inst, (int)g->plans.size(), Q, g->d_maps, n, sel);
     } else if (g->fwd_split) {
       // staged-psi tiles on the caller's stream, CPML-free tiles beside them
       RFXB_CUDA(cudaEventRecord(g->ev_fork, st));
@@ -1237,11 +1538,11 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, b
       // first, equal on one grid)
       auto plain = [&]() {
         fwd_kernel(1, em)<<<g->n_wf1, dim3(32, kTY), fwd_step_smem_bytes(1), g->side_stream>>>(g->d_inst, g->d_wf1,
-                                                                                            g->d_maps, n, par);
+                                                                                            g->d_maps, n, sel);
       };
       auto staged = [&]() {
         fwd_kernel(2, em)<<<g->n_wf2, dim3(32, kTY), fwd_step_smem_bytes(2), st>>>(g->d_inst, g->d_wf2, g->d_maps,
-                                                                                n, par);
+                                                                                n, sel);
       };
       if (g->fwd_order == 0) { plain(); staged(); }
       else { staged(); plain(); }
@@ -1249,15 +1550,12 @@ int launch_steps(RfxbBatch* g, int step0, int n_steps, int par0, bool has_dft, b
       RFXB_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0));
     } else {
       fwd_kernel(g->fwd_mode, em)<<<g->n_work, dim3(32, kTY), fwd_step_smem_bytes(g->fwd_mode), st>>>(
-          g->d_inst, g->d_work, g->d_maps, n, par);
+          g->d_inst, g->d_work, g->d_maps, n, sel);
     }
-    if (has_dft)
-      dft_kernel<<<g->dft_blocks, 256, 0, st>>>(g->d_inst, g->d_dft, (int)g->dft.size(), n, par ^ 1);
-    if (has_flux)
-      flux_kernel<<<g->flux_blocks, 256, 0, st>>>(g->d_inst, g->d_flux, (int)g->flux.size(), n, par ^ 1);
-    if (has_ntff)
-      ntff_kernel<<<g->ntff_blocks, 256, 0, st>>>(g->d_inst, g->d_ntff, (int)g->ntff.size(), n, par ^ 1);
+    observe(n, par ^ 1);
     par ^= 1;
+    pp ^= 1;
+    ++s;
   }
   RFXB_CUDA(cudaGetLastError());
   return 0;
@@ -1322,21 +1620,27 @@ int run_graph(RfxbBatch* g, const GraphKey& key, cudaStream_t st, F&& launch) {
 int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, cudaStream_t st) {
   if (n_steps < 0 || step0 < 0) return fail(RFXB_E_INVALID, "negative step range");
   if (n_steps == 0) return 0;
-  const int par0 = g->plans[0]->par;
+  const int par0 = g->plans[0]->par, ppar0 = g->plans[0]->ppar;
   for (auto* p : g->plans)
-    if (p->par != par0) return fail(RFXB_E_STATE, "plans of a batch must share the step parity");
+    if (p->par != par0 || p->ppar != ppar0) return fail(RFXB_E_STATE, "plans of a batch must share the step parity");
   bool has_dft = false, has_prb = false, has_flux = false, has_ntff = false;
   if (int rc = upload_group(g, ios, &has_dft, &has_prb, &has_flux, &has_ntff, st)) return rc;
   if (graphs_enabled() && n_steps >= 4) {
-    const GraphKey key{0, step0, n_steps, par0, 0, (has_dft ? 1 : 0) | (has_flux ? 2 : 0) | (has_ntff ? 4 : 0)};
+    const GraphKey key{0, step0, n_steps, par0, 0,
+                       (has_dft ? 1 : 0) | (has_flux ? 2 : 0) | (has_ntff ? 4 : 0) | (two_step(g) ? 8 : 0), ppar0};
     if (int rc = run_graph(g, key, st, [&](cudaStream_t cs) {
-          return launch_steps(g, step0, n_steps, par0, has_dft, has_flux, has_ntff, cs);
+          return launch_steps(g, step0, n_steps, par0, ppar0, has_dft, has_flux, has_ntff, cs);
         }))
       return rc;
   } else {
-    if (int rc = launch_steps(g, step0, n_steps, par0, has_dft, has_flux, has_ntff, st)) return rc;
+    if (int rc = launch_steps(g, step0, n_steps, par0, ppar0, has_dft, has_flux, has_ntff, st)) return rc;
   }
-  for (auto* p : g->plans) p->par = (par0 + n_steps) & 1;
+  int par = par0, ppar = ppar0;
+  end_parities(g, n_steps, par, ppar);
+  for (auto* p : g->plans) {
+    p->par = par;
+    p->ppar = ppar;
+  }
   return 0;
 }
 
@@ -1866,6 +2170,7 @@ int rfxb_plan_reset(RfxbPlan* p, void* stream) {
   for (size_t q = 0; q < p->dft_cmp.size(); ++q)
     RFXB_CUDA(cudaMemsetAsync(p->dft_cmp[q], 0, p->dft[q].n_freqs * p->dft_cells[q] * sizeof(float2), st));
   p->par = 0;
+  p->ppar = 0;
   return 0;
 }
 
@@ -1951,9 +2256,9 @@ int rfxb_plan_checkpoint_save(RfxbPlan* p, int slot, void* stream) {
   }
   for (int a = 0; a < 3; ++a) {
     if (p->psi_elems[a] == 0) continue;
-    RFXB_CUDA(cudaMemcpyAsync(dst, p->inst.psH[p->par][a], p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    RFXB_CUDA(cudaMemcpyAsync(dst, p->inst.psH[p->ppar][a], p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
     dst += p->psi_elems[a];
-    RFXB_CUDA(cudaMemcpyAsync(dst, p->inst.psE[p->par][a], p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    RFXB_CUDA(cudaMemcpyAsync(dst, p->inst.psE[p->ppar][a], p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
     dst += p->psi_elems[a];
   }
   p->ckpt_valid[slot] = 1;
@@ -1971,9 +2276,9 @@ int rfxb_plan_checkpoint_load(RfxbPlan* p, int slot, void* stream) {
   }
   for (int a = 0; a < 3; ++a) {
     if (p->psi_elems[a] == 0) continue;
-    RFXB_CUDA(cudaMemcpyAsync(p->inst.psH[p->par][a], src, p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    RFXB_CUDA(cudaMemcpyAsync(p->inst.psH[p->ppar][a], src, p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
     src += p->psi_elems[a];
-    RFXB_CUDA(cudaMemcpyAsync(p->inst.psE[p->par][a], src, p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    RFXB_CUDA(cudaMemcpyAsync(p->inst.psE[p->ppar][a], src, p->psi_elems[a] * sizeof(float), cudaMemcpyDeviceToDevice, st));
     src += p->psi_elems[a];
   }
   return 0;
@@ -2013,8 +2318,8 @@ std::vector<std::pair<void*, long long>> state_sections(RfxbPlan* p) {
   for (int c = 0; c < 6; ++c) v.emplace_back(p->inst.F[p->par][c], p->elems * (long long)sizeof(float));
   for (int a = 0; a < 3; ++a) {
     if (p->psi_elems[a] == 0) continue;
-    v.emplace_back(p->inst.psH[p->par][a], p->psi_elems[a] * (long long)sizeof(float));
-    v.emplace_back(p->inst.psE[p->par][a], p->psi_elems[a] * (long long)sizeof(float));
+    v.emplace_back(p->inst.psH[p->ppar][a], p->psi_elems[a] * (long long)sizeof(float));
+    v.emplace_back(p->inst.psE[p->ppar][a], p->psi_elems[a] * (long long)sizeof(float));
   }
   for (size_t q = 0; q < p->dft_cmp.size(); ++q)
     v.emplace_back(p->dft_cmp[q], p->dft[q].n_freqs * p->dft_cells[q] * (long long)sizeof(float2));
@@ -2193,7 +2498,10 @@ int rfxb_batch_forward_variant(const RfxbBatch* g) {
 
 namespace {
 void step_launches(const RfxbBatch* g, int* fwd, int* rev) {
-  if (fwd) *fwd = (g->fwd_persist > 0 && g->fwd_split_avail) ? 1 : g->fwd_split ? 2 : 1;
+  if (fwd) {
+    if (two_step(g)) *fwd = 1 + 2 * ((g->n_wd1 > 0 ? 1 : 0) + (g->n_wd2 > 0 ? 1 : 0));   // per pass of two steps
+    else *fwd = (g->fwd_persist > 0 && g->fwd_split_avail) ? 1 : g->fwd_split ? 2 : 1;
+  }
   if (rev) {
     if (g->adj_mode < 0) *rev = -1;
     else if (use_twopass()) *rev = 2;
@@ -2221,10 +2529,10 @@ namespace {
 void launch_config(const RfxbBatch* g, RfxbLaunchConfig* cur, RfxbLaunchConfig* lim) {
   if (cur)
     *cur = RfxbLaunchConfig{g->fwd_split ? 1 : 0, g->fwd_order, g->adj_lite ? 1 : 0, g->adj_order, g->fwd_persist,
-                            g->adj_persist, g->plans[0]->l2promo};
+                            g->adj_persist, g->plans[0]->l2promo, g->fwd_depth};
   if (lim)
     *lim = RfxbLaunchConfig{g->fwd_split_avail ? 1 : 0, g->fwd_split_avail ? 1 : 0, g->adj_lite_avail ? 1 : 0,
-                            g->adj_split ? 5 : 0, g->fwd_split_avail ? 3 : 0, adj_persist_avail(g) ? 1 : 0, 3};
+                            g->adj_split ? 5 : 0, g->fwd_split_avail ? 3 : 0, adj_persist_avail(g) ? 1 : 0, 3, g->fwd_depth_avail ? 2 : 1};
 }
 
 int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
@@ -2234,8 +2542,13 @@ int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
   auto in = [](int v, int hi) { return v >= 0 && v <= hi; };
   if (!in(c->fwd_split, lim.fwd_split) || !in(c->fwd_order, lim.fwd_order) || !in(c->adj_lite, lim.adj_lite) ||
       !in(c->adj_order, lim.adj_order) || !in(c->fwd_persist, lim.fwd_persist) ||
-      !in(c->adj_persist, lim.adj_persist) || !in(c->l2_promo, lim.l2_promo))
+      !in(c->adj_persist, lim.adj_persist) || !in(c->l2_promo, lim.l2_promo) || !in(c->fwd_depth, lim.fwd_depth))
     return fail(RFXB_E_INVALID, "launch configuration outside the limits of this plan/batch");
+  if (c->fwd_depth == 2 && c->fwd_persist > 0)
+    return fail(RFXB_E_INVALID, "two-step passes and persistent forward launches exclude each other");
+  if (c->fwd_depth == 2)
+    for (auto* p : g->plans)
+      if (int rc = ensure_mid(p)) return rc;
   // cached graphs hold the old launch sequence: drop them once nothing runs
   RFXB_CUDA(cudaDeviceSynchronize());
   for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second);
@@ -2247,6 +2560,7 @@ int set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* c) {
   g->adj_order = c->adj_order;
   g->fwd_persist = c->fwd_persist;
   g->adj_persist = c->adj_persist;
+  g->fwd_depth = c->fwd_depth == 2 ? 2 : 1;
   for (auto* p : g->plans)
     if (p->l2promo != c->l2_promo) {
       p->l2promo = c->l2_promo;
@@ -2314,7 +2628,7 @@ int rfxb_batch_set_launch_config(RfxbBatch* g, const RfxbLaunchConfig* config) {
 
 int rfxb_debug_work_lists(int n_plans, const int32_t* dims, int32_t resident, int32_t which, int32_t* out,
                           int32_t cap, int32_t* n_out) {
-  if (n_plans <= 0 || !dims || resident <= 0 || which < 0 || which > 6 || !n_out)
+  if (n_plans <= 0 || !dims || resident <= 0 || which < 0 || which > 9 || !n_out)
     return fail(RFXB_E_INVALID, "rfxb_debug_work_lists: bad arguments");
   std::vector<std::unique_ptr<RfxbPlan>> own;
   std::vector<RfxbPlan*> plans;
@@ -2343,10 +2657,19 @@ int rfxb_debug_work_lists(int n_plans, const int32_t* dims, int32_t resident, in
     std::vector<WorkSeg> plain, cpml;
     split_adj_segments(plans, slab, plain, cpml);
     balance_segments(which == 3 ? plain : cpml, resident, 3.0, w);
-  } else {
+  } else if (which <= 6) {
     std::vector<WorkSeg> plain, ys, noy;
     split_adj_segments(plans, slab, plain, ys, &noy);
     balance_segments(which == 5 ? ys : noy, resident, 3.0, w);
+  } else {
+    std::vector<WorkSeg> d2, plain, cpml;
+    split_depth2_segments(plans, slab, d2, plain, cpml);
+    balance_segments(which == 7 ? d2 : which == 8 ? plain : cpml, resident, 3.0, w);
+    if (which == 7)   // the intermediate-store flags ride in bits 16.. of the plan index
+      for (RfxbWork& it : w) {
+        const int mid = depth2_mid_flags(*plans[it.inst], it);
+        it.inst |= mid << 16;
+      }
   }
   *n_out = (int32_t)w.size();
   if (!out) return 0;

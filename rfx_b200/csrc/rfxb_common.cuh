@@ -48,9 +48,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: false if the phase did not complete within `limit` polls
-// (each poll may suspend the thread for a hardware-defined time).
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity, int limit = 1 << 22) {
+// Default poll limit of a pipeline wait (each poll may suspend the thread for
+// a hardware-defined time): a wait that never completes gives up instead of
+// hanging the launch.
+constexpr int kWaitLimit = 1 << 22;
+// Bounded wait: false if the phase did not complete within `limit` polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity, int limit = kWaitLimit) {
   for (int it = 0; it < limit; ++it)
     if (mbar_try_wait(addr, parity)) return true;
   return false;
@@ -70,8 +73,32 @@ struct StepPhases {
 // `wait_limit` polls and the CTA takes the time-out path.
 struct StepFault {
   int cta = -1;
-  int wait_limit = 1 << 22;
+  int wait_limit = kWaitLimit;
 };
+
+// Yee updates with their rounding spelled out (products and fused
+// multiply-adds written as intrinsics, nothing left to contraction), so every
+// kernel that updates a cell, the one-step and the two-step kernels alike,
+// produces the same bits.
+// a * pa - b * pb: one component of a curl
+__device__ __forceinline__ float yee_diff2(float a, float pa, float b, float pb) {
+  return __fmaf_rn(a, pa, -__fmul_rn(b, pb));
+}
+// H^{n+1/2} = H^{n-1/2} - ch * curl E
+__device__ __forceinline__ float yee_h(float h, float ch, float curl) { return __fmaf_rn(-ch, curl, h); }
+// E^{n+1} = ca * E^n + cb * curl H
+__device__ __forceinline__ float yee_e(float ca, float e, float cb, float curl) {
+  return __fmaf_rn(cb, curl, __fmul_rn(ca, e));
+}
+
+// Buffer selector of a forward step launch: the field state is read from
+// F[in] and written to F[out] (0 and 1: the ping-pong pair; 2: the
+// intermediate state of a two-step pass), the CPML psi are read from parity
+// `psi` and written to psi ^ 1.
+__host__ __device__ constexpr int step_sel(int in, int out, int psi) { return in | (out << 2) | (psi << 4); }
+__host__ __device__ constexpr int sel_in(int s) { return s & 3; }
+__host__ __device__ constexpr int sel_out(int s) { return (s >> 2) & 3; }
+__host__ __device__ constexpr int sel_psi(int s) { return (s >> 4) & 1; }
 
 // 4-D tiled TMA load of one box into shared memory, completing on an mbarrier.
 // The innermost coordinate c0 must be a multiple of 4 (16 bytes of float).

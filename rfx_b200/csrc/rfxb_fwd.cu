@@ -130,9 +130,9 @@ __device__ __forceinline__ void h_cell(const RfxbInst& P, const FwdSmem<TY>& S, 
   const float dEx_y = A.e[0][ly + 1][lz] - Ex;
   float chc = C.ch0;
   if (C.ch) chc = C.ch[C.off0 + (long long)i * C.ps + (long long)jj * C.zs + kk];
-  if (MASK & 1) hx = A.h[0][ly][lz] - chc * (dEz_y * yh - dEy_z * zh);
-  if (MASK & 2) hy = A.h[1][ly][lz] - chc * (dEx_z * zh - dEz_x * xh);
-  if (MASK & 4) hz = A.h[2][ly][lz] - chc * (dEy_x * xh - dEx_y * yh);
+  if (MASK & 1) hx = yee_h(A.h[0][ly][lz], chc, yee_diff2(dEz_y, yh, dEy_z, zh));
+  if (MASK & 2) hy = yee_h(A.h[1][ly][lz], chc, yee_diff2(dEx_z, zh, dEz_x, xh));
+  if (MASK & 4) hz = yee_h(A.h[2][ly][lz], chc, yee_diff2(dEy_x, xh, dEx_y, yh));
   const int n = C.ncp;
   const int par = C.par;
   int s, sd;
@@ -237,9 +237,9 @@ __device__ __forceinline__ void h_cell2(const RfxbInst& P, const FwdSmem<TY>& S,
   const float dEz_x = B.e[2][ly][lz] - Ez;
   const float dEy_x = B.e[1][ly][lz] - Ey;
   const float dEx_y = A.e[0][ly + 1][lz] - Ex;
-  if (MASK & 1) hx = A.h[0][ly][lz] - chc * (dEz_y * yh - dEy_z * zh);
-  if (MASK & 2) hy = A.h[1][ly][lz] - chc * (dEx_z * zh - dEz_x * xh);
-  if (MASK & 4) hz = A.h[2][ly][lz] - chc * (dEy_x * xh - dEx_y * yh);
+  if (MASK & 1) hx = yee_h(A.h[0][ly][lz], chc, yee_diff2(dEz_y, yh, dEy_z, zh));
+  if (MASK & 2) hy = yee_h(A.h[1][ly][lz], chc, yee_diff2(dEx_z, zh, dEz_x, xh));
+  if (MASK & 4) hz = yee_h(A.h[2][ly][lz], chc, yee_diff2(dEy_x, xh, dEx_y, yh));
   constexpr int RH = (TY + 1) * RFXB_HW;   // q stride of an H box
   const int par = C.par;
   if (X.on) {   // Hy += ch psi(dEz/dx) [q0], Hz -= ch psi(dEy/dx) [q1]
@@ -322,15 +322,17 @@ __device__ __forceinline__ void load_stage(FwdSmem<TY>& S, const FwdCtx& C, cons
 
 // Issue the TMA boxes of plane ip into its stage (one thread).  Tensor maps of
 // an instance: [0|1] field block of parity 0|1 with the E box, [2|3] the same
-// with the H box, [4] the coefficient block with the ca/cb box.
+// with the H box, [4] the coefficient block with the ca/cb box; the
+// intermediate block (fin = 2) has its own E and H box maps.
 template <int TY, bool EM>
-__device__ __forceinline__ void tma_stage(FwdSmem<TY>& S, const CUtensorMap* tm, int par, int y0, int z0, int ip) {
+__device__ __forceinline__ void tma_stage(FwdSmem<TY>& S, const CUtensorMap* tm, int fin, int y0, int z0, int ip) {
   const int s = stage_of(ip);
   const uint32_t mb = smem_u32(&S.mbar[s]);
+  const int me = fin < 2 ? fin : RFXB_MAP_MIDE, mh = fin < 2 ? 2 + fin : RFXB_MAP_MIDH;
   mbar_expect_tx(mb, FwdStageDims<TY>::BYTES + (EM ? (unsigned)(TY * RFXB_TZ) : 0u));
   if (EM) tma_load_4d(smem_u32(&S.st[s].em[0][0]), tm + RFXB_MAP_EMASK, z0, y0 + 1, ip + 1, 0, mb);
-  tma_load_4d(smem_u32(&S.st[s].e[0][0][0]), tm + par, z0 - 4, y0, ip + 1, 0, mb);
-  tma_load_4d(smem_u32(&S.st[s].h[0][0][0]), tm + 2 + par, z0 - 4, y0, ip + 1, 3, mb);
+  tma_load_4d(smem_u32(&S.st[s].e[0][0][0]), tm + me, z0 - 4, y0, ip + 1, 0, mb);
+  tma_load_4d(smem_u32(&S.st[s].h[0][0][0]), tm + mh, z0 - 4, y0, ip + 1, 3, mb);
   tma_load_4d(smem_u32(&S.st[s].cab[0][0][0]), tm + 4, z0, y0 + 1, ip + 1, 0, mb);
 }
 
@@ -390,7 +392,7 @@ struct FwdBounds<2> { static constexpr int MIN_CTAS = 3; };
 // (TMA modes); without EM the mask (if any) is read from global memory.
 template <int TY, int MODE, bool EM>
 __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const RfxbInst* __restrict__ insts,
-                                         const RfxbWork w, const CUtensorMap* __restrict__ maps, int n, int par,
+                                         const RfxbWork w, const CUtensorMap* __restrict__ maps, int n, int sel,
                                          StepPhases& ph, const StepFault& fault, bool first_item) {
   constexpr bool TMA = MODE != 0;
   using L = PsiSlot<TY>;
@@ -406,10 +408,12 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
   const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const RfxbInst& P = S.P;
   FwdCtx C;
+  // fields in F[fin] -> F[fout], psi parity par -> par ^ 1
+  const int fin = sel_in(sel), fout = sel_out(sel), par = sel_psi(sel);
   C.nx = P.nx; C.ny = P.ny; C.nz = P.nz; C.zs = P.zs; C.ncp = P.ncp; C.par = par;
   C.ps = P.ps; C.off0 = P.off0; C.cs = P.cs;
-  C.Fi = P.F[par][0];
-  C.Fo = P.F[par ^ 1][0];
+  C.Fi = P.F[fin][0];
+  C.Fo = P.F[fout][0];
   C.ch = P.ch;
   C.ch0 = P.ch0;
   const int y0 = w.y0, z0 = w.z0;
@@ -555,7 +559,7 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
   if (TMA) {
     if (tid == producer) {
       for (int p = xa - 1; p <= min(xa + 2, xb); ++p)
-        if (!(skip_first && p == xa)) tma_stage<TY, EM>(S, tm, par, y0, z0, p);
+        if (!(skip_first && p == xa)) tma_stage<TY, EM>(S, tm, fin, y0, z0, p);
     }
     psi_fill(xa - 1);
     psi_fill(xa);
@@ -624,7 +628,7 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
       // psi slot takes plane i+1
       const bool ok = mbar_wait_bounded(smem_u32(&S.mbar[stage_of(i + 1)]), sparity(i + 1), wlim) && psi_wait(i);
       if (__syncthreads_or(!ok)) { bail(min(i + 2, xb), i + 1); return false; }
-      if (tid == producer && i + 3 <= xb) tma_stage<TY, EM>(S, tm, par, y0, z0, i + 3);
+      if (tid == producer && i + 3 <= xb) tma_stage<TY, EM>(S, tm, fin, y0, z0, i + 3);
       if (i + 1 < xb) psi_fill(i + 1);
     } else {
       cp_async_wait<1>();   // planes up to i+1 have landed (i+2 may be in flight)
@@ -706,13 +710,13 @@ __device__ __forceinline__ bool fwd_item(FwdSmem<TY>& S, float* ring, const Rfxb
       const float dHz_x = hz - hz_prev;
       const float dHy_x = hy - hy_prev;
       const float dHx_y = hx - S.h[0][ly - 1][lh];
-      const float cx_ = dHz_y * ye - dHy_z * ze;
-      const float cy_ = dHx_z * ze - dHz_x * xe;
-      const float cz_ = dHy_x * xe - dHx_y * ye;
+      const float cx_ = yee_diff2(dHz_y, ye, dHy_z, ze);
+      const float cy_ = yee_diff2(dHx_z, ze, dHz_x, xe);
+      const float cz_ = yee_diff2(dHy_x, xe, dHx_y, ye);
       const float cav = A.cab[0][ty][lane], cbv = A.cab[1][ty][lane];
-      float ex = cav * Ex + cbv * cx_;
-      float ey = cav * Ey + cbv * cy_;
-      float ez = cav * Ez + cbv * cz_;
+      float ex = yee_e(cav, Ex, cbv, cx_);
+      float ey = yee_e(cav, Ey, cbv, cy_);
+      float ez = yee_e(cav, Ez, cbv, cz_);
       const int ncp = C.ncp;
       // CPML-E correction of each component before its ce scaling (the
       // factor d ce / d eps_r multiplies in the gradient) and this cell's ce
@@ -938,17 +942,18 @@ __device__ __forceinline__ void fwd_init_barriers(FwdSmem<TY>& S, int tid) {
   __syncthreads();
 }
 
-// One launch per step and variant: CTA b runs work item b.
+// One launch per step and variant: CTA b runs work item b.  `sel` selects
+// the field buffers and the psi parity (step_sel).
 template <int TY, int MODE, bool EM>
 __global__ void __launch_bounds__(32 * TY, FwdBounds<MODE>::MIN_CTAS)
 fwd_step_kernel(const RfxbInst* __restrict__ insts, const RfxbWork* __restrict__ work,
-                const CUtensorMap* __restrict__ maps, int n, int par) {
+                const CUtensorMap* __restrict__ maps, int n, int sel) {
   extern __shared__ __align__(128) unsigned char fwd_smem_raw[];
   FwdSmem<TY>& S = *reinterpret_cast<FwdSmem<TY>*>(fwd_smem_raw);
   float* ring = reinterpret_cast<float*>(fwd_smem_raw + sizeof(FwdSmem<TY>));   // mode 2: 2 slots
   fwd_init_barriers<TY, MODE>(S, threadIdx.y * 32 + threadIdx.x);
   StepPhases ph;
-  fwd_item<TY, MODE, EM>(S, ring, insts, work[blockIdx.x], maps, n, par, ph, StepFault{}, true);
+  fwd_item<TY, MODE, EM>(S, ring, insts, work[blockIdx.x], maps, n, sel, ph, StepFault{}, true);
 }
 
 // Whether a work item can be run: its instance exists and its tile and x
@@ -974,7 +979,7 @@ __device__ __forceinline__ bool work_item_valid(const RfxbWork& w, const RfxbIns
 template <int TY, bool EM>
 __global__ void __launch_bounds__(32 * TY, 3)
 fwd_persist_kernel(const RfxbInst* __restrict__ insts, int n_inst, RfxbFwdQueues Q,
-                   const CUtensorMap* __restrict__ maps, int n, int par) {
+                   const CUtensorMap* __restrict__ maps, int n, int sel) {
   extern __shared__ __align__(128) unsigned char fwd_smem_raw[];
   FwdSmem<TY>& S = *reinterpret_cast<FwdSmem<TY>*>(fwd_smem_raw);
   float* ring = reinterpret_cast<float*>(fwd_smem_raw + sizeof(FwdSmem<TY>));
@@ -1007,8 +1012,8 @@ fwd_persist_kernel(const RfxbInst* __restrict__ insts, int n_inst, RfxbFwdQueues
       if (tid == 0) atomicOr(Q.status, 2);
       continue;
     }
-    ok = q == 0 ? fwd_item<TY, 2, EM>(S, ring, insts, w, maps, n, par, ph, fault, first_item)
-                : fwd_item<TY, 1, EM>(S, ring, insts, w, maps, n, par, ph, fault, first_item);
+    ok = q == 0 ? fwd_item<TY, 2, EM>(S, ring, insts, w, maps, n, sel, ph, fault, first_item)
+                : fwd_item<TY, 1, EM>(S, ring, insts, w, maps, n, sel, ph, fault, first_item);
     first_item = false;
   }
   if (tid == 0) {

@@ -28,9 +28,18 @@
 // coefficient with the H box; then the adjoint psi of parity 0|1: [24|25]
 // E-side x (H box), [26|27] E-side y (E box), [28|29] E-side z (E rows),
 // [30|31] H-side x (tile box), [32|33] H-side y (H box), [34|35] H-side z
-// (H rows); [36] the PEC edge-mask bytes with the tile box.
-#define RFXB_NMAPS 37
+// (H rows); [36] the PEC edge-mask bytes with the tile box; [37] the
+// intermediate field state of a two-step pass with the E box, [38] with the
+// H box; the two-step kernel's boxes: [39|40] fields parity 0|1 with the
+// two-step E box, [41|42] with the two-step H box, [43] coefficients with the
+// two-step ca/cb box.
+#define RFXB_NMAPS 44
 #define RFXB_MAP_EMASK 36   // PEC edge mask bytes with the tile box
+#define RFXB_MAP_MIDE 37
+#define RFXB_MAP_MIDH 38
+#define RFXB_MAP_E2 39
+#define RFXB_MAP_H2 41
+#define RFXB_MAP_C2 43
 #define RFXB_MAP_PSH 11
 #define RFXB_MAP_PSE 17
 #define RFXB_MAP_APE 24
@@ -48,7 +57,8 @@ struct RfxbInst {
   long long ps;            // plane stride (elements)
   long long off0;          // element offset of cell (0,0,0)
   long long cs;            // component stride: F[p][c] = F[p][0] + c * cs (multiple of 32)
-  float* F[2][6];          // ping-pong field buffers: ex ey ez hx hy hz
+  float* F[3][6];          // ping-pong field buffers: ex ey ez hx hy hz; [2] the
+                           // intermediate state of two-step passes (or null)
   const float* ca;         // per cell, E decay coefficient
   const float* cb;         // per cell, E curl coefficient
   const float* ce;         // per cell, dt/(eps_r eps0) for CPML-E
@@ -106,6 +116,20 @@ struct RfxbWork {          // one CTA: a (y, z) tile over an x range
   int inst;
   int y0, z0;
   int xa, xb;
+};
+
+// One CTA of the two-step kernel: a tile over an x range, advanced two time
+// steps, and where the intermediate state must also be stored (the cells that
+// one-step neighbours or per-step observers read): bit 0 every plane, bit 1
+// plane xa, bit 2 plane xb-1.
+#define RFXB_MID_ALL 1
+#define RFXB_MID_LO 2
+#define RFXB_MID_HI 4
+struct RfxbWork2 {
+  int inst;
+  int y0, z0;
+  int xa, xb;
+  int mid;
 };
 
 // Work queues of the persistent forward step (one launch per step).

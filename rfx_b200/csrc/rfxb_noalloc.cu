@@ -318,7 +318,7 @@ extern "C" int rfxb_forward_noalloc(const RfxbDesc* d, const float* eps_r_dev, c
   int par = 0;
   for (int s = 0; s < n_steps; ++s) {
     fwd_step_kernel<TY, 0, false><<<(unsigned)n_work, dim3(32, TY), fwd_step_smem_bytes(0), st>>>(dI, dW, nullptr, step0 + s,
-                                                                                           par);
+                                                                                           step_sel(par, par ^ 1, par));
     par ^= 1;
   }
   for (int c = 0; c < 6; ++c) unpack_kernel<<<blocks, 256, 0, st>>>(fields_dev[c], I.F[par][c], I);

@@ -43,7 +43,8 @@ def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-_LAUNCH_FIELDS = ("fwd_split", "fwd_order", "adj_lite", "adj_order", "fwd_persist", "adj_persist", "l2_promo")
+_LAUNCH_FIELDS = ("fwd_split", "fwd_order", "adj_lite", "adj_order", "fwd_persist", "adj_persist", "l2_promo",
+                  "fwd_depth")
 
 
 def _get_launch(getter, h):

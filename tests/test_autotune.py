@@ -82,6 +82,29 @@ def test_candidates_cover_the_limits():
     assert r == [{"adj_lite": 0, "adj_order": 1}, {"adj_lite": 0, "adj_order": 0}]
 
 
+def test_depth_candidates_and_choice():
+    """With two-step tiles (fwd_depth limit 2) the forward search adds one
+    two-step candidate (no persistent launch) and keeps depth 1 unless two
+    steps per pass are faster by more than the margin."""
+    lim = dict(FULL, fwd_persist=3, adj_persist=1, fwd_depth=2)
+    cur = {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": 0, "adj_persist": 0,
+           "fwd_depth": 1}
+    f = at.forward_candidates(lim, cur)
+    assert f[0] == {"fwd_split": 1, "fwd_order": 0, "fwd_persist": 0, "fwd_depth": 1} and len(f) == 7
+    assert [d for d in f if d["fwd_depth"] == 2] == [{"fwd_split": 1, "fwd_order": 0, "fwd_persist": 0,
+                                                       "fwd_depth": 2}]
+    assert all(d["fwd_persist"] == 0 for d in f if d["fwd_depth"] == 2)
+    # the current setting on two-step passes comes first
+    f2 = at.forward_candidates(lim, dict(cur, fwd_depth=2))
+    assert f2[0]["fwd_depth"] == 2 and len(f2) == 7
+    for gain, want in ((0.3, 2), (0.005, 1)):
+        t = FakeTarget(lim, dict(cur))
+        fwd = lambda c, g=gain: 10.0 * (1.0 - g * (c.get("fwd_depth", 1) == 2))
+        timer, rf, rr, _ = _timer_for(t, fwd, lambda c: 20.0)
+        res = at.autotune(t, rf, rr, timer=timer, repeats=1)
+        assert res.config["fwd_depth"] == want and t.cur["fwd_depth"] == want
+
+
 def test_picks_the_fastest_configuration():
     t = FakeTarget(FULL)
     fwd = lambda c: 10.0 - 3.0 * (c["fwd_split"] == 1 and c["fwd_order"] == 1)
@@ -176,7 +199,7 @@ def test_launch_config_bindings_validate_fields():
     lib.get.__func__.__name__ = "rfxb_batch_launch_config"
     cur, lim = engine._get_launch(lib.get, None)
     assert cur == {"fwd_split": 1, "fwd_order": 0, "adj_lite": 1, "adj_order": 0, "fwd_persist": 0, "adj_persist": 0,
-                   "l2_promo": 0}
+                   "l2_promo": 0, "fwd_depth": 0}
     assert lim["adj_order"] == 5
     engine._set_launch(lib.get, lib.set, None, {"adj_order": 3})
     assert engine._get_launch(lib.get, None)[0]["adj_order"] == 3
@@ -226,13 +249,15 @@ def test_every_launch_configuration_gives_the_same_sweep(cuda):
         # the L2 promotion of the TMA boxes moves no value
         assert lim["l2_promo"] == 3
         configs += [{"l2_promo": v} for v in (0, 1, 3, 2)]
+        # two steps per pass compute every cell with the same rounding
+        configs += [{"fwd_depth": 2}, {"fwd_depth": 1}]
         for c in configs:
             if any(v > lim[k] for k, v in c.items()):
                 continue
             sw.batch.set_launch_config(**c)
             J, g = _run(sw)
-            order_only = set(c) <= {"fwd_order", "adj_order", "l2_promo"} or c.get("fwd_persist", 0) > 0 or (
-                c == {"fwd_persist": 0, "adj_persist": 0})
+            order_only = (set(c) <= {"fwd_order", "adj_order", "l2_promo", "fwd_depth"}
+                          or c.get("fwd_persist", 0) > 0 or c == {"fwd_persist": 0, "adj_persist": 0})
             for a, b in zip(g, g0):
                 # the launch order cannot change a value; another kernel
                 # variant on the same tiles may round differently

@@ -12,7 +12,12 @@ and planes whose update needs no CPML term:
 * reverse: CPML-free (3) + CPML (4), or CPML-free (3) + y-slab (5) + the
   rest (6); a reverse CPML-free item's rows y0-1 .. y0+8 and columns z0-1 ..
   z0+32 reach no slab and its planes lie in ncp+1 .. nx-ncp-2; a variant-4
-  item (6) reaches no y slab.
+  item (6) reaches no y slab;
+* two-step passes: two-step tiles (7) + one-step CPML-free work (8) + one-step
+  CPML work (9); every cell a two-step item computes (rows y0-2 .. y0+8,
+  columns z0-2 .. z0+32, planes xa-1 .. xb) lies inside the grid off the
+  faces and the slabs, and an item stores its intermediate state wherever
+  one-step work reads it.
 """
 
 import ctypes as C
@@ -74,9 +79,10 @@ CASES = [
 @pytest.mark.parametrize("resident", [148, 592])
 def test_work_lists_cover_each_plane_once(case, resident):
     plans = CASES[case] if case < len(CASES) else _random_plans(np.random.default_rng(case), 4)
-    groups = {"all": [0], "fwd split": [1, 2], "rev split": [3, 4], "rev lite": [3, 5, 6]}
+    groups = {"all": [0], "fwd split": [1, 2], "rev split": [3, 4], "rev lite": [3, 5, 6], "two-step": [7, 8, 9]}
     for name, ids in groups.items():
         items = np.concatenate([_lists(plans, w, resident) for w in ids])
+        items[:, 0] &= 0xFFFF   # the two-step list's intermediate-store flags
         for q, c in enumerate(_coverage(plans, items)):
             assert c.min() == 1 and c.max() == 1, (name, plans[q])
 
@@ -105,6 +111,62 @@ def test_cpml_free_lists_touch_no_slab(case):
         assert not ((ax & 2) and _reaches(y0 - 1, y0 + TY, ny, ncp))
 
 
+def _two_step_column(plan, y0, z0):
+    """Whether tile column (y0, z0) runs two steps per pass (a plan without
+    sources, probes or gradient region)."""
+    nx, ny, nz, ncp, ax = plan
+    ax = ax if ncp else 0
+    ylo, zlo = max(1, ncp if ax & 2 else 0), max(1, ncp if ax & 4 else 0)
+    yhi = min(ny - 2, ny - ncp - 1 if ax & 2 else ny - 2)
+    zhi = min(nz - 2, nz - ncp - 1 if ax & 4 else nz - 2)
+    return y0 - 2 >= ylo and y0 + TY <= yhi and z0 - 2 >= zlo and z0 + TZ <= zhi
+
+
+def _two_step_xrange(plan):
+    nx, ny, nz, ncp, ax = plan
+    ncpx = ncp if (ncp and ax & 1) else 0
+    return max(ncpx + 1, 2), min(nx - ncpx - 1, nx - 2)
+
+
+TWO_STEP_CASES = CASES + [[(129, 129, 129, 0, 0)], [(117, 117, 117, 10, 7), (90, 200, 75, 8, 7)]]
+
+
+@pytest.mark.parametrize("case", range(len(TWO_STEP_CASES) + 4))
+def test_two_step_tiles_stay_clear_and_store_what_one_step_work_reads(case):
+    plans = (TWO_STEP_CASES[case] if case < len(TWO_STEP_CASES)
+             else _random_plans(np.random.default_rng(200 + case), 4))
+    items = _lists(plans, 7)
+    cols = set()
+    for code, y0, z0, xa, xb in items:
+        q, mid = code & 0xFFFF, code >> 16
+        plan = plans[q]
+        assert _two_step_column(plan, y0, z0), (plan, y0, z0)
+        lo, hi = _two_step_xrange(plan)
+        assert lo <= xa < xb <= hi
+        cols.add((q, y0, z0))
+        # first / last plane of the column's two-step range: one-step work
+        # continues beyond it and reads that plane's intermediate state
+        assert bool(mid & 2) == (xa == lo) and bool(mid & 4) == (xb == hi)
+        ring = all(_two_step_column(plan, y0 + dy * TY, z0 + dz * TZ)
+                   for dy in (-1, 0, 1) for dz in (-1, 0, 1))
+        assert bool(mid & 1) == (not ring)
+    # a plan large enough for it has two-step tiles; the one-step CPML-free
+    # work of a pass keeps the CPML-free kernel's bounds
+    for q, plan in enumerate(plans):
+        nx, ny, nz, ncp, ax = plan
+        lo, hi = _two_step_xrange(plan)
+        any_col = any(_two_step_column(plan, y0, z0) for y0 in range(0, ny, TY) for z0 in range(0, nz, TZ))
+        assert any(qq == q for (qq, _, _) in cols) == (any_col and hi - lo >= 8)
+    for q, y0, z0, xa, xb in _lists(plans, 8):
+        nx, ny, nz, ncp, ax = plans[q]
+        if not ncp or not ax:
+            continue
+        assert not ((ax & 2) and _reaches(y0 - 1, y0 + TY - 1, ny, ncp))
+        assert not ((ax & 4) and _reaches(z0 - 1, z0 + TZ - 1, nz, ncp))
+        if ax & 1:
+            assert xa >= ncp + 1 and xb <= nx - ncp
+
+
 def test_bad_arguments_are_rejected():
     lib = _lib.load()
     n = C.c_int32()
@@ -112,7 +174,7 @@ def test_bad_arguments_are_rejected():
     invalid = -1   # RFXB_E_INVALID
     assert lib.rfxb_debug_work_lists(1, dims, 100, 0, None, 0, C.byref(n)) == invalid
     dims = (C.c_int32 * 5)(20, 20, 20, 4, 7)
-    assert lib.rfxb_debug_work_lists(1, dims, 100, 7, None, 0, C.byref(n)) == invalid
+    assert lib.rfxb_debug_work_lists(1, dims, 100, 10, None, 0, C.byref(n)) == invalid
     assert lib.rfxb_debug_work_lists(1, dims, 100, 0, None, 0, C.byref(n)) == 0 and n.value > 0
     small = (C.c_int32 * 5)()
     assert lib.rfxb_debug_work_lists(1, dims, 100, 0, small, 1, C.byref(n)) == invalid
