@@ -499,37 +499,43 @@ void split_adj_segments(const std::vector<RfxbPlan*>& plans, double slab, std::v
 
 // Two-step passes.  A tile column (y0, z0) of plan p runs on the two-step
 // kernel when every cell its two steps compute -- rows y0-2 .. y0+TY,
-// columns z0-2 .. z0+32 -- lies inside the grid, off the PEC faces and out of
-// every CPML slab, and no source, probe or gradient-history cell lies within
-// reach (rows y0-2 .. y0+TY+1, columns z0-2 .. z0+33); the plan must have
-// uniform H coefficients and no PEC edge mask.
+// columns z0-2 .. z0+32 -- lies out of every CPML slab, and no source, probe
+// or gradient-history cell lies within reach (rows y0-2 .. y0+TY+1, columns
+// z0-2 .. z0+33); the plan must have uniform H coefficients and no PEC edge
+// mask.  On an axis without CPML the cells may reach the grid faces: such a
+// column is a face column (the kernel's guarded path: zero outside the grid,
+// PEC faces on E); 0 = not a two-step column, 1 = interior, 2 = face column.
 bool depth2_plan(const RfxbPlan& p) { return p.inst.emask == nullptr && p.inst.ch == nullptr; }
 
-bool depth2_column(const RfxbPlan& p, int y0, int z0) {
+int depth2_column(const RfxbPlan& p, int y0, int z0) {
+  if (y0 < 0 || y0 >= p.ny || z0 < 0 || z0 >= p.nz) return 0;
   const int n = p.inst.ncp;
   const unsigned ax = n > 0 ? p.inst.cpml_axes : 0u;
-  const int ylo = std::max(1, (ax & 2u) ? n : 0), zlo = std::max(1, (ax & 4u) ? n : 0);
-  const int yhi = std::min(p.ny - 2, (ax & 2u) ? p.ny - n - 1 : p.ny - 2);
-  const int zhi = std::min(p.nz - 2, (ax & 4u) ? p.nz - n - 1 : p.nz - 2);
-  if (y0 - 2 < ylo || y0 + kTY > yhi || z0 - 2 < zlo || z0 + 32 > zhi) return false;
+  if ((ax & 2u) && (y0 - 2 < n || y0 + kTY > p.ny - n - 1)) return 0;
+  if ((ax & 4u) && (z0 - 2 < n || z0 + 32 > p.nz - n - 1)) return 0;
   auto near = [&](int j, int k) { return j >= y0 - 2 && j <= y0 + kTY + 1 && k >= z0 - 2 && k <= z0 + 33; };
   for (const int4& c : p.src)
-    if (near(c.y, c.z)) return false;
+    if (near(c.y, c.z)) return 0;
   for (const int4& c : p.prb)
-    if (near(c.y, c.z)) return false;
+    if (near(c.y, c.z)) return 0;
   const int* hb = p.inst.hb;
   if (hb[0] < hb[1] && hb[2] <= y0 + kTY + 1 && hb[3] - 1 >= y0 - 2 && hb[4] <= z0 + 33 && hb[5] - 1 >= z0 - 2)
-    return false;
-  return true;
+    return 0;
+  // interior: the first step's E cells (rows y0-1 .. y0+TY) off the faces,
+  // its H cells (rows y0-2 ..) inside the grid
+  const bool yin = y0 - 1 >= 1 && y0 + kTY <= p.ny - 2;
+  const bool zin = z0 - 1 >= 1 && z0 + 32 <= p.nz - 2;
+  return (yin && zin) ? 1 : 2;
 }
 
-// The x range of a plan's two-step segments: planes whose x-1 .. x+1
-// neighbours are off the x slabs and the PEC x faces.
+// The x range of a plan's two-step segments: all planes without x CPML (the
+// items at the x faces take the guarded path), else the planes whose x-1 ..
+// x+1 neighbours are off the x slabs.
 void depth2_xrange(const RfxbPlan& p, int& dlo, int& dhi) {
   const int n = p.inst.ncp;
   const int ncpx = (n > 0 && (p.inst.cpml_axes & 1u)) ? n : 0;
-  dlo = std::max(ncpx + 1, 2);
-  dhi = std::min(p.nx - ncpx - 1, p.nx - 2);
+  dlo = ncpx > 0 ? ncpx + 1 : 0;
+  dhi = ncpx > 0 ? p.nx - ncpx - 1 : p.nx;
 }
 
 // Work of a two-step pass: two-step segments (d2), the other CPML-free work
@@ -567,8 +573,15 @@ void split_depth2_segments(const std::vector<RfxbPlan*>& plans, double slab, std
           if (hi < p.nx) cpml.push_back(WorkSeg{(int)q, y0, z0, hi, p.nx, p.nx, ncpx, 1.0, cx});
         }
         const int a = std::max(lo, dlo), b = std::min(hi, dhi);
-        if (plan_ok && b - a >= 8 && depth2_column(p, y0, z0)) {
-          d2.push_back(WorkSeg{(int)q, y0, z0, a, b, p.nx, 0, 1.0, 0.0});
+        if (plan_ok && b - a >= 8 && depth2_column(p, y0, z0) > 0) {
+          if (a < 2 && b > p.nx - 2 && b - a >= 32) {
+            // the x faces' end pieces apart, so the rest takes the interior path
+            d2.push_back(WorkSeg{(int)q, y0, z0, a, a + 8, p.nx, 0, 1.0, 0.0});
+            d2.push_back(WorkSeg{(int)q, y0, z0, a + 8, b - 8, p.nx, 0, 1.0, 0.0});
+            d2.push_back(WorkSeg{(int)q, y0, z0, b - 8, b, p.nx, 0, 1.0, 0.0});
+          } else {
+            d2.push_back(WorkSeg{(int)q, y0, z0, a, b, p.nx, 0, 1.0, 0.0});
+          }
           if (a > lo) plain.push_back(WorkSeg{(int)q, y0, z0, lo, a, p.nx, 0, 1.0, 0.0});
           if (b < hi) plain.push_back(WorkSeg{(int)q, y0, z0, b, hi, p.nx, 0, 1.0, 0.0});
         } else {
@@ -579,20 +592,24 @@ void split_depth2_segments(const std::vector<RfxbPlan*>& plans, double slab, std
 }
 
 // Where a two-step item also stores its intermediate state (RfxbWork2::mid):
-// at its first / last plane when that is the end of its column's two-step
-// range (one-step work continues beyond), on every plane when one of the
-// eight neighbouring columns runs one-step work (its halo reads this tile)
-// or when a DFT plane, flux monitor or NTFF face of the plan passes through
-// the item (the observers read every step's state).
+// at its first / last plane when one-step work continues beyond it in x, on
+// every plane when one of the eight neighbouring columns runs one-step work
+// (its halo reads this tile) or when a DFT plane, flux monitor or NTFF face
+// of the plan passes through the item (the observers read every step's
+// state).  RFXB_MID_EDGE marks items whose cells reach a grid face.
 int depth2_mid_flags(const RfxbPlan& p, const RfxbWork& w) {
   int dlo, dhi;
   depth2_xrange(p, dlo, dhi);
   int mid = 0;
-  if (w.xa == dlo) mid |= RFXB_MID_LO;
-  if (w.xb == dhi) mid |= RFXB_MID_HI;
+  if (w.xa == dlo && dlo > 0) mid |= RFXB_MID_LO;
+  if (w.xb == dhi && dhi < p.nx) mid |= RFXB_MID_HI;
   for (int dy = -1; dy <= 1; ++dy)
-    for (int dz = -1; dz <= 1; ++dz)
-      if ((dy || dz) && !depth2_column(p, w.y0 + dy * kTY, w.z0 + dz * 32)) mid |= RFXB_MID_ALL;
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int y = w.y0 + dy * kTY, z = w.z0 + dz * 32;
+      const bool in_grid = y >= 0 && y < p.ny && z >= 0 && z < p.nz;
+      if ((dy || dz) && in_grid && depth2_column(p, y, z) == 0) mid |= RFXB_MID_ALL;
+    }
+  if (depth2_column(p, w.y0, w.z0) == 2 || w.xa < 2 || w.xb > p.nx - 2) mid |= RFXB_MID_EDGE;
   auto through = [&](int axis, int index) {
     const int lo = axis == 0 ? w.xa : axis == 1 ? w.y0 : w.z0;
     const int hi = axis == 0 ? w.xb : axis == 1 ? w.y0 + kTY : w.z0 + 32;
@@ -739,11 +756,22 @@ int fwd2_resident() {
   return r;
 }
 
-// Default depth of the forward passes (RFXB_FWD_DEPTH=2: two steps per pass
-// where the group has two-step tiles; otherwise one).
-int fwd_depth_default() {
+// Default depth of the forward passes: RFXB_FWD_DEPTH=1 or 2 sets it for
+// every group with two-step tiles; unset, groups without any CPML of at least
+// 2^24 cells take two steps per pass (the 513^3 PEC benchmark: 78.1 -> 98.1
+// G cells/s) and the others one (with CPML the gain measured 0-2 %, and on
+// small grids the directly launched passes lose the graphs' launch rate;
+// the autotuner chooses per workload).
+int fwd_depth_default(const RfxbBatch* g) {
   const char* e = getenv("RFXB_FWD_DEPTH");
-  return (e && std::string(e) == "2") ? 2 : 1;
+  if (e && std::string(e) == "2") return 2;
+  if (e && std::string(e) == "1") return 1;
+  long long cells = 0;
+  for (const RfxbPlan* p : g->plans) {
+    if (p->inst.ncp > 0 && p->inst.cpml_axes != 0u) return 1;
+    cells += (long long)p->nx * p->ny * p->nz;
+  }
+  return cells >= (1LL << 24) ? 2 : 1;
 }
 
 using FwdPersistKernel = void (*)(const RfxbInst*, int, RfxbFwdQueues, const CUtensorMap*, int, int);
@@ -1244,7 +1272,7 @@ int build_group(RfxbBatch* g) {
         RFXB_CUDA(cudaEventCreateWithFlags(&g->ev_join2, cudaEventDisableTiming));
       }
       g->fwd_depth_avail = true;
-      if (fwd_depth_default() == 2) {
+      if (fwd_depth_default(g) == 2) {
         for (auto* p : g->plans)
           if (int rc = ensure_mid(p)) return rc;
         g->fwd_depth = 2;
@@ -1625,9 +1653,13 @@ int group_advance(RfxbBatch* g, const RfxbStepIO* ios, int step0, int n_steps, c
     if (p->par != par0 || p->ppar != ppar0) return fail(RFXB_E_STATE, "plans of a batch must share the step parity");
   bool has_dft = false, has_prb = false, has_flux = false, has_ntff = false;
   if (int rc = upload_group(g, ios, &has_dft, &has_prb, &has_flux, &has_ntff, st)) return rc;
-  if (graphs_enabled() && n_steps >= 4) {
-    const GraphKey key{0, step0, n_steps, par0, 0,
-                       (has_dft ? 1 : 0) | (has_flux ? 2 : 0) | (has_ntff ? 4 : 0) | (two_step(g) ? 8 : 0), ppar0};
+  // two-step passes launch directly: each pass is milliseconds of device
+  // work, and their captured graphs measured slower to build and to replay
+  // (1000 steps of a 513^3 grid: 0.9 s to capture, 1.58 s against 1.49 s per
+  // replay)
+  if (graphs_enabled() && n_steps >= 4 && !two_step(g)) {
+    const GraphKey key{0, step0, n_steps, par0, 0, (has_dft ? 1 : 0) | (has_flux ? 2 : 0) | (has_ntff ? 4 : 0),
+                       ppar0};
     if (int rc = run_graph(g, key, st, [&](cudaStream_t cs) {
           return launch_steps(g, step0, n_steps, par0, ppar0, has_dft, has_flux, has_ntff, cs);
         }))

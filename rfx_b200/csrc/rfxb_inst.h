@@ -121,10 +121,12 @@ struct RfxbWork {          // one CTA: a (y, z) tile over an x range
 // One CTA of the two-step kernel: a tile over an x range, advanced two time
 // steps, and where the intermediate state must also be stored (the cells that
 // one-step neighbours or per-step observers read): bit 0 every plane, bit 1
-// plane xa, bit 2 plane xb-1.
+// plane xa, bit 2 plane xb-1; bit 3: the item's cells reach a grid face (the
+// kernel then keeps cells outside the grid at zero and applies PEC faces).
 #define RFXB_MID_ALL 1
 #define RFXB_MID_LO 2
 #define RFXB_MID_HI 4
+#define RFXB_MID_EDGE 8
 struct RfxbWork2 {
   int inst;
   int y0, z0;

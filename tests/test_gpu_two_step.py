@@ -13,7 +13,9 @@ identical, not merely close:
 * the uniform CPML grid of the 277^3 configuration at 117^3 (8 probes, a
   source, a z-plane DFT through two-step tiles), from random fields in every
   cell, over odd and even step counts and cut into chunks of odd lengths;
-* the reference's own PEC benchmark (no CPML, PEC faces) at 129^3;
+* the reference's own PEC benchmark (no CPML, PEC faces) at 129^3, and grids
+  mixing CPML, PEC and open faces by axis (the guarded path of the tiles
+  whose cells reach a face);
 * a graded-z grid with CPML (the spacing tables of the non-uniform lane);
 * the batched sweep (history recording, adjoint gradients);
 * a saved and restored state blob and checkpoints taken mid-run.
@@ -85,6 +87,25 @@ def test_two_step_pec_cube_equals_one_step(cuda):
         _check_two_step_available(r)
         init = _random_fields(g.shape, 6)
         _same(_run(r, n, init, 1), _run(r, n, init, 2), "pec cube")
+    finally:
+        r.plan.close()
+
+
+@pytest.mark.parametrize("cpml_axes,pec_axes", [("z", "x"), ("xy", ""), ("", "yz"), ("", "")])
+def test_two_step_mixed_faces_equal_one_step(cuda, cpml_axes, pec_axes):
+    """Axes with CPML, with PEC faces and open (zero guards only): the tiles
+    whose cells reach a PEC or open face take the guarded path."""
+    from rfx_b200.simulation import MaterialArrays, init_dft_plane_probe, prepare_device_run
+    n = 29
+    g, eps, sig, src, probes, dft = workloads.large_uniform(n_steps=n, n_interior=80)
+    planes = [init_dft_plane_probe(a, ix, c, f, g.shape) for (a, ix, c, f) in dft]
+    r = prepare_device_run(g, MaterialArrays(eps, sig, np.ones_like(eps)), n, cpml_axes=cpml_axes,
+                           pec_axes=pec_axes, sources=src, probes=[p[:4] for p in probes], dft_planes=planes,
+                           pec_mask=None, dft_time_offset=1)
+    try:
+        _check_two_step_available(r)
+        init = _random_fields(g.shape, 10)
+        _same(_run(r, n, init, 1), _run(r, n, init, 2), f"cpml {cpml_axes!r}, pec {pec_axes!r}")
     finally:
         r.plan.close()
 

@@ -15,9 +15,9 @@ and planes whose update needs no CPML term:
   item (6) reaches no y slab;
 * two-step passes: two-step tiles (7) + one-step CPML-free work (8) + one-step
   CPML work (9); every cell a two-step item computes (rows y0-2 .. y0+8,
-  columns z0-2 .. z0+32, planes xa-1 .. xb) lies inside the grid off the
-  faces and the slabs, and an item stores its intermediate state wherever
-  one-step work reads it.
+  columns z0-2 .. z0+32, planes xa-2 .. xb) lies out of the slabs, an item
+  whose cells reach a grid face or guard takes the guarded path, and an item
+  stores its intermediate state wherever one-step work reads it.
 """
 
 import ctypes as C
@@ -112,23 +112,30 @@ def test_cpml_free_lists_touch_no_slab(case):
 
 
 def _two_step_column(plan, y0, z0):
-    """Whether tile column (y0, z0) runs two steps per pass (a plan without
-    sources, probes or gradient region)."""
+    """0: tile column (y0, z0) runs one-step work in a two-step pass; 1: it
+    runs on the two-step kernel's interior path; 2: on its guarded path (cells
+    reach a grid face) -- for a plan without sources, probes or gradient
+    region."""
     nx, ny, nz, ncp, ax = plan
     ax = ax if ncp else 0
-    ylo, zlo = max(1, ncp if ax & 2 else 0), max(1, ncp if ax & 4 else 0)
-    yhi = min(ny - 2, ny - ncp - 1 if ax & 2 else ny - 2)
-    zhi = min(nz - 2, nz - ncp - 1 if ax & 4 else nz - 2)
-    return y0 - 2 >= ylo and y0 + TY <= yhi and z0 - 2 >= zlo and z0 + TZ <= zhi
+    if not (0 <= y0 < ny and 0 <= z0 < nz):
+        return 0
+    if ax & 2 and (y0 - 2 < ncp or y0 + TY > ny - ncp - 1):
+        return 0
+    if ax & 4 and (z0 - 2 < ncp or z0 + TZ > nz - ncp - 1):
+        return 0
+    inner = y0 - 1 >= 1 and y0 + TY <= ny - 2 and z0 - 1 >= 1 and z0 + TZ <= nz - 2
+    return 1 if inner else 2
 
 
 def _two_step_xrange(plan):
     nx, ny, nz, ncp, ax = plan
     ncpx = ncp if (ncp and ax & 1) else 0
-    return max(ncpx + 1, 2), min(nx - ncpx - 1, nx - 2)
+    return (ncpx + 1, nx - ncpx - 1) if ncpx else (0, nx)
 
 
-TWO_STEP_CASES = CASES + [[(129, 129, 129, 0, 0)], [(117, 117, 117, 10, 7), (90, 200, 75, 8, 7)]]
+TWO_STEP_CASES = CASES + [[(129, 129, 129, 0, 0)], [(117, 117, 117, 10, 7), (90, 200, 75, 8, 7)],
+                          [(100, 90, 77, 10, 5), (64, 64, 64, 8, 1)]]
 
 
 @pytest.mark.parametrize("case", range(len(TWO_STEP_CASES) + 4))
@@ -140,16 +147,21 @@ def test_two_step_tiles_stay_clear_and_store_what_one_step_work_reads(case):
     for code, y0, z0, xa, xb in items:
         q, mid = code & 0xFFFF, code >> 16
         plan = plans[q]
-        assert _two_step_column(plan, y0, z0), (plan, y0, z0)
+        nx = plan[0]
+        kind = _two_step_column(plan, y0, z0)
+        assert kind > 0, (plan, y0, z0)
         lo, hi = _two_step_xrange(plan)
         assert lo <= xa < xb <= hi
         cols.add((q, y0, z0))
         # first / last plane of the column's two-step range: one-step work
         # continues beyond it and reads that plane's intermediate state
-        assert bool(mid & 2) == (xa == lo) and bool(mid & 4) == (xb == hi)
-        ring = all(_two_step_column(plan, y0 + dy * TY, z0 + dz * TZ)
+        assert bool(mid & 2) == (xa == lo and lo > 0) and bool(mid & 4) == (xb == hi and hi < nx)
+        ring = all(_two_step_column(plan, y0 + dy * TY, z0 + dz * TZ) > 0 or
+                   not (0 <= y0 + dy * TY < plan[1] and 0 <= z0 + dz * TZ < plan[2])
                    for dy in (-1, 0, 1) for dz in (-1, 0, 1))
         assert bool(mid & 1) == (not ring)
+        # the guarded path wherever a computed cell reaches a face or a guard
+        assert bool(mid & 8) == (kind == 2 or xa < 2 or xb > nx - 2)
     # a plan large enough for it has two-step tiles; the one-step CPML-free
     # work of a pass keeps the CPML-free kernel's bounds
     for q, plan in enumerate(plans):
