@@ -170,15 +170,15 @@ def cpu_baseline_port(args, n_workers=1, n_time=60):
 # our arm
 # ---------------------------------------------------------------------------
 
-def _traffic_per_cell(kernel):
+def _traffic_per_cell(kernel, key="small_case_dram_bytes_per_cell_per_step"):
     """DRAM bytes per cell and time step of a step kernel (all its launches
     of one step), measured by ncu on the 4-instance case of the same sweep
-    (committed in profiles/<kernel>.md) and scaled by cells to the workload;
-    None if the summary has no such line."""
+    (committed in profiles/<kernel>.md as ``key: value``) and scaled by cells
+    to the workload; None if the summary has no such line."""
     path = os.path.join(ROOT, "profiles", f"{kernel}.md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"small_case_dram_bytes_per_cell_per_step:\s*([0-9.eE+-]+)", open(path).read())
+    m = re.search(re.escape(key) + r":\s*([0-9.eE+-]+)", open(path).read())
     return float(m.group(1)) if m else None
 
 
@@ -270,10 +270,10 @@ def run_ours(args, rank, world, local_rank):
     # rooflines of the two step kernels: algorithmic bytes per launch over the
     # average launch time (one launch per time step in each phase; the
     # backward phase also holds one adjoint-init launch per bench step)
-    def roof(kernel, alg, ms, what):
+    def roof(kernel, alg, ms, what, key="small_case_dram_bytes_per_cell_per_step"):
         step_s = ms / 1e3 / (N * args.steps)
         achieved = alg / step_s / 1e9
-        tpc = _traffic_per_cell(kernel)
+        tpc = _traffic_per_cell(kernel, key)
         return {"kernel": kernel, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4),
                 "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
@@ -284,9 +284,18 @@ def run_ours(args, rank, world, local_rank):
                     "fused reverse step, batched over all instances: variant 2 on the tiles that reach a y slab, "
                     "variant 4 on the other CPML work, variant 3 on the plain tiles, three streams; one step = "
                     "the three launches")
-    roof_fwd = roof("fwd_step_kernel", sum(p.algorithmic_bytes_per_step() for p in sw.plans), fwd_ms,
-                    "fused forward step, batched over all instances: variant 2 on the CPML tiles and variant 1 "
-                    "on the plain tiles, two streams; one step = both launches")
+    two_step = (sw.batch or sw.plans[0]).launch_config()[0].get("fwd_depth", 1) == 2
+    if two_step:
+        roof_fwd = roof("fwd_step_kernel", sum(p.algorithmic_bytes_per_step() for p in sw.plans), fwd_ms,
+                        "forward in two-step passes, batched over all instances: fwd2_step_kernel advances the "
+                        "tiles clear of CPML, sources, probes and the gradient region two steps per read of the "
+                        "state, beside two launches of variant 2 (CPML tiles) and variant 1 (the other CPML-free "
+                        "work) per pass; algorithmic bytes counted per step",
+                        key="small_case_dram_bytes_per_cell_per_step_two_step")
+    else:
+        roof_fwd = roof("fwd_step_kernel", sum(p.algorithmic_bytes_per_step() for p in sw.plans), fwd_ms,
+                        "fused forward step, batched over all instances: variant 2 on the CPML tiles and variant 1 "
+                        "on the plain tiles, two streams; one step = both launches")
     roofline, roofline_other = (roof_adj, roof_fwd) if adj_ms >= fwd_ms else (roof_fwd, roof_adj)
 
     # single-instance comparison (each simulation launched on its own)
@@ -597,8 +606,12 @@ def run_pec_uniform(args, emit, hbm_peak, peak_src):
                "wall_s": round(wall, 3), "walls_s": [round(x, 3) for x in walls],
                "h2d_bytes_per_step": int(eps.nbytes + sig.nbytes + eps.nbytes), "d2h_bytes_per_step": int(4 * N)}
     step_s = ms / 1e3 / (args.steps * N)
+    depth2 = cfg.get("fwd_depth", 1) == 2
     kernel = ("fwd2_step_kernel (two steps per pass; algorithmic bytes counted per step)"
-              if cfg.get("fwd_depth", 1) == 2 else "fwd_step_kernel (CPML-free variant)")
+              if depth2 else "fwd_step_kernel (CPML-free variant)")
+    # DRAM bytes per cell-step of the 257^3 capture of the same scene
+    tpc = _traffic_per_cell("fwd2_step_kernel", "pec_257_dram_bytes_per_cell_per_step_" +
+                            ("two_step" if depth2 else "one_step"))
     line = {"metric": "Mcells/s (cell updates per second), PEC-only uniform run(): the reference's rfx.gpu.benchmark",
             "value": round(cells * N * args.steps / (ms / 1e3) / 1e6, 1), "unit": "Mcells/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2),
@@ -613,7 +626,8 @@ def run_pec_uniform(args, emit, hbm_peak, peak_src):
             "e2e": e2e,
             "roofline": {"kernel": kernel, "bound": "hbm",
                          "achieved": round(alg / step_s / 1e9, 1), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(alg / step_s / 1e9 / hbm_peak, 4), "peak_source": peak_src, "traffic": None,
+                         "frac": round(alg / step_s / 1e9 / hbm_peak, 4), "peak_source": peak_src,
+                         "traffic": round(tpc * cells) if tpc else None,
                          "algorithmic_bytes_per_step": int(alg)},
             "clocks": clk.summary()}
     if emit:
