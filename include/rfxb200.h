@@ -320,7 +320,7 @@ int rfxb_plan_box_energy_weighted(RfxbPlan* plan, const int* box, const double* 
 int rfxb_plan_box_flux(RfxbPlan* plan, const int* box, double* flux_dev, void* stream);
 
 /* Bytes of device memory a plan holds (state, coefficients, psi, history,
- * checkpoints). */
+ * checkpoints, and the intermediate state of two-step passes once used). */
 int64_t rfxb_plan_device_bytes(const RfxbPlan* plan);
 
 /* Which forward step kernel the launches of a plan (or batch) use: 0 the

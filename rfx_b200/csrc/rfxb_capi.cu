@@ -2731,6 +2731,7 @@ int64_t rfxb_plan_device_bytes(const RfxbPlan* p) {
   if (!p) return 0;
   int64_t b = 0;
   b += 12 * p->elems * 4;                  // fields
+  if (p->mid) b += 6 * p->elems * 4;       // intermediate state of two-step passes
   b += 3 * p->elems * 4;                   // ca cb ce
   if (p->ch) b += p->elems * 4;
   if (p->emask) b += p->elems;
