@@ -17,6 +17,8 @@ identical, not merely close:
   mixing CPML, PEC and open faces by axis (the guarded path of the tiles
   whose cells reach a face);
 * a graded-z grid with CPML (the spacing tables of the non-uniform lane);
+* a DFT plane, a flux monitor and an NTFF box through two-step tiles (the
+  observers read each pass's intermediate state);
 * the batched sweep (history recording, adjoint gradients);
 * a saved and restored state blob and checkpoints taken mid-run.
 """
@@ -106,6 +108,49 @@ def test_two_step_mixed_faces_equal_one_step(cuda, cpml_axes, pec_axes):
         _check_two_step_available(r)
         init = _random_fields(g.shape, 10)
         _same(_run(r, n, init, 1), _run(r, n, init, 2), f"cpml {cpml_axes!r}, pec {pec_axes!r}")
+    finally:
+        r.plan.close()
+
+
+def test_two_step_observers_equal_one_step(cuda):
+    """A DFT plane, a flux monitor and an NTFF box whose planes pass through
+    two-step tiles: their accumulators read the intermediate state of every
+    pass (stored by those tiles) and match one step per pass bit for bit,
+    over an odd step count (a pass of two and a last single step)."""
+    import rfx_b200
+    from rfx_b200.simulation import prepare_device_run
+    g = rfx_b200.Grid(freq_max=20e9, domain=(0.08, 0.08, 0.08), dx=1e-3, cpml_layers=4)
+    n = 51
+    t = np.arange(n, dtype=np.float32) * np.float32(g.dt)
+    w = rfx_b200.GaussianPulse(f0=28e9, bandwidth=0.5)(t).astype(np.float32)
+    c = (g.nx // 2, g.ny // 2, g.nz // 2)
+    eps = (1.0 + np.random.default_rng(4).random(g.shape)).astype(np.float32)
+    mats = rfx_b200.MaterialArrays(eps, np.zeros(g.shape, np.float32), np.ones(g.shape, np.float32))
+    planes = [rfx_b200.init_dft_plane_probe(1, c[1] - 13, "ex", [24e9, 29e9], g.shape)]
+    mons = [rfx_b200.init_flux_monitor(2, c[2] + 13, [26e9], g.shape, g.dx, g.dx, lo1=3, hi1=g.nx - 3)]
+    box = (20, g.nx - 20, 22, g.ny - 22, 18, g.nz - 18, np.array([25e9, 30e9], np.float32))
+    r = prepare_device_run(g, mats, n, cpml_axes="xyz", pec_axes="", sources=[(*c, "ez", w)],
+                           probes=[(c[0], c[1] + 1, c[2], "ey")], dft_planes=planes, pec_mask=None,
+                           dft_time_offset=1, flux_monitors=mons, ntff_box=rfx_b200.NTFFBox(*box))
+
+    def run(depth):
+        p = r.plan
+        p.set_launch_config(fwd_depth=depth)
+        p.reset()
+        for a in list(r.dft_accs) + list(r.flux_accs) + [r.ntff[0], r.ntff[1]]:   # (NTFF: sums, residuals)
+            a.zero_()
+        p.advance(0, n, r.src_table, r.probe_out, r.dft_accs, r.dft_phases, r.flux_accs, r.flux_kernels, r.ntff)
+        torch.cuda.synchronize()
+        p.check_device()
+        return ([a.cpu().numpy().copy() for a in r.dft_accs] + [a.cpu().numpy().copy() for a in r.flux_accs] +
+                [r.ntff[0].cpu().numpy().copy(), r.probe_out.cpu().numpy().copy()] + _fields(r))
+
+    try:
+        _check_two_step_available(r)
+        one, two = run(1), run(2)
+        for q, (x, y) in enumerate(zip(one, two)):
+            assert np.abs(x).max() > 0, q
+            assert np.array_equal(x, y), q
     finally:
         r.plan.close()
 
