@@ -384,8 +384,8 @@ int rfxb_batch_step_launches(const RfxbBatch* batch, int* fwd, int* rev);
  *                 kernel while the rest runs one launch per step through an
  *                 intermediate field buffer (allocated on first use, 24 bytes
  *                 per cell); an odd remaining step runs alone, and every
- *                 step does while a plan has per-cell mu_r or a PEC edge
- *                 mask.  Excludes fwd_persist > 0.  Results equal depth 1
+ *                 step does while a plan has per-cell mu_r.  Excludes
+ *                 fwd_persist > 0.  Results equal depth 1
  *                 bit for bit (rfxb_*_step_launches then counts the
  *                 launches of one pass of two steps).
  * rfxb_*_launch_config writes the current setting to *current and the

@@ -501,11 +501,12 @@ void split_adj_segments(const std::vector<RfxbPlan*>& plans, double slab, std::v
 // kernel when every cell its two steps compute -- rows y0-2 .. y0+TY,
 // columns z0-2 .. z0+32 -- lies out of every CPML slab, and no source, probe
 // or gradient-history cell lies within reach (rows y0-2 .. y0+TY+1, columns
-// z0-2 .. z0+33); the plan must have uniform H coefficients and no PEC edge
-// mask.  On an axis without CPML the cells may reach the grid faces: such a
+// z0-2 .. z0+33); the plan must have uniform H coefficients (a PEC edge mask
+// is applied by the kernel).  On an axis without CPML the cells may reach the
+// grid faces: such a
 // column is a face column (the kernel's guarded path: zero outside the grid,
 // PEC faces on E); 0 = not a two-step column, 1 = interior, 2 = face column.
-bool depth2_plan(const RfxbPlan& p) { return p.inst.emask == nullptr && p.inst.ch == nullptr; }
+bool depth2_plan(const RfxbPlan& p) { return p.inst.ch == nullptr; }
 
 int depth2_column(const RfxbPlan& p, int y0, int z0) {
   if (y0 < 0 || y0 >= p.ny || z0 < 0 || z0 >= p.nz) return 0;
@@ -1465,8 +1466,8 @@ int upload_group(RfxbBatch* g, const RfxbStepIO* ios, bool* has_dft, bool* has_p
 }
 
 // Two-step passes run when chosen, when the group has two-step tiles and
-// while every plan still has uniform H coefficients and no PEC edge mask
-// (materials set after the lists were built may add either).
+// while every plan still has uniform H coefficients (materials set after the
+// lists were built may add per-cell mu_r).
 bool two_step(const RfxbBatch* g) {
   if (g->fwd_depth != 2 || !g->fwd_depth_avail) return false;
   for (const RfxbPlan* p : g->plans)

@@ -20,9 +20,11 @@
 // one the one-step kernel computes, bit for bit.
 //
 // The host gives this kernel only tiles whose cells, halo included, lie in no
-// CPML slab, on no PEC face, hold no source, probe, PEC edge mask or
-// gradient-history cell, and have uniform H coefficients; everything else
-// runs two one-step launches per pass through the intermediate buffer F[2].
+// CPML slab and hold no source, probe or gradient-history cell, in plans with
+// uniform H coefficients; cells at a grid face take the guarded path (zero
+// outside the grid, PEC faces) and a PEC edge mask applies to every E cell as
+// in the one-step kernel.  Everything else runs two one-step launches per
+// pass through the intermediate buffer F[2].
 // Where a one-step neighbour or a per-step observer (DFT plane, flux monitor,
 // NTFF face) reads this tile's intermediate state, the CTA also stores it to
 // F[2] (RfxbWork2::mid).
@@ -106,6 +108,16 @@ __device__ __forceinline__ void pec_faces(unsigned pec, int i, int j, int k, int
   if ((pec & 4u) && k == nz - 1) ez = 0.f;
 }
 
+// PEC edge mask of one E cell (rfx/boundaries/pec.py:179-208), as the
+// one-step kernel applies it after the PEC faces.
+__device__ __forceinline__ void edge_mask(unsigned m, float& ex, float& ey, float& ez) {
+  if (m) {
+    ex = ex * (1.f - (float)(m & 1u));
+    ey = ey * (1.f - (float)((m >> 1) & 1u));
+    ez = ez * (1.f - (float)((m >> 2) & 1u));
+  }
+}
+
 // One work item.  EDGE: the item's cells reach a grid face (no CPML on that
 // axis): cells outside the grid stay zero (the guards the one-step kernel
 // reads) and E takes the PEC faces; otherwise every computed cell is an
@@ -120,6 +132,7 @@ __device__ __forceinline__ void fwd2_item(Fwd2Smem<TY>& S, const RfxbWork2& w, c
   const int y0 = w.y0, z0 = w.z0, xa = w.xa, xb = w.xb;
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const unsigned pec = P.pec_axes;
+  const unsigned char* emask = P.emask;   // PEC edge mask bits (1 ex, 2 ey, 4 ez) or null
   const CUtensorMap* tm = maps + (size_t)w.inst * RFXB_NMAPS;
   const int producer = NT - 32;   // lane 0 of the last warp issues the boxes
   const int wlim = kWaitLimit;
@@ -235,6 +248,7 @@ __device__ __forceinline__ void fwd2_item(Fwd2Smem<TY>& S, const RfxbWork2& w, c
         float ey = yee_e(cav, A.e[1][hr][q + 3], cbv, cy_);
         float ez = yee_e(cav, A.e[2][hr][q + 3], cbv, cz_);
         if (EDGE) pec_faces(pec, p, j, k, nx, ny, nz, ex, ey, ez);
+        if (emask) edge_mask(emask[P.off0 + (long long)p * P.ps + (long long)j * P.zs + k], ex, ey, ez);
         E1[0][r][q] = ex;
         E1[1][r][q] = ey;
         E1[2][r][q] = ez;
@@ -295,6 +309,7 @@ __device__ __forceinline__ void fwd2_item(Fwd2Smem<TY>& S, const RfxbWork2& w, c
       float ey = yee_e(cav, E1[1][r][s], cbv, cy_);
       float ez = yee_e(cav, E1[2][r][s], cbv, cz_);
       if (EDGE) pec_faces(pec, q, jt, kt, nx, ny, nz, ex, ey, ez);
+      if (emask) edge_mask(emask[e_row + (long long)q * P.ps], ex, ey, ez);
       const long long e = e_row + (long long)q * P.ps;
       Fo[e] = ex;
       Fo[cs + e] = ey;

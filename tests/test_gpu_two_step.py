@@ -16,7 +16,8 @@ identical, not merely close:
 * the reference's own PEC benchmark (no CPML, PEC faces) at 129^3, and grids
   mixing CPML, PEC and open faces by axis (the guarded path of the tiles
   whose cells reach a face);
-* a graded-z grid with CPML (the spacing tables of the non-uniform lane);
+* a graded-z grid with CPML and a PEC sheet (the spacing tables of the
+  non-uniform lane, the PEC edge mask in both steps of a pass);
 * a DFT plane, a flux monitor and an NTFF box through two-step tiles (the
   observers read each pass's intermediate state);
 * the batched sweep (history recording, adjoint gradients);
@@ -168,7 +169,11 @@ def test_two_step_graded_grid_equals_one_step(cuda):
     src = [(*c, "ez", rng.standard_normal(n).astype(np.float32))]
     probes = [(c[0] + 7, c[1] - 5, c[2], "ez")]
     dft = [(2, c[2] + 11, "ex", np.linspace(10e9, 30e9, 4).astype(np.float32))]
-    r = _device(g, eps, sig, n, src, probes, dft, "graded")
+    # a PEC sheet with a hole, through the two-step tiles (edge mask)
+    pec = np.zeros(g.shape, bool)
+    pec[15:g.nx - 15, 12:g.ny - 12, c[2] - 6] = True
+    pec[40:60, 40:60, c[2] - 6] = False
+    r = _device(g, eps, sig, n, src, probes, dft, "graded", pec=pec)
     try:
         _check_two_step_available(r)
         init = _random_fields(g.shape, 8)
