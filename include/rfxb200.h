@@ -189,7 +189,9 @@ typedef struct {
 int rfxb_version(void);
 const char* rfxb_last_error(void);
 
-/* Create / destroy a plan.  Replaces the trace-time setup named above. */
+/* Create / destroy a plan.  Replaces the trace-time setup named above.
+ * A plan lives on the device current at its creation; destroy waits for the
+ * current device before freeing, so call it with that device current. */
 int rfxb_plan_create(const RfxbDesc* desc, RfxbPlan** out);
 void rfxb_plan_destroy(RfxbPlan* plan);
 
@@ -262,6 +264,7 @@ int rfxb_plan_adjoint_advance(RfxbPlan* plan, const RfxbAdjointIO* aio, int step
  * batching the reference offers for uneven grids (rfx/vmap_sweep.py:871
  * batches equal grids only). */
 int rfxb_batch_create(RfxbPlan* const* plans, int n_plans, RfxbBatch** out);
+/* Like rfxb_plan_destroy: call with the plans' device current. */
 void rfxb_batch_destroy(RfxbBatch* batch);
 int rfxb_batch_advance(RfxbBatch* batch, const RfxbStepIO* ios, int step0, int n_steps, void* stream);
 int rfxb_batch_record_history(RfxbBatch* batch, int step0, int n_steps);

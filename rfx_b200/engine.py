@@ -178,8 +178,11 @@ class Plan:
 
     # -- lifecycle ---------------------------------------------------------
     def close(self):
+        # rfxb_plan_destroy synchronises the current device before freeing:
+        # make that the plan's own device
         if getattr(self, "_h", None) and self._h.value:
-            self._lib.rfxb_plan_destroy(self._h)
+            with torch.cuda.device(self.device):
+                self._lib.rfxb_plan_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -442,7 +445,8 @@ class Batch:
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
-            self._lib.rfxb_batch_destroy(self._h)
+            with torch.cuda.device(self.plans[0].device):
+                self._lib.rfxb_batch_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
